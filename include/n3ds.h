@@ -1,0 +1,190 @@
+/*
+ * n3ds: B200-native (sm_100a) stroke field of Neural 3D Strokes, C ABI.
+ *
+ * Every entry point takes device pointers, int64 sizes and a CUDA stream, launches
+ * asynchronously on that stream, allocates nothing, and returns 0 or an N3DS_ERR_*
+ * code; n3ds_last_error() gives the message of the last failure on the calling
+ * thread. Float buffers are float32, C-contiguous.
+ *
+ * Two layers:
+ *  1. The four operators of the reference's native module `_strokelib`
+ *     (source/strokelib/src/bindings.cpp:6-11), same argument meaning and order,
+ *     with tensors replaced by pointers + sizes. Gradient outputs accumulate into
+ *     caller-zeroed buffers, as in the reference (strokes.py:212-216, 365-367).
+ *  2. The fused stroke field: stroke evaluation, soft step, overlay compositing and
+ *     volume rendering in one forward, its exact adjoint in one backward, for one
+ *     scene or a batch of uneven scenes, graph-capturable (no host syncs, no
+ *     allocation; scratch lives in a caller-provided workspace).
+ */
+#ifndef N3DS_H_
+#define N3DS_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* n3ds_stream_t; /* = cudaStream_t */
+
+#define N3DS_OK 0
+#define N3DS_ERR_INVALID 1     /* bad argument (shape, null pointer, size) */
+#define N3DS_ERR_UNSUPPORTED 2 /* sdf_id / colour type outside the implemented set */
+#define N3DS_ERR_CUDA 3        /* a CUDA call failed */
+#define N3DS_ERR_WORKSPACE 4   /* workspace too small */
+#define N3DS_ERR_DEVICE 5      /* a kernel reported a device-side error status */
+
+#define N3DS_GRAD_EXACT 0  /* exact adjoint of the forward (checked against float64 finite differences) */
+#define N3DS_GRAD_COMPAT 1 /* the reference's hand-written backward formulas */
+
+/* Message of the last failure on this thread (empty string if none). */
+const char* n3ds_last_error(void);
+/* Library version, major * 10000 + minor * 100 + patch. */
+int n3ds_version(void);
+
+/* ------------------------------------------------------------------------------
+ * Layer 1: reference `_strokelib` operators
+ * ------------------------------------------------------------------------------ */
+
+/* Workspace bytes needed by n3ds_stroke_forward / n3ds_stroke_backward for
+ * n_strokes strokes (prepared per-stroke records). */
+size_t n3ds_stroke_workspace_bytes(int64_t n_strokes);
+
+/* Replaces stroke_forward (strokes_forward.cu:170-225; declared strokes.h:14-27).
+ * alpha_out [P,S], color_out [P,S,3], sdf_out [P,S] or NULL; texcoord output is not
+ * implemented (pass n_texcoord = 0). x [P,3], radius [P], viewdir [R,3] (unused by
+ * constant_rgb; only its count n_viewdirs is checked: P must be a multiple),
+ * shape_params [S,Ps], color_params [S,Pc]. sdf_id / color_id as produced by the
+ * reference get_stroke (strokes.py:95-106); color_id must be 0 (constant_rgb). */
+int n3ds_stroke_forward(float* alpha_out, float* color_out, float* sdf_out, int64_t n_texcoord,
+                        const float* x, const float* radius, const float* viewdir,
+                        const float* shape_params, const float* color_params, int64_t n_points,
+                        int64_t n_viewdirs, int64_t n_strokes, int64_t n_shape_params,
+                        int64_t n_color_params, uint32_t sdf_id, uint32_t color_id, float sdf_delta,
+                        int use_laplace_transform, int inv_scale_radius, void* workspace,
+                        size_t workspace_bytes, n3ds_stream_t stream);
+
+/* Replaces stroke_backward (strokes_backward.cu:224-287; declared strokes.h:38-54).
+ * Accumulates into grad_shape_params [S,Ps], grad_color_params [S,Pc] and grad_x [P,3]
+ * (NULL to skip). grad_sdf may be NULL. alpha is the forward's alpha_out.
+ * grad_mode: N3DS_GRAD_EXACT or N3DS_GRAD_COMPAT. */
+int n3ds_stroke_backward(float* grad_shape_params, float* grad_color_params, float* grad_x,
+                         const float* grad_alpha, const float* grad_color, const float* grad_sdf,
+                         const float* x, const float* radius, const float* viewdir,
+                         const float* alpha, const float* shape_params, const float* color_params,
+                         int64_t n_points, int64_t n_viewdirs, int64_t n_strokes,
+                         int64_t n_shape_params, int64_t n_color_params, uint32_t sdf_id,
+                         uint32_t color_id, float sdf_delta, int use_laplace_transform,
+                         int inv_scale_radius, int grad_mode, void* workspace,
+                         size_t workspace_bytes, n3ds_stream_t stream);
+
+/* Replaces compose_forward (compositing.cu:159-204; declared compositing.h:10-14).
+ * density_out [P], color_out [P,C], alphas [P,S], colors [P,S,C], density_params [S];
+ * C in {1, 3}. */
+int n3ds_compose_forward(float* density_out, float* color_out, const float* alphas,
+                         const float* colors, const float* density_params, int64_t n_points,
+                         int64_t n_strokes, int64_t color_dim, n3ds_stream_t stream);
+
+/* Workspace bytes of n3ds_compose_backward: P*S floats in exact mode (the
+ * transmittance in front of every stroke), 0 in compat mode. */
+size_t n3ds_compose_workspace_bytes(int64_t n_points, int64_t n_strokes, int grad_mode);
+
+/* Replaces compose_backward (compositing.cu:206-262; declared compositing.h:24-31).
+ * Accumulates into grad_alphas [P,S], grad_colors [P,S,C], grad_density_params [S].
+ * grad_density_out [P] and grad_color_out [P,C] may be NULL (treated as zero).
+ * Exact mode is division-free (a top-down and a bottom-up sweep) and needs
+ * n3ds_compose_workspace_bytes of scratch. */
+int n3ds_compose_backward(float* grad_alphas, float* grad_colors, float* grad_density_params,
+                          const float* grad_density_out, const float* grad_color_out,
+                          const float* alphas, const float* colors, const float* density_params,
+                          int64_t n_points, int64_t n_strokes, int64_t color_dim, int grad_mode,
+                          void* workspace, size_t workspace_bytes, n3ds_stream_t stream);
+
+/* ------------------------------------------------------------------------------
+ * Layer 2: fused stroke field
+ * (StrokeField.predict_density models.py:660-711 + compute_alpha_weights /
+ *  volumetric_rendering render.py:29-88, as driven by Model.forward models.py:191-235)
+ * ------------------------------------------------------------------------------ */
+
+/* Scene batch: scene i owns n_rays[i] consecutive rays and n_strokes[i] consecutive
+ * strokes of the concatenated arrays. Host arrays. */
+typedef struct n3ds_batch {
+  int32_t n_scenes;
+  const int64_t* n_rays;    /* host [n_scenes] */
+  const int32_t* n_strokes; /* host [n_scenes] */
+  int32_t n_samples;        /* samples per ray, all scenes */
+} n3ds_batch_t;
+
+typedef struct n3ds_rays {
+  const float* x;      /* [R*N*3] sample positions */
+  const float* radius; /* [R*N] sample radii */
+  const float* tdist;  /* [R*(N+1)] fence-post distances */
+  const float* dirs;   /* [R*3] ray directions (their norm scales the intervals) */
+  const float* bg;     /* [R*3] background colour, or NULL to use bg_value */
+  float bg_value;
+  int32_t opaque_background;
+} n3ds_rays_t;
+
+typedef struct n3ds_strokes {
+  const int32_t* sdf_ids;     /* [S] reference sdf_id per stroke (device) */
+  const float* shape_params;  /* [S*param_stride], reference layout, zero-padded */
+  int32_t param_stride;
+  const float* color_params;  /* [S*3] constant rgb */
+  const float* density;       /* [S] density (already times density_scale) */
+  const float* sdf_delta;     /* [S] softness per stroke */
+  int32_t use_laplace_transform;
+  int32_t inv_scale_radius;
+} n3ds_strokes_t;
+
+typedef struct n3ds_options {
+  float cull_alpha;   /* drop a stroke where its alpha provably stays below this; <= 0: no culling */
+  int32_t chunk_fwd;  /* strokes per shared-memory stage, forward (0 = auto) */
+  int32_t chunk_bwd;  /* strokes per shared-memory stage, backward (0 = auto) */
+  int32_t warps;      /* warps per CTA: 4, 8 or 16 (0 = auto) */
+  int32_t segs_per_tile; /* 32-sample segments per CTA work tile (0 = auto) */
+  int32_t grad_mode;  /* N3DS_GRAD_EXACT or N3DS_GRAD_COMPAT */
+} n3ds_options_t;
+
+/* Fill *opt with the defaults. */
+void n3ds_default_options(n3ds_options_t* opt);
+
+/* Workspace bytes for a batch (forward checkpoint, backward seeds and state,
+ * prepared records, reduction slots, counters). total_strokes = sum of n_strokes. */
+size_t n3ds_field_workspace_bytes(const n3ds_batch_t* batch, const n3ds_options_t* opt);
+
+/* Forward: rgb [R*3], acc [R], depth [R]. Leaves the checkpoint in the workspace. */
+int n3ds_field_forward(const n3ds_batch_t* batch, const n3ds_rays_t* rays,
+                       const n3ds_strokes_t* strokes, const n3ds_options_t* opt, float* rgb,
+                       float* acc, float* depth, void* workspace, size_t workspace_bytes,
+                       n3ds_stream_t stream);
+
+/* Backward of the preceding n3ds_field_forward with the same inputs and workspace.
+ * Upstream grads may be NULL (zero). Writes (overwrites) grad_x [R*N*3] (NULL to
+ * skip), grad_shape [S*param_stride], grad_color [S*3], grad_density [S],
+ * grad_sdf_delta [S] (NULL to skip). */
+int n3ds_field_backward(const n3ds_batch_t* batch, const n3ds_rays_t* rays,
+                        const n3ds_strokes_t* strokes, const n3ds_options_t* opt,
+                        const float* grad_rgb, const float* grad_acc, const float* grad_depth,
+                        float* grad_x, float* grad_shape, float* grad_color, float* grad_density,
+                        float* grad_sdf_delta, void* workspace, size_t workspace_bytes,
+                        n3ds_stream_t stream);
+
+/* Synchronously read (and clear) the device status word and the count of evaluated
+ * (sample, stroke) pairs of the last forward. status 0 = fine. */
+int n3ds_field_read_status(void* workspace, int32_t* status, uint64_t* evaluated_pairs,
+                           n3ds_stream_t stream);
+
+/* Adam step fused with the reference's parameter clamp (utils/training.py:119-136,
+ * models.py:576-584) over n floats: m = b1 m + (1-b1) g; v = b2 v + (1-b2) g^2;
+ * p -= lr * mhat / (sqrt(vhat) + eps); then p = clamp(p, lo, hi) where lo/hi may be
+ * NULL. step is read from device memory (incremented by the caller's graph). */
+int n3ds_adam_step(float* param, const float* grad, float* exp_avg, float* exp_avg_sq,
+                   const float* lo, const float* hi, int64_t n, float lr, float beta1, float beta2,
+                   float eps, const int32_t* step, n3ds_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* N3DS_H_ */

@@ -1,0 +1,638 @@
+// C ABI of the stroke-field library: argument validation, workspace layout, pass
+// planning and kernel dispatch. Allocates nothing; every launch goes to the caller's
+// stream; no host synchronisation except in n3ds_field_read_status.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/n3ds.h"
+#include "n3ds_field.cuh"
+#include "n3ds_record.cuh"
+#include "n3ds_unfused.cuh"
+#include "n3ds_adam.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define N3DS_CUDA_TRY(expr)                                                              \
+  do {                                                                                   \
+    cudaError_t e_ = (expr);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return fail(N3DS_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_));   \
+  } while (0)
+
+struct DevInfo {
+  int sms = 0;
+  int smem_optin = 0;
+};
+
+DevInfo dev_info() {
+  static DevInfo cache[64];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) dev = 0;
+  DevInfo& d = cache[dev];
+  if (d.sms == 0) {
+    cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&d.smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (d.sms <= 0) d.sms = 148;
+    if (d.smem_optin <= 0) d.smem_optin = 227 * 1024;
+  }
+  return d;
+}
+
+constexpr size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+struct WsLayout {
+  size_t recs, cull_a, cull_b, state, seeds, bstate, gslots, counters, status, stats, total;
+};
+constexpr int N_COUNTERS = 128;
+
+WsLayout ws_layout(long long total_rays, int N, long long S) {
+  WsLayout w{};
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t o = off;
+    off = align256(off + bytes);
+    return o;
+  };
+  const size_t P = size_t(total_rays) * size_t(N);
+  w.status = take(256);  // header: int32 status at +0, uint64 evaluated-pair count at +8
+  w.stats = w.status + 8;
+  w.recs = take(size_t(S) * n3ds::REC_FLOATS * 4);
+  w.cull_a = take(size_t(S) * 16);
+  w.cull_b = take(size_t(S + 4) * 4);
+  w.state = take(P * 5 * 4);
+  w.seeds = take(P * 5 * 4);
+  w.bstate = take(P * 8 * 4);
+  w.gslots = take(size_t(S) * n3ds::GRAD_SLOTS * 4);
+  w.counters = take(N_COUNTERS * 4);
+  w.total = off;
+  return w;
+}
+
+struct Resolved {
+  float cull_m;
+  int chunk_fwd, chunk_bwd, warps, segs_per_tile, grad_mode;
+};
+
+Resolved resolve(const n3ds_options_t* o) {
+  n3ds_options_t d;
+  n3ds_default_options(&d);
+  if (!o) o = &d;
+  Resolved r;
+  // alpha = exp(-m)/2 beyond the cut: m_cut = -ln(2 alpha_cut)
+  r.cull_m = o->cull_alpha > 0.f ? -logf(2.f * o->cull_alpha) : -1.f;
+  if (o->cull_alpha > 0.f && r.cull_m < 0.f) r.cull_m = 0.f;
+  const DevInfo di = dev_info();
+  r.warps = o->warps > 0 ? o->warps : 16;
+  r.segs_per_tile = o->segs_per_tile > 0 ? o->segs_per_tile : 4 * r.warps;
+  const size_t budget = size_t(di.smem_optin) - 64;
+  int cf = o->chunk_fwd > 0 ? o->chunk_fwd : 768;
+  int cb = o->chunk_bwd > 0 ? o->chunk_bwd : 512;
+  while (cf > 32 && n3ds::seg_fwd_smem(cf) > budget) cf -= 32;
+  while (cb > 32 && n3ds::seg_bwd_smem(cb) > budget) cb -= 32;
+  r.chunk_fwd = cf;
+  r.chunk_bwd = cb;
+  r.grad_mode = o->grad_mode;
+  return r;
+}
+
+int check_batch(const n3ds_batch_t* b, long long* total_rays, long long* total_strokes) {
+  if (!b || b->n_scenes < 1 || !b->n_rays || !b->n_strokes)
+    return fail(N3DS_ERR_INVALID, "batch: n_scenes >= 1 and host n_rays / n_strokes arrays required");
+  if (b->n_samples < 1) return fail(N3DS_ERR_INVALID, "batch: n_samples must be >= 1");
+  long long R = 0, S = 0;
+  for (int i = 0; i < b->n_scenes; i++) {
+    if (b->n_rays[i] < 0 || b->n_strokes[i] < 0)
+      return fail(N3DS_ERR_INVALID, "batch: negative ray or stroke count");
+    if (b->n_rays[i] * ((b->n_samples + 31) / 32) > 0x7fffffffLL)
+      return fail(N3DS_ERR_INVALID, "batch: too many segments in one scene");
+    R += b->n_rays[i];
+    S += b->n_strokes[i];
+  }
+  if (S > 0x7fffffffLL) return fail(N3DS_ERR_INVALID, "batch: too many strokes");
+  *total_rays = R;
+  *total_strokes = S;
+  return N3DS_OK;
+}
+
+// Plan and launch the segment passes of one direction.
+int run_seg_passes(bool backward, const n3ds_batch_t* b, const Resolved& rv, n3ds::SegLaunch base,
+                   int counter_base, cudaStream_t st) {
+  const int cap = backward ? rv.chunk_bwd : rv.chunk_fwd;
+  const int spr = (b->n_samples + 31) / 32;
+  std::vector<long long> ray_begin(b->n_scenes), stroke_begin(b->n_scenes);
+  std::vector<int> nch(b->n_scenes);
+  long long r0 = 0, s0 = 0;
+  int passes = 1;
+  for (int i = 0; i < b->n_scenes; i++) {
+    ray_begin[i] = r0;
+    stroke_begin[i] = s0;
+    r0 += b->n_rays[i];
+    s0 += b->n_strokes[i];
+    nch[i] = std::max(1, (b->n_strokes[i] + cap - 1) / cap);
+    passes = std::max(passes, nch[i]);
+  }
+  const DevInfo di = dev_info();
+  const size_t smem = backward ? n3ds::seg_bwd_smem(cap) : n3ds::seg_fwd_smem(cap);
+  int counter = counter_base;
+  for (int pass = 0; pass < passes; pass++) {
+    std::vector<int> scenes;
+    for (int i = 0; i < b->n_scenes; i++)
+      if (nch[i] > pass && b->n_rays[i] > 0) scenes.push_back(i);
+    for (size_t g = 0; g < scenes.size(); g += n3ds::MAX_SCENES_PER_LAUNCH) {
+      n3ds::SegLaunch L = base;
+      L.chunk_cap = cap;
+      L.segs_per_ray = spr;
+      L.segs_per_tile = rv.segs_per_tile;
+      L.n_scenes = 0;
+      int tiles = 0;
+      for (size_t k = g; k < scenes.size() && k < g + n3ds::MAX_SCENES_PER_LAUNCH; k++) {
+        const int i = scenes[k];
+        n3ds::SceneDesc& d = L.sc[L.n_scenes++];
+        d.ray_begin = ray_begin[i];
+        d.n_rays = (int)b->n_rays[i];
+        d.stroke_begin = (int)stroke_begin[i];
+        d.n_strokes = b->n_strokes[i];
+        const int hi = b->n_strokes[i] - pass * cap;
+        const int lo = std::max(0, hi - cap);
+        d.chunk_lo = lo;
+        d.chunk_n = std::max(0, hi - lo);
+        d.first_pass = pass == 0;
+        d.last_pass = pass == nch[i] - 1;
+        d.tile_begin = tiles;
+        const long long segs = (long long)d.n_rays * spr;
+        tiles += (int)((segs + rv.segs_per_tile - 1) / rv.segs_per_tile);
+      }
+      if (tiles == 0) continue;
+      if (counter >= N_COUNTERS) return fail(N3DS_ERR_INVALID, "batch needs too many launches (raise chunk size or split the batch)");
+      L.tiles_total = tiles;
+      L.tile_counter = base.tile_counter + counter++;
+      const int grid = std::min(tiles, di.sms);
+      cudaError_t e = backward ? n3ds::launch_seg_bwd(L, grid, rv.warps, smem, st)
+                               : n3ds::launch_seg_fwd(L, grid, rv.warps, smem, st);
+      if (e != cudaSuccess) return fail(N3DS_ERR_CUDA, std::string("segment kernel launch: ") + cudaGetErrorString(e));
+    }
+  }
+  return N3DS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* n3ds_last_error(void) { return g_last_error.c_str(); }
+int n3ds_version(void) { return 100; }
+
+void n3ds_default_options(n3ds_options_t* opt) {
+  if (!opt) return;
+  opt->cull_alpha = 1e-9f;
+  opt->chunk_fwd = 0;
+  opt->chunk_bwd = 0;
+  opt->warps = 0;
+  opt->segs_per_tile = 0;
+  opt->grad_mode = N3DS_GRAD_EXACT;
+}
+
+size_t n3ds_field_workspace_bytes(const n3ds_batch_t* batch, const n3ds_options_t* opt) {
+  (void)opt;
+  long long R = 0, S = 0;
+  if (check_batch(batch, &R, &S) != N3DS_OK) return 0;
+  return ws_layout(R, batch->n_samples, S).total;
+}
+
+static int field_common(const n3ds_batch_t* batch, const n3ds_rays_t* rays, const n3ds_strokes_t* strokes,
+                        void* ws, size_t ws_bytes, long long* R, long long* S, WsLayout* lay) {
+  int rc = check_batch(batch, R, S);
+  if (rc) return rc;
+  if (!rays || !rays->x || !rays->radius || !rays->tdist || !rays->dirs)
+    return fail(N3DS_ERR_INVALID, "rays: x, radius, tdist and dirs are required");
+  if (!strokes || (*S > 0 && (!strokes->sdf_ids || !strokes->shape_params || !strokes->color_params ||
+                              !strokes->density || !strokes->sdf_delta)))
+    return fail(N3DS_ERR_INVALID, "strokes: sdf_ids, shape_params, color_params, density, sdf_delta required");
+  if (*S > 0 && (strokes->param_stride < 1 || strokes->param_stride > 64))
+    return fail(N3DS_ERR_INVALID, "strokes: param_stride must be in [1, 64]");
+  *lay = ws_layout(*R, batch->n_samples, *S);
+  if (!ws || ws_bytes < lay->total)
+    return fail(N3DS_ERR_WORKSPACE, "workspace too small: need " + std::to_string(lay->total) + " bytes");
+  if (reinterpret_cast<uintptr_t>(ws) % 256)
+    return fail(N3DS_ERR_INVALID, "workspace must be 256-byte aligned");
+  return N3DS_OK;
+}
+
+static n3ds::PrepLaunch make_prep(const n3ds_strokes_t* s, long long S, const Resolved& rv, char* ws,
+                                  const WsLayout& lay, bool zero_slots) {
+  n3ds::PrepLaunch p{};
+  p.sdf_ids = s->sdf_ids;
+  p.uniform_sdf_id = -1;
+  p.shape_params = s->shape_params;
+  p.param_stride = s->param_stride;
+  p.color_params = s->color_params;
+  p.color_stride = 3;
+  p.density = s->density;
+  p.sdf_delta = s->sdf_delta;
+  p.use_laplace = s->use_laplace_transform;
+  p.inv_scale_radius = s->inv_scale_radius;
+  p.cull_m = rv.cull_m;
+  p.n_strokes = S;
+  p.recs = reinterpret_cast<float*>(ws + lay.recs);
+  p.cull_a = reinterpret_cast<float*>(ws + lay.cull_a);
+  p.cull_b = reinterpret_cast<float*>(ws + lay.cull_b);
+  p.status = reinterpret_cast<int*>(ws + lay.status);
+  p.counters = reinterpret_cast<int*>(ws + lay.counters);
+  p.n_counters = N_COUNTERS;
+  p.gslots = zero_slots ? reinterpret_cast<float*>(ws + lay.gslots) : nullptr;
+  p.stats = zero_slots ? nullptr : reinterpret_cast<unsigned long long*>(ws + lay.stats);
+  return p;
+}
+
+static n3ds::SegLaunch make_seg(const n3ds_batch_t* b, const n3ds_rays_t* rays, char* ws, const WsLayout& lay,
+                                int compat) {
+  n3ds::SegLaunch L{};
+  L.x = rays->x;
+  L.radius = rays->radius;
+  L.n_samples = b->n_samples;
+  L.recs = reinterpret_cast<const float*>(ws + lay.recs);
+  L.cull_a = reinterpret_cast<const float*>(ws + lay.cull_a);
+  L.cull_b = reinterpret_cast<const float*>(ws + lay.cull_b);
+  L.state = reinterpret_cast<float*>(ws + lay.state);
+  L.seeds = reinterpret_cast<const float*>(ws + lay.seeds);
+  L.bstate = reinterpret_cast<float*>(ws + lay.bstate);
+  L.gslots = reinterpret_cast<float*>(ws + lay.gslots);
+  L.compat = compat;
+  L.tile_counter = reinterpret_cast<int*>(ws + lay.counters);
+  L.status = reinterpret_cast<int*>(ws + lay.status);
+  L.stats = reinterpret_cast<unsigned long long*>(ws + lay.stats);
+  return L;
+}
+
+static n3ds::RayLaunch make_ray(const n3ds_batch_t* b, const n3ds_rays_t* rays, char* ws, const WsLayout& lay,
+                                long long R) {
+  n3ds::RayLaunch L{};
+  L.state = reinterpret_cast<const float*>(ws + lay.state);
+  L.tdist = rays->tdist;
+  L.dirs = rays->dirs;
+  L.bg = rays->bg;
+  L.bg_value = rays->bg_value;
+  L.opaque = rays->opaque_background;
+  L.n_rays = R;
+  L.n_samples = b->n_samples;
+  L.seeds = reinterpret_cast<float*>(ws + lay.seeds);
+  return L;
+}
+
+int n3ds_field_forward(const n3ds_batch_t* batch, const n3ds_rays_t* rays, const n3ds_strokes_t* strokes,
+                       const n3ds_options_t* opt, float* rgb, float* acc, float* depth, void* workspace,
+                       size_t workspace_bytes, n3ds_stream_t stream) {
+  long long R, S;
+  WsLayout lay;
+  int rc = field_common(batch, rays, strokes, workspace, workspace_bytes, &R, &S, &lay);
+  if (rc) return rc;
+  if (!rgb || !acc || !depth) return fail(N3DS_ERR_INVALID, "rgb, acc and depth outputs are required");
+  const Resolved rv = resolve(opt);
+  char* ws = static_cast<char*>(workspace);
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  n3ds::launch_prep(make_prep(strokes, S, rv, ws, lay, false), st);
+  N3DS_CUDA_TRY(cudaGetLastError());
+  rc = run_seg_passes(false, batch, rv, make_seg(batch, rays, ws, lay, 0), 0, st);
+  if (rc) return rc;
+  if (R > 0) {
+    n3ds::RayLaunch L = make_ray(batch, rays, ws, lay, R);
+    L.rgb = rgb;
+    L.acc = acc;
+    L.depth = depth;
+    n3ds::launch_ray_fwd(L, st);
+    N3DS_CUDA_TRY(cudaGetLastError());
+  }
+  return N3DS_OK;
+}
+
+int n3ds_field_backward(const n3ds_batch_t* batch, const n3ds_rays_t* rays, const n3ds_strokes_t* strokes,
+                        const n3ds_options_t* opt, const float* grad_rgb, const float* grad_acc,
+                        const float* grad_depth, float* grad_x, float* grad_shape, float* grad_color,
+                        float* grad_density, float* grad_sdf_delta, void* workspace, size_t workspace_bytes,
+                        n3ds_stream_t stream) {
+  long long R, S;
+  WsLayout lay;
+  int rc = field_common(batch, rays, strokes, workspace, workspace_bytes, &R, &S, &lay);
+  if (rc) return rc;
+  if (S > 0 && (!grad_shape || !grad_color || !grad_density))
+    return fail(N3DS_ERR_INVALID, "grad_shape, grad_color and grad_density outputs are required");
+  const Resolved rv = resolve(opt);
+  const int compat = rv.grad_mode == N3DS_GRAD_COMPAT;
+  char* ws = static_cast<char*>(workspace);
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  n3ds::launch_prep(make_prep(strokes, S, rv, ws, lay, true), st);
+  N3DS_CUDA_TRY(cudaGetLastError());
+  if (R > 0) {
+    n3ds::RayLaunch L = make_ray(batch, rays, ws, lay, R);
+    L.g_rgb = grad_rgb;
+    L.g_acc = grad_acc;
+    L.g_depth = grad_depth;
+    n3ds::launch_ray_bwd(L, st);
+    N3DS_CUDA_TRY(cudaGetLastError());
+  }
+  n3ds::SegLaunch SL = make_seg(batch, rays, ws, lay, compat);
+  SL.grad_x = grad_x;
+  SL.stats = nullptr;
+  rc = run_seg_passes(true, batch, rv, SL, N_COUNTERS / 2, st);
+  if (rc) return rc;
+  if (S > 0) {
+    n3ds::FinalizeLaunch F{};
+    F.sdf_ids = strokes->sdf_ids;
+    F.shape_params = strokes->shape_params;
+    F.param_stride = strokes->param_stride;
+    F.sdf_delta = strokes->sdf_delta;
+    F.recs = reinterpret_cast<const float*>(ws + lay.recs);
+    F.gslots = reinterpret_cast<const float*>(ws + lay.gslots);
+    F.n_strokes = S;
+    F.compat = compat;
+    F.grad_shape = grad_shape;
+    F.grad_color = grad_color;
+    F.grad_density = grad_density;
+    F.grad_delta = grad_sdf_delta;
+    F.accumulate = 0;
+    F.color_stride = 3;
+    n3ds::launch_finalize(F, st);
+    N3DS_CUDA_TRY(cudaGetLastError());
+  }
+  return N3DS_OK;
+}
+
+int n3ds_field_read_status(void* workspace, int32_t* status, uint64_t* evaluated_pairs, n3ds_stream_t stream) {
+  if (!workspace) return fail(N3DS_ERR_INVALID, "workspace required");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  unsigned long long hdr[2] = {0ull, 0ull};
+  N3DS_CUDA_TRY(cudaMemcpyAsync(hdr, workspace, sizeof(hdr), cudaMemcpyDeviceToHost, st));
+  N3DS_CUDA_TRY(cudaStreamSynchronize(st));
+  N3DS_CUDA_TRY(cudaMemsetAsync(workspace, 0, sizeof(int32_t), st));
+  int32_t sv;
+  std::memcpy(&sv, &hdr[0], sizeof(sv));
+  if (status) *status = sv;
+  if (evaluated_pairs) *evaluated_pairs = hdr[1];
+  return N3DS_OK;
+}
+
+
+// ------------------------------------------------------------- layer 1 operators
+
+size_t n3ds_stroke_workspace_bytes(int64_t n_strokes) {
+  if (n_strokes < 0) return 0;
+  // header, records, culling arrays (unused but written by the shared prep kernel),
+  // reduced gradient slots
+  return 256 + align256(size_t(n_strokes) * n3ds::REC_FLOATS * 4) + align256(size_t(n_strokes) * 16) +
+         align256(size_t(n_strokes + 4) * 4) + align256(size_t(n_strokes) * n3ds::GRAD_SLOTS * 4) + 256;
+}
+
+namespace {
+struct StrokeWs {
+  float *recs, *cull_a, *cull_b, *gslots;
+  int* status;
+};
+StrokeWs stroke_ws(void* ws, int64_t S) {
+  char* b = static_cast<char*>(ws);
+  StrokeWs w;
+  size_t off = 0;
+  w.status = reinterpret_cast<int*>(b + off);
+  off += 256;
+  w.recs = reinterpret_cast<float*>(b + off);
+  off += align256(size_t(S) * n3ds::REC_FLOATS * 4);
+  w.cull_a = reinterpret_cast<float*>(b + off);
+  off += align256(size_t(S) * 16);
+  w.cull_b = reinterpret_cast<float*>(b + off);
+  off += align256(size_t(S + 4) * 4);
+  w.gslots = reinterpret_cast<float*>(b + off);
+  return w;
+}
+
+int check_stroke_args(uint32_t sdf_id, uint32_t color_id, int64_t n_points, int64_t n_viewdirs, int64_t n_strokes,
+                      int64_t n_shape_params, int64_t n_color_params, int64_t n_texcoord, void* ws, size_t ws_bytes) {
+  // fn_id bound as strokes_forward.cu:202-204, then this build's implemented subset
+  if (sdf_id * 4u + color_id >= 12u * 16u * 4u) return fail(N3DS_ERR_INVALID, "fn_id must be in [0, num_fn_ids]");
+  if (color_id != 0) return fail(N3DS_ERR_UNSUPPORTED, "only color_id 0 (constant_rgb) is implemented");
+  const int base = (int)(sdf_id >> 4);
+  if (!n3ds::base_supported(base))
+    return fail(N3DS_ERR_UNSUPPORTED, "sdf base " + std::to_string(base) +
+                                          " is outside the implemented set (sphere, cube, round cube, capsule, "
+                                          "octahedron, tetrahedron, quadratic and cubic Bezier)");
+  if (base > n3ds::B_TETRAHEDRON && (sdf_id & 15u))
+    return fail(N3DS_ERR_UNSUPPORTED, "Bezier strokes take no transform flags");
+  if (n_texcoord != 0) return fail(N3DS_ERR_UNSUPPORTED, "texcoord output is not implemented");
+  if (n_points < 0 || n_strokes < 0) return fail(N3DS_ERR_INVALID, "negative sizes");
+  if (n_viewdirs <= 0 && n_points > 0) return fail(N3DS_ERR_INVALID, "viewdir must have at least one row");
+  if (n_strokes > 0 && n_shape_params < n3ds::sdf_id_param_count((int)sdf_id))
+    return fail(N3DS_ERR_INVALID, "shape_params has " + std::to_string(n_shape_params) + " columns, sdf_id needs " +
+                                      std::to_string(n3ds::sdf_id_param_count((int)sdf_id)));
+  if (n_strokes > 0 && n_color_params < 3) return fail(N3DS_ERR_INVALID, "color_params needs 3 columns");
+  if (n_strokes > 65535LL * 32) return fail(N3DS_ERR_INVALID, "too many strokes");
+  if (!ws || ws_bytes < n3ds_stroke_workspace_bytes(n_strokes))
+    return fail(N3DS_ERR_WORKSPACE, "workspace too small: need " + std::to_string(n3ds_stroke_workspace_bytes(n_strokes)));
+  if (reinterpret_cast<uintptr_t>(ws) % 256) return fail(N3DS_ERR_INVALID, "workspace must be 256-byte aligned");
+  return N3DS_OK;
+}
+
+n3ds::PrepLaunch uniform_prep(const StrokeWs& w, const float* shape_params, int64_t n_shape_params,
+                              const float* color_params, int64_t n_color_params, int64_t S, uint32_t sdf_id,
+                              float sdf_delta, int laplace, int inv_scale, bool zero_slots) {
+  n3ds::PrepLaunch p{};
+  p.sdf_ids = nullptr;
+  p.uniform_sdf_id = (int)sdf_id;
+  p.shape_params = shape_params;
+  p.param_stride = (int)n_shape_params;
+  p.color_params = color_params;
+  p.color_stride = (int)n_color_params;
+  p.density = nullptr;
+  p.sdf_delta = nullptr;
+  p.uniform_delta = sdf_delta;
+  p.use_laplace = laplace;
+  p.inv_scale_radius = inv_scale;
+  p.cull_m = -1.f;
+  p.n_strokes = S;
+  p.recs = w.recs;
+  p.cull_a = w.cull_a;
+  p.cull_b = w.cull_b;
+  p.status = w.status;
+  p.counters = nullptr;
+  p.n_counters = 0;
+  p.gslots = zero_slots ? w.gslots : nullptr;
+  p.stats = nullptr;
+  return p;
+}
+}  // namespace
+
+int n3ds_stroke_forward(float* alpha_out, float* color_out, float* sdf_out, int64_t n_texcoord, const float* x,
+                        const float* radius, const float* viewdir, const float* shape_params,
+                        const float* color_params, int64_t n_points, int64_t n_viewdirs, int64_t n_strokes,
+                        int64_t n_shape_params, int64_t n_color_params, uint32_t sdf_id, uint32_t color_id,
+                        float sdf_delta, int use_laplace_transform, int inv_scale_radius, void* workspace,
+                        size_t workspace_bytes, n3ds_stream_t stream) {
+  (void)viewdir;
+  int rc = check_stroke_args(sdf_id, color_id, n_points, n_viewdirs, n_strokes, n_shape_params, n_color_params,
+                             n_texcoord, workspace, workspace_bytes);
+  if (rc) return rc;
+  if (n_points == 0 || n_strokes == 0) return N3DS_OK;
+  if (!alpha_out || !color_out || !x || !radius || !shape_params || !color_params)
+    return fail(N3DS_ERR_INVALID, "null tensor pointer");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  StrokeWs w = stroke_ws(workspace, n_strokes);
+  n3ds::launch_prep(uniform_prep(w, shape_params, n_shape_params, color_params, n_color_params, n_strokes, sdf_id,
+                                 sdf_delta, use_laplace_transform, inv_scale_radius, false),
+                    st);
+  N3DS_CUDA_TRY(cudaGetLastError());
+  n3ds::UfStroke L{};
+  L.x = x;
+  L.radius = radius;
+  L.recs = w.recs;
+  L.n_points = n_points;
+  L.n_strokes = (int)n_strokes;
+  L.alpha = alpha_out;
+  L.color = color_out;
+  L.sdf = sdf_out;
+  N3DS_CUDA_TRY(n3ds::launch_uf_stroke_fwd(L, (int)(sdf_id >> 4), st));
+  return N3DS_OK;
+}
+
+int n3ds_stroke_backward(float* grad_shape_params, float* grad_color_params, float* grad_x, const float* grad_alpha,
+                         const float* grad_color, const float* grad_sdf, const float* x, const float* radius,
+                         const float* viewdir, const float* alpha, const float* shape_params,
+                         const float* color_params, int64_t n_points, int64_t n_viewdirs, int64_t n_strokes,
+                         int64_t n_shape_params, int64_t n_color_params, uint32_t sdf_id, uint32_t color_id,
+                         float sdf_delta, int use_laplace_transform, int inv_scale_radius, int grad_mode,
+                         void* workspace, size_t workspace_bytes, n3ds_stream_t stream) {
+  (void)viewdir;
+  int rc = check_stroke_args(sdf_id, color_id, n_points, n_viewdirs, n_strokes, n_shape_params, n_color_params, 0,
+                             workspace, workspace_bytes);
+  if (rc) return rc;
+  if (n_strokes == 0) return N3DS_OK;
+  if (!grad_shape_params || !grad_color_params || !grad_alpha || !grad_color || !x || !radius || !alpha ||
+      !shape_params || !color_params)
+    return fail(N3DS_ERR_INVALID, "null tensor pointer");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  StrokeWs w = stroke_ws(workspace, n_strokes);
+  n3ds::launch_prep(uniform_prep(w, shape_params, n_shape_params, color_params, n_color_params, n_strokes, sdf_id,
+                                 sdf_delta, use_laplace_transform, inv_scale_radius, true),
+                    st);
+  N3DS_CUDA_TRY(cudaGetLastError());
+  const int compat = grad_mode == N3DS_GRAD_COMPAT;
+  if (n_points > 0) {
+    n3ds::UfStroke L{};
+    L.x = x;
+    L.radius = radius;
+    L.recs = w.recs;
+    L.n_points = n_points;
+    L.n_strokes = (int)n_strokes;
+    L.g_alpha = grad_alpha;
+    L.g_color = grad_color;
+    L.g_sdf = grad_sdf;
+    L.alpha_in = alpha;
+    L.grad_x = grad_x;
+    L.gslots = w.gslots;
+    L.compat = compat;
+    N3DS_CUDA_TRY(n3ds::launch_uf_stroke_bwd(L, (int)(sdf_id >> 4), st));
+  }
+  n3ds::FinalizeLaunch F{};
+  F.sdf_ids = nullptr;
+  F.uniform_sdf_id = (int)sdf_id;
+  F.shape_params = shape_params;
+  F.param_stride = (int)n_shape_params;
+  F.sdf_delta = nullptr;
+  F.uniform_delta = sdf_delta;
+  F.recs = w.recs;
+  F.gslots = w.gslots;
+  F.n_strokes = n_strokes;
+  F.compat = compat;
+  F.grad_shape = grad_shape_params;
+  F.grad_color = grad_color_params;
+  F.color_stride = (int)n_color_params;
+  F.grad_density = nullptr;
+  F.grad_delta = nullptr;
+  F.accumulate = 1;
+  n3ds::launch_finalize(F, st);
+  N3DS_CUDA_TRY(cudaGetLastError());
+  return N3DS_OK;
+}
+
+int n3ds_compose_forward(float* density_out, float* color_out, const float* alphas, const float* colors,
+                         const float* density_params, int64_t n_points, int64_t n_strokes, int64_t color_dim,
+                         n3ds_stream_t stream) {
+  if (color_dim != 1 && color_dim != 3)
+    return fail(N3DS_ERR_UNSUPPORTED, "Unsupported color dimension: " + std::to_string(color_dim));
+  if (n_points < 0 || n_strokes < 0) return fail(N3DS_ERR_INVALID, "negative sizes");
+  if (n_points == 0) return N3DS_OK;
+  if (!density_out || !color_out || (n_strokes > 0 && (!alphas || !colors || !density_params)))
+    return fail(N3DS_ERR_INVALID, "null tensor pointer");
+  if (n_strokes > 0x7fffffffLL) return fail(N3DS_ERR_INVALID, "too many strokes");
+  n3ds::UfCompose L{};
+  L.alphas = alphas;
+  L.colors = colors;
+  L.density = density_params;
+  L.n_points = n_points;
+  L.n_strokes = (int)n_strokes;
+  L.color_dim = (int)color_dim;
+  L.density_out = density_out;
+  L.color_out = color_out;
+  N3DS_CUDA_TRY(n3ds::launch_uf_compose_fwd(L, reinterpret_cast<cudaStream_t>(stream)));
+  return N3DS_OK;
+}
+
+size_t n3ds_compose_workspace_bytes(int64_t n_points, int64_t n_strokes, int grad_mode) {
+  if (grad_mode == N3DS_GRAD_COMPAT || n_points <= 0 || n_strokes <= 0) return 0;
+  return size_t(n_points) * size_t(n_strokes) * 4;
+}
+
+int n3ds_compose_backward(float* grad_alphas, float* grad_colors, float* grad_density_params,
+                          const float* grad_density_out, const float* grad_color_out, const float* alphas,
+                          const float* colors, const float* density_params, int64_t n_points, int64_t n_strokes,
+                          int64_t color_dim, int grad_mode, void* workspace, size_t workspace_bytes,
+                          n3ds_stream_t stream) {
+  if (color_dim != 1 && color_dim != 3)
+    return fail(N3DS_ERR_UNSUPPORTED, "Unsupported color dimension: " + std::to_string(color_dim));
+  if (n_points < 0 || n_strokes < 0) return fail(N3DS_ERR_INVALID, "negative sizes");
+  if (n_points == 0 || n_strokes == 0) return N3DS_OK;
+  if (!grad_alphas || !grad_colors || !grad_density_params || !alphas || !colors || !density_params)
+    return fail(N3DS_ERR_INVALID, "null tensor pointer");
+  const int compat = grad_mode == N3DS_GRAD_COMPAT;
+  if (!compat && (!workspace || workspace_bytes < n3ds_compose_workspace_bytes(n_points, n_strokes, grad_mode)))
+    return fail(N3DS_ERR_WORKSPACE, "exact compose backward needs P*S*4 bytes of workspace");
+  n3ds::UfCompose L{};
+  L.alphas = alphas;
+  L.colors = colors;
+  L.density = density_params;
+  L.n_points = n_points;
+  L.n_strokes = (int)n_strokes;
+  L.color_dim = (int)color_dim;
+  L.g_density = grad_density_out;
+  L.g_color = grad_color_out;
+  L.g_alphas = grad_alphas;
+  L.g_colors = grad_colors;
+  L.g_density_params = grad_density_params;
+  L.t_scratch = static_cast<float*>(workspace);
+  L.compat = compat;
+  N3DS_CUDA_TRY(n3ds::launch_uf_compose_bwd(L, reinterpret_cast<cudaStream_t>(stream)));
+  return N3DS_OK;
+}
+
+// ---------------------------------------------------------------------- Adam
+
+int n3ds_adam_step(float* param, const float* grad, float* exp_avg, float* exp_avg_sq, const float* lo,
+                   const float* hi, int64_t n, float lr, float beta1, float beta2, float eps, const int32_t* step,
+                   n3ds_stream_t stream) {
+  if (n < 0) return fail(N3DS_ERR_INVALID, "negative size");
+  if (n == 0) return N3DS_OK;
+  if (!param || !grad || !exp_avg || !exp_avg_sq || !step) return fail(N3DS_ERR_INVALID, "null pointer");
+  N3DS_CUDA_TRY(n3ds::launch_adam(param, grad, exp_avg, exp_avg_sq, lo, hi, n, lr, beta1, beta2, eps, step,
+                                  reinterpret_cast<cudaStream_t>(stream)));
+  return N3DS_OK;
+}
+
+}  // extern "C"

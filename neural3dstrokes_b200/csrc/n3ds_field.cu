@@ -1,0 +1,917 @@
+// Fused stroke-field kernels for sm_100a.
+//
+// Work decomposition. A ray's N samples are split into segments of up to 32
+// consecutive samples; one warp owns one segment at a time (lane = sample). Stroke
+// records of the current scene are staged into shared memory by one bulk
+// (cp.async.bulk / TMA) copy per chunk of strokes, completed on an mbarrier. For each
+// segment the warp first culls the chunk: lane j tests stroke (top - j) of a
+// 32-stroke block against the segment's bounding capsule, and a ballot gives the
+// surviving strokes in descending index order, i.e. the reference compositing order
+// (compositing.cu:34, last stroke on top). Every lane then evaluates the surviving
+// strokes for its own sample; the stroke (and so the SDF type) is warp-uniform, so
+// mixed-type scenes run without divergence.
+//
+// Persistent CTAs (one per SM) pull tiles of segments from a global counter; a tile
+// never spans two scenes, so a CTA restages records only when its scene changes.
+// Scenes with more strokes than one stage holds run in several passes (one launch
+// each), carrying the per-sample composite state through HBM.
+//
+// The backward recomputes each sample's stroke alphas from the forward checkpoint
+// (final T, density and colour sum per sample), evaluates the exact adjoint of the
+// overlay composite in the division-safe form
+//   (1 - a_s) dL/da_s = g_sigma (T_{s+1} d_s - suffix_sigma)
+//                     + g_C . (T_{s+1} c_s - suffix_C) - g_T T_final,
+// and reduces per-stroke gradients across the warp with a transpose reduction
+// before one shared-memory atomic per value; CTAs flush to global memory once per
+// staged chunk.
+#include "n3ds_eval.cuh"
+#include "n3ds_field.cuh"
+
+namespace n3ds {
+
+// ----------------------------------------------------------- async-copy helpers
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  // make the initialised barrier visible to the async (bulk-copy) proxy
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Wait for the mbarrier phase with a one-second limit; false on timeout.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase) {
+  if (mbar_try_wait(bar, phase)) return true;
+  uint64_t t0 = globaltimer_ns();
+  while (!mbar_try_wait(bar, phase)) {
+    if (globaltimer_ns() - t0 > 1000000000ull) return false;
+  }
+  return true;
+}
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ float seg_dist(V3 c, V3 A, V3 AB, float invL2) {
+  V3 w = c - A;
+  float tt = clampf(dot(w, AB) * invL2, 0.f, 1.f);
+  V3 d = w - AB * tt;
+  return sqrtf(dot(d, d));
+}
+
+__device__ __forceinline__ V3 shfl3(V3 v, int src) {
+  return {__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src),
+          __shfl_sync(0xffffffffu, v.z, src)};
+}
+
+__device__ __forceinline__ int find_scene(const SegLaunch& L, int tile) {
+  int lo = 0;
+  for (int i = 1; i < L.n_scenes; i++)
+    if (L.sc[i].tile_begin <= tile) lo = i;
+  return lo;
+}
+
+__host__ __device__ constexpr size_t align16(size_t v) { return (v + 15) & ~size_t(15); }
+
+size_t seg_fwd_smem(int cap) { return align16(cap * 16) + align16(cap * 4) + size_t(cap) * REC_FLOATS * 4; }
+size_t seg_bwd_smem(int cap) { return seg_fwd_smem(cap) + size_t(cap) * GRAD_SLOTS * 4; }
+
+struct Stage {
+  float4* cull_a;
+  float* cull_b;
+  float* recs;
+  float* gacc;
+};
+
+__device__ __forceinline__ Stage carve(unsigned char* smem, int cap, bool with_grads) {
+  Stage s;
+  s.cull_a = reinterpret_cast<float4*>(smem);
+  s.cull_b = reinterpret_cast<float*>(smem + align16(cap * 16));
+  s.recs = reinterpret_cast<float*>(smem + align16(cap * 16) + align16(cap * 4));
+  s.gacc = with_grads ? s.recs + size_t(cap) * REC_FLOATS : nullptr;
+  return s;
+}
+
+// Stage the scene's current chunk: records and culling spheres by bulk copy,
+// culling margins by plain loads. Returns false on an mbarrier timeout.
+__device__ bool stage_chunk(const SegLaunch& L, const SceneDesc& sc, const Stage& S, uint64_t* bar,
+                            uint32_t& phase, int* s_fail) {
+  const int n = sc.chunk_n;
+  const long long g0 = (long long)sc.stroke_begin + sc.chunk_lo;
+  if (n > 0) {
+    if (threadIdx.x == 0) {
+      fence_proxy_async();
+      const uint32_t b_rec = uint32_t(n) * REC_FLOATS * 4;
+      const uint32_t b_cull = uint32_t(n) * 16;
+      mbar_expect_tx(bar, b_rec + b_cull);
+      bulk_g2s(S.recs, L.recs + g0 * REC_FLOATS, b_rec, bar);
+      bulk_g2s(S.cull_a, L.cull_a + g0 * 4, b_cull, bar);
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) S.cull_b[i] = L.cull_b[g0 + i];
+    if (!mbar_wait_bounded(bar, phase)) *s_fail = 1;
+    phase ^= 1u;
+  }
+  __syncthreads();
+  return *s_fail == 0;
+}
+
+// Segment geometry shared by both directions.
+struct SegCtx {
+  long long si;   // this lane's sample index
+  bool active;
+  V3 x;
+  float r, rinv;
+  V3 A, AB;
+  float invL2, rho, rmax;
+};
+
+__device__ __forceinline__ SegCtx seg_setup(const SegLaunch& L, const SceneDesc& sc, int seg, int lane) {
+  SegCtx c;
+  const int spr = L.segs_per_ray;
+  const int ray_local = seg / spr;
+  const int g = seg - ray_local * spr;
+  const long long ray = sc.ray_begin + ray_local;
+  const int i0 = g * 32;
+  const int cnt = min(32, L.n_samples - i0);
+  c.active = lane < cnt;
+  c.si = ray * L.n_samples + i0 + (c.active ? lane : 0);
+  c.x = v3(L.x[3 * c.si], L.x[3 * c.si + 1], L.x[3 * c.si + 2]);
+  c.r = L.radius[c.si];
+  c.rinv = 1.f / c.r;
+  c.A = shfl3(c.x, 0);
+  V3 B = shfl3(c.x, cnt - 1);
+  c.AB = B - c.A;
+  float l2 = dot(c.AB, c.AB);
+  c.invL2 = l2 > 0.f ? 1.f / l2 : 0.f;
+  c.rho = warp_max(c.active ? seg_dist(c.x, c.A, c.AB, c.invL2) : 0.f);
+  c.rmax = warp_max(c.active ? fabsf(c.r) : 0.f);
+  return c;
+}
+
+__device__ __forceinline__ unsigned cull_block(const Stage& S, const SegCtx& c, int hi, int lane) {
+  const int sl = hi - lane;
+  bool cand = false;
+  if (sl >= 0) {
+    float4 ca = S.cull_a[sl];
+    float d = seg_dist(v3(ca.x, ca.y, ca.z), c.A, c.AB, c.invL2);
+    cand = !(d - c.rho > ca.w + S.cull_b[sl] * c.rmax);
+  }
+  return __ballot_sync(0xffffffffu, cand);
+}
+
+// ================================================================== forward
+
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_constant__ SegLaunch L) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ uint64_t bar;
+  __shared__ int s_tile, s_seg, s_fail;
+  const Stage S = carve(smem, L.chunk_cap, false);
+  const int lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    s_fail = 0;
+  }
+  __syncthreads();
+  uint32_t phase = 0;
+  int staged = -1;
+  unsigned long long pairs = 0;
+  while (true) {
+    if (threadIdx.x == 0) {
+      s_tile = atomicAdd(L.tile_counter, 1);
+      s_seg = 0;
+    }
+    __syncthreads();
+    const int tile = s_tile;
+    if (tile >= L.tiles_total) break;
+    const int sci = find_scene(L, tile);
+    const SceneDesc& sc = L.sc[sci];
+    if (sci != staged) {
+      if (!stage_chunk(L, sc, S, &bar, phase, &s_fail)) {
+        if (threadIdx.x == 0) atomicOr(L.status, ST_WAIT_TIMEOUT);
+        return;
+      }
+      staged = sci;
+    }
+    const int seg_lo = (tile - sc.tile_begin) * L.segs_per_tile;
+    const int seg_hi = min(seg_lo + L.segs_per_tile, sc.n_rays * L.segs_per_ray);
+    while (true) {
+      int k = 0;
+      if (lane == 0) k = atomicAdd(&s_seg, 1);
+      k = __shfl_sync(0xffffffffu, k, 0);
+      const int seg = seg_lo + k;
+      if (seg >= seg_hi) break;
+      SegCtx c = seg_setup(L, sc, seg, lane);
+      float T, sig, cr, cg, cb;
+      if (sc.first_pass) {
+        T = 1.f; sig = cr = cg = cb = 0.f;
+      } else {
+        const float* st = L.state + 5 * c.si;
+        T = st[0]; sig = st[1]; cr = st[2]; cg = st[3]; cb = st[4];
+      }
+      unsigned cand_total = 0;
+      for (int hi = sc.chunk_n - 1; hi >= 0; hi -= 32) {
+        unsigned mask = cull_block(S, c, hi, lane);
+        cand_total += __popc(mask);
+        while (mask) {
+          const int b = __ffs(mask) - 1;
+          mask &= mask - 1;
+          const float* rec = S.recs + size_t(hi - b) * REC_FLOATS;
+          const float a = pair_alpha(rec, c.x, c.rinv);
+          const float w = a * T;
+          T *= (1.0f - a);
+          sig += rec[R_DENSITY] * w;
+          cr += rec[R_COLOR] * w;
+          cg += rec[R_COLOR + 1] * w;
+          cb += rec[R_COLOR + 2] * w;
+        }
+      }
+      if (c.active) {
+        float* st = L.state + 5 * c.si;
+        st[0] = T; st[1] = sig; st[2] = cr; st[3] = cg; st[4] = cb;
+      }
+      if (lane == 0) pairs += (unsigned long long)cand_total * (unsigned)min(32, L.n_samples - (seg % L.segs_per_ray) * 32);
+    }
+    __syncthreads();
+  }
+  if (lane == 0 && L.stats && pairs) atomicAdd(L.stats, pairs);
+}
+
+// ================================================================= backward
+
+__device__ __forceinline__ void gacc_add(float* row, int idx, float v) {
+  if (v != 0.f) atomicAdd(row + idx, v);
+}
+
+template <int NV>
+__device__ __forceinline__ void reduce_into(float (&v)[NV], float* row, int lane) {
+  int idx;
+  float tot = warp_transpose_reduce<NV>(v, lane, &idx);
+  if (NV == 32 || lane < 16) gacc_add(row, idx, tot);
+}
+
+struct CompAdj {
+  float T, Ps, Pr, Pg, Pb;          // running (through the previous stroke)
+  float gs, gcr, gcg, gcb, gT;      // seeds
+  float sig, Cr, Cg, Cb, Tf;        // forward totals
+};
+
+// Compose step + exact adjoint for one stroke; returns dL/dm. Writes colour /
+// density slots. compat: the reference compose adjoint (compositing.cu:104-155).
+__device__ __forceinline__ float compose_step(const float* rec, float a, float m, int mode, CompAdj& s,
+                                              float* v, int compat) {
+  const float d = rec[R_DENSITY];
+  const float c0 = rec[R_COLOR], c1 = rec[R_COLOR + 1], c2 = rec[R_COLOR + 2];
+  const float w = a * s.T;
+  const float T1 = s.T * (1.0f - a);
+  s.Ps += d * w;
+  s.Pr += c0 * w;
+  s.Pg += c1 * w;
+  s.Pb += c2 * w;
+  v[G_COLOR + 0] += s.gcr * w;
+  v[G_COLOR + 1] += s.gcg * w;
+  v[G_COLOR + 2] += s.gcb * w;
+  v[G_DENSITY] += s.gs * w;
+  float dm;
+  if (!compat) {
+    const float G = s.gs * (T1 * d - (s.sig - s.Ps)) + s.gcr * (T1 * c0 - (s.Cr - s.Pr)) +
+                    s.gcg * (T1 * c1 - (s.Cg - s.Pg)) + s.gcb * (T1 * c2 - (s.Cb - s.Pb)) - s.gT * s.Tf;
+    dm = soft_dm_from_G(mode, m, a, G);
+  } else {
+    // reference: dL/da = [g_d (T' d - suf_d) + sum g_c O (T' c (O - a) - suf_c) / O^2] / max(1 - a, 1e-6)
+    const float O = 1.0f + 1e-6f - s.Tf;
+    const float sc = 1.f / fmaxf(1.0f - a, 1e-6f);
+    float ga = s.gs * (T1 * d - (s.sig - s.Ps)) * sc;
+    ga += (s.gcr * (T1 * c0 * (O - a) - (s.Cr - s.Pr)) + s.gcg * (T1 * c1 * (O - a) - (s.Cg - s.Pg)) +
+           s.gcb * (T1 * c2 * (O - a) - (s.Cb - s.Pb))) * (sc / O);
+    dm = soft_dm(mode, m, a, ga);
+  }
+  s.T = T1;
+  return dm;
+}
+
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_constant__ SegLaunch L) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ uint64_t bar;
+  __shared__ int s_tile, s_seg, s_fail;
+  const Stage S = carve(smem, L.chunk_cap, true);
+  const int lane = threadIdx.x & 31;
+  const int nthr = blockDim.x;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    s_fail = 0;
+  }
+  for (int i = threadIdx.x; i < L.chunk_cap * GRAD_SLOTS; i += nthr) S.gacc[i] = 0.f;
+  __syncthreads();
+  uint32_t phase = 0;
+  int staged = -1;
+  const int compat = L.compat;
+
+  auto flush = [&](int sci) {
+    const SceneDesc& o = L.sc[sci];
+    float* dst = L.gslots + ((long long)o.stroke_begin + o.chunk_lo) * GRAD_SLOTS;
+    for (int i = threadIdx.x; i < o.chunk_n * GRAD_SLOTS; i += nthr) {
+      float v = S.gacc[i];
+      if (v != 0.f) {
+        atomicAdd(dst + i, v);
+        S.gacc[i] = 0.f;
+      }
+    }
+  };
+
+  while (true) {
+    if (threadIdx.x == 0) {
+      s_tile = atomicAdd(L.tile_counter, 1);
+      s_seg = 0;
+    }
+    __syncthreads();
+    const int tile = s_tile;
+    if (tile >= L.tiles_total) break;
+    const int sci = find_scene(L, tile);
+    const SceneDesc& sc = L.sc[sci];
+    if (sci != staged) {
+      if (staged >= 0) {
+        flush(staged);
+        __syncthreads();
+      }
+      if (!stage_chunk(L, sc, S, &bar, phase, &s_fail)) {
+        if (threadIdx.x == 0) atomicOr(L.status, ST_WAIT_TIMEOUT);
+        return;
+      }
+      staged = sci;
+    }
+    const int seg_lo = (tile - sc.tile_begin) * L.segs_per_tile;
+    const int seg_hi = min(seg_lo + L.segs_per_tile, sc.n_rays * L.segs_per_ray);
+    while (true) {
+      int k = 0;
+      if (lane == 0) k = atomicAdd(&s_seg, 1);
+      k = __shfl_sync(0xffffffffu, k, 0);
+      const int seg = seg_lo + k;
+      if (seg >= seg_hi) break;
+      SegCtx c = seg_setup(L, sc, seg, lane);
+      CompAdj s;
+      {
+        const float* st = L.state + 5 * c.si;
+        s.Tf = st[0]; s.sig = st[1]; s.Cr = st[2]; s.Cg = st[3]; s.Cb = st[4];
+        const float* sd = L.seeds + 5 * c.si;
+        s.gs = sd[0]; s.gcr = sd[1]; s.gcg = sd[2]; s.gcb = sd[3]; s.gT = sd[4];
+        if (!c.active) {
+          s.gs = s.gcr = s.gcg = s.gcb = s.gT = 0.f;
+        }
+      }
+      V3 gx;
+      if (sc.first_pass) {
+        s.T = 1.f; s.Ps = s.Pr = s.Pg = s.Pb = 0.f;
+        gx = v3(0.f, 0.f, 0.f);
+      } else {
+        const float* b = L.bstate + 8 * c.si;
+        s.T = b[0]; s.Ps = b[1]; s.Pr = b[2]; s.Pg = b[3]; s.Pb = b[4];
+        gx = v3(b[5], b[6], b[7]);
+      }
+      for (int hi = sc.chunk_n - 1; hi >= 0; hi -= 32) {
+        unsigned mask = cull_block(S, c, hi, lane);
+        while (mask) {
+          const int b = __ffs(mask) - 1;
+          mask &= mask - 1;
+          const int sl = hi - b;
+          const float* rec = S.recs + size_t(sl) * REC_FLOATS;
+          float* row = S.gacc + size_t(sl) * GRAD_SLOTS;
+          const int kind = __float_as_int(rec[R_KIND]);
+          const int base = kind & 15;
+          const int mode = (kind >> 8) & 3;
+          if (base <= B_TETRAHEDRON) {
+            float v[16];
+#pragma unroll
+            for (int j = 0; j < 16; j++) v[j] = 0.f;
+            const V3 p = prim_local(rec, c.x);
+            const float sdf = prim_sdf(base, p, rec[R_BP]);
+            const float f = (kind & K_S3FAC) ? s3_factor(base, p, ld3(rec + R_S)) : 1.f;
+            const float kk = rec[R_KFIX] * f * c.rinv;
+            const float m = -sdf * kk;
+            const float a = mode == STEP_HARD ? (sdf <= 0.f ? 1.f : 0.f) : soft_alpha(mode, m);
+            const float dm = compose_step(rec, a, m, mode, s, v, compat);
+            const float K = m * dm;
+            v[G_K] += K;
+            gx += prim_backprop(rec, kind, p, -kk * dm, K, v, compat);
+            reduce_into<16>(v, row, lane);
+          } else if (base == B_QUAD_BEZIER) {
+            float v[16];
+#pragma unroll
+            for (int j = 0; j < 16; j++) v[j] = 0.f;
+            QuadFwd qf;
+            const float sdf = quad_eval(rec, c.x, qf);
+            const float kk = rec[R_KFIX] * c.rinv;
+            const float m = -sdf * kk;
+            const float a = mode == STEP_HARD ? (sdf <= 0.f ? 1.f : 0.f) : soft_alpha(mode, m);
+            const float dm = compose_step(rec, a, m, mode, s, v, compat);
+            v[G_K] += m * dm;
+            gx += quad_adjoint(rec, qf, -kk * dm, v + G_CTRL);
+            reduce_into<16>(v, row, lane);
+          } else {
+            float v[32];
+#pragma unroll
+            for (int j = 0; j < 32; j++) v[j] = 0.f;
+            CubicFwd cf;
+            const float sdf = cubic_eval(rec, c.x, cf);
+            const float kk = rec[R_KFIX] * c.rinv;
+            const float m = -sdf * kk;
+            const float a = mode == STEP_HARD ? (sdf <= 0.f ? 1.f : 0.f) : soft_alpha(mode, m);
+            const float dm = compose_step(rec, a, m, mode, s, v, compat);
+            const float dsdf = -kk * dm;
+            v[G_K] += m * dm;
+            V3 g = cubic_adjoint(rec, c.x, cf, dsdf, v + G_CTRL, compat);
+            if (compat) g = g * dsdf;  // the reference multiplies by dL/dSDF again
+            gx += g;
+            reduce_into<32>(v, row, lane);
+          }
+        }
+      }
+      if (c.active) {
+        if (sc.last_pass) {
+          if (L.grad_x) {
+            L.grad_x[3 * c.si] = gx.x;
+            L.grad_x[3 * c.si + 1] = gx.y;
+            L.grad_x[3 * c.si + 2] = gx.z;
+          }
+        } else {
+          float* b = L.bstate + 8 * c.si;
+          b[0] = s.T; b[1] = s.Ps; b[2] = s.Pr; b[3] = s.Pg; b[4] = s.Pb;
+          b[5] = gx.x; b[6] = gx.y; b[7] = gx.z;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (staged >= 0) flush(staged);
+}
+
+// ============================================================== ray kernels
+
+// One warp per ray: volume rendering of the composited samples
+// (render.py:29-48 compute_alpha_weights, 51-88 volumetric_rendering).
+__global__ void ray_fwd_kernel(const RayLaunch L) {
+  const long long ray = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (ray >= L.n_rays) return;
+  const int N = L.n_samples;
+  const float* td = L.tdist + ray * (N + 1);
+  const float dn = sqrtf(L.dirs[3 * ray] * L.dirs[3 * ray] + L.dirs[3 * ray + 1] * L.dirs[3 * ray + 1] +
+                         L.dirs[3 * ray + 2] * L.dirs[3 * ray + 2]);
+  float carry = 0.f, acc = 0.f, r = 0.f, g = 0.f, b = 0.f, D = 0.f;
+  for (int i0 = 0; i0 < N; i0 += 32) {
+    const int i = i0 + lane;
+    const bool on = i < N;
+    float tau = 0.f, cr = 0.f, cg = 0.f, cb = 0.f, tm = 0.f;
+    if (on) {
+      const float* st = L.state + 5 * (ray * N + i);
+      const float T = st[0], sig = st[1];
+      const float inv = 1.0f / (1.0f + 1e-6f - T);
+      cr = clampf(st[2] * inv, 0.f, 1.f);
+      cg = clampf(st[3] * inv, 0.f, 1.f);
+      cb = clampf(st[4] * inv, 0.f, 1.f);
+      const float t0 = td[i], t1 = td[i + 1];
+      tm = 0.5f * (t0 + t1);
+      tau = sig * ((t1 - t0) * dn);
+      if (L.opaque && i == N - 1) tau = __int_as_float(0x7f800000);
+    }
+    const float incl = warp_inclusive_scan(on && isfinite(tau) ? tau : 0.f, lane);
+    const float excl = incl - (on && isfinite(tau) ? tau : 0.f);
+    const float tr = expf(-(carry + excl));
+    const float a = isinf(tau) ? 1.f : -expm1f(-tau);
+    const float w = on ? a * tr : 0.f;
+    acc += w;
+    r += w * cr; g += w * cg; b += w * cb;
+    D += w * tm;
+    carry += __shfl_sync(0xffffffffu, incl, 31);
+  }
+  acc = warp_sum(acc);
+  r = warp_sum(r); g = warp_sum(g); b = warp_sum(b);
+  D = warp_sum(D);
+  if (lane == 0) {
+    const float bgw = fmaxf(1.f - acc, 0.f);
+    float br = L.bg_value, bgg = L.bg_value, bb = L.bg_value;
+    if (L.bg) { br = L.bg[3 * ray]; bgg = L.bg[3 * ray + 1]; bb = L.bg[3 * ray + 2]; }
+    L.rgb[3 * ray] = r + bgw * br;
+    L.rgb[3 * ray + 1] = g + bgw * bgg;
+    L.rgb[3 * ray + 2] = b + bgw * bb;
+    L.acc[ray] = acc;
+    const float eps = 1.1920929e-07f;  // float32 machine epsilon (render.py:76)
+    float val = D / fmaxf(acc, eps);
+    if (isnan(val)) val = __int_as_float(0x7f800000);
+    L.depth[ray] = clampf(val, td[0], td[N]);
+  }
+}
+
+// One warp per ray: adjoint of the volume rendering, producing per-sample seeds
+// g_sigma = dL/dsigma, g_C = dL/d(colour sum), g_T = dL/dT_final.
+__global__ void ray_bwd_kernel(const RayLaunch L) {
+  const long long ray = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (ray >= L.n_rays) return;
+  const int N = L.n_samples;
+  const float* td = L.tdist + ray * (N + 1);
+  const float dn = sqrtf(L.dirs[3 * ray] * L.dirs[3 * ray] + L.dirs[3 * ray + 1] * L.dirs[3 * ray + 1] +
+                         L.dirs[3 * ray + 2] * L.dirs[3 * ray + 2]);
+  float grr = 0.f, grg = 0.f, grb = 0.f, gacc = 0.f, gdep = 0.f;
+  if (L.g_rgb) { grr = L.g_rgb[3 * ray]; grg = L.g_rgb[3 * ray + 1]; grb = L.g_rgb[3 * ray + 2]; }
+  if (L.g_acc) gacc = L.g_acc[ray];
+  if (L.g_depth) gdep = L.g_depth[ray];
+  float br = L.bg_value, bgg = L.bg_value, bb = L.bg_value;
+  if (L.bg) { br = L.bg[3 * ray]; bgg = L.bg[3 * ray + 1]; bb = L.bg[3 * ray + 2]; }
+
+  // Per-sample forward quantities (recomputed in each sweep).
+  struct Smp { float w, tr_next, delta, cr, cg, cb, inv, tm, Cr, Cg, Cb; bool on, opq; };
+  auto sample = [&](int i, float carry_in, float* incl_out) {
+    Smp s;
+    s.on = i < N;
+    float tau = 0.f;
+    s.cr = s.cg = s.cb = s.tm = s.delta = s.inv = s.Cr = s.Cg = s.Cb = 0.f;
+    s.opq = false;
+    if (s.on) {
+      const float* st = L.state + 5 * (ray * N + i);
+      const float T = st[0], sig = st[1];
+      s.inv = 1.0f / (1.0f + 1e-6f - T);
+      s.Cr = st[2]; s.Cg = st[3]; s.Cb = st[4];
+      s.cr = clampf(s.Cr * s.inv, 0.f, 1.f);
+      s.cg = clampf(s.Cg * s.inv, 0.f, 1.f);
+      s.cb = clampf(s.Cb * s.inv, 0.f, 1.f);
+      const float t0 = td[i], t1 = td[i + 1];
+      s.tm = 0.5f * (t0 + t1);
+      s.delta = (t1 - t0) * dn;
+      tau = sig * s.delta;
+      s.opq = L.opaque && i == N - 1;
+    }
+    const float ft = (s.on && !s.opq) ? tau : 0.f;
+    const float incl = warp_inclusive_scan(ft, lane);
+    const float excl = incl - ft;
+    const float tr = expf(-(carry_in + excl));
+    const float a = s.opq ? 1.f : -expm1f(-tau);
+    s.w = s.on ? a * tr : 0.f;
+    s.tr_next = s.opq ? 0.f : expf(-(carry_in + incl));
+    *incl_out = __shfl_sync(0xffffffffu, incl, 31);
+    return s;
+  };
+
+  // sweep 1: totals
+  float carry = 0.f, acc = 0.f, D = 0.f;
+  for (int i0 = 0; i0 < N; i0 += 32) {
+    float tot;
+    Smp s = sample(i0 + lane, carry, &tot);
+    acc += s.w;
+    D += s.w * s.tm;
+    carry += tot;
+  }
+  acc = warp_sum(acc);
+  D = warp_sum(D);
+  const float eps = 1.1920929e-07f;
+  float dacc = gacc;
+  if (1.f - acc >= 0.f) dacc -= grr * br + grg * bgg + grb * bb;
+  float gD = 0.f;
+  {
+    const float val = D / fmaxf(acc, eps);
+    if (isfinite(val) && val >= td[0] && val <= td[N]) {
+      gD = gdep / fmaxf(acc, eps);
+      if (acc >= eps) dacc += -gdep * D / (acc * acc);
+    }
+  }
+  // sweep 2: Z = sum_j dL/dw_j w_j
+  carry = 0.f;
+  float Z = 0.f;
+  for (int i0 = 0; i0 < N; i0 += 32) {
+    float tot;
+    Smp s = sample(i0 + lane, carry, &tot);
+    const float gw = dacc + grr * s.cr + grg * s.cg + grb * s.cb + gD * s.tm;
+    Z += gw * s.w;
+    carry += tot;
+  }
+  Z = warp_sum(Z);
+  // sweep 3: seeds
+  carry = 0.f;
+  float zcarry = 0.f;
+  for (int i0 = 0; i0 < N; i0 += 32) {
+    const int i = i0 + lane;
+    float tot;
+    Smp s = sample(i, carry, &tot);
+    const float gw = dacc + grr * s.cr + grg * s.cg + grb * s.cb + gD * s.tm;
+    const float zi = warp_inclusive_scan(gw * s.w, lane);
+    const float suffix = Z - (zcarry + zi);
+    zcarry += __shfl_sync(0xffffffffu, zi, 31);
+    carry += tot;
+    if (s.on) {
+      const float gtau = gw * s.tr_next - suffix;
+      const float gsig = s.opq ? 0.f : gtau * s.delta;
+      // colour normalisation c = clamp(C / O, 0, 1), O = 1 + 1e-6 - T
+      const float mr = (s.Cr * s.inv >= 0.f && s.Cr * s.inv <= 1.f) ? 1.f : 0.f;
+      const float mg = (s.Cg * s.inv >= 0.f && s.Cg * s.inv <= 1.f) ? 1.f : 0.f;
+      const float mb = (s.Cb * s.inv >= 0.f && s.Cb * s.inv <= 1.f) ? 1.f : 0.f;
+      const float dcr = mr * s.w * grr, dcg = mg * s.w * grg, dcb = mb * s.w * grb;
+      float* sd = L.seeds + 5 * (ray * N + i);
+      sd[0] = gsig;
+      sd[1] = dcr * s.inv;
+      sd[2] = dcg * s.inv;
+      sd[3] = dcb * s.inv;
+      sd[4] = (dcr * s.Cr + dcg * s.Cg + dcb * s.Cb) * s.inv * s.inv;
+    }
+  }
+}
+
+// ============================================================ prep/finalize
+
+__global__ void prep_kernel(const PrepLaunch P) {
+  const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (s < P.n_counters) P.counters[s] = 0;
+  if (s == 0 && P.stats) P.stats[0] = 0ull;
+  if (s >= P.n_strokes) return;
+  if (P.gslots) {
+    float* g = P.gslots + s * GRAD_SLOTS;
+#pragma unroll
+    for (int j = 0; j < GRAD_SLOTS; j++) g[j] = 0.f;
+  }
+  const int sid = P.sdf_ids ? P.sdf_ids[s] : P.uniform_sdf_id;
+  const int base = (sid >> 4) & 15;
+  const int flags = sid & 15;
+  const float* prm = P.shape_params + s * (long long)P.param_stride;
+  float* rec = P.recs + s * REC_FLOATS;
+  const int np = sdf_id_param_count(sid);
+  const bool s1 = flags & F_S1;
+  const bool s3 = !s1 && (flags & F_S3);
+  if (!base_supported(base) || np > P.param_stride || sid < 0 || sid > 255 ||
+      ((base > B_TETRAHEDRON) && flags != 0)) {
+    // Unsupported stroke: flag it, never read its parameters, and make every
+    // sample that meets it NaN (the culling sphere is infinite) so that the error
+    // cannot pass silently.
+    atomicOr(P.status, ST_BAD_KIND);
+    rec[R_KIND] = __int_as_float(B_CAPPED_TORUS | (STEP_LAPLACE << 8));
+    rec[R_KFIX] = __int_as_float(0x7fc00000);
+    for (int j = R_COLOR; j < R_CULL_R; j++) rec[j] = 0.f;
+    P.cull_a[4 * s] = 0.f; P.cull_a[4 * s + 1] = 0.f; P.cull_a[4 * s + 2] = 0.f;
+    P.cull_a[4 * s + 3] = __int_as_float(0x7f800000);
+    P.cull_b[s] = 0.f;
+    return;
+  }
+  const float delta = P.sdf_delta ? P.sdf_delta[s] : P.uniform_delta;
+  const int mode = delta > 0.f ? (P.use_laplace ? STEP_LAPLACE : STEP_LINEAR) : STEP_HARD;
+  const float kappa = P.use_laplace ? 2.f : 0.5f;
+  int off = np;
+  V3 t = v3(0.f, 0.f, 0.f), sc = v3(1.f, 1.f, 1.f);
+  M3 R;
+  R.r0 = v3(1.f, 0.f, 0.f); R.r1 = v3(0.f, 1.f, 0.f); R.r2 = v3(0.f, 0.f, 1.f);
+  if (flags & F_T) { off -= 3; t = v3(prm[off], prm[off + 1], prm[off + 2]); }
+  if (flags & F_R) { off -= 3; R = euler_matrix(v3(prm[off], prm[off + 1], prm[off + 2])); }
+  if (s1) { off -= 1; sc = v3(prm[off], prm[off], prm[off]); }
+  else if (s3) { off -= 3; sc = v3(prm[off], prm[off + 1], prm[off + 2]); }
+  int kind = base | (flags << 4) | (mode << 8);
+  const bool s1k = s1 && P.inv_scale_radius;
+  const bool s3f = s3 && P.inv_scale_radius;
+  if (s1k) kind |= K_S1K;
+  if (s3f) kind |= K_S3FAC;
+  rec[R_KIND] = __int_as_float(kind);
+  const float* col = P.color_params + s * (long long)P.color_stride;
+  rec[R_COLOR] = col[0];
+  rec[R_COLOR + 1] = col[1];
+  rec[R_COLOR + 2] = col[2];
+  rec[R_DENSITY] = P.density ? P.density[s] : 0.f;
+  rec[R_KFIX] = kappa / delta * (s1k ? sc.x : 1.f);
+  rec[R_DELTA] = delta;
+
+  // culling: sdf_local >= Lg (|p| - rho0) with p the local point; world centre cw
+  float rho0 = 1.f, Lg = 1.f, smax = fmaxf(sc.x, fmaxf(sc.y, sc.z)), smin = fminf(sc.x, fminf(sc.y, sc.z));
+  V3 cw = t;
+  float Rb;
+  if (base <= B_TETRAHEDRON) {
+    // M = S^-1 R^T: row i is column i of R divided by s_i
+    rec[R_M + 0] = R.r0.x / sc.x; rec[R_M + 1] = R.r1.x / sc.x; rec[R_M + 2] = R.r2.x / sc.x;
+    rec[R_M + 3] = R.r0.y / sc.y; rec[R_M + 4] = R.r1.y / sc.y; rec[R_M + 5] = R.r2.y / sc.y;
+    rec[R_M + 6] = R.r0.z / sc.z; rec[R_M + 7] = R.r1.z / sc.z; rec[R_M + 8] = R.r2.z / sc.z;
+    rec[R_T] = t.x; rec[R_T + 1] = t.y; rec[R_T + 2] = t.z;
+    rec[R_S] = sc.x; rec[R_S + 1] = sc.y; rec[R_S + 2] = sc.z;
+    rec[R_SINV] = 1.f / sc.x; rec[R_SINV + 1] = 1.f / sc.y; rec[R_SINV + 2] = 1.f / sc.z;
+    const float bp = base_param_count(base) > 0 ? prm[0] : 0.f;
+    rec[R_BP] = bp;
+    switch (base) {
+      case B_SPHERE: rho0 = 1.f; Lg = 1.f; break;
+      case B_CUBE: rho0 = 1.7320509f; Lg = 1.f; break;
+      case B_ROUND_CUBE: rho0 = fmaxf(1.7320509f + bp, 0.f); Lg = 1.f; break;
+      case B_CAPSULE: rho0 = 1.f + fabsf(bp); Lg = 1.f; break;
+      case B_OCTAHEDRON: rho0 = 1.f; Lg = 0.5773502f; break;
+      case B_TETRAHEDRON: rho0 = 1.7320511f; Lg = 0.3333333f; break;
+      default: break;
+    }
+    Rb = smax * rho0;
+  } else if (base == B_QUAD_BEZIER) {
+    V3 A = v3(prm[0], prm[1], prm[2]), B = v3(prm[3], prm[4], prm[5]), C = v3(prm[6], prm[7], prm[8]);
+    V3 a = B - A;
+    V3 b = (A - B * 2.0f) + C;
+    V3 c = a * 2.0f;
+    for (int j = 0; j < 3; j++) {
+      rec[R_QA + j] = (&A.x)[j]; rec[R_QB + j] = (&B.x)[j]; rec[R_QC + j] = (&C.x)[j];
+      rec[R_Qa + j] = (&a.x)[j]; rec[R_Qb + j] = (&b.x)[j]; rec[R_Qc + j] = (&c.x)[j];
+    }
+    rec[R_QR1] = prm[9];
+    rec[R_QR2] = prm[10];
+    const float kk = 1.0f / dot(b, b);
+    rec[R_QKK] = kk;
+    rec[R_QKX] = kk * dot(a, b);
+    rec[R_QAA2] = 2.0f * dot(a, a);
+    rec[R_QAB] = dot(a, b);
+    cw = (A + B + C) * (1.f / 3.f);
+    float rc = fmaxf(sqrtf(dot(A - cw, A - cw)), fmaxf(sqrtf(dot(B - cw, B - cw)), sqrtf(dot(C - cw, C - cw))));
+    Rb = rc + fmaxf(prm[9], prm[10]);
+    smax = smin = 1.f;
+  } else {
+    V3 P4[4];
+    for (int k = 0; k < 4; k++) {
+      P4[k] = v3(prm[3 * k], prm[3 * k + 1], prm[3 * k + 2]);
+      rec[R_CA + 3 * k] = P4[k].x; rec[R_CA + 3 * k + 1] = P4[k].y; rec[R_CA + 3 * k + 2] = P4[k].z;
+    }
+    rec[R_CR1] = prm[12];
+    rec[R_CR2] = prm[13];
+    constexpr float step = 1.0f / CUBIC_SEGMENTS;
+    for (int i = 0; i <= CUBIC_SEGMENTS; i++) {
+      const float ti = i * step;
+      float w[4];
+      cubic_weights(ti, w);
+      V3 v = P4[0] * w[0] + P4[1] * w[1] + P4[2] * w[2] + P4[3] * w[3];
+      rec[R_CV + 3 * i] = v.x; rec[R_CV + 3 * i + 1] = v.y; rec[R_CV + 3 * i + 2] = v.z;
+    }
+    cw = (P4[0] + P4[1] + P4[2] + P4[3]) * 0.25f;
+    float rc = 0.f;
+    for (int k = 0; k < 4; k++) rc = fmaxf(rc, sqrtf(dot(P4[k] - cw, P4[k] - cw)));
+    Rb = rc + fmaxf(prm[12], prm[13]);
+    smax = smin = 1.f;
+  }
+  // margin per unit sample radius: the soft-step argument m = sdf * k exceeds the
+  // cut m_cut (alpha = exp(-m_cut)/2) beyond Rb + cm * r.
+  float cm = 0.f;
+  bool cull = true;
+  if (mode != STEP_HARD) {
+    const float mcut = mode == STEP_LINEAR ? 0.5f : P.cull_m;
+    if (mode == STEP_LAPLACE && P.cull_m < 0.f) cull = false;
+    if (base > B_TETRAHEDRON) {
+      cm = mcut * delta / kappa;
+    } else if (s1) {
+      cm = mcut * delta * (P.inv_scale_radius ? 1.f : sc.x) / (kappa * Lg);
+    } else if (s3) {
+      if (P.inv_scale_radius)
+        cm = base == B_SPHERE ? mcut * delta / kappa : mcut * delta * smax / (kappa * Lg * smin);
+      else
+        cm = mcut * delta * smax / (kappa * Lg);
+    } else {
+      cm = mcut * delta / (kappa * Lg);
+    }
+  }
+  if (!cull) Rb = __int_as_float(0x7f800000);
+  rec[R_CULL_R] = Rb * 1.0001f + 1e-6f;
+  rec[R_CULL_C] = cw.x; rec[R_CULL_C + 1] = cw.y; rec[R_CULL_C + 2] = cw.z;
+  rec[R_CULL_M] = cm * 1.0001f;
+  P.cull_a[4 * s] = cw.x; P.cull_a[4 * s + 1] = cw.y; P.cull_a[4 * s + 2] = cw.z;
+  P.cull_a[4 * s + 3] = rec[R_CULL_R];
+  P.cull_b[s] = rec[R_CULL_M];
+}
+
+__device__ void prim_param_grads(const FinalizeLaunch& F, long long s, int base, int flags, const float* g,
+                                 const float* rec, float* out);
+
+// Convert reduced slots into gradients of the raw reference-layout parameters.
+__global__ void finalize_kernel(const FinalizeLaunch F) {
+  const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (s >= F.n_strokes) return;
+  const float* g = F.gslots + s * GRAD_SLOTS;
+  const float* rec = F.recs + s * REC_FLOATS;
+  const int sid = F.sdf_ids ? F.sdf_ids[s] : F.uniform_sdf_id;
+  const int base = (sid >> 4) & 15;
+  const int flags = sid & 15;
+  const bool acc = F.accumulate != 0;
+  auto put = [&](float* dst, float v) { *dst = acc ? *dst + v : v; };
+  float* gc = F.grad_color + s * (long long)F.color_stride;
+  put(gc, g[G_COLOR]);
+  put(gc + 1, g[G_COLOR + 1]);
+  put(gc + 2, g[G_COLOR + 2]);
+  if (F.grad_density) put(F.grad_density + s, g[G_DENSITY]);
+  const float delta = F.sdf_delta ? F.sdf_delta[s] : F.uniform_delta;
+  if (F.grad_delta) put(F.grad_delta + s, (delta > 0.f && !F.compat) ? -g[G_K] / delta : 0.f);
+  float* out = F.grad_shape + s * (long long)F.param_stride;
+  float o[64];
+  for (int j = 0; j < F.param_stride && j < 64; j++) o[j] = 0.f;
+  if (base == B_QUAD_BEZIER) {
+    for (int j = 0; j < 11; j++) o[j] = g[G_CTRL + j];
+  } else if (base == B_CUBIC_BEZIER) {
+    for (int j = 0; j < 14; j++) o[j] = g[G_CTRL + j];
+  } else if (base <= B_TETRAHEDRON) {
+    prim_param_grads(F, s, base, flags, g, rec, o);
+  }
+  for (int j = 0; j < F.param_stride && j < 64; j++) put(out + j, o[j]);
+}
+
+// Primitive slots -> [base, scale (1|3), euler (3), translation (3)] gradients.
+__device__ void prim_param_grads(const FinalizeLaunch& F, long long s, int base, int flags, const float* g,
+                                 const float* rec, float* out) {
+  const bool s1 = flags & F_S1;
+  const bool s3 = !s1 && (flags & F_S3);
+  int off = 0;
+  const int nb = base_param_count(base);
+  if (nb > 0) out[0] = g[G_BP];
+  off = nb;
+  if (s1) { out[off] = g[G_SCALE]; off += 1; }
+  else if (s3) { out[off] = g[G_SCALE]; out[off + 1] = g[G_SCALE + 1]; out[off + 2] = g[G_SCALE + 2]; off += 3; }
+  if (flags & F_R) {
+    const float* e = F.shape_params + s * (long long)F.param_stride + off;
+    const float sx = sinf(e[0]), cx = cosf(e[0]), sy = sinf(e[1]), cy = cosf(e[1]);
+    const float tx = g[G_TORQUE], ty = g[G_TORQUE + 1], tz = g[G_TORQUE + 2];
+    // dL/de = w_k . torque with w_x = e_x, w_y = Rx^T e_y, w_z = R^T e_z
+    out[off] = tx;
+    out[off + 1] = cx * ty - sx * tz;
+    out[off + 2] = -sy * tx + sx * cy * ty + cx * cy * tz;
+    off += 3;
+  }
+  if (flags & F_T) {
+    // dL/dt = -M^T sum g_p
+    const float gx = g[G_GP], gy = g[G_GP + 1], gz = g[G_GP + 2];
+    for (int j = 0; j < 3; j++)
+      out[off + j] = -(rec[R_M + j] * gx + rec[R_M + 3 + j] * gy + rec[R_M + 6 + j] * gz);
+  }
+}
+
+// ================================================================ launchers
+
+void launch_prep(const PrepLaunch& p, cudaStream_t st) {
+  long long n = p.n_strokes > p.n_counters ? p.n_strokes : p.n_counters;
+  if (n < 1) n = 1;
+  const int threads = 128;
+  prep_kernel<<<(unsigned)((n + threads - 1) / threads), threads, 0, st>>>(p);
+}
+
+template <int W>
+static cudaError_t launch_fwd_w(const SegLaunch& L, int grid, size_t smem, cudaStream_t st) {
+  cudaError_t e = cudaFuncSetAttribute(seg_fwd_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  seg_fwd_kernel<W><<<grid, W * 32, smem, st>>>(L);
+  return cudaGetLastError();
+}
+template <int W>
+static cudaError_t launch_bwd_w(const SegLaunch& L, int grid, size_t smem, cudaStream_t st) {
+  cudaError_t e = cudaFuncSetAttribute(seg_bwd_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  seg_bwd_kernel<W><<<grid, W * 32, smem, st>>>(L);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_seg_fwd(const SegLaunch& L, int grid, int warps, size_t smem, cudaStream_t st) {
+  switch (warps) {
+    case 4: return launch_fwd_w<4>(L, grid, smem, st);
+    case 8: return launch_fwd_w<8>(L, grid, smem, st);
+    case 16: return launch_fwd_w<16>(L, grid, smem, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+cudaError_t launch_seg_bwd(const SegLaunch& L, int grid, int warps, size_t smem, cudaStream_t st) {
+  switch (warps) {
+    case 4: return launch_bwd_w<4>(L, grid, smem, st);
+    case 8: return launch_bwd_w<8>(L, grid, smem, st);
+    case 16: return launch_bwd_w<16>(L, grid, smem, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+void launch_ray_fwd(const RayLaunch& L, cudaStream_t st) {
+  const long long threads = L.n_rays * 32;
+  const int bs = 256;
+  ray_fwd_kernel<<<(unsigned)((threads + bs - 1) / bs), bs, 0, st>>>(L);
+}
+void launch_ray_bwd(const RayLaunch& L, cudaStream_t st) {
+  const long long threads = L.n_rays * 32;
+  const int bs = 256;
+  ray_bwd_kernel<<<(unsigned)((threads + bs - 1) / bs), bs, 0, st>>>(L);
+}
+void launch_finalize(const FinalizeLaunch& L, cudaStream_t st) {
+  const int bs = 128;
+  finalize_kernel<<<(unsigned)((L.n_strokes + bs - 1) / bs), bs, 0, st>>>(L);
+}
+
+}  // namespace n3ds

@@ -1,0 +1,126 @@
+// Launch descriptors and kernel declarations of the fused stroke field.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace n3ds {
+
+constexpr int MAX_SCENES_PER_LAUNCH = 40;
+
+// One scene of a (possibly batched) launch. Rays, samples and strokes of all
+// scenes are concatenated; these give the scene's slice.
+struct SceneDesc {
+  long long ray_begin;   // first ray (global)
+  int n_rays;
+  int stroke_begin;      // first stroke (global)
+  int n_strokes;
+  int tile_begin;        // first tile of this scene in the current launch
+  int chunk_lo;          // stroke range of the current pass, scene-local
+  int chunk_n;
+  int first_pass;        // 1: composite state starts fresh
+  int last_pass;         // 1: the pass that finishes the scene
+};
+
+struct SegLaunch {
+  const float* x;          // [P*3]
+  const float* radius;     // [P]
+  int n_samples;           // samples per ray
+  int segs_per_ray;        // ceil(n_samples / 32)
+  const float* recs;       // [S*64] prepared stroke records
+  const float* cull_a;     // [S*4]  culling sphere (cx, cy, cz, R)
+  const float* cull_b;     // [S(+pad)] culling margin per unit radius
+  float* state;            // [P*5] composite state / forward checkpoint (T, sigma, C)
+  const float* seeds;      // [P*5] backward seeds (g_sigma, g_C, g_T)
+  float* bstate;           // [P*8] backward running state between passes
+  float* grad_x;           // [P*3] or null
+  float* gslots;           // [S*32] reduced per-stroke gradient slots
+  int compat;              // reference gradient formulas
+  int n_scenes;
+  int tiles_total;
+  int segs_per_tile;
+  int chunk_cap;           // strokes per shared-memory stage
+  int* tile_counter;
+  int* status;
+  unsigned long long* stats;  // [0] evaluated (sample, stroke) pairs
+  SceneDesc sc[MAX_SCENES_PER_LAUNCH];
+};
+
+struct RayLaunch {
+  const float* state;      // [P*5]
+  const float* tdist;      // [R*(N+1)]
+  const float* dirs;       // [R*3]
+  const float* bg;         // [R*3] or null
+  float bg_value;
+  int opaque;
+  long long n_rays;
+  int n_samples;
+  float* rgb;              // [R*3]
+  float* acc;              // [R]
+  float* depth;            // [R]
+  // backward
+  const float* g_rgb;      // [R*3] or null
+  const float* g_acc;      // [R] or null
+  const float* g_depth;    // [R] or null
+  float* seeds;            // [P*5]
+};
+
+struct PrepLaunch {
+  const int* sdf_ids;      // [S], or null with uniform_sdf_id
+  int uniform_sdf_id;
+  const float* shape_params;
+  int param_stride;
+  const float* color_params;
+  int color_stride;
+  const float* density;    // [S] or null (zero density)
+  const float* sdf_delta;  // [S] or null with uniform_delta
+  float uniform_delta;
+  int use_laplace;
+  int inv_scale_radius;
+  float cull_m;            // soft-step argument beyond which a stroke is dropped; <0 disables
+  long long n_strokes;
+  float* recs;
+  float* cull_a;
+  float* cull_b;
+  int* status;
+  // zeroed by the prep kernel (graph-capture friendly resets)
+  int* counters;
+  int n_counters;
+  float* gslots;           // zeroed when non-null
+  unsigned long long* stats;
+};
+
+struct FinalizeLaunch {
+  const int* sdf_ids;      // [S], or null with uniform_sdf_id
+  int uniform_sdf_id;
+  const float* shape_params;
+  int param_stride;
+  const float* sdf_delta;  // [S] or null with uniform_delta
+  float uniform_delta;
+  const float* recs;
+  const float* gslots;
+  long long n_strokes;
+  int compat;
+  float* grad_shape;       // [S*param_stride]
+  float* grad_color;       // [S*3]
+  float* grad_density;     // [S]
+  float* grad_delta;       // [S] or null
+  int accumulate;          // 1: add into the outputs instead of overwriting
+  int color_stride;        // floats per stroke row of grad_color (3 for the fused path)
+};
+
+// status word bits
+constexpr int ST_BAD_KIND = 1;
+constexpr int ST_WAIT_TIMEOUT = 2;
+
+void launch_prep(const PrepLaunch& p, cudaStream_t st);
+cudaError_t launch_seg_fwd(const SegLaunch& L, int grid, int warps, size_t smem, cudaStream_t st);
+cudaError_t launch_seg_bwd(const SegLaunch& L, int grid, int warps, size_t smem, cudaStream_t st);
+void launch_ray_fwd(const RayLaunch& L, cudaStream_t st);
+void launch_ray_bwd(const RayLaunch& L, cudaStream_t st);
+void launch_finalize(const FinalizeLaunch& L, cudaStream_t st);
+
+size_t seg_fwd_smem(int chunk_cap);
+size_t seg_bwd_smem(int chunk_cap);
+
+}  // namespace n3ds

@@ -1,0 +1,362 @@
+// Signed distance primitives of the stroke field: values and exact adjoints.
+//
+// Values follow the reference definitions (strokes_sdf.h, cited per function),
+// including their 1e-8 regularisers, so outputs agree with the reference op.
+// Adjoints are the exact derivatives of these computed functions (what float64
+// autograd of the same definitions gives): the quadratic Bezier is differentiated
+// in reverse mode through its closed-form closest-parameter solve, the cubic Bezier
+// through its polyline projection, so both include the dependence of the closest
+// parameter t on the sample and the control points.
+#pragma once
+#include "n3ds_record.cuh"
+
+namespace n3ds {
+
+constexpr float OCTA_K = 0.57735027f;  // strokes_sdf.h:587,612
+constexpr float BEZ_SQRT3 = 1.732050808f;  // strokes_sdf.h:686
+
+__device__ __forceinline__ V3 sub1(V3 a, float s) { return {a.x - s, a.y - s, a.z - s}; }
+
+// Axis chosen by the reference's inside-cube argmax tie-breaking (strokes_sdf.h:283-286).
+__device__ __forceinline__ V3 cube_inside_axis(V3 q, V3 sg) {
+  return {(q.x >= q.y && q.x >= q.z) ? sg.x : 0.f,
+          (q.x < q.y && q.y >= q.z) ? sg.y : 0.f,
+          (q.x < q.z && q.y < q.z) ? sg.z : 0.f};
+}
+
+// ------------------------------------------------------------------ primitives
+// p is the local-frame sample, bp the base parameter.
+
+__device__ __forceinline__ float prim_sdf(int base, V3 p, float bp) {
+  switch (base) {
+    case B_SPHERE:  // strokes_sdf.h:245-249
+      return sqrtf(dot(p, p) + 1e-8f) - 1.f;
+    case B_CUBE: {  // 273-277
+      V3 q = sub1(vabs(p), 1.f);
+      V3 qp = vmax0(q);
+      return sqrtf(dot(qp, qp)) + fminf(max3(q), 0.f);
+    }
+    case B_ROUND_CUBE: {  // 316-325
+      V3 q = sub1(vabs(p), 1.f);
+      V3 qp = vmax0(q);
+      return sqrtf(dot(qp, qp) + 1e-8f) + fminf(max3(q), 0.f) - bp;
+    }
+    case B_CAPSULE: {  // 434-440
+      p.y -= clampf(p.y, -bp, bp);
+      return sqrtf(dot(p, p) + 1e-8f) - 1.f;
+    }
+    case B_OCTAHEDRON:  // 584-588
+      return (fabsf(p.x) + fabsf(p.y) + fabsf(p.z) - 1.f) * OCTA_K;
+    case B_TETRAHEDRON:  // 610-613
+      return (fmaxf(fabsf(p.x + p.y) - p.z, fabsf(p.x - p.y) + p.z) - 1.f) * OCTA_K;
+    default:
+      return __int_as_float(0x7fc00000);
+  }
+}
+
+// Exact dSDF/dp of prim_sdf; *gbp receives dSDF/d(base parameter).
+// compat != 0 reproduces the reference's cube exterior formula 2*max(q,0)
+// (strokes_sdf.h:289) instead of the normalised one.
+__device__ __forceinline__ V3 prim_grad(int base, V3 p, float bp, float* gbp, int compat) {
+  *gbp = 0.f;
+  switch (base) {
+    case B_SPHERE: {
+      float inv = rsqrtf(dot(p, p) + 1e-8f);
+      return p * inv;
+    }
+    case B_CUBE: {
+      V3 q = sub1(vabs(p), 1.f);
+      V3 sg = vsgn(p);
+      if (max3(q) <= 0.f) return cube_inside_axis(q, sg);
+      V3 qp = vmax0(q);
+      if (compat) return sg * (qp * 2.f);
+      return sg * (qp * rsqrtf(dot(qp, qp)));
+    }
+    case B_ROUND_CUBE: {
+      V3 q = sub1(vabs(p), 1.f);
+      V3 sg = vsgn(p);
+      V3 qp = vmax0(q);
+      V3 g = sg * (qp * rsqrtf(dot(qp, qp) + 1e-8f));
+      if (max3(q) < 0.f) g += cube_inside_axis(q, sg);
+      *gbp = -1.f;
+      return g;
+    }
+    case B_CAPSULE: {
+      float y = p.y;
+      p.y -= clampf(y, -bp, bp);
+      float inv = rsqrtf(dot(p, p) + 1e-8f);
+      *gbp = -sgn(y) * p.y * inv;  // p.y == 0 on the straight part
+      return p * inv;
+    }
+    case B_OCTAHEDRON:
+      return vsgn(p) * OCTA_K;
+    case B_TETRAHEDRON: {
+      float a = p.x + p.y, c = p.x - p.y;
+      if (fabsf(a) - p.z > fabsf(c) + p.z) {
+        float sa = sgn(a) * OCTA_K;
+        return {sa, sa, -OCTA_K};
+      }
+      float sc = sgn(c) * OCTA_K;
+      return {sc, -sc, OCTA_K};
+    }
+    default:
+      return {0.f, 0.f, 0.f};
+  }
+}
+
+// Radius factor f of a multi-scale transform under inv_scale_radius
+// (strokes_forward.cu:74-81): f = |g*s| / |g| with g the SDF gradient direction.
+// For the sphere base g is parallel to p, so f = |s*p| / |p|.
+__device__ __forceinline__ float s3_factor(int base, V3 p, V3 s) {
+  V3 g;
+  if (base == B_SPHERE) {
+    g = p;
+  } else {
+    float unused;
+    g = prim_grad(base, p, 0.f, &unused, 0);
+  }
+  V3 gs = g * s;
+  return sqrtf(dot(gs, gs)) / sqrtf(dot(g, g));
+}
+
+// ---------------------------------------------------------- quadratic Bezier
+// strokes_sdf.h:649-715, with per-stroke constants from the record.
+
+struct QuadFwd {
+  float t, t_raw, dist;
+  V3 d, e;
+  float kx, ky, p, q, h;
+  // h >= 0 branch
+  float H, x0, x1, u0, u1;
+  // h < 0 branch
+  float z, den, arg, v, m, n, sigma;  // sigma = +1 for the (m+n) root, -1 for -(m+n)
+  int pos_branch;
+};
+
+__device__ __forceinline__ float quad_eval(const float* rec, V3 pos, QuadFwd& s) {
+  V3 A = ld3(rec + R_QA), a = ld3(rec + R_Qa), b = ld3(rec + R_Qb), c = ld3(rec + R_Qc);
+  float kk = rec[R_QKK], kx = rec[R_QKX];
+  V3 d = A - pos;
+  float ky = kk * (rec[R_QAA2] + dot(d, b)) / 3.0f;
+  float kz = kk * dot(d, a);
+  float p = ky - kx * kx;
+  float p3 = p * p * p;
+  float q = kx * (2.0f * kx * kx - 3.0f * ky) + kz;
+  float h = q * q + 4.0f * p3;
+  s.d = d; s.kx = kx; s.ky = ky; s.p = p; s.q = q; s.h = h;
+  float t, t_raw;
+  if (h >= 0.0f) {
+    s.pos_branch = 1;
+    float H = sqrtf(h + 1e-8f);
+    float x0 = (H - q) * 0.5f, x1 = -(H + q) * 0.5f;
+    float u0 = copysignf(cbrtf(fabsf(x0)), x0), u1 = copysignf(cbrtf(fabsf(x1)), x1);
+    t_raw = (u0 + u1) - kx;
+    t = clampf(t_raw, 0.f, 1.f);
+    s.H = H; s.x0 = x0; s.x1 = x1; s.u0 = u0; s.u1 = u1;
+  } else {
+    s.pos_branch = 0;
+    float z = sqrtf(-p + 1e-8f);
+    float den = p * z * 2.0f + 1e-8f;
+    float arg = q / den;
+    float v = acosf(arg) / 3.0f;
+    float sv, cv;
+    sincosf(v, &sv, &cv);
+    float m = cv, n = sv * BEZ_SQRT3;
+    float ra = (m + n) * z - kx, rb = (-n - m) * z - kx;
+    float ta = clampf(ra, 0.f, 1.f), tb = clampf(rb, 0.f, 1.f);
+    V3 ea = d + (c + b * ta) * ta, eb = d + (c + b * tb) * tb;
+    float da = dot(ea, ea), db = dot(eb, eb);
+    bool use_b = db < da;
+    t = use_b ? tb : ta;
+    t_raw = use_b ? rb : ra;
+    s.z = z; s.den = den; s.arg = arg; s.v = v; s.m = m; s.n = n; s.sigma = use_b ? -1.f : 1.f;
+  }
+  V3 e = d + (c + b * t) * t;
+  float dist = sqrtf(dot(e, e) + 1e-8f);
+  s.t = t; s.t_raw = t_raw; s.e = e; s.dist = dist;
+  float r1 = rec[R_QR1], r2 = rec[R_QR2];
+  return dist - (r1 + t * (r2 - r1));
+}
+
+// Reverse mode of quad_eval for upstream w = dL/dSDF.
+// Returns dL/dpos; g[0..8] += dL/d(A,B,C), g[9], g[10] += dL/d(r1, r2).
+__device__ __forceinline__ V3 quad_adjoint(const float* rec, const QuadFwd& s, float w, float* g) {
+  V3 a = ld3(rec + R_Qa), b = ld3(rec + R_Qb), c = ld3(rec + R_Qc);
+  float kk = rec[R_QKK];
+  float r1 = rec[R_QR1], r2 = rec[R_QR2];
+  float t = s.t;
+  V3 ge = s.e * (w / s.dist);           // dL/de
+  V3 gd = ge;                           // e = d + c t + b t^2
+  V3 gc = ge * t;
+  V3 gb = ge * (t * t);
+  float gt = -w * (r2 - r1) + dot(ge, c + b * (2.f * t));
+  g[9] += -w * (1.f - t);
+  g[10] += -w * t;
+  float gtr = (s.t_raw > 0.f && s.t_raw < 1.f) ? gt : 0.f;
+  float gkx = -gtr, gky = 0.f, gkz = 0.f, gp = 0.f, gq = 0.f;
+  if (gtr == 0.f) {
+    // t is clamped (or the solve gave NaN): no dependence through the root
+  } else if (s.pos_branch) {
+    float gx0 = s.x0 != 0.f ? gtr / (3.f * s.u0 * s.u0) : 0.f;
+    float gx1 = s.x1 != 0.f ? gtr / (3.f * s.u1 * s.u1) : 0.f;
+    float gH = 0.5f * (gx0 - gx1);
+    gq = -0.5f * (gx0 + gx1);
+    float gh = gH * 0.5f / s.H;
+    gq += 2.f * s.q * gh;
+    gp = 12.f * s.p * s.p * gh;
+  } else {
+    float gz = gtr * s.sigma * (s.m + s.n);
+    float gm = gtr * s.sigma * s.z;
+    float gn = gm;
+    float sv = sinf(s.v), cv = cosf(s.v);
+    float gv = -sv * gm + BEZ_SQRT3 * cv * gn;
+    float garg = -(gv / 3.f) * rsqrtf(1.f - s.arg * s.arg);
+    gq = garg / s.den;
+    float gden = -garg * s.arg / s.den;
+    gp = 2.f * s.z * gden;
+    gz += 2.f * s.p * gden;
+    gp += gz * (-0.5f / s.z);
+  }
+  // p = ky - kx^2 ; q = kx (2 kx^2 - 3 ky) + kz
+  gky += gp;
+  gkx += -2.f * s.kx * gp;
+  gkx += gq * (6.f * s.kx * s.kx - 3.f * s.ky);
+  gky += -3.f * s.kx * gq;
+  gkz += gq;
+  // ky = kk (aa2 + d.b) / 3 ; kz = kk (d.a)
+  float db = dot(s.d, b), da = dot(s.d, a);
+  float gkk = gky * (rec[R_QAA2] + db) / 3.f + gkz * da;
+  float gaa2 = gky * kk / 3.f;
+  float gdb = gky * kk / 3.f;
+  float gda = gkz * kk;
+  gd += b * gdb + a * gda;
+  gb += s.d * gdb;
+  V3 ga = s.d * gda;
+  // stroke constants: kx = kk (a.b), kk = 1/(b.b), aa2 = 2 a.a, c = 2 a
+  gkk += gkx * rec[R_QAB];
+  ga += b * (gkx * kk);
+  gb += a * (gkx * kk);
+  gb += b * (-2.f * kk * kk * gkk);
+  ga += a * (4.f * gaa2);
+  ga += gc * 2.f;
+  // a = B - A ; b = A - 2B + C ; d = A - pos
+  V3 gA = gd - ga + gb, gB = ga - gb * 2.f, gC = gb;
+  g[0] += gA.x; g[1] += gA.y; g[2] += gA.z;
+  g[3] += gB.x; g[4] += gB.y; g[5] += gB.z;
+  g[6] += gC.x; g[7] += gC.y; g[8] += gC.z;
+  return -gd;
+}
+
+// -------------------------------------------------------------- cubic Bezier
+// strokes_sdf.h:1238-1294: the closest parameter is taken from a 10-segment
+// polyline (vertices precomputed per stroke), then the distance to the curve point.
+
+__device__ __forceinline__ void cubic_weights(float t, float w[4]) {
+  float u = 1.0f - t;
+  w[0] = u * u * u;
+  w[1] = 3.0f * u * u * t;
+  w[2] = 3.0f * u * t * t;
+  w[3] = t * t * t;
+}
+
+struct CubicFwd {
+  float t, tau, tau_raw, dist;
+  int seg;  // winning segment 1..10, 0 when none
+  V3 v;     // B(t) - pos
+};
+
+__device__ __forceinline__ float cubic_eval(const float* rec, V3 pos, CubicFwd& s) {
+  constexpr float step = 1.0f / CUBIC_SEGMENTS;
+  float best = 1e18f, t_min = 0.f, tau_best = 0.f, tau_raw_best = 0.f;
+  int seg = 0;
+  float t_start = 0.f;
+  V3 s0 = ld3(rec + R_CV);
+#pragma unroll
+  for (int i = 1; i <= CUBIC_SEGMENTS; i++) {
+    float t_end = i * step;
+    V3 s1 = ld3(rec + R_CV + 3 * i);
+    V3 ab = s1 - s0;
+    float tr = dot(pos - s0, ab) / dot(ab, ab);
+    float tt = clampf(tr, 0.f, 1.f);
+    V3 dv = pos - (s0 + ab * tt);
+    float d2 = dot(dv, dv);
+    if (d2 < best) {
+      best = d2;
+      t_min = t_start * (1.0f - tt) + t_end * tt;
+      tau_best = tt;
+      tau_raw_best = tr;
+      seg = i;
+    }
+    t_start = t_end;
+    s0 = s1;
+  }
+  float w[4];
+  cubic_weights(t_min, w);
+  V3 P = ld3(rec + R_CA) * w[0] + ld3(rec + R_CB) * w[1] + ld3(rec + R_CC) * w[2] + ld3(rec + R_CD) * w[3];
+  V3 v = P - pos;
+  float dist = sqrtf(dot(v, v));
+  s.t = t_min; s.tau = tau_best; s.tau_raw = tau_raw_best; s.seg = seg; s.v = v; s.dist = dist;
+  float r1 = rec[R_CR1], r2 = rec[R_CR2];
+  return dist - (r1 + t_min * (r2 - r1));
+}
+
+// Reverse mode of cubic_eval. compat != 0 reproduces the reference gradient
+// (strokes_sdf.h:1296-1322): -w*2v for position, 2w v * weights for control points,
+// no dependence of t on the inputs. Returns dL/dpos (before the reference's second
+// multiplication by dL/dSDF, which the caller applies in compat mode).
+// g[0..11] += dL/d(A,B,C,D); g[12], g[13] += dL/d(r1, r2).
+__device__ __forceinline__ V3 cubic_adjoint(const float* rec, V3 pos, const CubicFwd& s, float w,
+                                            float* g, int compat) {
+  constexpr float step = 1.0f / CUBIC_SEGMENTS;
+  float r1 = rec[R_CR1], r2 = rec[R_CR2];
+  float t = s.t;
+  float bw[4];
+  cubic_weights(t, bw);
+  g[12] += -w * (1.f - t);
+  g[13] += -w * t;
+  if (compat) {
+    V3 gv = s.v * (2.f * w);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      g[3 * k + 0] += gv.x * bw[k];
+      g[3 * k + 1] += gv.y * bw[k];
+      g[3 * k + 2] += gv.z * bw[k];
+    }
+    return -gv;
+  }
+  V3 A = ld3(rec + R_CA), B = ld3(rec + R_CB), C = ld3(rec + R_CC), D = ld3(rec + R_CD);
+  V3 gv = s.v * (w / s.dist);
+  float u = 1.f - t;
+  V3 dB = (B - A) * (3.f * u * u) + (C - B) * (6.f * u * t) + (D - C) * (3.f * t * t);
+  float gt = -w * (r2 - r1) + dot(gv, dB);
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    g[3 * k + 0] += gv.x * bw[k];
+    g[3 * k + 1] += gv.y * bw[k];
+    g[3 * k + 2] += gv.z * bw[k];
+  }
+  V3 gpos = -gv;
+  if (s.seg > 0 && s.tau_raw > 0.f && s.tau_raw < 1.f) {
+    float t0 = (s.seg - 1) * step, t1 = s.seg * step;
+    float gtau = gt * (t1 - t0);
+    V3 s0 = ld3(rec + R_CV + 3 * (s.seg - 1)), s1 = ld3(rec + R_CV + 3 * s.seg);
+    V3 ab = s1 - s0;
+    V3 wv = pos - s0;
+    float inv = 1.f / dot(ab, ab);
+    gpos += ab * (gtau * inv);
+    V3 g0 = (ab * (2.f * s.tau - 1.f) - wv) * (gtau * inv);
+    V3 g1 = (wv - ab * (2.f * s.tau)) * (gtau * inv);
+    float w0[4], w1[4];
+    cubic_weights(t0, w0);
+    cubic_weights(t1, w1);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      g[3 * k + 0] += g0.x * w0[k] + g1.x * w1[k];
+      g[3 * k + 1] += g0.y * w0[k] + g1.y * w1[k];
+      g[3 * k + 2] += g0.z * w0[k] + g1.z * w1[k];
+    }
+  }
+  return gpos;
+}
+
+}  // namespace n3ds

@@ -1,0 +1,427 @@
+// The reference `_strokelib` operators over dense [P, S] tensors, B200 style.
+//
+// The reference runs one thread per (sample, stroke) with 32-bit indices and up to
+// 14 global atomics per pair (strokes_backward.cu), and one thread per sample with
+// row-strided reads (compositing.cu). Here:
+// - stroke forward: a warp evaluates 32 samples x 32 strokes with the stroke record
+//   broadcast from shared memory, and writes alpha / colour rows coalesced through a
+//   transposed shared-memory tile;
+// - stroke backward: lane = stroke; each lane accumulates its stroke's reduced
+//   gradient slots in registers across all samples the warp visits (no per-pair
+//   atomics), grad_x is a warp sum per sample;
+// - compose forward / backward: lane = sample with the serial stroke loop of the
+//   reference (same multiplication order), fed by coalesced tile loads transposed in
+//   shared memory. The exact backward uses a top-down sweep for T_s and a bottom-up
+//   "under" sweep, so it needs no division by (1 - alpha).
+// All indices are 64-bit.
+#include "n3ds_eval.cuh"
+#include "n3ds_unfused.cuh"
+
+namespace n3ds {
+
+constexpr int UF_WARPS = 4;
+
+__global__ void __launch_bounds__(UF_WARPS * 32) uf_stroke_fwd_kernel(const UfStroke L) {
+  __shared__ float recs[32 * REC_FLOATS];
+  __shared__ float ta[UF_WARPS][32][33];
+  __shared__ float tsd[UF_WARPS][32][33];
+  const int s0 = blockIdx.y * 32;
+  const int ns = min(32, L.n_strokes - s0);
+  for (int i = threadIdx.x; i < ns * REC_FLOATS; i += blockDim.x) recs[i] = L.recs[(long long)s0 * REC_FLOATS + i];
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long S = L.n_strokes;
+  for (long long p0 = ((long long)blockIdx.x * UF_WARPS + warp) * 32; p0 < L.n_points;
+       p0 += (long long)gridDim.x * UF_WARPS * 32) {
+    const long long p = p0 + lane;
+    const long long pp = p < L.n_points ? p : p0;
+    const V3 x = v3(L.x[3 * pp], L.x[3 * pp + 1], L.x[3 * pp + 2]);
+    const float rinv = 1.f / L.radius[pp];
+    for (int j = 0; j < ns; j++) {
+      float sdf;
+      ta[warp][lane][j] = pair_alpha(recs + j * REC_FLOATS, x, rinv, &sdf);
+      tsd[warp][lane][j] = sdf;
+    }
+    __syncwarp();
+    const int rows = (int)min(32LL, L.n_points - p0);
+    for (int rr = 0; rr < rows; rr++) {
+      const long long row = (p0 + rr) * S + s0;
+      if (lane < ns) {
+        L.alpha[row + lane] = ta[warp][rr][lane];
+        if (L.sdf) L.sdf[row + lane] = tsd[warp][rr][lane];
+      }
+      for (int e = lane; e < 3 * ns; e += 32) L.color[row * 3 + e] = recs[(e / 3) * REC_FLOATS + R_COLOR + e % 3];
+    }
+    __syncwarp();
+  }
+}
+
+template <int NV>
+__global__ void __launch_bounds__(UF_WARPS * 32) uf_stroke_bwd_kernel(const UfStroke L) {
+  constexpr int RS = REC_FLOATS + 1;  // padded stride: lane-indexed record reads hit distinct banks
+  __shared__ float recs[32 * RS];
+  const int s0 = blockIdx.y * 32;
+  const int ns = min(32, L.n_strokes - s0);
+  for (int i = threadIdx.x; i < ns * REC_FLOATS; i += blockDim.x)
+    recs[(i / REC_FLOATS) * RS + (i % REC_FLOATS)] = L.recs[(long long)s0 * REC_FLOATS + i];
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const bool active = lane < ns;
+  const float* rec = recs + (active ? lane : 0) * RS;
+  const int kind = __float_as_int(rec[R_KIND]);
+  const int base = kind & 15;
+  const int mode = (kind >> 8) & 3;
+  const long long S = L.n_strokes;
+  float v[NV];
+#pragma unroll
+  for (int j = 0; j < NV; j++) v[j] = 0.f;
+  for (long long p = (long long)blockIdx.x * UF_WARPS + warp; p < L.n_points; p += (long long)gridDim.x * UF_WARPS) {
+    const V3 x = v3(L.x[3 * p], L.x[3 * p + 1], L.x[3 * p + 2]);
+    const float rinv = 1.f / L.radius[p];
+    const long long pi = p * S + s0 + lane;
+    const float ga = active ? L.g_alpha[pi] : 0.f;
+    const float a = active ? L.alpha_in[pi] : 0.f;
+    const float gs = (active && L.g_sdf) ? L.g_sdf[pi] : 0.f;
+    if (active) {
+      v[G_COLOR] += L.g_color[3 * pi];
+      v[G_COLOR + 1] += L.g_color[3 * pi + 1];
+      v[G_COLOR + 2] += L.g_color[3 * pi + 2];
+    }
+    float sdf, f = 1.f;
+    V3 pl;
+    QuadFwd qf;
+    CubicFwd cf;
+    if (base <= B_TETRAHEDRON) {
+      pl = prim_local(rec, x);
+      sdf = prim_sdf(base, pl, rec[R_BP]);
+      if (kind & K_S3FAC) f = s3_factor(base, pl, ld3(rec + R_S));
+    } else if (base == B_QUAD_BEZIER) {
+      sdf = quad_eval(rec, x, qf);
+    } else {
+      sdf = cubic_eval(rec, x, cf);
+    }
+    const float kk = rec[R_KFIX] * f * rinv;
+    const float m = -sdf * kk;
+    float dsdf, K;
+    if (mode == STEP_HARD) {
+      dsdf = gs;
+      K = 0.f;
+    } else if (L.compat) {
+      // strokes_backward.cu:85-94: dAlpha/dSDF from the saved alpha
+      const float dad = mode == STEP_LAPLACE ? (a < 0.5f ? a : 1.0f - a) * -kk
+                                             : ((a > 0.f && a < 0.9999f) ? -kk : 0.f);
+      dsdf = ga * dad + gs;
+      K = 0.f;
+    } else {
+      const float dm = soft_dm(mode, m, a, ga);
+      dsdf = -kk * dm + gs;
+      K = m * dm;
+    }
+    v[G_K] += K;
+    V3 gx;
+    if (base <= B_TETRAHEDRON) {
+      gx = prim_backprop(rec, kind, pl, dsdf, K, v, L.compat);
+    } else if (base == B_QUAD_BEZIER) {
+      gx = quad_adjoint(rec, qf, dsdf, v + G_CTRL);
+    } else {
+      gx = cubic_adjoint(rec, x, cf, dsdf, v + G_CTRL, L.compat);
+      if (L.compat) gx = gx * dsdf;  // the reference multiplies by dL/dSDF again
+    }
+    if (L.grad_x) {
+      const float sx = warp_sum(gx.x), sy = warp_sum(gx.y), sz = warp_sum(gx.z);
+      if (lane == 0) {
+        atomicAdd(L.grad_x + 3 * p, sx);
+        atomicAdd(L.grad_x + 3 * p + 1, sy);
+        atomicAdd(L.grad_x + 3 * p + 2, sz);
+      }
+    }
+  }
+  if (active) {
+    float* dst = L.gslots + (long long)(s0 + lane) * GRAD_SLOTS;
+#pragma unroll
+    for (int j = 0; j < NV; j++)
+      if (v[j] != 0.f) atomicAdd(dst + j, v[j]);
+  }
+}
+
+// ------------------------------------------------------------------ compose
+
+constexpr int UC_WARPS = 4;     // compose forward
+constexpr int UCB_WARPS = 2;    // compose backward (twice the tiles per warp)
+
+template <int C, int W>
+struct ComposeTiles {
+  float a[W][32][33];
+  float c[W][32][32 * C + 1];
+};
+template <int C, int W>
+struct ComposeBwdTiles {
+  ComposeTiles<C, W> t;
+  float x[W][32][33];          // per-pair alpha grad / T_s tile
+  float g[W][32][32 * C + 1];  // per-pair colour grad tile
+};
+
+// Load a tile of 32 sample rows x nb strokes starting at stroke s_first, stroke
+// order descending (dir = -1) or ascending (dir = +1), into the warp's tiles.
+template <int C, int W>
+__device__ __forceinline__ void load_tile(ComposeTiles<C, W>& t, int warp, int lane, const UfCompose& L, long long p0,
+                                          int rows, int s_first, int nb, int dir, const float* extra,
+                                          float (*te)[33]) {
+  const long long S = L.n_strokes;
+  for (int rr = 0; rr < rows; rr++) {
+    const long long row = (p0 + rr) * S;
+    if (lane < nb) {
+      const long long s = s_first + dir * lane;
+      t.a[warp][rr][lane] = L.alphas[row + s];
+      if (extra) te[rr][lane] = extra[row + s];
+    }
+    for (int e = lane; e < nb * C; e += 32) {
+      const int j = e / C, ch = e - j * C;
+      t.c[warp][rr][j * C + ch] = L.colors[(row + s_first + dir * j) * C + ch];
+    }
+  }
+}
+
+template <int C>
+__global__ void __launch_bounds__(UC_WARPS * 32) uf_compose_fwd_kernel(const UfCompose L) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  ComposeTiles<C, UC_WARPS>& t = *reinterpret_cast<ComposeTiles<C, UC_WARPS>*>(dsm);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int S = L.n_strokes;
+  for (long long p0 = ((long long)blockIdx.x * UC_WARPS + warp) * 32; p0 < L.n_points;
+       p0 += (long long)gridDim.x * UC_WARPS * 32) {
+    const int rows = (int)min(32LL, L.n_points - p0);
+    float T = 1.0f, dens = 0.0f, col[C];
+#pragma unroll
+    for (int ch = 0; ch < C; ch++) col[ch] = 0.0f;
+    for (int hi = S - 1; hi >= 0; hi -= 32) {
+      const int nb = min(32, hi + 1);
+      load_tile<C, UC_WARPS>(t, warp, lane, L, p0, rows, hi, nb, -1, nullptr, nullptr);
+      __syncwarp();
+      if (lane < rows) {
+        for (int j = 0; j < nb; j++) {
+          const float a = t.a[warp][lane][j];
+          if (a == 0.0f) continue;  // compositing.cu:37
+          const float w = a * T;
+          T *= (1.0f - a);
+          dens += L.density[hi - j] * w;
+#pragma unroll
+          for (int ch = 0; ch < C; ch++) col[ch] += t.c[warp][lane][j * C + ch] * w;
+        }
+      }
+      __syncwarp();
+    }
+    if (lane < rows) {
+      const long long p = p0 + lane;
+      const float scale = 1.0f / (1.0f + 1e-6f - T);
+      L.density_out[p] = dens;
+#pragma unroll
+      for (int ch = 0; ch < C; ch++) L.color_out[p * C + ch] = clampf(col[ch] * scale, 0.0f, 1.0f);
+    }
+  }
+}
+
+template <int C>
+__global__ void __launch_bounds__(UCB_WARPS * 32) uf_compose_bwd_kernel(const UfCompose L) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  ComposeBwdTiles<C, UCB_WARPS>& bt = *reinterpret_cast<ComposeBwdTiles<C, UCB_WARPS>*>(dsm);
+  ComposeTiles<C, UCB_WARPS>& t = bt.t;
+  auto& tx = bt.x;
+  auto& tg = bt.g;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int S = L.n_strokes;
+  const long long SS = S;
+  for (long long p0 = ((long long)blockIdx.x * UCB_WARPS + warp) * 32; p0 < L.n_points;
+       p0 += (long long)gridDim.x * UCB_WARPS * 32) {
+    const int rows = (int)min(32LL, L.n_points - p0);
+    const long long p = p0 + lane;
+    const bool on = lane < rows;
+    // sweep 1 (top-down): totals; exact mode also stores T before each stroke
+    float T = 1.0f, dens = 0.0f, col[C];
+#pragma unroll
+    for (int ch = 0; ch < C; ch++) col[ch] = 0.0f;
+    for (int hi = S - 1; hi >= 0; hi -= 32) {
+      const int nb = min(32, hi + 1);
+      load_tile<C, UCB_WARPS>(t, warp, lane, L, p0, rows, hi, nb, -1, nullptr, nullptr);
+      __syncwarp();
+      if (on) {
+        for (int j = 0; j < nb; j++) {
+          const float a = t.a[warp][lane][j];
+          tx[warp][lane][j] = T;
+          if (a == 0.0f) continue;
+          const float w = a * T;
+          T *= (1.0f - a);
+          dens += L.density[hi - j] * w;
+#pragma unroll
+          for (int ch = 0; ch < C; ch++) col[ch] += t.c[warp][lane][j * C + ch] * w;
+        }
+      }
+      __syncwarp();
+      if (!L.compat) {
+        for (int rr = 0; rr < rows; rr++)
+          if (lane < nb) L.t_scratch[(p0 + rr) * SS + hi - lane] = tx[warp][rr][lane];
+        __syncwarp();
+      }
+    }
+    const float gd = (on && L.g_density) ? L.g_density[p] : 0.0f;
+    const float O = 1.0f + 1e-6f - T;
+    const float scale = 1.0f / O;
+    float gc[C];
+#pragma unroll
+    for (int ch = 0; ch < C; ch++) {
+      const float sc = col[ch] * scale;
+      gc[ch] = (on && L.g_color && sc >= 0.0f && sc <= 1.0f) ? L.g_color[p * C + ch] : 0.0f;
+    }
+    if (L.compat) {
+      // compositing.cu:116-156, top-down
+      float T2 = 1.0f, d2 = 0.0f, c2[C];
+#pragma unroll
+      for (int ch = 0; ch < C; ch++) c2[ch] = 0.0f;
+      for (int hi = S - 1; hi >= 0; hi -= 32) {
+        const int nb = min(32, hi + 1);
+        load_tile<C, UCB_WARPS>(t, warp, lane, L, p0, rows, hi, nb, -1, nullptr, nullptr);
+        __syncwarp();
+        for (int j = 0; j < nb; j++) {
+          const float a = t.a[warp][lane][j];
+          const float ds = L.density[hi - j];
+          float w = 0.0f;
+          if (a > 0.0f) {
+            w = a * T2;
+            T2 *= (1.0f - a);
+            d2 += ds * w;
+#pragma unroll
+            for (int ch = 0; ch < C; ch++) c2[ch] += t.c[warp][lane][j * C + ch] * w;
+          }
+          float sd = 1.0f / fmaxf(1.0f - a, 1e-6f);
+          float ga = gd * (T2 * ds - (dens - d2)) * sd;
+          sd *= scale * scale;
+#pragma unroll
+          for (int ch = 0; ch < C; ch++) {
+            ga += gc[ch] * (T2 * t.c[warp][lane][j * C + ch] * (O - a) - (col[ch] - c2[ch])) * sd;
+            tg[warp][lane][j * C + ch] = on ? gc[ch] * scale * w : 0.0f;
+          }
+          tx[warp][lane][j] = on ? ga : 0.0f;
+          t.a[warp][lane][j] = on ? gd * w : 0.0f;  // reuse: density-param contribution
+        }
+        __syncwarp();
+        for (int rr = 0; rr < rows; rr++) {
+          const long long row = (p0 + rr) * SS;
+          if (lane < nb) L.g_alphas[row + hi - lane] += tx[warp][rr][lane];
+          for (int e = lane; e < nb * C; e += 32) {
+            const int j = e / C, ch = e - j * C;
+            L.g_colors[(row + hi - j) * C + ch] += tg[warp][rr][j * C + ch];
+          }
+        }
+        if (lane < nb) {
+          float sum = 0.0f;
+          for (int rr = 0; rr < rows; rr++) sum += t.a[warp][rr][lane];
+          if (sum != 0.0f) atomicAdd(L.g_density_params + hi - lane, sum);
+        }
+        __syncwarp();
+      }
+    } else {
+      // exact: dL/da_s = T_s [g_d (d_s - U) + g_C.(c_s - V) - g_T B], U/V/B composited
+      // bottom-up over the strokes below s
+      float gC[C], gT = 0.0f;
+#pragma unroll
+      for (int ch = 0; ch < C; ch++) {
+        gC[ch] = gc[ch] * scale;
+        gT += gc[ch] * col[ch] * scale * scale;
+      }
+      float U = 0.0f, V[C], B = 1.0f;
+#pragma unroll
+      for (int ch = 0; ch < C; ch++) V[ch] = 0.0f;
+      for (int lo = 0; lo < S; lo += 32) {
+        const int nb = min(32, S - lo);
+        load_tile<C, UCB_WARPS>(t, warp, lane, L, p0, rows, lo, nb, +1, L.t_scratch, tx[warp]);
+        __syncwarp();
+        for (int j = 0; j < nb; j++) {
+          const float a = t.a[warp][lane][j];
+          const float Ts = tx[warp][lane][j];
+          const float ds = L.density[lo + j];
+          const float w = a * Ts;
+          float inner = gd * (ds - U) - gT * B;
+#pragma unroll
+          for (int ch = 0; ch < C; ch++) {
+            const float cs = t.c[warp][lane][j * C + ch];
+            inner += gC[ch] * (cs - V[ch]);
+            tg[warp][lane][j * C + ch] = on ? gC[ch] * w : 0.0f;
+            V[ch] = cs * a + (1.0f - a) * V[ch];
+          }
+          U = ds * a + (1.0f - a) * U;
+          B *= (1.0f - a);
+          tx[warp][lane][j] = on ? Ts * inner : 0.0f;
+          t.a[warp][lane][j] = on ? gd * w : 0.0f;
+        }
+        __syncwarp();
+        for (int rr = 0; rr < rows; rr++) {
+          const long long row = (p0 + rr) * SS;
+          if (lane < nb) L.g_alphas[row + lo + lane] += tx[warp][rr][lane];
+          for (int e = lane; e < nb * C; e += 32) {
+            const int j = e / C, ch = e - j * C;
+            L.g_colors[(row + lo + j) * C + ch] += tg[warp][rr][j * C + ch];
+          }
+        }
+        if (lane < nb) {
+          float sum = 0.0f;
+          for (int rr = 0; rr < rows; rr++) sum += t.a[warp][rr][lane];
+          if (sum != 0.0f) atomicAdd(L.g_density_params + lo + lane, sum);
+        }
+        __syncwarp();
+      }
+    }
+  }
+}
+
+static int grid_for(long long items, int per_block) {
+  long long g = (items + per_block - 1) / per_block;
+  if (g > 148LL * 16) g = 148LL * 16;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+cudaError_t launch_uf_stroke_fwd(const UfStroke& L, int base, cudaStream_t st) {
+  (void)base;
+  dim3 grid(grid_for(L.n_points, UF_WARPS * 32), (L.n_strokes + 31) / 32);
+  uf_stroke_fwd_kernel<<<grid, UF_WARPS * 32, 0, st>>>(L);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_uf_stroke_bwd(const UfStroke& L, int base, cudaStream_t st) {
+  // enough sample-parallel blocks per stroke block to fill the machine
+  const int sblocks = (L.n_strokes + 31) / 32;
+  long long want = (148LL * 8 + sblocks - 1) / sblocks;
+  long long cap = (L.n_points + UF_WARPS - 1) / UF_WARPS;
+  if (want > cap) want = cap;
+  if (want < 1) want = 1;
+  dim3 grid((unsigned)want, sblocks);
+  if (base == B_CUBIC_BEZIER)
+    uf_stroke_bwd_kernel<32><<<grid, UF_WARPS * 32, 0, st>>>(L);
+  else
+    uf_stroke_bwd_kernel<16><<<grid, UF_WARPS * 32, 0, st>>>(L);
+  return cudaGetLastError();
+}
+
+template <typename K>
+static cudaError_t launch_dyn(K kernel, int grid, int threads, size_t smem, const UfCompose& L, cudaStream_t st) {
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  kernel<<<grid, threads, smem, st>>>(L);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_uf_compose_fwd(const UfCompose& L, cudaStream_t st) {
+  const int grid = grid_for(L.n_points, UC_WARPS * 32);
+  if (L.color_dim == 1)
+    return launch_dyn(uf_compose_fwd_kernel<1>, grid, UC_WARPS * 32, sizeof(ComposeTiles<1, UC_WARPS>), L, st);
+  return launch_dyn(uf_compose_fwd_kernel<3>, grid, UC_WARPS * 32, sizeof(ComposeTiles<3, UC_WARPS>), L, st);
+}
+
+cudaError_t launch_uf_compose_bwd(const UfCompose& L, cudaStream_t st) {
+  const int grid = grid_for(L.n_points, UCB_WARPS * 32);
+  if (L.color_dim == 1)
+    return launch_dyn(uf_compose_bwd_kernel<1>, grid, UCB_WARPS * 32, sizeof(ComposeBwdTiles<1, UCB_WARPS>), L, st);
+  return launch_dyn(uf_compose_bwd_kernel<3>, grid, UCB_WARPS * 32, sizeof(ComposeBwdTiles<3, UCB_WARPS>), L, st);
+}
+
+}  // namespace n3ds

@@ -1,0 +1,51 @@
+// The reference `_strokelib` operators over dense [P, S] tensors (drop-in layer).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace n3ds {
+
+struct UfStroke {
+  const float* x;          // [P*3]
+  const float* radius;     // [P]
+  const float* recs;       // [S*64] prepared records (uniform sdf_id)
+  long long n_points;
+  int n_strokes;
+  // forward outputs
+  float* alpha;            // [P*S]
+  float* color;            // [P*S*3]
+  float* sdf;              // [P*S] or null
+  // backward
+  const float* g_alpha;    // [P*S]
+  const float* g_color;    // [P*S*3]
+  const float* g_sdf;      // [P*S] or null
+  const float* alpha_in;   // [P*S] saved alpha
+  float* grad_x;           // [P*3] or null (accumulated)
+  float* gslots;           // [S*32] reduced slots
+  int compat;
+};
+
+struct UfCompose {
+  const float* alphas;     // [P*S]
+  const float* colors;     // [P*S*C]
+  const float* density;    // [S]
+  long long n_points;
+  int n_strokes;
+  int color_dim;
+  float* density_out;      // [P]
+  float* color_out;        // [P*C]
+  const float* g_density;  // [P] or null
+  const float* g_color;    // [P*C] or null
+  float* g_alphas;         // [P*S] accumulated
+  float* g_colors;         // [P*S*C] accumulated
+  float* g_density_params; // [S] accumulated
+  float* t_scratch;        // [P*S] exact mode only
+  int compat;
+};
+
+cudaError_t launch_uf_stroke_fwd(const UfStroke& L, int base, cudaStream_t st);
+cudaError_t launch_uf_stroke_bwd(const UfStroke& L, int base, cudaStream_t st);
+cudaError_t launch_uf_compose_fwd(const UfCompose& L, cudaStream_t st);
+cudaError_t launch_uf_compose_bwd(const UfCompose& L, cudaStream_t st);
+
+}  // namespace n3ds

@@ -1,0 +1,170 @@
+"""The fused stroke field as a torch.autograd.Function over the C ABI.
+
+One forward call replaces, for one scene or a batch of uneven scenes, the reference
+chain StrokeField.predict_density -> stroke_fn per primitive group -> compose_strokes
+('over') -> compute_alpha_weights -> volumetric_rendering (models.py:660-711, 191-235;
+render.py:29-88): it returns rgb, opacity (acc) and depth per ray without any
+[samples x strokes] tensor. The backward is the hand-written exact adjoint (or the
+reference's formulas with ``grad_mode='compat'``) and returns gradients for the sample
+positions and every stroke parameter: shape (translation, rotation, scale, base
+parameters, Bezier control points and radii), colour, density and softness.
+"""
+import ctypes
+from dataclasses import dataclass
+from typing import Optional, Sequence
+
+import torch
+
+from . import _lib
+
+
+@dataclass
+class FieldOptions:
+    cull_alpha: float = 1e-9   # strokes whose alpha provably stays below this are skipped; 0 disables
+    chunk_fwd: int = 0         # strokes per shared-memory stage (0: auto)
+    chunk_bwd: int = 0
+    warps: int = 0             # warps per CTA: 4, 8, 16 (0: auto)
+    segs_per_tile: int = 0     # 32-sample segments per CTA work tile (0: auto)
+    grad_mode: str = "exact"   # 'exact' or 'compat'
+
+    def c(self):
+        return _lib.Options(float(self.cull_alpha), int(self.chunk_fwd), int(self.chunk_bwd), int(self.warps),
+                            int(self.segs_per_tile),
+                            _lib.N3DS_GRAD_COMPAT if self.grad_mode == "compat" else _lib.N3DS_GRAD_EXACT)
+
+
+class _Native:
+    """ctypes argument blocks for one call (kept alive for the call's duration)."""
+
+    def __init__(self, scene_rays, scene_strokes, n_samples, x, radius, tdist, dirs, bg, bg_value, opaque,
+                 sdf_ids, shape_params, color_params, density, delta, laplace, inv_scale, options):
+        n = len(scene_rays)
+        self.nr = (ctypes.c_int64 * n)(*[int(v) for v in scene_rays])
+        self.ns = (ctypes.c_int32 * n)(*[int(v) for v in scene_strokes])
+        self.batch = _lib.Batch(n, self.nr, self.ns, int(n_samples))
+        self.rays = _lib.Rays(_lib.ptr(x), _lib.ptr(radius), _lib.ptr(tdist), _lib.ptr(dirs), _lib.ptr(bg),
+                              float(bg_value), int(bool(opaque)))
+        self.strokes = _lib.Strokes(_lib.ptr(sdf_ids), _lib.ptr(shape_params), int(shape_params.shape[1]),
+                                    _lib.ptr(color_params), _lib.ptr(density), _lib.ptr(delta), int(bool(laplace)),
+                                    int(bool(inv_scale)))
+        self.opt = options.c()
+
+    def ws_bytes(self):
+        return _lib.load().n3ds_field_workspace_bytes(ctypes.byref(self.batch), ctypes.byref(self.opt))
+
+
+def _f32(t, name):
+    if not (t.is_cuda and t.dtype == torch.float32):
+        raise RuntimeError(f"{name} must be a CUDA float32 tensor")
+    return t.contiguous()
+
+
+class _FieldFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x, radius, tdist, dirs, shape_params, color_params, density, delta, bg_t, sdf_ids,
+                scene_rays, scene_strokes, bg_value, opaque, laplace, inv_scale, options):
+        R, N = x.shape[0], x.shape[1]
+        x, radius, tdist, dirs = (_f32(t, n) for t, n in ((x, "x"), (radius, "radius"), (tdist, "tdist"),
+                                                           (dirs, "dirs")))
+        shape_params, color_params, density, delta = (
+            _f32(t, n) for t, n in ((shape_params, "shape_params"), (color_params, "color_params"),
+                                    (density, "density"), (delta, "sdf_delta")))
+        if sdf_ids.dtype != torch.int32 or not sdf_ids.is_cuda:
+            raise RuntimeError("sdf_ids must be a CUDA int32 tensor")
+        sdf_ids = sdf_ids.contiguous()
+        bg_c = _f32(bg_t, "bg") if bg_t is not None else None
+        nat = _Native(scene_rays, scene_strokes, N, x, radius, tdist, dirs, bg_c, bg_value, opaque, sdf_ids,
+                      shape_params, color_params, density, delta, laplace, inv_scale, options)
+        lib = _lib.load()
+        with torch.cuda.device(x.device):
+            ws_bytes = nat.ws_bytes()
+            if ws_bytes == 0:
+                raise RuntimeError("invalid batch description")
+            ws = _lib.workspace(ws_bytes, x.device)
+            rgb = torch.empty(R, 3, device=x.device)
+            acc = torch.empty(R, device=x.device)
+            depth = torch.empty(R, device=x.device)
+            rc = lib.n3ds_field_forward(ctypes.byref(nat.batch), ctypes.byref(nat.rays), ctypes.byref(nat.strokes),
+                                        ctypes.byref(nat.opt), _lib.ptr(rgb), _lib.ptr(acc), _lib.ptr(depth),
+                                        _lib.ptr(ws), ws_bytes, _lib.stream_ptr())
+        _lib.check(rc)
+        ctx.save_for_backward(x, radius, tdist, dirs, shape_params, color_params, density, delta, sdf_ids)
+        ctx.bg = bg_c
+        ctx.ws, ctx.ws_bytes = ws, ws_bytes
+        ctx.meta = (scene_rays, scene_strokes, bg_value, opaque, laplace, inv_scale, options)
+        return rgb, acc, depth
+
+    @staticmethod
+    def backward(ctx, g_rgb, g_acc, g_depth):
+        x, radius, tdist, dirs, shape_params, color_params, density, delta, sdf_ids = ctx.saved_tensors
+        scene_rays, scene_strokes, bg_value, opaque, laplace, inv_scale, options = ctx.meta
+        N = x.shape[1]
+        nat = _Native(scene_rays, scene_strokes, N, x, radius, tdist, dirs, ctx.bg, bg_value, opaque, sdf_ids,
+                      shape_params, color_params, density, delta, laplace, inv_scale, options)
+        gx = torch.empty_like(x) if ctx.needs_input_grad[0] else None
+        gshape = torch.empty_like(shape_params)
+        gcol = torch.empty_like(color_params)
+        gden = torch.empty_like(density)
+        gdel = torch.empty_like(delta)
+        g = [t.contiguous().float() if t is not None else None for t in (g_rgb, g_acc, g_depth)]
+        lib = _lib.load()
+        with torch.cuda.device(x.device):
+            rc = lib.n3ds_field_backward(ctypes.byref(nat.batch), ctypes.byref(nat.rays), ctypes.byref(nat.strokes),
+                                         ctypes.byref(nat.opt), _lib.ptr(g[0]), _lib.ptr(g[1]), _lib.ptr(g[2]),
+                                         _lib.ptr(gx), _lib.ptr(gshape), _lib.ptr(gcol), _lib.ptr(gden),
+                                         _lib.ptr(gdel), _lib.ptr(ctx.ws), ctx.ws_bytes, _lib.stream_ptr())
+        _lib.check(rc)
+        return (gx, None, None, None, gshape, gcol, gden, gdel, None, None, None, None, None, None, None, None,
+                None)
+
+
+def render_strokes(x: torch.Tensor, radius: torch.Tensor, tdist: torch.Tensor, dirs: torch.Tensor,
+                   shape_params: torch.Tensor, sdf_ids: torch.Tensor, color_params: torch.Tensor,
+                   density: torch.Tensor, sdf_delta, use_laplace_transform: bool = True,
+                   inv_scale_radius: bool = True, bg=1.0, opaque_background: bool = False,
+                   options: Optional[FieldOptions] = None, scene_sizes: Optional[Sequence] = None):
+    """Render rays through a stroke field.
+
+    x [R,N,3] sample positions, radius [R,N], tdist [R,N+1], dirs [R,3];
+    shape_params [S,P] in the reference layout (zero-padded rows), sdf_ids int32 [S],
+    color_params [S,3], density [S] (already multiplied by density_scale), sdf_delta a
+    float, a 0-d tensor or a per-stroke [S] tensor. ``scene_sizes``: list of
+    (n_rays, n_strokes) for a batch of scenes concatenated along rays and strokes
+    (default: one scene). bg: float or [R,3] tensor.
+    Returns rgb [R,3], acc [R], depth [R].
+    """
+    S = int(sdf_ids.numel())
+    R = int(x.shape[0])
+    dev = x.device
+    if torch.is_tensor(sdf_delta):
+        delta = sdf_delta.to(dev, torch.float32)
+        if delta.dim() == 0:
+            delta = delta.expand(S)
+    else:
+        delta = torch.full((S,), float(sdf_delta), device=dev)
+    if scene_sizes is None:
+        scene_sizes = [(R, S)]
+    scene_rays = [int(a) for a, _ in scene_sizes]
+    scene_strokes = [int(b) for _, b in scene_sizes]
+    if sum(scene_rays) != R or sum(scene_strokes) != S:
+        raise ValueError("scene_sizes do not add up to the ray / stroke counts")
+    if x.dim() != 3 or x.shape[2] != 3 or radius.shape != x.shape[:2] or tdist.shape != (R, x.shape[1] + 1) \
+            or dirs.shape != (R, 3):
+        raise ValueError("expected x [R,N,3], radius [R,N], tdist [R,N+1], dirs [R,3]")
+    if shape_params.dim() != 2 or shape_params.shape[0] != S or color_params.shape != (S, 3) or \
+            density.shape != (S,):
+        raise ValueError("expected shape_params [S,P], color_params [S,3], density [S]")
+    bg_t, bg_value = (bg, 0.0) if torch.is_tensor(bg) else (None, float(bg))
+    opts = options or FieldOptions()
+    return _FieldFn.apply(x, radius, tdist, dirs, shape_params, color_params, density, delta, bg_t, sdf_ids,
+                          scene_rays, scene_strokes, bg_value, opaque_background, use_laplace_transform,
+                          inv_scale_radius, opts)
+
+
+def field_status(workspace):
+    """(status, evaluated pairs) of the last forward that used ``workspace`` (synchronises)."""
+    st = ctypes.c_int32(0)
+    pairs = ctypes.c_uint64(0)
+    _lib.check(_lib.load().n3ds_field_read_status(_lib.ptr(workspace), ctypes.byref(st), ctypes.byref(pairs),
+                                                  _lib.stream_ptr()))
+    return int(st.value), int(pairs.value)

@@ -1,0 +1,135 @@
+"""Parity of the fused stroke field (CUDA, through the C ABI) with the float64 oracle.
+
+Tolerances (helpers.rel, normwise): forward 1e-5, gradients 1e-4.
+"""
+import pytest
+import torch
+
+from helpers import (FWD_TOL, GRAD_TOL, depth_errors, oracle_forward, oracle_grads, rel, shape_param_mask,
+                     small_workload)
+from neural3dstrokes_b200 import scenes
+from neural3dstrokes_b200.field import FieldOptions, render_strokes
+
+pytestmark = pytest.mark.gpu
+
+KINDS = ["sphere", "ellipsoid", "cube", "roundcube", "capsule", "octahedron", "tetrahedron",
+         "quadratic_bezier", "cubic_bezier", "mixed"]
+
+
+def run_field(sc, rays, dev, delta=0.02, laplace=True, inv=True, bg=1.0, opaque=False, opts=None,
+              requires_grad=False):
+    x = rays.x.to(dev).requires_grad_(requires_grad)
+    sp = sc.shape_params.to(dev).requires_grad_(requires_grad)
+    col = sc.color_params.to(dev).requires_grad_(requires_grad)
+    den = sc.density.to(dev).requires_grad_(requires_grad)
+    dl = torch.full((sc.n_strokes,), float(delta), device=dev, requires_grad=requires_grad)
+    out = render_strokes(x, rays.radius.to(dev), rays.tdist.to(dev), rays.dirs.to(dev), sp, sc.sdf_ids.to(dev),
+                         col, den, dl, laplace, inv, bg.to(dev) if torch.is_tensor(bg) else bg, opaque, opts)
+    return out, (x, sp, col, den, dl)
+
+
+@pytest.mark.parametrize("kind", KINDS)
+def test_forward_matches_oracle(cuda, kind):
+    sc, rays = small_workload(kind)
+    (rgb, acc, depth), _ = run_field(sc, rays, cuda)
+    rgb_r, acc_r, depth_r = oracle_forward(sc, rays)
+    assert rel(rgb, rgb_r) < FWD_TOL
+    assert rel(acc, acc_r) < FWD_TOL
+    e1, e2 = depth_errors(depth.cpu(), acc.cpu(), depth_r, acc_r)
+    assert e1 < FWD_TOL and e2 < FWD_TOL
+
+
+@pytest.mark.parametrize("kind", KINDS)
+def test_backward_matches_float64_autograd(cuda, kind):
+    sc, rays = small_workload(kind, n_strokes=16, n_rays=64, n_samples=40, seed=3)
+    g = torch.Generator().manual_seed(7)
+    g_rgb = torch.randn(rays.n_rays, 3, generator=g)
+    g_acc = torch.randn(rays.n_rays, generator=g)
+    g_depth = torch.randn(rays.n_rays, generator=g)
+    (rgb, acc, depth), (x, sp, col, den, dl) = run_field(sc, rays, cuda, requires_grad=True)
+    L = (rgb * g_rgb.to(cuda)).sum() + (acc * g_acc.to(cuda)).sum() + (depth * g_depth.to(cuda)).sum()
+    L.backward()
+    ref = oracle_grads(sc, rays, g_rgb, g_acc, g_depth)
+    m = shape_param_mask(sc)
+    errs = {
+        "x": rel(x.grad, ref["x"]),
+        "shape": rel(sp.grad.cpu()[m], ref["shape"][m]),
+        "color": rel(col.grad, ref["color"]),
+        "density": rel(den.grad, ref["density"]),
+        "delta": rel(dl.grad, ref["delta"]),
+    }
+    assert all(v < GRAD_TOL for v in errs.values()), errs
+    # unused padding slots get exactly zero gradient
+    assert float(sp.grad.cpu()[~m].abs().max()) == 0.0
+
+
+def test_config0_forward(cuda):
+    w = scenes.config(0, scale=0.25)
+    sc, rays = w.scenes[0], w.rays[0]
+    (rgb, acc, depth), _ = run_field(sc, rays, cuda)
+    rgb_r, acc_r, depth_r = oracle_forward(sc, rays)
+    assert rel(rgb, rgb_r) < FWD_TOL and rel(acc, acc_r) < FWD_TOL
+    e1, e2 = depth_errors(depth.cpu(), acc.cpu(), depth_r, acc_r)
+    assert e1 < FWD_TOL and e2 < FWD_TOL
+
+
+def test_culling_is_invisible(cuda):
+    sc, rays = small_workload("mixed", n_strokes=64, n_rays=256, n_samples=64, seed=11)
+    (a, acc_a, _), _ = run_field(sc, rays, cuda, opts=FieldOptions(cull_alpha=1e-9))
+    (b, acc_b, _), _ = run_field(sc, rays, cuda, opts=FieldOptions(cull_alpha=0.0))
+    assert rel(a, b) < 1e-6 and rel(acc_a, acc_b) < 1e-6
+
+
+def test_multipass_matches_single_pass(cuda):
+    sc, rays = small_workload("mixed", n_strokes=100, n_rays=96, n_samples=70, seed=5)
+    g_rgb = torch.randn(rays.n_rays, 3, generator=torch.Generator().manual_seed(1)).to(cuda)
+    outs = []
+    for opts in (FieldOptions(), FieldOptions(chunk_fwd=32, chunk_bwd=32)):
+        (rgb, acc, depth), (x, sp, col, den, dl) = run_field(sc, rays, cuda, opts=opts, requires_grad=True)
+        (rgb * g_rgb).sum().backward()
+        outs.append((rgb.detach(), x.grad, sp.grad, col.grad, den.grad, dl.grad))
+    for a, b in zip(*outs):
+        assert rel(a, b) < 1e-5
+
+
+def test_batched_scenes_match_individual(cuda):
+    parts = [small_workload(k, n_strokes=n, n_rays=r, n_samples=48, seed=i)
+             for i, (k, n, r) in enumerate([("mixed", 40, 64), ("cube", 7, 33), ("cubic_bezier", 19, 90)])]
+    x = torch.cat([p[1].x for p in parts]).to(cuda).requires_grad_(True)
+    sp = torch.cat([p[0].shape_params for p in parts]).to(cuda).requires_grad_(True)
+    col = torch.cat([p[0].color_params for p in parts]).to(cuda)
+    den = torch.cat([p[0].density for p in parts]).to(cuda)
+    ids = torch.cat([p[0].sdf_ids for p in parts]).to(cuda)
+    cat = lambda f: torch.cat([f(p[1]) for p in parts]).to(cuda)
+    rgb, acc, depth = render_strokes(x, cat(lambda r: r.radius), cat(lambda r: r.tdist), cat(lambda r: r.dirs), sp,
+                                     ids, col, den, 0.02,
+                                     scene_sizes=[(p[1].n_rays, p[0].n_strokes) for p in parts])
+    rgb.sum().backward()
+    r0 = s0 = 0
+    for sc, rays in parts:
+        (rgb1, _, _), (x1, sp1, _, _, _) = run_field(sc, rays, cuda, requires_grad=True)
+        rgb1.sum().backward()
+        assert rel(rgb[r0:r0 + rays.n_rays], rgb1) < 1e-6
+        assert rel(x.grad[r0:r0 + rays.n_rays], x1.grad) < 1e-5
+        assert rel(sp.grad[s0:s0 + sc.n_strokes], sp1.grad) < 1e-5
+        r0 += rays.n_rays
+        s0 += sc.n_strokes
+
+
+@pytest.mark.parametrize("laplace,delta,opaque", [(False, 0.05, False), (True, 0.02, True), (True, 0.0, False)])
+def test_step_modes_and_opaque_background(cuda, laplace, delta, opaque):
+    sc, rays = small_workload("mixed", n_strokes=20, n_rays=64, n_samples=32, seed=9)
+    bg = torch.rand(rays.n_rays, 3, generator=torch.Generator().manual_seed(2))
+    (rgb, acc, depth), _ = run_field(sc, rays, cuda, delta=delta, laplace=laplace, bg=bg, opaque=opaque)
+    rgb_r, acc_r, depth_r = oracle_forward(sc, rays, delta=delta, laplace=laplace, bg=bg, opaque=opaque)
+    assert rel(rgb, rgb_r) < FWD_TOL and rel(acc, acc_r) < FWD_TOL
+
+
+def test_empty_scene_and_rays(cuda):
+    sc, rays = small_workload("sphere", n_strokes=0, n_rays=16, n_samples=32)
+    (rgb, acc, depth), _ = run_field(sc, rays, cuda)
+    assert float(acc.abs().max()) == 0.0
+    assert torch.allclose(rgb, torch.ones_like(rgb))
+    sc2, rays2 = small_workload("sphere", n_strokes=4, n_rays=0, n_samples=32)
+    (rgb2, acc2, _), _ = run_field(sc2, rays2, cuda)
+    assert rgb2.shape == (0, 3) and acc2.shape == (0,)

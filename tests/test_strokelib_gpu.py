@@ -1,0 +1,251 @@
+"""Parity of the drop-in ``_strokelib`` operators (CUDA via the C ABI) with
+(a) the float64 oracle (forward and exact backward), (b) the oracle's restatement of
+the reference backward formulas (compat mode), and (c) when ``oracle/_ref`` holds the
+reference extension built from its own sources, the reference op itself.
+
+Tolerances (helpers.rel, normwise): forward 1e-5, gradients 1e-4.
+"""
+import glob
+import importlib.machinery
+import importlib.util
+import os
+
+import pytest
+import torch
+
+from helpers import FWD_TOL, GRAD_TOL, rel
+from neural3dstrokes_b200 import scenes
+from neural3dstrokes_b200 import strokelib as sl
+from oracle import strokefield as sf
+
+pytestmark = pytest.mark.gpu
+
+SDF_KINDS = ["sphere", "ellipsoid", "cube", "roundcube", "capsule", "octahedron", "tetrahedron",
+             "quadratic_bezier", "cubic_bezier"]
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def ref_ext():
+    hits = glob.glob(os.path.join(ROOT, "oracle", "_ref", "_strokelib*.so"))
+    if not hits:
+        return None
+    loader = importlib.machinery.ExtensionFileLoader("_strokelib", hits[0])
+    spec = importlib.util.spec_from_file_location("_strokelib", hits[0], loader=loader)
+    mod = importlib.util.module_from_spec(spec)
+    loader.exec_module(mod)
+    return mod
+
+
+def group(kind, n_strokes=40, n_points=3000, seed=0):
+    g = torch.Generator().manual_seed(seed)
+    sc = scenes.make_strokes([kind] * n_strokes, g)
+    rays = scenes.make_rays(max(1, n_points // 30), 30, g)
+    sid = scenes.SDF_ID[kind]
+    ps = sc.shape_params[:, :sf.num_shape_params(sid)].contiguous()
+    x = rays.x.reshape(-1, 3)
+    r = rays.radius.reshape(-1)
+    return sid, ps, sc.color_params.contiguous(), x, r, rays.dirs, sc
+
+
+def run_forward(impl, sid, ps, col, x, r, vd, delta, lap, inv, dev, want_sdf=True):
+    P, S = x.shape[0], ps.shape[0]
+    a = torch.empty(P, S, device=dev)
+    c = torch.empty(P, S, 3, device=dev)
+    sdf = torch.empty(P, S, device=dev) if want_sdf else torch.empty(0, device=dev)
+    impl.stroke_forward(a, c, sdf, torch.empty(0, device=dev), x.to(dev), r.to(dev), vd.to(dev), ps.to(dev),
+                        col.to(dev), sid, 0, delta, lap, inv)
+    return a, c, sdf
+
+
+@pytest.mark.parametrize("kind", SDF_KINDS)
+@pytest.mark.parametrize("lap,inv", [(True, True), (False, True), (True, False)])
+def test_stroke_forward_matches_oracle(cuda, kind, lap, inv):
+    sid, ps, col, x, r, vd, _ = group(kind)
+    a, c, sdf = run_forward(sl, sid, ps, col, x, r, vd, 0.02, lap, inv, cuda)
+    a_r, c_r, sdf_r = sf.stroke_forward(x.double(), r.double(), ps.double(), col.double(), sid, 0.02, lap, inv,
+                                        return_sdf=True)
+    assert rel(a, a_r) < FWD_TOL
+    assert rel(c, c_r) < FWD_TOL
+    assert rel(sdf, sdf_r) < FWD_TOL
+
+
+@pytest.mark.parametrize("kind", SDF_KINDS)
+def test_stroke_backward_exact_matches_autograd(cuda, kind):
+    sid, ps, col, x, r, vd, _ = group(kind, n_strokes=24, n_points=1500, seed=2)
+    g = torch.Generator().manual_seed(3)
+    P, S = x.shape[0], ps.shape[0]
+    ga = torch.randn(P, S, generator=g)
+    gc = torch.randn(P, S, 3, generator=g)
+    a, c, _ = run_forward(sl, sid, ps, col, x, r, vd, 0.02, True, True, cuda, want_sdf=False)
+    gps = torch.zeros_like(ps, device=cuda)
+    gcol = torch.zeros_like(col, device=cuda)
+    gx = torch.zeros(P, 3, device=cuda)
+    sl.set_grad_mode("exact")
+    sl.stroke_backward(gps, gcol, gx, ga.to(cuda), gc.to(cuda), torch.empty(0, device=cuda), x.to(cuda),
+                       r.to(cuda), vd.to(cuda), a, ps.to(cuda), col.to(cuda), sid, 0, 0.02, True, True)
+    xd = x.double().requires_grad_(True)
+    pd = ps.double().requires_grad_(True)
+    cd = col.double().requires_grad_(True)
+    a_r, c_r = sf.stroke_forward(xd, r.double(), pd, cd, sid, 0.02, True, True)
+    L = (a_r * ga.double()).sum() + (c_r * gc.double()).sum()
+    gx_r, gp_r, gc_r = torch.autograd.grad(L, [xd, pd, cd])
+    assert rel(gps, gp_r) < GRAD_TOL, rel(gps, gp_r)
+    assert rel(gx, gx_r) < GRAD_TOL, rel(gx, gx_r)
+    assert rel(gcol, gc_r) < GRAD_TOL
+
+
+@pytest.mark.parametrize("kind", SDF_KINDS)
+def test_stroke_backward_compat_matches_reference_formulas(cuda, kind):
+    sid, ps, col, x, r, vd, _ = group(kind, n_strokes=24, n_points=1500, seed=4)
+    g = torch.Generator().manual_seed(5)
+    P, S = x.shape[0], ps.shape[0]
+    ga = torch.randn(P, S, generator=g)
+    gc = torch.randn(P, S, 3, generator=g)
+    a, _, _ = run_forward(sl, sid, ps, col, x, r, vd, 0.02, True, True, cuda, want_sdf=False)
+    gps = torch.zeros_like(ps, device=cuda)
+    gcol = torch.zeros_like(col, device=cuda)
+    gx = torch.zeros(P, 3, device=cuda)
+    sl.set_grad_mode("compat")
+    try:
+        sl.stroke_backward(gps, gcol, gx, ga.to(cuda), gc.to(cuda), torch.empty(0, device=cuda), x.to(cuda),
+                           r.to(cuda), vd.to(cuda), a, ps.to(cuda), col.to(cuda), sid, 0, 0.02, True, True)
+    finally:
+        sl.set_grad_mode("exact")
+    gp_r, gc_r, gx_r = sf.stroke_backward_compat(ga.double(), gc.double(), x.double(), r.double(),
+                                                 a.double().cpu(), ps.double(), col.double(), sid, 0.02, True,
+                                                 True)
+    assert rel(gps, gp_r) < GRAD_TOL, rel(gps, gp_r)
+    assert rel(gx, gx_r) < GRAD_TOL, rel(gx, gx_r)
+    assert rel(gcol, gc_r) < GRAD_TOL
+
+
+def compose_inputs(P=700, S=45, C=3, seed=0):
+    g = torch.Generator().manual_seed(seed)
+    a = torch.rand(P, S, generator=g) ** 3
+    a[torch.rand(P, S, generator=g) < 0.3] = 0.0
+    c = torch.rand(P, S, C, generator=g)
+    d = torch.rand(S, generator=g) * 10
+    return a, c, d
+
+
+@pytest.mark.parametrize("C", [1, 3])
+def test_compose_forward_matches_oracle(cuda, C):
+    a, c, d = compose_inputs(C=C)
+    dens = torch.empty(a.shape[0], device=cuda)
+    col = torch.empty(a.shape[0], C, device=cuda)
+    sl.compose_forward(dens, col, a.to(cuda), c.to(cuda), d.to(cuda))
+    dr, cr = sf.compose_forward(a.double(), c.double(), d.double())
+    assert rel(dens, dr) < FWD_TOL and rel(col, cr) < FWD_TOL
+
+
+@pytest.mark.parametrize("mode", ["exact", "compat"])
+def test_compose_backward(cuda, mode):
+    a, c, d = compose_inputs(seed=1)
+    g = torch.Generator().manual_seed(2)
+    gd = torch.randn(a.shape[0], generator=g)
+    gcol = torch.randn(a.shape[0], 3, generator=g)
+    ga = torch.zeros_like(a, device=cuda)
+    gc = torch.zeros_like(c, device=cuda)
+    gdp = torch.zeros_like(d, device=cuda)
+    sl.set_grad_mode(mode)
+    try:
+        sl.compose_backward(ga, gc, gdp, gd.to(cuda), gcol.to(cuda), a.to(cuda), c.to(cuda), d.to(cuda))
+    finally:
+        sl.set_grad_mode("exact")
+    if mode == "exact":
+        ad = a.double().requires_grad_(True)
+        cd = c.double().requires_grad_(True)
+        dd = d.double().requires_grad_(True)
+        dr, cr = sf.compose_forward(ad, cd, dd)
+        ga_r, gc_r, gd_r = torch.autograd.grad((dr * gd.double()).sum() + (cr * gcol.double()).sum(), [ad, cd, dd])
+    else:
+        ga_r, gc_r, gd_r = sf.compose_backward_compat(gd.double(), gcol.double(), a.double(), c.double(),
+                                                      d.double())
+    assert rel(ga, ga_r) < GRAD_TOL, rel(ga, ga_r)
+    assert rel(gc, gc_r) < GRAD_TOL
+    assert rel(gdp, gd_r) < GRAD_TOL
+
+
+def test_errors_are_runtime_errors(cuda):
+    sid, ps, col, x, r, vd, _ = group("sphere", n_strokes=4, n_points=60)
+    with pytest.raises(RuntimeError, match="must be a CUDA tensor"):
+        sl.stroke_forward(torch.empty(60, 4), torch.empty(60, 4, 3), torch.empty(0), torch.empty(0), x, r, vd, ps,
+                          col, sid, 0, 0.02, True, True)
+    with pytest.raises(RuntimeError, match="implemented set"):
+        run_forward(sl, 0x37, torch.zeros(4, 9), col, x, r, vd, 0.02, True, True, cuda)  # capped torus
+    with pytest.raises(RuntimeError, match="fn_id"):
+        run_forward(sl, 0xc0, ps, col, x, r, vd, 0.02, True, True, cuda)
+    with pytest.raises(RuntimeError, match="Unsupported color dimension"):
+        sl.compose_forward(torch.empty(5, device=cuda), torch.empty(5, 2, device=cuda),
+                           torch.rand(5, 3, device=cuda), torch.rand(5, 3, 2, device=cuda),
+                           torch.rand(3, device=cuda))
+
+
+# ------------------------------------------------------- the reference op itself
+
+@pytest.mark.parametrize("kind", SDF_KINDS)
+def test_forward_matches_reference_op(cuda, kind):
+    ref = ref_ext()
+    if ref is None:
+        pytest.skip("reference extension not built (oracle/_ref)")
+    sid, ps, col, x, r, vd, _ = group(kind, n_points=2000, seed=8)
+    for lap, inv in [(True, True), (False, False)]:
+        a, c, sdf = run_forward(sl, sid, ps, col, x, r, vd, 0.02, lap, inv, cuda)
+        a_r, c_r, sdf_r = run_forward(ref, sid, ps, col, x, r, vd, 0.02, lap, inv, cuda)
+        assert rel(a, a_r) < FWD_TOL and rel(c, c_r) == 0.0 and rel(sdf, sdf_r) < FWD_TOL
+
+
+@pytest.mark.parametrize("kind", ["sphere", "ellipsoid", "cube", "roundcube", "capsule", "octahedron",
+                                  "tetrahedron", "cubic_bezier"])
+def test_compat_backward_matches_reference_op(cuda, kind):
+    ref = ref_ext()
+    if ref is None:
+        pytest.skip("reference extension not built (oracle/_ref)")
+    sid, ps, col, x, r, vd, _ = group(kind, n_strokes=24, n_points=1500, seed=9)
+    g = torch.Generator().manual_seed(10)
+    P, S = x.shape[0], ps.shape[0]
+    ga = torch.randn(P, S, generator=g).to(cuda)
+    gc = torch.randn(P, S, 3, generator=g).to(cuda)
+    a, _, _ = run_forward(ref, sid, ps, col, x, r, vd, 0.02, True, True, cuda, want_sdf=False)
+    outs = []
+    for impl in (sl, ref):
+        gps = torch.zeros_like(ps, device=cuda)
+        gcol = torch.zeros_like(col, device=cuda)
+        gx = torch.zeros(P, 3, device=cuda)
+        sl.set_grad_mode("compat")
+        try:
+            impl.stroke_backward(gps, gcol, gx, ga, gc, torch.empty(0, device=cuda), x.to(cuda), r.to(cuda),
+                                 vd.to(cuda), a, ps.to(cuda), col.to(cuda), sid, 0, 0.02, True, True)
+        finally:
+            sl.set_grad_mode("exact")
+        outs.append((gps, gcol, gx))
+    for m, rr in zip(*outs):
+        assert rel(m, rr) < GRAD_TOL, rel(m, rr)
+
+
+def test_compose_matches_reference_op(cuda):
+    ref = ref_ext()
+    if ref is None:
+        pytest.skip("reference extension not built (oracle/_ref)")
+    a, c, d = [t.to(cuda) for t in compose_inputs(seed=3)]
+    res = []
+    for impl in (sl, ref):
+        dens = torch.empty(a.shape[0], device=cuda)
+        col = torch.empty(a.shape[0], 3, device=cuda)
+        impl.compose_forward(dens, col, a, c, d)
+        res.append((dens, col))
+    assert rel(res[0][0], res[1][0]) < FWD_TOL and rel(res[0][1], res[1][1]) < FWD_TOL
+    g = torch.Generator().manual_seed(4)
+    gd = torch.randn(a.shape[0], generator=g).to(cuda)
+    gcol = torch.randn(a.shape[0], 3, generator=g).to(cuda)
+    res = []
+    for impl in (sl, ref):
+        ga, gc, gdp = torch.zeros_like(a), torch.zeros_like(c), torch.zeros_like(d)
+        sl.set_grad_mode("compat")
+        try:
+            impl.compose_backward(ga, gc, gdp, gd, gcol, a, c, d)
+        finally:
+            sl.set_grad_mode("exact")
+        res.append((ga, gc, gdp))
+    for m, rr in zip(*res):
+        assert rel(m, rr) < GRAD_TOL
