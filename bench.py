@@ -1,0 +1,439 @@
+#!/usr/bin/env python
+"""Stroke-field benchmark: forward + backward stroke x sample evaluations per second.
+
+One step = one forward + adjoint backward of the fused stroke field over every scene
+of the workload (all rays, all strokes), captured once into a CUDA graph and
+replayed; inputs are resident in HBM. Upstream gradients are N(0, 1) on rgb,
+opacity and depth. An "eval" is one (stroke, sample) pair of the nominal dense
+product S x P per scene, the same count whatever culling skips.
+
+Default workload: 16 uneven scenes (strokes log-uniform in [50, 2000], rays
+log-uniform in [4096, 65536], 64 samples each, six primitive types mixed) in one
+batched launch per pass + CUDA graph. Other workloads: --config 0..4.
+
+Usage:
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--config C] [--impl reference]
+Multi-GPU (torchrun): every rank runs the same workload on its own GPU (replicas, no
+data-path collective); the value is the sum over ranks of evals divided by the
+slowest rank's time.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+bwd stroke×sample evals/s on 1 B200: batched+graph vs plain op @≤1e-4 rel"
+UNIT = "evals/s"
+
+# Algorithmic FP32 flops per evaluated (sample, stroke) pair, forward: inverse
+# transform + SDF + 15 (soft step 4 + over-composite 11); sphere transform is 6
+# (translate + scale only), the Beziers have none. Backward = 2.5 x forward
+# (recompute, adjoint of each step, reduction share). Survey 8(d) table.
+FWD_FLOPS_BY_KIND = {
+    "sphere": 6 + 6 + 15, "ellipsoid": 21 + 6 + 10 + 15, "cube": 21 + 14 + 15, "roundcube": 21 + 16 + 15,
+    "capsule": 21 + 9 + 15, "octahedron": 21 + 6 + 15, "tetrahedron": 21 + 8 + 15,
+    "quadratic_bezier": 75 + 15, "cubic_bezier": 190 + 15,
+}
+BWD_FACTOR = 2.5
+KIND_BASE = {"sphere": 0, "ellipsoid": 0, "cube": 1, "roundcube": 2, "capsule": 4, "octahedron": 7,
+             "tetrahedron": 8, "quadratic_bezier": 9, "cubic_bezier": 10}
+CLOCK_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+def base_flops(kinds):
+    """Forward flops per evaluated pair for each base SDF index, weighted by the
+    workload's stroke mix (sphere and ellipsoid share base 0)."""
+    acc, cnt = {}, {}
+    for k in kinds:
+        b = KIND_BASE[k]
+        acc[b] = acc.get(b, 0.0) + FWD_FLOPS_BY_KIND[k]
+        cnt[b] = cnt.get(b, 0) + 1
+    return {b: acc[b] / cnt[b] for b in acc}
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={CLOCK_FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [v.strip() for v in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        torch.distributed.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        torch.distributed.barrier()
+
+
+def max_over_ranks(v, world, device):
+    if world == 1:
+        return v
+    t = torch.tensor([float(v)], device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(local_step_s, pairs_per_rank, world, device):
+    """Whole-job evals/s of N replicas: every rank processes pairs_per_rank per step;
+    the job's step time is the slowest rank's. Returns (value, max step seconds)."""
+    step = max_over_ranks(local_step_s, world, device)
+    return pairs_per_rank * world / step, step
+
+
+def workload_upstream(field, seed=7):
+    g = torch.Generator().manual_seed(seed)
+    R = field.rgb.shape[0]
+    return (torch.randn(R, 3, generator=g), torch.randn(R, generator=g), torch.randn(R, generator=g))
+
+
+def fp32_peak(device, repeats=8):
+    """Measured FP32 FMA throughput (TFLOP/s) of this GPU with the library's probe."""
+    from neural3dstrokes_b200 import _lib
+    lib = _lib.load()
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    blocks, iters = sms * 8, 8192
+    out = torch.empty(blocks * 256, device=device)
+    best = 0.0
+    for _ in range(repeats + 2):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        _lib.check(lib.n3ds_fp32_probe(_lib.ptr(out), blocks, iters, _lib.stream_ptr(device)))
+        e.record()
+        e.synchronize()
+        best = max(best, blocks * 256.0 * iters * 32 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    return best
+
+
+def cpu_baseline(workload, budget_s=15.0):
+    """The labelled float32 CPU port of the reference step (oracle/cpu_port.py) on a
+    bounded ray sample of the same workload, all host threads."""
+    from oracle import cpu_port
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    g = torch.Generator().manual_seed(11)
+
+    def run(k):
+        t0 = time.perf_counter()
+        pairs = 0
+        for sc, rays in zip(workload.scenes, workload.rays):
+            n = min(k, rays.n_rays)
+            sl = slice(0, n)
+            gr = (torch.randn(n, 3, generator=g), torch.randn(n, generator=g), torch.randn(n, generator=g))
+            cpu_port.port_step(sc, rays.x[sl], rays.radius[sl], rays.tdist[sl], rays.dirs[sl], *gr,
+                               delta=workload.sdf_delta, laplace=workload.use_laplace, inv=workload.inv_scale_radius)
+            pairs += sc.n_strokes * n * rays.n_samples
+        return pairs, time.perf_counter() - t0
+
+    # size the sample from a small probe so the measured round takes about budget_s
+    k = 2
+    pairs, dt = run(k)
+    k = max(k, min(4096, int(k * budget_s / max(dt, 1e-3))))
+    pairs, dt = run(k)
+    return {"value": pairs / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"first {k} rays of each scene ({pairs} nominal pairs, {dt:.1f} s): float32 torch "
+                      f"restatement of the reference strokelib kernels + render.py, forward + backward"}
+
+
+def run_reference(args, world, rank):
+    """Reference arm: the reference implementation of the path timed on the host cores
+    (its kernels are CUDA-only, so its CPU form is the labelled float32 port), plus,
+    as an extra field, the unmodified reference CUDA op on this GPU."""
+    if rank != 0:
+        return
+    from neural3dstrokes_b200 import scenes
+    from oracle import cpu_port
+    w = scenes.config(args.config)
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    g = torch.Generator().manual_seed(5)
+    # one step = a bounded ray sample of every scene (sized for ~2-4 s of CPU work)
+    n = 4 if args.config in (3, 4) else 16
+    rates = []
+    for it in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        pairs = 0
+        for sc, rays in zip(w.scenes, w.rays):
+            m = min(n, rays.n_rays)
+            r0 = (it * m) % max(1, rays.n_rays - m)
+            sl = slice(r0, r0 + m)
+            gr = (torch.randn(m, 3, generator=g), torch.randn(m, generator=g), torch.randn(m, generator=g))
+            cpu_port.port_step(sc, rays.x[sl], rays.radius[sl], rays.tdist[sl], rays.dirs[sl], *gr,
+                               delta=w.sdf_delta, laplace=w.use_laplace, inv=w.inv_scale_radius)
+            pairs += sc.n_strokes * m * rays.n_samples
+        dt = time.perf_counter() - t0
+        if it >= args.warmup:
+            rates.append(pairs / dt)
+        if it == 0 and dt > 20 and n > 1:
+            n = max(1, n // 4)
+    value = statistics.mean(rates)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": w.name, "nominal_pairs_per_full_step": w.nominal_pairs},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{n} rays of each scene per step, float32 torch restatement of the "
+                                       f"reference strokelib kernels + render.py, forward + backward"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if torch.cuda.is_available() and not args.no_plain_op:
+        try:
+            line["plain_op_gpu"] = plain_op_gpu(w, args)
+        except Exception as e:  # the extra field must not sink the arm
+            line["plain_op_gpu"] = {"unavailable": f"{type(e).__name__}: {e}"[:300]}
+    print(json.dumps(line), flush=True)
+
+
+def plain_op_gpu(w, args, max_seconds=60.0):
+    """The unmodified reference CUDA op (oracle/_ref) driven as models.py drives it,
+    one scene at a time, over the whole workload; CUDA events."""
+    from oracle import cpu_port
+    ref = cpu_port.reference_extension()
+    if ref is None:
+        return {"unavailable": "reference extension not built (oracle/_ref)"}
+    dev = torch.device("cuda")
+    g = torch.Generator().manual_seed(7)
+    data = []
+    for sc, rays in zip(w.scenes, w.rays):
+        R = rays.n_rays
+        data.append((sc.to(dev), rays.to(dev), torch.randn(R, 3, generator=g).to(dev),
+                     torch.randn(R, generator=g).to(dev), torch.randn(R, generator=g).to(dev)))
+
+    def step():
+        for sc, rays, a, b, c in data:
+            cpu_port.plain_op_step(ref, sc, rays.x, rays.radius, rays.tdist, rays.dirs, a, b, c, w.sdf_delta,
+                                   w.use_laplace, w.inv_scale_radius)
+    step()  # warm-up
+    torch.cuda.synchronize()
+    times = []
+    t_start = time.perf_counter()
+    while len(times) < 3 and (time.perf_counter() - t_start) < max_seconds:
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        step()
+        e.record()
+        e.synchronize()
+        times.append(s.elapsed_time(e) * 1e-3)
+    t = statistics.median(times)
+    return {"value": w.nominal_pairs / t, "unit": UNIT, "ms_per_step": t * 1e3, "steps": len(times),
+            "note": "reference _strokelib built from its own sources for sm_100a, per scene, per primitive "
+                    "group, ray-chunked (P_chunk*S < 2^29), torch autograd for render.py, grad_x requested"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--config", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--scale", type=float, default=1.0, help="ray-count scale (profiling small cases)")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain-op", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup(args.gpus)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+
+    from neural3dstrokes_b200 import scenes
+    from neural3dstrokes_b200.train import BatchedField, GraphedTrainer, capture
+
+    dev = torch.device("cuda", local)
+    w = scenes.config(args.config, scale=args.scale)
+    field = BatchedField(w.scenes, w.rays, w.sdf_delta, w.use_laplace, w.inv_scale_radius, device=dev)
+    g_rgb, g_acc, g_depth = workload_upstream(field)
+    trainer = None
+    if args.config == 4:
+        # target image: render of a separate seeded 2000-stroke scene per ray set
+        tf = BatchedField(w.target_scenes, w.rays, w.sdf_delta, w.use_laplace, w.inv_scale_radius, device=dev,
+                          need_grad_x=False)
+        tf.forward()
+        trainer = GraphedTrainer(field, tf.rgb.clone(), lr=1e-3)
+        del tf
+        step_fn = trainer._step
+    else:
+        field.g_rgb.copy_(g_rgb)
+        field.g_acc.copy_(g_acc)
+        field.g_depth.copy_(g_depth)
+        step_fn = field.step
+    pairs = field.nominal_pairs
+
+    # statistics pass (not timed): evaluated pairs per primitive type, status word
+    field.forward()
+    torch.cuda.synchronize(dev)
+    per_base = field.pair_counts()
+    status, evaluated = field.status()
+    if status != 0:
+        raise SystemExit(f"device status {status}")
+
+    graph = capture(step_fn, dev, warmup=1) if trainer is None else trainer.capture()
+    for _ in range(args.warmup):
+        graph.replay()
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    clocks = ClockSampler(torch.cuda.current_device() if world == 1 else local)
+    clocks.start()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    t0.record()
+    for _ in range(args.steps):
+        graph.replay()
+    t1.record()
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    clk = clocks.stop()
+    value, step_s = replica_throughput(t0.elapsed_time(t1) * 1e-3 / args.steps, pairs, world, dev)
+
+    # dominant-kernel timing with CUDA events recorded on the launching stream
+    from neural3dstrokes_b200 import _lib
+    import ctypes
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    field.c_opt = field.options.c(ev)
+    fwd_t, bwd_t = [], []
+    for _ in range(max(3, min(10, args.steps))):
+        field.forward()
+        field.backward()
+        ev[3].synchronize()
+        fwd_t.append(ev[0].elapsed_time(ev[1]) * 1e-3)
+        bwd_t.append(ev[2].elapsed_time(ev[3]) * 1e-3)
+    field.c_opt = field.options.c()
+    t_fwd, t_bwd = statistics.mean(fwd_t), statistics.mean(bwd_t)
+    bf = base_flops(field.kinds)
+    fwd_flops = sum(per_base[b] * bf.get(b, 0.0) for b in range(16))
+    bwd_flops = BWD_FACTOR * fwd_flops
+    peak = fp32_peak(dev)
+    roofline = {"bound": "fp32", "kernel": "seg_bwd_kernel (segment adjoint)", "achieved": bwd_flops / t_bwd / 1e12,
+                "peak": peak, "unit": "TFLOP/s", "frac": bwd_flops / t_bwd / 1e12 / peak, "traffic": None,
+                "peak_source": "measured: FP32 FMA probe kernel on this GPU (no FP32 figure in the peaks file)",
+                "flops_per_launch": bwd_flops, "launch_ms": t_bwd * 1e3,
+                "seg_fwd": {"achieved": fwd_flops / t_fwd / 1e12, "launch_ms": t_fwd * 1e3,
+                            "frac": fwd_flops / t_fwd / 1e12 / peak}}
+
+    # end to end through the public API with host buffers: H2D of the step's inputs,
+    # the step, D2H of its results, every step
+    e2e = None
+    if not args.no_e2e:
+        ins = [field.x, field.radius, field.tdist, field.dirs, field.g_rgb, field.g_acc, field.g_depth, field.shape,
+               field.color, field.density, field.delta, field.sdf_ids]
+        outs = [field.rgb, field.acc, field.depth, field.grad_shape, field.grad_color, field.grad_density,
+                field.grad_delta]
+        h_in = [t.detach().cpu().pin_memory() for t in ins]
+        h_out = [torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for t in outs]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n_e2e = max(3, min(args.steps, 10))
+
+        def e2e_step():
+            for d, h in zip(ins, h_in):
+                d.copy_(h, non_blocking=True)
+            graph.replay()
+            for h, d in zip(h_out, outs):
+                h.copy_(d, non_blocking=True)
+        e2e_step()
+        torch.cuda.synchronize(dev)
+        barrier(world)
+        e0.record()
+        for _ in range(n_e2e):
+            e2e_step()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        t_e2e = max_over_ranks(e0.elapsed_time(e1) * 1e-3 / n_e2e, world, dev)
+        e2e = {"value": pairs * world / t_e2e, "unit": UNIT, "ms_per_step": t_e2e * 1e3,
+               "h2d_bytes_per_step": sum(t.numel() * t.element_size() for t in h_in),
+               "d2h_bytes_per_step": sum(t.numel() * t.element_size() for t in h_out)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(w, args.cpu_seconds)
+
+    lf, lb = field.launch_count()
+    launches_per_step = lf + lb + (3 if trainer is not None else 0)  # + 3 Adam launches when training
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators, no dataset)",
+            "config": {"workload": w.name, "scenes": len(w.scenes), "nominal_pairs_per_step": pairs,
+                       "evaluated_pairs_per_step": int(evaluated), "rays": int(field.rgb.shape[0]),
+                       "samples_per_ray": field.n_samples, "strokes": int(field.shape.shape[0]),
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                       "l2": "inputs larger than L2 (x alone %.0f MB)" % (field.x.numel() * 4 / 1e6),
+                       "graph": "forward+backward captured in one CUDA graph" if trainer is None
+                       else "forward+MSE+backward+Adam captured in one CUDA graph"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+            "gpu_launches": launches_per_step * args.steps,
+            "gpu_launches_per_step": launches_per_step,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        del graph
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -144,6 +144,9 @@ typedef struct n3ds_options {
   int32_t warps;      /* warps per CTA: 4, 8 or 16 (0 = auto) */
   int32_t segs_per_tile; /* 32-sample segments per CTA work tile (0 = auto) */
   int32_t grad_mode;  /* N3DS_GRAD_EXACT or N3DS_GRAD_COMPAT */
+  /* optional: 4 cudaEvent_t recorded on the stream around the segment kernels
+   * (forward begin/end, backward begin/end), or NULL */
+  void* const* timing_events;
 } n3ds_options_t;
 
 /* Fill *opt with the defaults. */
@@ -175,6 +178,15 @@ int n3ds_field_backward(const n3ds_batch_t* batch, const n3ds_rays_t* rays,
 int n3ds_field_read_status(void* workspace, int32_t* status, uint64_t* evaluated_pairs,
                            n3ds_stream_t stream);
 
+/* Number of kernel launches one n3ds_field_forward / n3ds_field_backward makes for
+ * this batch and these options (host-only planning, no device work). */
+int n3ds_field_launch_count(const n3ds_batch_t* batch, const n3ds_options_t* opt, int32_t* forward,
+                            int32_t* backward);
+
+/* Synchronously read the evaluated (sample, stroke) pairs of the last forward per base
+ * SDF type (16 counters, indexed by sdf_id >> 4). */
+int n3ds_field_read_pair_counts(void* workspace, uint64_t* per_base, n3ds_stream_t stream);
+
 /* Adam step fused with the reference's parameter clamp (utils/training.py:119-136,
  * models.py:576-584) over n floats: m = b1 m + (1-b1) g; v = b2 v + (1-b2) g^2;
  * p -= lr * mhat / (sqrt(vhat) + eps); then p = clamp(p, lo, hi) where lo/hi may be
@@ -182,6 +194,12 @@ int n3ds_field_read_status(void* workspace, int32_t* status, uint64_t* evaluated
 int n3ds_adam_step(float* param, const float* grad, float* exp_avg, float* exp_avg_sq,
                    const float* lo, const float* hi, int64_t n, float lr, float beta1, float beta2,
                    float eps, const int32_t* step, n3ds_stream_t stream);
+
+/* FP32 FMA throughput probe (no counterpart in the reference; a measurement aid for
+ * the roofline of these FP32-bound kernels): one launch of `blocks` x 256 threads,
+ * each doing iters x 16 fused multiply-adds, i.e. blocks*256*iters*32 flops.
+ * out needs blocks*256 floats (written only to keep the work alive). */
+int n3ds_fp32_probe(float* out, int32_t blocks, int32_t iters, n3ds_stream_t stream);
 
 #ifdef __cplusplus
 }

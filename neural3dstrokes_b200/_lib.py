@@ -42,7 +42,8 @@ class Strokes(ctypes.Structure):
 
 class Options(ctypes.Structure):
     _fields_ = [("cull_alpha", ctypes.c_float), ("chunk_fwd", c_i32), ("chunk_bwd", c_i32),
-                ("warps", c_i32), ("segs_per_tile", c_i32), ("grad_mode", c_i32)]
+                ("warps", c_i32), ("segs_per_tile", c_i32), ("grad_mode", c_i32),
+                ("timing_events", ctypes.POINTER(ctypes.c_void_p))]
 
 
 _P = ctypes.c_void_p
@@ -70,6 +71,10 @@ _SIGS = {
     "n3ds_field_read_status": (ctypes.c_int, [_P, ctypes.POINTER(c_i32), ctypes.POINTER(ctypes.c_uint64), _P]),
     "n3ds_adam_step": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, c_i64, ctypes.c_float, ctypes.c_float,
                                       ctypes.c_float, ctypes.c_float, _P, _P]),
+    "n3ds_fp32_probe": (ctypes.c_int, [_P, c_i32, c_i32, _P]),
+    "n3ds_field_read_pair_counts": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64), _P]),
+    "n3ds_field_launch_count": (ctypes.c_int, [ctypes.POINTER(Batch), ctypes.POINTER(Options),
+                                               ctypes.POINTER(c_i32), ctypes.POINTER(c_i32)]),
 }
 
 EXPORTED = tuple(_SIGS)

@@ -66,7 +66,8 @@ WsLayout ws_layout(long long total_rays, int N, long long S) {
     return o;
   };
   const size_t P = size_t(total_rays) * size_t(N);
-  w.status = take(256);  // header: int32 status at +0, uint64 evaluated-pair count at +8
+  // header: int32 status at +0, uint64 evaluated pairs at +8, uint64 per-base counts at +16
+  w.status = take(256);
   w.stats = w.status + 8;
   w.recs = take(size_t(S) * n3ds::REC_FLOATS * 4);
   w.cull_a = take(size_t(S) * 16);
@@ -83,7 +84,12 @@ WsLayout ws_layout(long long total_rays, int N, long long S) {
 struct Resolved {
   float cull_m;
   int chunk_fwd, chunk_bwd, warps, segs_per_tile, grad_mode;
+  void* const* events;
 };
+
+void record_event(const Resolved& rv, int i, cudaStream_t st) {
+  if (rv.events && rv.events[i]) cudaEventRecord(static_cast<cudaEvent_t>(rv.events[i]), st);
+}
 
 Resolved resolve(const n3ds_options_t* o) {
   n3ds_options_t d;
@@ -104,6 +110,7 @@ Resolved resolve(const n3ds_options_t* o) {
   r.chunk_fwd = cf;
   r.chunk_bwd = cb;
   r.grad_mode = o->grad_mode;
+  r.events = o->timing_events;
   return r;
 }
 
@@ -128,7 +135,7 @@ int check_batch(const n3ds_batch_t* b, long long* total_rays, long long* total_s
 
 // Plan and launch the segment passes of one direction.
 int run_seg_passes(bool backward, const n3ds_batch_t* b, const Resolved& rv, n3ds::SegLaunch base,
-                   int counter_base, cudaStream_t st) {
+                   int counter_base, cudaStream_t st, int* launch_count = nullptr) {
   const int cap = backward ? rv.chunk_bwd : rv.chunk_fwd;
   const int spr = (b->n_samples + 31) / 32;
   std::vector<long long> ray_begin(b->n_scenes), stroke_begin(b->n_scenes);
@@ -176,6 +183,10 @@ int run_seg_passes(bool backward, const n3ds_batch_t* b, const Resolved& rv, n3d
       }
       if (tiles == 0) continue;
       if (counter >= N_COUNTERS) return fail(N3DS_ERR_INVALID, "batch needs too many launches (raise chunk size or split the batch)");
+      if (launch_count) {  // planning only
+        ++*launch_count;
+        continue;
+      }
       L.tiles_total = tiles;
       L.tile_counter = base.tile_counter + counter++;
       const int grid = std::min(tiles, di.sms);
@@ -202,6 +213,7 @@ void n3ds_default_options(n3ds_options_t* opt) {
   opt->warps = 0;
   opt->segs_per_tile = 0;
   opt->grad_mode = N3DS_GRAD_EXACT;
+  opt->timing_events = nullptr;
 }
 
 size_t n3ds_field_workspace_bytes(const n3ds_batch_t* batch, const n3ds_options_t* opt) {
@@ -215,7 +227,7 @@ static int field_common(const n3ds_batch_t* batch, const n3ds_rays_t* rays, cons
                         void* ws, size_t ws_bytes, long long* R, long long* S, WsLayout* lay) {
   int rc = check_batch(batch, R, S);
   if (rc) return rc;
-  if (!rays || !rays->x || !rays->radius || !rays->tdist || !rays->dirs)
+  if (!rays || (*R > 0 && (!rays->x || !rays->radius || !rays->tdist || !rays->dirs)))
     return fail(N3DS_ERR_INVALID, "rays: x, radius, tdist and dirs are required");
   if (!strokes || (*S > 0 && (!strokes->sdf_ids || !strokes->shape_params || !strokes->color_params ||
                               !strokes->density || !strokes->sdf_delta)))
@@ -298,14 +310,16 @@ int n3ds_field_forward(const n3ds_batch_t* batch, const n3ds_rays_t* rays, const
   WsLayout lay;
   int rc = field_common(batch, rays, strokes, workspace, workspace_bytes, &R, &S, &lay);
   if (rc) return rc;
-  if (!rgb || !acc || !depth) return fail(N3DS_ERR_INVALID, "rgb, acc and depth outputs are required");
+  if (R > 0 && (!rgb || !acc || !depth)) return fail(N3DS_ERR_INVALID, "rgb, acc and depth outputs are required");
   const Resolved rv = resolve(opt);
   char* ws = static_cast<char*>(workspace);
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   n3ds::launch_prep(make_prep(strokes, S, rv, ws, lay, false), st);
   N3DS_CUDA_TRY(cudaGetLastError());
+  record_event(rv, 0, st);
   rc = run_seg_passes(false, batch, rv, make_seg(batch, rays, ws, lay, 0), 0, st);
   if (rc) return rc;
+  record_event(rv, 1, st);
   if (R > 0) {
     n3ds::RayLaunch L = make_ray(batch, rays, ws, lay, R);
     L.rgb = rgb;
@@ -345,8 +359,10 @@ int n3ds_field_backward(const n3ds_batch_t* batch, const n3ds_rays_t* rays, cons
   n3ds::SegLaunch SL = make_seg(batch, rays, ws, lay, compat);
   SL.grad_x = grad_x;
   SL.stats = nullptr;
+  record_event(rv, 2, st);
   rc = run_seg_passes(true, batch, rv, SL, N_COUNTERS / 2, st);
   if (rc) return rc;
+  record_event(rv, 3, st);
   if (S > 0) {
     n3ds::FinalizeLaunch F{};
     F.sdf_ids = strokes->sdf_ids;
@@ -366,6 +382,32 @@ int n3ds_field_backward(const n3ds_batch_t* batch, const n3ds_rays_t* rays, cons
     n3ds::launch_finalize(F, st);
     N3DS_CUDA_TRY(cudaGetLastError());
   }
+  return N3DS_OK;
+}
+
+int n3ds_field_launch_count(const n3ds_batch_t* batch, const n3ds_options_t* opt, int32_t* forward,
+                            int32_t* backward) {
+  long long R = 0, S = 0;
+  int rc = check_batch(batch, &R, &S);
+  if (rc) return rc;
+  const Resolved rv = resolve(opt);
+  int f = 0, b = 0;
+  n3ds::SegLaunch dummy{};
+  run_seg_passes(false, batch, rv, dummy, 0, nullptr, &f);
+  run_seg_passes(true, batch, rv, dummy, 0, nullptr, &b);
+  // forward: prep + segment passes + ray render; backward: prep + ray adjoint +
+  // segment passes + finalize
+  if (forward) *forward = 1 + f + (R > 0 ? 1 : 0);
+  if (backward) *backward = 1 + (R > 0 ? 1 : 0) + b + (S > 0 ? 1 : 0);
+  return N3DS_OK;
+}
+
+int n3ds_field_read_pair_counts(void* workspace, uint64_t* per_base, n3ds_stream_t stream) {
+  if (!workspace || !per_base) return fail(N3DS_ERR_INVALID, "workspace and per_base required");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  N3DS_CUDA_TRY(cudaMemcpyAsync(per_base, static_cast<char*>(workspace) + 16, 16 * sizeof(uint64_t),
+                                cudaMemcpyDeviceToHost, st));
+  N3DS_CUDA_TRY(cudaStreamSynchronize(st));
   return N3DS_OK;
 }
 

@@ -191,16 +191,17 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_con
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t bar;
   __shared__ int s_tile, s_seg, s_fail;
+  __shared__ unsigned long long s_kcount[16];  // evaluated (sample, stroke) pairs per base
   const Stage S = carve(smem, L.chunk_cap, false);
   const int lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     mbar_init(&bar, 1);
     s_fail = 0;
   }
+  if (threadIdx.x < 16) s_kcount[threadIdx.x] = 0ull;
   __syncthreads();
   uint32_t phase = 0;
   int staged = -1;
-  unsigned long long pairs = 0;
   while (true) {
     if (threadIdx.x == 0) {
       s_tile = atomicAdd(L.tile_counter, 1);
@@ -234,14 +235,14 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_con
         const float* st = L.state + 5 * c.si;
         T = st[0]; sig = st[1]; cr = st[2]; cg = st[3]; cb = st[4];
       }
-      unsigned cand_total = 0;
+      const unsigned nact = __popc(__ballot_sync(0xffffffffu, c.active));
       for (int hi = sc.chunk_n - 1; hi >= 0; hi -= 32) {
         unsigned mask = cull_block(S, c, hi, lane);
-        cand_total += __popc(mask);
         while (mask) {
           const int b = __ffs(mask) - 1;
           mask &= mask - 1;
           const float* rec = S.recs + size_t(hi - b) * REC_FLOATS;
+          if (lane == 0) atomicAdd(&s_kcount[__float_as_int(rec[R_KIND]) & 15], (unsigned long long)nact);
           const float a = pair_alpha(rec, c.x, c.rinv);
           const float w = a * T;
           T *= (1.0f - a);
@@ -255,11 +256,14 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_con
         float* st = L.state + 5 * c.si;
         st[0] = T; st[1] = sig; st[2] = cr; st[3] = cg; st[4] = cb;
       }
-      if (lane == 0) pairs += (unsigned long long)cand_total * (unsigned)min(32, L.n_samples - (seg % L.segs_per_ray) * 32);
     }
     __syncthreads();
   }
-  if (lane == 0 && L.stats && pairs) atomicAdd(L.stats, pairs);
+  __syncthreads();
+  if (L.stats && threadIdx.x < 16 && s_kcount[threadIdx.x]) {
+    atomicAdd(L.stats, s_kcount[threadIdx.x]);
+    atomicAdd(L.stats + 1 + threadIdx.x, s_kcount[threadIdx.x]);
+  }
 }
 
 // ================================================================= backward
@@ -646,7 +650,7 @@ __global__ void ray_bwd_kernel(const RayLaunch L) {
 __global__ void prep_kernel(const PrepLaunch P) {
   const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (s < P.n_counters) P.counters[s] = 0;
-  if (s == 0 && P.stats) P.stats[0] = 0ull;
+  if (P.stats && s < 17) P.stats[s] = 0ull;
   if (s >= P.n_strokes) return;
   if (P.gslots) {
     float* g = P.gslots + s * GRAD_SLOTS;

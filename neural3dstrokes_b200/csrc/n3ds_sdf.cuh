@@ -193,36 +193,21 @@ __device__ __forceinline__ V3 quad_adjoint(const float* rec, const QuadFwd& s, f
   g[9] += -w * (1.f - t);
   g[10] += -w * t;
   float gtr = (s.t_raw > 0.f && s.t_raw < 1.f) ? gt : 0.f;
-  float gkx = -gtr, gky = 0.f, gkz = 0.f, gp = 0.f, gq = 0.f;
-  if (gtr == 0.f) {
-    // t is clamped (or the solve gave NaN): no dependence through the root
-  } else if (s.pos_branch) {
-    float gx0 = s.x0 != 0.f ? gtr / (3.f * s.u0 * s.u0) : 0.f;
-    float gx1 = s.x1 != 0.f ? gtr / (3.f * s.u1 * s.u1) : 0.f;
-    float gH = 0.5f * (gx0 - gx1);
-    gq = -0.5f * (gx0 + gx1);
-    float gh = gH * 0.5f / s.H;
-    gq += 2.f * s.q * gh;
-    gp = 12.f * s.p * s.p * gh;
-  } else {
-    float gz = gtr * s.sigma * (s.m + s.n);
-    float gm = gtr * s.sigma * s.z;
-    float gn = gm;
-    float sv = sinf(s.v), cv = cosf(s.v);
-    float gv = -sv * gm + BEZ_SQRT3 * cv * gn;
-    float garg = -(gv / 3.f) * rsqrtf(1.f - s.arg * s.arg);
-    gq = garg / s.den;
-    float gden = -garg * s.arg / s.den;
-    gp = 2.f * s.z * gden;
-    gz += 2.f * s.p * gden;
-    gp += gz * (-0.5f / s.z);
+  // t_raw is a root of G(t) = t^3 + 3 kx t^2 + 3 ky t + kz (the stationarity condition
+  // of |B(t) - pos|^2 divided by 2 |b|^2). Its derivative follows from the implicit
+  // function theorem, dt = -(3t^2 dkx + 3t dky + dkz) / G'(t): well conditioned for a
+  // simple root, unlike differentiating the cube roots of the closed form, whose
+  // 1/(3 u^2) factors blow up when one Cardano term approaches zero.
+  float gkx = 0.f, gky = 0.f, gkz = 0.f;
+  if (gtr != 0.f) {
+    const float tr = s.t_raw;
+    float Gp = 3.f * tr * tr + 6.f * s.kx * tr + 3.f * s.ky;
+    if (fabsf(Gp) < 1e-20f) Gp = copysignf(1e-20f, Gp);
+    const float f = -gtr / Gp;
+    gkx = f * 3.f * tr * tr;
+    gky = f * 3.f * tr;
+    gkz = f;
   }
-  // p = ky - kx^2 ; q = kx (2 kx^2 - 3 ky) + kz
-  gky += gp;
-  gkx += -2.f * s.kx * gp;
-  gkx += gq * (6.f * s.kx * s.kx - 3.f * s.ky);
-  gky += -3.f * s.kx * gq;
-  gkz += gq;
   // ky = kk (aa2 + d.b) / 3 ; kz = kk (d.a)
   float db = dot(s.d, b), da = dot(s.d, a);
   float gkk = gky * (rec[R_QAA2] + db) / 3.f + gkz * da;

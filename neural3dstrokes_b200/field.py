@@ -27,10 +27,20 @@ class FieldOptions:
     segs_per_tile: int = 0     # 32-sample segments per CTA work tile (0: auto)
     grad_mode: str = "exact"   # 'exact' or 'compat'
 
-    def c(self):
+    def c(self, events=None):
+        """ctypes options; ``events``: optional 4 torch.cuda.Event(enable_timing=True)
+        recorded around the forward and backward segment kernels."""
+        ev = None
+        if events is not None:
+            for e in events:
+                if not e.cuda_event:  # torch creates the event on its first record
+                    e.record()
+            arr = (ctypes.c_void_p * 4)(*[ctypes.c_void_p(e.cuda_event) for e in events])
+            ev = ctypes.cast(arr, ctypes.POINTER(ctypes.c_void_p))
+            self._ev_keepalive = arr
         return _lib.Options(float(self.cull_alpha), int(self.chunk_fwd), int(self.chunk_bwd), int(self.warps),
                             int(self.segs_per_tile),
-                            _lib.N3DS_GRAD_COMPAT if self.grad_mode == "compat" else _lib.N3DS_GRAD_EXACT)
+                            _lib.N3DS_GRAD_COMPAT if self.grad_mode == "compat" else _lib.N3DS_GRAD_EXACT, ev)
 
 
 class _Native:

@@ -37,8 +37,11 @@ def compute_alpha_weights(density, tdist, dirs, opaque_background=False):
     return weights, alpha, trans
 
 
-def volumetric_rendering(rgbs, weights, tdist, bg_rgbs):
-    eps = torch.finfo(rgbs.dtype).eps
+def volumetric_rendering(rgbs, weights, tdist, bg_rgbs, eps=None):
+    """render.py:51-88; ``eps`` defaults to the machine epsilon of the input dtype as
+    the reference does (render.py:76)."""
+    if eps is None:
+        eps = torch.finfo(rgbs.dtype).eps
     acc = weights.sum(dim=-1)
     bg_w = (1 - acc[..., None]).clamp_min(0.)
     rgb = (weights[..., None] * rgbs).sum(dim=-2) + bg_w * bg_rgbs
@@ -56,6 +59,10 @@ def render_strokes(x, radius, tdist, dirs, shape_params, sdf_ids, color_params, 
     x [R,N,3], radius [R,N], tdist [R,N+1], dirs [R,3]; shape_params [S,Pmax] padded,
     sdf_ids [S]; color_params [S,3]; density [S] (already times density_scale).
     Returns rgb [R,3], acc [R], depth [R]. Differentiable by torch.autograd.
+
+    The depth guard max(acc, eps) uses float32's epsilon whatever the oracle dtype:
+    the reference path runs in float32 (render.py:76 takes eps from the input dtype),
+    so that constant is part of the function being reproduced.
     """
     R, N, _ = x.shape
     xf = x.reshape(-1, 3)
@@ -64,5 +71,6 @@ def render_strokes(x, radius, tdist, dirs, shape_params, sdf_ids, color_params, 
                                            sdf_delta, use_laplace, inv_scale_radius)
     dens, col = sf.compose_forward(alpha, color, density)
     weights = compute_alpha_weights(dens.reshape(R, N), tdist, dirs, opaque_background)[0]
-    rgb, depth, acc = volumetric_rendering(col.reshape(R, N, -1), weights, tdist, bg)
+    rgb, depth, acc = volumetric_rendering(col.reshape(R, N, -1), weights, tdist, bg,
+                                           eps=float(torch.finfo(torch.float32).eps))
     return rgb, acc, depth

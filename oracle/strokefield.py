@@ -35,6 +35,8 @@ N_BASE_PARAMS = {0: 0, 1: 0, 2: 1, 3: 2, 4: 1, 5: 2, 6: 1, 7: 0, 8: 0, 9: 11, 10
 # the bases this build implements (the stroke-field hot path's primitive set)
 SUPPORTED_BASES = (0, 1, 2, 4, 7, 8, 9, 10)
 INV_SQRT3 = 0.57735027  # strokes_sdf.h:587,612
+# the linear soft step's upper clamp 0.9999f (strokes_forward.cu:88) as float32 rounds it
+ALPHA_MAX = float(torch.tensor(0.9999, dtype=torch.float32))
 SQRT3_BEZ = 1.732050808  # strokes_sdf.h:686
 
 
@@ -426,7 +428,7 @@ def soft_step(sdf, radius_eff, sdf_delta, use_laplace):
         e = torch.exp(-s.abs())
         soft = torch.where(s <= 0, 0.5 * e, 1.0 - 0.5 * e)
     else:
-        soft = cu_clamp(s + 0.5, 0.0, 0.9999)
+        soft = cu_clamp(s + 0.5, 0.0, ALPHA_MAX)
     hard = (sdf <= 0).to(sdf.dtype)
     return torch.where(pos, soft, hard)
 
@@ -572,7 +574,7 @@ def stroke_backward_compat(grad_alpha, grad_color, x, radius, alpha, shape_param
         if use_laplace:
             dadsdf = torch.where(alpha < 0.5, alpha, 1.0 - alpha) * -sdf_scale
         else:
-            dadsdf = torch.where((alpha > 0) & (alpha < 0.9999), -sdf_scale, torch.zeros_like(alpha))
+            dadsdf = torch.where((alpha > 0) & (alpha < ALPHA_MAX), -sdf_scale, torch.zeros_like(alpha))
     else:
         dadsdf = torch.zeros_like(alpha)
     dl_dsdf = grad_alpha * dadsdf

@@ -1,0 +1,171 @@
+"""Generate the golden fixtures under tests/golden/ from the reference itself.
+
+Three sources, each a seeded, small input set:
+
+--layouts   (CPU, needs the reference checkout): imports the reference
+            source/strokelib/strokes.py with a stub ``_strokelib`` module and records,
+            per shape type, the sdf_id, parameter count and clamp ranges that
+            get_stroke produces (strokes.py:95-106, 227-313). -> layouts.json
+--render    (CPU, needs the reference checkout): imports the reference
+            source/utils/render.py and runs compute_alpha_weights (plain and opaque
+            background) and volumetric_rendering in float64 on seeded inputs.
+            -> render_golden.npz
+--strokelib (GPU, needs oracle/_ref built from the reference sources by
+            oracle/build_ref.py): runs the reference CUDA operators stroke_forward,
+            stroke_backward, compose_forward, compose_backward on seeded inputs for
+            every implemented primitive. -> strokelib_golden.npz
+
+Usage: python tests/golden/make_golden.py [--layouts] [--render] [--strokelib]
+       [--ref /root/reference] [--out tests/golden]
+"""
+import argparse
+import copy
+import glob
+import importlib.machinery
+import importlib.util
+import json
+import os
+import sys
+import types
+
+import numpy as np
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+
+def make_layouts(ref_root, out):
+    sys.modules["_strokelib"] = types.ModuleType("_strokelib")  # stub backend: never called
+    path = os.path.join(ref_root, "source", "strokelib", "strokes.py")
+    spec = importlib.util.spec_from_file_location("ref_strokes", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    pristine = copy.deepcopy(mod._sdf_dict)
+    res = {}
+    for name in pristine:
+        mod._sdf_dict = copy.deepcopy(pristine)  # get_stroke mutates the range lists in place
+        base, _, _, t, r, s1, s3 = mod._sdf_dict[name]
+        _, d_shape, d_color, sranges, cranges, _, _ = mod.get_stroke(name, "constant_rgb", "recon")
+        res[name] = {
+            "sdf_id": mod._make_sdf_id(base, t, r, s1, s3),
+            "dim_shape": d_shape,
+            "dim_color": d_color,
+            "shape_ranges": [[None if a is None else float(a), None if b is None else float(b)] for a, b in sranges],
+        }
+    del sys.modules["_strokelib"]
+    with open(os.path.join(out, "layouts.json"), "w") as f:
+        json.dump(res, f, indent=1, sort_keys=True)
+    print("layouts:", len(res), "shape types")
+
+
+def make_render(ref_root, out):
+    sys.path.insert(0, ref_root)
+    from source.utils import render as ref_render  # noqa: E402
+    g = torch.Generator().manual_seed(1234)
+    R, N = 96, 40
+    density = (torch.rand(R, N, generator=g, dtype=torch.float64) ** 4) * 30
+    density[torch.rand(R, N, generator=g) < 0.3] = 0
+    rgbs = torch.rand(R, N, 3, generator=g, dtype=torch.float64)
+    t0 = 2 + torch.rand(R, 1, generator=g, dtype=torch.float64)
+    steps = torch.rand(R, N, generator=g, dtype=torch.float64) * 0.2 + 0.01
+    tdist = torch.cat([t0, t0 + torch.cumsum(steps, -1)], -1)
+    dirs = torch.randn(R, 3, generator=g, dtype=torch.float64)
+    bg = torch.rand(R, 3, generator=g, dtype=torch.float64)
+    w, a, tr = ref_render.compute_alpha_weights(density, tdist, dirs)
+    wo, ao, tro = ref_render.compute_alpha_weights(density, tdist, dirs, opaque_background=True)
+    rend = ref_render.volumetric_rendering(rgbs, w, tdist, bg, tdist[..., -1:], False)
+    rend1 = ref_render.volumetric_rendering(rgbs, wo, tdist, 1.0, tdist[..., -1:], False)
+    np.savez_compressed(os.path.join(out, "render_golden.npz"), density=density.numpy(), rgbs=rgbs.numpy(),
+                        tdist=tdist.numpy(), dirs=dirs.numpy(), bg=bg.numpy(), weights=w.numpy(),
+                        alpha=a.numpy(), trans=tr.numpy(), weights_opaque=wo.numpy(), rgb=rend["rgb"].numpy(),
+                        depth=rend["depth"].numpy(), acc=rend["acc"].numpy(), rgb_opaque=rend1["rgb"].numpy(),
+                        depth_opaque=rend1["depth"].numpy(), acc_opaque=rend1["acc"].numpy())
+    print("render golden written")
+
+
+KINDS = ["sphere", "ellipsoid", "cube", "roundcube", "capsule", "octahedron", "tetrahedron",
+         "quadratic_bezier", "cubic_bezier"]
+
+
+def make_strokelib(out):
+    from neural3dstrokes_b200 import scenes
+    from oracle import strokefield as sf
+    hits = glob.glob(os.path.join(ROOT, "oracle", "_ref", "_strokelib*.so"))
+    if not hits:
+        raise SystemExit("oracle/_ref/_strokelib*.so missing: run python oracle/build_ref.py")
+    loader = importlib.machinery.ExtensionFileLoader("_strokelib", hits[0])
+    spec = importlib.util.spec_from_file_location("_strokelib", hits[0], loader=loader)
+    ref = importlib.util.module_from_spec(spec)
+    loader.exec_module(ref)
+    dev = torch.device("cuda:0")
+    arrays = {}
+    for ki, kind in enumerate(KINDS):
+        g = torch.Generator().manual_seed(500 + ki)
+        sc = scenes.make_strokes([kind] * 12, g)
+        rays = scenes.make_rays(20, 16, g)
+        sid = scenes.SDF_ID[kind]
+        ps = sc.shape_params[:, :sf.num_shape_params(sid)].contiguous()
+        x = rays.x.reshape(-1, 3).contiguous()
+        r = rays.radius.reshape(-1).contiguous()
+        P, S = x.shape[0], ps.shape[0]
+        # laplace step with delta 0.02 (the benchmark softness); linear step with a wide
+        # delta 0.5 so that samples fall inside its 0 < alpha < 0.9999 band
+        for lap, inv, delta in [(True, True, 0.02), (False, False, 0.5)]:
+            tag = f"{kind}_{int(lap)}{int(inv)}"
+            a = torch.empty(P, S, device=dev)
+            c = torch.empty(P, S, 3, device=dev)
+            sdf = torch.empty(P, S, device=dev)
+            ref.stroke_forward(a, c, sdf, torch.empty(0, device=dev), x.to(dev), r.to(dev), rays.dirs.to(dev),
+                               ps.to(dev), sc.color_params.to(dev), sid, 0, delta, lap, inv)
+            ga = torch.randn(P, S, generator=g)
+            gc = torch.randn(P, S, 3, generator=g)
+            gps = torch.zeros_like(ps, device=dev)
+            gcol = torch.zeros(S, 3, device=dev)
+            gx = torch.zeros(P, 3, device=dev)
+            ref.stroke_backward(gps, gcol, gx, ga.to(dev), gc.to(dev), torch.empty(0, device=dev), x.to(dev),
+                                r.to(dev), rays.dirs.to(dev), a, ps.to(dev), sc.color_params.to(dev), sid, 0, delta,
+                                lap, inv)
+            for k, v in dict(x=x, radius=r, shape=ps, color=sc.color_params, alpha=a, colors=c, sdf=sdf,
+                             g_alpha=ga, g_color=gc, grad_shape=gps, grad_color=gcol, grad_x=gx).items():
+                arrays[f"{tag}/{k}"] = v.detach().cpu().numpy()
+            arrays[f"{tag}/sdf_id"] = np.array(sid)
+            arrays[f"{tag}/delta"] = np.array(delta)
+    g = torch.Generator().manual_seed(99)
+    P, S = 300, 37
+    al = torch.rand(P, S, generator=g) ** 3
+    al[torch.rand(P, S, generator=g) < 0.3] = 0
+    co = torch.rand(P, S, 3, generator=g)
+    dp = torch.rand(S, generator=g) * 10
+    dens = torch.empty(P, device=dev)
+    col = torch.empty(P, 3, device=dev)
+    ref.compose_forward(dens, col, al.to(dev), co.to(dev), dp.to(dev))
+    gd = torch.randn(P, generator=g)
+    gcol = torch.randn(P, 3, generator=g)
+    ga = torch.zeros(P, S, device=dev)
+    gc = torch.zeros(P, S, 3, device=dev)
+    gdp = torch.zeros(S, device=dev)
+    ref.compose_backward(ga, gc, gdp, gd.to(dev), gcol.to(dev), al.to(dev), co.to(dev), dp.to(dev))
+    for k, v in dict(alphas=al, colors=co, density_params=dp, density=dens, color=col, g_density=gd, g_color=gcol,
+                     grad_alphas=ga, grad_colors=gc, grad_density_params=gdp).items():
+        arrays[f"compose/{k}"] = v.detach().cpu().numpy()
+    np.savez_compressed(os.path.join(out, "strokelib_golden.npz"), **arrays)
+    print("strokelib golden written:", len(arrays), "arrays")
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--layouts", action="store_true")
+    ap.add_argument("--render", action="store_true")
+    ap.add_argument("--strokelib", action="store_true")
+    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--out", default=HERE)
+    a = ap.parse_args()
+    os.makedirs(a.out, exist_ok=True)
+    if a.layouts:
+        make_layouts(a.ref, a.out)
+    if a.render:
+        make_render(a.ref, a.out)
+    if a.strokelib:
+        make_strokelib(a.out)

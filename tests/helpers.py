@@ -43,6 +43,13 @@ def oracle_forward(sc, rays, delta=0.02, laplace=True, inv=True, bg=1.0, opaque=
                               bg if not torch.is_tensor(bg) else d(bg), opaque)
 
 
+def depth_upstream(sc, rays, g, delta=0.02, thresh=0.05):
+    """Random upstream depth gradient, zero on rays less than 5% opaque (where
+    depth = D / acc is ill-conditioned and culling-sensitive)."""
+    _, acc, _ = oracle_forward(sc, rays, delta=delta)
+    return torch.randn(rays.n_rays, generator=g) * (acc > thresh).float()
+
+
 def oracle_grads(sc, rays, g_rgb, g_acc, g_depth, delta=0.02, laplace=True, inv=True, bg=1.0, opaque=False):
     """Exact float64 gradients (torch.autograd of the oracle) of
     L = <rgb, g_rgb> + <acc, g_acc> + <depth, g_depth>."""

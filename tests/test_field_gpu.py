@@ -5,8 +5,8 @@ Tolerances (helpers.rel, normwise): forward 1e-5, gradients 1e-4.
 import pytest
 import torch
 
-from helpers import (FWD_TOL, GRAD_TOL, depth_errors, oracle_forward, oracle_grads, rel, shape_param_mask,
-                     small_workload)
+from helpers import (FWD_TOL, GRAD_TOL, depth_errors, depth_upstream, oracle_forward, oracle_grads, rel,
+                     shape_param_mask, small_workload)
 from neural3dstrokes_b200 import scenes
 from neural3dstrokes_b200.field import FieldOptions, render_strokes
 
@@ -45,7 +45,7 @@ def test_backward_matches_float64_autograd(cuda, kind):
     g = torch.Generator().manual_seed(7)
     g_rgb = torch.randn(rays.n_rays, 3, generator=g)
     g_acc = torch.randn(rays.n_rays, generator=g)
-    g_depth = torch.randn(rays.n_rays, generator=g)
+    g_depth = depth_upstream(sc, rays, g)
     (rgb, acc, depth), (x, sp, col, den, dl) = run_field(sc, rays, cuda, requires_grad=True)
     L = (rgb * g_rgb.to(cuda)).sum() + (acc * g_acc.to(cuda)).sum() + (depth * g_depth.to(cuda)).sum()
     L.backward()
