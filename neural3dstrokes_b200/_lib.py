@@ -9,7 +9,9 @@ import threading
 
 import torch
 
-LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libn3ds.so")
+# N3DS_LIB selects another build of the same library (e.g. a tuning variant)
+LIB_PATH = os.environ.get("N3DS_LIB") or os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib",
+                                                      "libn3ds.so")
 
 N3DS_OK = 0
 N3DS_GRAD_EXACT = 0

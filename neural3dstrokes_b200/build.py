@@ -18,14 +18,18 @@ import sys
 PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
-LIBDIR = os.path.join(PKG, "lib")
+LIBDIR = os.environ.get("N3DS_BUILD_DIR") or os.path.join(PKG, "lib")
 OBJDIR = os.path.join(LIBDIR, "obj")
 LIB = os.path.join(LIBDIR, "libn3ds.so")
 INCLUDE = os.path.join(ROOT, "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
-         "-I", INCLUDE, "-I", CSRC]
+# Approximate (MUFU-based) sqrt and division and flush-to-zero of denormals: the
+# stroke kernels are FP32 issue-bound and their IEEE-rounded sqrt/div sequences cost
+# several instructions each; the 1-2 ulp difference is far inside the 1e-5 tolerance.
+FAST_MATH = ["-prec-sqrt=false", "-prec-div=false", "-ftz=true"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INCLUDE, "-I", CSRC] + \
+    ([] if os.environ.get("N3DS_IEEE_MATH") else FAST_MATH)
 
 
 def nvcc_path():

@@ -177,9 +177,8 @@ int run_seg_passes(bool backward, const n3ds_batch_t* b, const Resolved& rv, n3d
         d.chunk_n = std::max(0, hi - lo);
         d.first_pass = pass == 0;
         d.last_pass = pass == nch[i] - 1;
-        d.tile_begin = tiles;
-        const long long segs = (long long)d.n_rays * spr;
-        tiles += (int)((segs + rv.segs_per_tile - 1) / rv.segs_per_tile);
+        d.tile_begin = tiles;  // work items are rays: this scene's first ray in the launch
+        tiles += d.n_rays;
       }
       if (tiles == 0) continue;
       if (counter >= N_COUNTERS) return fail(N3DS_ERR_INVALID, "batch needs too many launches (raise chunk size or split the batch)");

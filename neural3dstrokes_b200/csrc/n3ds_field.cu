@@ -11,8 +11,10 @@
 // strokes for its own sample; the stroke (and so the SDF type) is warp-uniform, so
 // mixed-type scenes run without divergence.
 //
-// Persistent CTAs (one per SM) pull tiles of segments from a global counter; a tile
-// never spans two scenes, so a CTA restages records only when its scene changes.
+// Persistent CTAs (one per SM); each warp takes whole rays (all their segments) from a
+// global counter and keeps the next one it took in shared memory. The CTA synchronises
+// only when the smallest ray held by its warps belongs to another scene: then it
+// restages that scene's records, and warps whose ray belongs to it carry on.
 // Scenes with more strokes than one stage holds run in several passes (one launch
 // each), carrying the per-sample composite state through HBM.
 //
@@ -190,74 +192,77 @@ template <int WARPS>
 __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_constant__ SegLaunch L) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t bar;
-  __shared__ int s_tile, s_seg, s_fail;
+  __shared__ int s_hold[WARPS];
+  __shared__ int s_scene, s_fail;
   __shared__ unsigned long long s_kcount[16];  // evaluated (sample, stroke) pairs per base
   const Stage S = carve(smem, L.chunk_cap, false);
   const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
   if (threadIdx.x == 0) {
     mbar_init(&bar, 1);
     s_fail = 0;
   }
   if (threadIdx.x < 16) s_kcount[threadIdx.x] = 0ull;
-  __syncthreads();
+  if (lane == 0) s_hold[warp] = atomicAdd(L.tile_counter, 1);
   uint32_t phase = 0;
   int staged = -1;
   while (true) {
+    __syncthreads();
     if (threadIdx.x == 0) {
-      s_tile = atomicAdd(L.tile_counter, 1);
-      s_seg = 0;
+      int best = 0x7fffffff;
+      for (int w = 0; w < WARPS; w++) best = min(best, s_hold[w]);
+      s_scene = best < L.tiles_total ? find_scene(L, best) : -1;
     }
     __syncthreads();
-    const int tile = s_tile;
-    if (tile >= L.tiles_total) break;
-    const int sci = find_scene(L, tile);
-    const SceneDesc& sc = L.sc[sci];
+    const int sci = s_scene;
+    if (sci < 0) break;
     if (sci != staged) {
-      if (!stage_chunk(L, sc, S, &bar, phase, &s_fail)) {
+      if (!stage_chunk(L, L.sc[sci], S, &bar, phase, &s_fail)) {
         if (threadIdx.x == 0) atomicOr(L.status, ST_WAIT_TIMEOUT);
         return;
       }
       staged = sci;
     }
-    const int seg_lo = (tile - sc.tile_begin) * L.segs_per_tile;
-    const int seg_hi = min(seg_lo + L.segs_per_tile, sc.n_rays * L.segs_per_ray);
-    while (true) {
-      int k = 0;
-      if (lane == 0) k = atomicAdd(&s_seg, 1);
-      k = __shfl_sync(0xffffffffu, k, 0);
-      const int seg = seg_lo + k;
-      if (seg >= seg_hi) break;
-      SegCtx c = seg_setup(L, sc, seg, lane);
-      float T, sig, cr, cg, cb;
-      if (sc.first_pass) {
-        T = 1.f; sig = cr = cg = cb = 0.f;
-      } else {
-        const float* st = L.state + 5 * c.si;
-        T = st[0]; sig = st[1]; cr = st[2]; cg = st[3]; cb = st[4];
-      }
-      const unsigned nact = __popc(__ballot_sync(0xffffffffu, c.active));
-      for (int hi = sc.chunk_n - 1; hi >= 0; hi -= 32) {
-        unsigned mask = cull_block(S, c, hi, lane);
-        while (mask) {
-          const int b = __ffs(mask) - 1;
-          mask &= mask - 1;
-          const float* rec = S.recs + size_t(hi - b) * REC_FLOATS;
-          if (lane == 0) atomicAdd(&s_kcount[__float_as_int(rec[R_KIND]) & 15], (unsigned long long)nact);
-          const float a = pair_alpha(rec, c.x, c.rinv);
-          const float w = a * T;
-          T *= (1.0f - a);
-          sig += rec[R_DENSITY] * w;
-          cr += rec[R_COLOR] * w;
-          cg += rec[R_COLOR + 1] * w;
-          cb += rec[R_COLOR + 2] * w;
+    const SceneDesc& sc = L.sc[sci];
+    const int item_end = sc.tile_begin + sc.n_rays;
+    int item = s_hold[warp];
+    while (item >= sc.tile_begin && item < item_end) {
+      const int ray_local = item - sc.tile_begin;
+      for (int g = 0; g < L.segs_per_ray; g++) {
+        SegCtx c = seg_setup(L, sc, ray_local * L.segs_per_ray + g, lane);
+        float T, sig, cr, cg, cb;
+        if (sc.first_pass) {
+          T = 1.f; sig = cr = cg = cb = 0.f;
+        } else {
+          const float* st = L.state + 5 * c.si;
+          T = st[0]; sig = st[1]; cr = st[2]; cg = st[3]; cb = st[4];
+        }
+        const unsigned nact = __popc(__ballot_sync(0xffffffffu, c.active));
+        for (int hi = sc.chunk_n - 1; hi >= 0; hi -= 32) {
+          unsigned mask = cull_block(S, c, hi, lane);
+          while (mask) {
+            const int b = __ffs(mask) - 1;
+            mask &= mask - 1;
+            const float* rec = S.recs + size_t(hi - b) * REC_FLOATS;
+            if (lane == 0) atomicAdd(&s_kcount[__float_as_int(rec[R_KIND]) & 15], (unsigned long long)nact);
+            const float a = pair_alpha(rec, c.x, c.rinv);
+            const float w = a * T;
+            T *= (1.0f - a);
+            sig += rec[R_DENSITY] * w;
+            cr += rec[R_COLOR] * w;
+            cg += rec[R_COLOR + 1] * w;
+            cb += rec[R_COLOR + 2] * w;
+          }
+        }
+        if (c.active) {
+          float* st = L.state + 5 * c.si;
+          st[0] = T; st[1] = sig; st[2] = cr; st[3] = cg; st[4] = cb;
         }
       }
-      if (c.active) {
-        float* st = L.state + 5 * c.si;
-        st[0] = T; st[1] = sig; st[2] = cr; st[3] = cg; st[4] = cb;
-      }
+      if (lane == 0) item = atomicAdd(L.tile_counter, 1);
+      item = __shfl_sync(0xffffffffu, item, 0);
     }
-    __syncthreads();
+    if (lane == 0) s_hold[warp] = item;
   }
   __syncthreads();
   if (L.stats && threadIdx.x < 16 && s_kcount[threadIdx.x]) {
@@ -323,9 +328,11 @@ template <int WARPS>
 __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_constant__ SegLaunch L) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t bar;
-  __shared__ int s_tile, s_seg, s_fail;
+  __shared__ int s_hold[WARPS];
+  __shared__ int s_scene, s_fail;
   const Stage S = carve(smem, L.chunk_cap, true);
   const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
   const int nthr = blockDim.x;
   if (threadIdx.x == 0) {
     mbar_init(&bar, 1);
@@ -349,129 +356,132 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
     }
   };
 
+  if (lane == 0) s_hold[warp] = atomicAdd(L.tile_counter, 1);
   while (true) {
+    __syncthreads();
     if (threadIdx.x == 0) {
-      s_tile = atomicAdd(L.tile_counter, 1);
-      s_seg = 0;
+      int best = 0x7fffffff;
+      for (int w = 0; w < WARPS; w++) best = min(best, s_hold[w]);
+      s_scene = best < L.tiles_total ? find_scene(L, best) : -1;
     }
     __syncthreads();
-    const int tile = s_tile;
-    if (tile >= L.tiles_total) break;
-    const int sci = find_scene(L, tile);
-    const SceneDesc& sc = L.sc[sci];
+    const int sci = s_scene;
+    if (sci < 0) break;
     if (sci != staged) {
       if (staged >= 0) {
         flush(staged);
         __syncthreads();
       }
-      if (!stage_chunk(L, sc, S, &bar, phase, &s_fail)) {
+      if (!stage_chunk(L, L.sc[sci], S, &bar, phase, &s_fail)) {
         if (threadIdx.x == 0) atomicOr(L.status, ST_WAIT_TIMEOUT);
         return;
       }
       staged = sci;
     }
-    const int seg_lo = (tile - sc.tile_begin) * L.segs_per_tile;
-    const int seg_hi = min(seg_lo + L.segs_per_tile, sc.n_rays * L.segs_per_ray);
-    while (true) {
-      int k = 0;
-      if (lane == 0) k = atomicAdd(&s_seg, 1);
-      k = __shfl_sync(0xffffffffu, k, 0);
-      const int seg = seg_lo + k;
-      if (seg >= seg_hi) break;
-      SegCtx c = seg_setup(L, sc, seg, lane);
-      CompAdj s;
-      {
-        const float* st = L.state + 5 * c.si;
-        s.Tf = st[0]; s.sig = st[1]; s.Cr = st[2]; s.Cg = st[3]; s.Cb = st[4];
-        const float* sd = L.seeds + 5 * c.si;
-        s.gs = sd[0]; s.gcr = sd[1]; s.gcg = sd[2]; s.gcb = sd[3]; s.gT = sd[4];
-        if (!c.active) {
-          s.gs = s.gcr = s.gcg = s.gcb = s.gT = 0.f;
-        }
-      }
-      V3 gx;
-      if (sc.first_pass) {
-        s.T = 1.f; s.Ps = s.Pr = s.Pg = s.Pb = 0.f;
-        gx = v3(0.f, 0.f, 0.f);
-      } else {
-        const float* b = L.bstate + 8 * c.si;
-        s.T = b[0]; s.Ps = b[1]; s.Pr = b[2]; s.Pg = b[3]; s.Pb = b[4];
-        gx = v3(b[5], b[6], b[7]);
-      }
-      for (int hi = sc.chunk_n - 1; hi >= 0; hi -= 32) {
-        unsigned mask = cull_block(S, c, hi, lane);
-        while (mask) {
-          const int b = __ffs(mask) - 1;
-          mask &= mask - 1;
-          const int sl = hi - b;
-          const float* rec = S.recs + size_t(sl) * REC_FLOATS;
-          float* row = S.gacc + size_t(sl) * GRAD_SLOTS;
-          const int kind = __float_as_int(rec[R_KIND]);
-          const int base = kind & 15;
-          const int mode = (kind >> 8) & 3;
-          if (base <= B_TETRAHEDRON) {
-            float v[16];
-#pragma unroll
-            for (int j = 0; j < 16; j++) v[j] = 0.f;
-            const V3 p = prim_local(rec, c.x);
-            const float sdf = prim_sdf(base, p, rec[R_BP]);
-            const float f = (kind & K_S3FAC) ? s3_factor(base, p, ld3(rec + R_S)) : 1.f;
-            const float kk = rec[R_KFIX] * f * c.rinv;
-            const float m = -sdf * kk;
-            const float a = mode == STEP_HARD ? (sdf <= 0.f ? 1.f : 0.f) : soft_alpha(mode, m);
-            const float dm = compose_step(rec, a, m, mode, s, v, compat);
-            const float K = m * dm;
-            v[G_K] += K;
-            gx += prim_backprop(rec, kind, p, -kk * dm, K, v, compat);
-            reduce_into<16>(v, row, lane);
-          } else if (base == B_QUAD_BEZIER) {
-            float v[16];
-#pragma unroll
-            for (int j = 0; j < 16; j++) v[j] = 0.f;
-            QuadFwd qf;
-            const float sdf = quad_eval(rec, c.x, qf);
-            const float kk = rec[R_KFIX] * c.rinv;
-            const float m = -sdf * kk;
-            const float a = mode == STEP_HARD ? (sdf <= 0.f ? 1.f : 0.f) : soft_alpha(mode, m);
-            const float dm = compose_step(rec, a, m, mode, s, v, compat);
-            v[G_K] += m * dm;
-            gx += quad_adjoint(rec, qf, -kk * dm, v + G_CTRL);
-            reduce_into<16>(v, row, lane);
-          } else {
-            float v[32];
-#pragma unroll
-            for (int j = 0; j < 32; j++) v[j] = 0.f;
-            CubicFwd cf;
-            const float sdf = cubic_eval(rec, c.x, cf);
-            const float kk = rec[R_KFIX] * c.rinv;
-            const float m = -sdf * kk;
-            const float a = mode == STEP_HARD ? (sdf <= 0.f ? 1.f : 0.f) : soft_alpha(mode, m);
-            const float dm = compose_step(rec, a, m, mode, s, v, compat);
-            const float dsdf = -kk * dm;
-            v[G_K] += m * dm;
-            V3 g = cubic_adjoint(rec, c.x, cf, dsdf, v + G_CTRL, compat);
-            if (compat) g = g * dsdf;  // the reference multiplies by dL/dSDF again
-            gx += g;
-            reduce_into<32>(v, row, lane);
+    const SceneDesc& sc = L.sc[sci];
+    const int item_end = sc.tile_begin + sc.n_rays;
+    int item = s_hold[warp];
+    while (item >= sc.tile_begin && item < item_end) {
+      const int ray_local = item - sc.tile_begin;
+      for (int g = 0; g < L.segs_per_ray; g++) {
+        SegCtx c = seg_setup(L, sc, ray_local * L.segs_per_ray + g, lane);
+        CompAdj s;
+        {
+          const float* st = L.state + 5 * c.si;
+          s.Tf = st[0]; s.sig = st[1]; s.Cr = st[2]; s.Cg = st[3]; s.Cb = st[4];
+          const float* sd = L.seeds + 5 * c.si;
+          s.gs = sd[0]; s.gcr = sd[1]; s.gcg = sd[2]; s.gcb = sd[3]; s.gT = sd[4];
+          if (!c.active) {
+            s.gs = s.gcr = s.gcg = s.gcb = s.gT = 0.f;
           }
         }
-      }
-      if (c.active) {
-        if (sc.last_pass) {
-          if (L.grad_x) {
-            L.grad_x[3 * c.si] = gx.x;
-            L.grad_x[3 * c.si + 1] = gx.y;
-            L.grad_x[3 * c.si + 2] = gx.z;
-          }
+        V3 gx;
+        if (sc.first_pass) {
+          s.T = 1.f; s.Ps = s.Pr = s.Pg = s.Pb = 0.f;
+          gx = v3(0.f, 0.f, 0.f);
         } else {
-          float* b = L.bstate + 8 * c.si;
-          b[0] = s.T; b[1] = s.Ps; b[2] = s.Pr; b[3] = s.Pg; b[4] = s.Pb;
-          b[5] = gx.x; b[6] = gx.y; b[7] = gx.z;
+          const float* b = L.bstate + 8 * c.si;
+          s.T = b[0]; s.Ps = b[1]; s.Pr = b[2]; s.Pg = b[3]; s.Pb = b[4];
+          gx = v3(b[5], b[6], b[7]);
+        }
+        for (int hi = sc.chunk_n - 1; hi >= 0; hi -= 32) {
+          unsigned mask = cull_block(S, c, hi, lane);
+          while (mask) {
+            const int b = __ffs(mask) - 1;
+            mask &= mask - 1;
+            const int sl = hi - b;
+            const float* rec = S.recs + size_t(sl) * REC_FLOATS;
+            float* row = S.gacc + size_t(sl) * GRAD_SLOTS;
+            const int kind = __float_as_int(rec[R_KIND]);
+            const int base = kind & 15;
+            const int mode = (kind >> 8) & 3;
+            if (base <= B_TETRAHEDRON) {
+              float v[16];
+  #pragma unroll
+              for (int j = 0; j < 16; j++) v[j] = 0.f;
+              const V3 p = prim_local(rec, c.x);
+              const float sdf = prim_sdf(base, p, rec[R_BP]);
+              const float f = (kind & K_S3FAC) ? s3_factor(base, p, ld3(rec + R_S)) : 1.f;
+              const float kk = rec[R_KFIX] * f * c.rinv;
+              const float m = -sdf * kk;
+              const float a = mode == STEP_HARD ? (sdf <= 0.f ? 1.f : 0.f) : soft_alpha(mode, m);
+              const float dm = compose_step(rec, a, m, mode, s, v, compat);
+              const float K = m * dm;
+              v[G_K] += K;
+              gx += prim_backprop(rec, kind, p, -kk * dm, K, v, compat);
+              reduce_into<16>(v, row, lane);
+            } else if (base == B_QUAD_BEZIER) {
+              float v[16];
+  #pragma unroll
+              for (int j = 0; j < 16; j++) v[j] = 0.f;
+              QuadFwd qf;
+              const float sdf = quad_eval(rec, c.x, qf);
+              const float kk = rec[R_KFIX] * c.rinv;
+              const float m = -sdf * kk;
+              const float a = mode == STEP_HARD ? (sdf <= 0.f ? 1.f : 0.f) : soft_alpha(mode, m);
+              const float dm = compose_step(rec, a, m, mode, s, v, compat);
+              v[G_K] += m * dm;
+              gx += quad_adjoint(rec, qf, -kk * dm, v + G_CTRL);
+              reduce_into<16>(v, row, lane);
+            } else {
+              float v[32];
+  #pragma unroll
+              for (int j = 0; j < 32; j++) v[j] = 0.f;
+              CubicFwd cf;
+              const float sdf = cubic_eval(rec, c.x, cf);
+              const float kk = rec[R_KFIX] * c.rinv;
+              const float m = -sdf * kk;
+              const float a = mode == STEP_HARD ? (sdf <= 0.f ? 1.f : 0.f) : soft_alpha(mode, m);
+              const float dm = compose_step(rec, a, m, mode, s, v, compat);
+              const float dsdf = -kk * dm;
+              v[G_K] += m * dm;
+              V3 g = cubic_adjoint(rec, c.x, cf, dsdf, v + G_CTRL, compat);
+              if (compat) g = g * dsdf;  // the reference multiplies by dL/dSDF again
+              gx += g;
+              reduce_into<32>(v, row, lane);
+            }
+          }
+        }
+        if (c.active) {
+          if (sc.last_pass) {
+            if (L.grad_x) {
+              L.grad_x[3 * c.si] = gx.x;
+              L.grad_x[3 * c.si + 1] = gx.y;
+              L.grad_x[3 * c.si + 2] = gx.z;
+            }
+          } else {
+            float* b = L.bstate + 8 * c.si;
+            b[0] = s.T; b[1] = s.Ps; b[2] = s.Pr; b[3] = s.Pg; b[4] = s.Pb;
+            b[5] = gx.x; b[6] = gx.y; b[7] = gx.z;
+          }
         }
       }
+      if (lane == 0) item = atomicAdd(L.tile_counter, 1);
+      item = __shfl_sync(0xffffffffu, item, 0);
     }
-    __syncthreads();
+    if (lane == 0) s_hold[warp] = item;
   }
+  __syncthreads();
   if (staged >= 0) flush(staged);
 }
 

@@ -15,7 +15,7 @@ struct SceneDesc {
   int n_rays;
   int stroke_begin;      // first stroke (global)
   int n_strokes;
-  int tile_begin;        // first tile of this scene in the current launch
+  int tile_begin;        // first work item (ray) of this scene in the current launch
   int chunk_lo;          // stroke range of the current pass, scene-local
   int chunk_n;
   int first_pass;        // 1: composite state starts fresh
@@ -37,8 +37,8 @@ struct SegLaunch {
   float* gslots;           // [S*32] reduced per-stroke gradient slots
   int compat;              // reference gradient formulas
   int n_scenes;
-  int tiles_total;
-  int segs_per_tile;
+  int tiles_total;         // work items (rays) in the launch
+  int segs_per_tile;       // unused (kept for layout stability)
   int chunk_cap;           // strokes per shared-memory stage
   int* tile_counter;
   int* status;

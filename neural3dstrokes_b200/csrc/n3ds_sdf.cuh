@@ -125,13 +125,26 @@ __device__ __forceinline__ float s3_factor(int base, V3 p, V3 s) {
 struct QuadFwd {
   float t, t_raw, dist;
   V3 d, e;
-  float kx, ky, p, q, h;
-  // h >= 0 branch
-  float H, x0, x1, u0, u1;
+  float kx, ky, p, q;
+  float sr, pt;  // refined depressed-cubic root s = t_raw + kx and the regularised p
   // h < 0 branch
-  float z, den, arg, v, m, n, sigma;  // sigma = +1 for the (m+n) root, -1 for -(m+n)
+  float z, den, arg, v, m, n, sigma;  // sigma = +1 for the (m+n) candidate, -1 for -(m+n)
   int pos_branch;
 };
+
+// Two Newton steps on the regularised depressed cubic s^3 + 3 pt s + q = 0 whose
+// exact root the closed form represents (see quad_adjoint). The single-precision
+// Cardano / trigonometric evaluation loses up to ~1e-3 in t to cancellation; the
+// refinement restores the root to float32 accuracy.
+__device__ __forceinline__ float quad_newton(float s, float pt, float q) {
+#pragma unroll
+  for (int it = 0; it < 2; it++) {
+    const float g = (s * s + 3.f * pt) * s + q;
+    const float gd = 3.f * (s * s + pt);
+    if (fabsf(gd) > 1e-12f) s -= g / gd;
+  }
+  return s;
+}
 
 __device__ __forceinline__ float quad_eval(const float* rec, V3 pos, QuadFwd& s) {
   V3 A = ld3(rec + R_QA), a = ld3(rec + R_Qa), b = ld3(rec + R_Qb), c = ld3(rec + R_Qc);
@@ -143,16 +156,19 @@ __device__ __forceinline__ float quad_eval(const float* rec, V3 pos, QuadFwd& s)
   float p3 = p * p * p;
   float q = kx * (2.0f * kx * kx - 3.0f * ky) + kz;
   float h = q * q + 4.0f * p3;
-  s.d = d; s.kx = kx; s.ky = ky; s.p = p; s.q = q; s.h = h;
+  s.d = d; s.kx = kx; s.ky = ky; s.p = p; s.q = q;
+  const float pt = cbrtf(p3 + 2.5e-9f);
+  s.pt = pt;
   float t, t_raw;
   if (h >= 0.0f) {
     s.pos_branch = 1;
     float H = sqrtf(h + 1e-8f);
     float x0 = (H - q) * 0.5f, x1 = -(H + q) * 0.5f;
     float u0 = copysignf(cbrtf(fabsf(x0)), x0), u1 = copysignf(cbrtf(fabsf(x1)), x1);
-    t_raw = (u0 + u1) - kx;
+    const float sr = quad_newton(u0 + u1, pt, q);
+    s.sr = sr;
+    t_raw = sr - kx;
     t = clampf(t_raw, 0.f, 1.f);
-    s.H = H; s.x0 = x0; s.x1 = x1; s.u0 = u0; s.u1 = u1;
   } else {
     s.pos_branch = 0;
     float z = sqrtf(-p + 1e-8f);
@@ -162,13 +178,17 @@ __device__ __forceinline__ float quad_eval(const float* rec, V3 pos, QuadFwd& s)
     float sv, cv;
     sincosf(v, &sv, &cv);
     float m = cv, n = sv * BEZ_SQRT3;
-    float ra = (m + n) * z - kx, rb = (-n - m) * z - kx;
+    // (m + n) z is the reference's first candidate (not a root, kept as computed);
+    // (-n - m) z is a true root and is refined
+    const float sb = quad_newton((-n - m) * z, pt, q);
+    float ra = (m + n) * z - kx, rb = sb - kx;
     float ta = clampf(ra, 0.f, 1.f), tb = clampf(rb, 0.f, 1.f);
     V3 ea = d + (c + b * ta) * ta, eb = d + (c + b * tb) * tb;
     float da = dot(ea, ea), db = dot(eb, eb);
     bool use_b = db < da;
     t = use_b ? tb : ta;
     t_raw = use_b ? rb : ra;
+    s.sr = sb;
     s.z = z; s.den = den; s.arg = arg; s.v = v; s.m = m; s.n = n; s.sigma = use_b ? -1.f : 1.f;
   }
   V3 e = d + (c + b * t) * t;
@@ -193,20 +213,52 @@ __device__ __forceinline__ V3 quad_adjoint(const float* rec, const QuadFwd& s, f
   g[9] += -w * (1.f - t);
   g[10] += -w * t;
   float gtr = (s.t_raw > 0.f && s.t_raw < 1.f) ? gt : 0.f;
-  // t_raw is a root of G(t) = t^3 + 3 kx t^2 + 3 ky t + kz (the stationarity condition
-  // of |B(t) - pos|^2 divided by 2 |b|^2). Its derivative follows from the implicit
-  // function theorem, dt = -(3t^2 dkx + 3t dky + dkz) / G'(t): well conditioned for a
-  // simple root, unlike differentiating the cube roots of the closed form, whose
-  // 1/(3 u^2) factors blow up when one Cardano term approaches zero.
+  // One-real-root branch: t_raw + kx is a root of a depressed cubic (the stationarity
+  // condition of |B(t) - pos|^2 divided by 2 |b|^2), differentiated by the implicit
+  // function theorem. That stays well conditioned for a simple root, unlike
+  // differentiating the cube roots of the closed form, whose 1/(3 u^2) factors blow up
+  // when one Cardano term approaches zero.
+  //
+  // The three-real-root branch is differentiated through its trigonometric formula
+  // instead: the reference's first candidate there is (m + n) z - kx
+  // (strokes_sdf.h:687), which is not a root of G (the trigonometric root is 2 m z - kx),
+  // so the implicit derivative does not apply when that candidate is the closest.
+  //
+  // With the reference's regulariser H = sqrt(h + 1e-8), the computed s = u0 + u1 is
+  // exactly a root of the depressed cubic s^3 + 3 pt s + q = 0 with
+  // pt^3 = p^3 + 2.5e-9 (Cardano: u0^3 + u1^3 = -q, u0 u1 = -pt), so differentiating
+  // that cubic gives the exact derivative of the regularised closed form:
+  //   ds = -(3 s dpt + dq) / (3 (s^2 + pt)),  dpt/dp = p^2 / pt^2.
   float gkx = 0.f, gky = 0.f, gkz = 0.f;
-  if (gtr != 0.f) {
-    const float tr = s.t_raw;
-    float Gp = 3.f * tr * tr + 6.f * s.kx * tr + 3.f * s.ky;
-    if (fabsf(Gp) < 1e-20f) Gp = copysignf(1e-20f, Gp);
-    const float f = -gtr / Gp;
-    gkx = f * 3.f * tr * tr;
-    gky = f * 3.f * tr;
-    gkz = f;
+  if (gtr != 0.f && (s.pos_branch || s.sigma < 0.f)) {
+    // a (refined) true root: one-real-root branch, or the trig branch's -(m+n) root
+    const float sr = s.sr;
+    const float pt = s.pt;
+    float den = 3.f * (sr * sr + pt);
+    if (fabsf(den) < 1e-30f) den = copysignf(1e-30f, den);
+    const float gq = -gtr / den;
+    const float gp = -3.f * sr * (s.p * s.p) / (pt * pt) * gtr / den;
+    gkx = -gtr - 2.f * s.kx * gp + gq * (6.f * s.kx * s.kx - 3.f * s.ky);
+    gky = gp - 3.f * s.kx * gq;
+    gkz = gq;
+  } else if (gtr != 0.f) {
+    // t_raw = sigma (m + n) z - kx, m = cos v, n = sqrt3 sin v, v = acos(q / (2 p z + 1e-8)) / 3,
+    // z = sqrt(-p + 1e-8); p = ky - kx^2, q = kx (2 kx^2 - 3 ky) + kz
+    float gz = gtr * s.sigma * (s.m + s.n);
+    const float gm = gtr * s.sigma * s.z;
+    const float gn = gm;
+    float sv, cv;
+    sincosf(s.v, &sv, &cv);
+    const float gv = -sv * gm + BEZ_SQRT3 * cv * gn;
+    const float garg = -(gv / 3.f) * rsqrtf(fmaxf(1.f - s.arg * s.arg, 1e-30f));
+    const float gq = garg / s.den;
+    const float gden = -garg * s.arg / s.den;
+    float gp = 2.f * s.z * gden;
+    gz += 2.f * s.p * gden;
+    gp += gz * (-0.5f / s.z);
+    gkx = -gtr - 2.f * s.kx * gp + gq * (6.f * s.kx * s.kx - 3.f * s.ky);
+    gky = gp - 3.f * s.kx * gq;
+    gkz = gq;
   }
   // ky = kk (aa2 + d.b) / 3 ; kz = kk (d.a)
   float db = dot(s.d, b), da = dot(s.d, a);

@@ -195,11 +195,19 @@ def test_forward_matches_reference_op(cuda, kind):
     if ref is None:
         pytest.skip("reference extension not built (oracle/_ref)")
     sid, ps, col, x, r, vd, _ = group(kind, n_points=2000, seed=8)
+    tol = 1e-4 if "bezier" in kind else FWD_TOL
     for lap, inv in [(True, True), (False, False)]:
         a, c, sdf = run_forward(sl, sid, ps, col, x, r, vd, 0.02, lap, inv, cuda)
         a_r, c_r, sdf_r = run_forward(ref, sid, ps, col, x, r, vd, 0.02, lap, inv, cuda)
-        assert rel(a, a_r) < FWD_TOL and rel(c, c_r) == 0.0
-        assert rel(sdf, sdf_r) < (1e-4 if "bezier" in kind else FWD_TOL)
+        a64, _, sdf64 = sf.stroke_forward(x.double(), r.double(), ps.double(), col.double(), sid, 0.02, lap, inv,
+                                          return_sdf=True)
+        assert rel(c, c_r) == 0.0
+        # within tolerance of float64, and never further from the reference op than the
+        # reference op itself is from float64 (its single-precision closed-form Bezier
+        # solve loses up to ~1e-3 in t; this implementation refines the root)
+        assert rel(a, a64) < FWD_TOL and rel(sdf, sdf64) < tol
+        assert rel(a, a_r) <= rel(a_r, a64) + FWD_TOL
+        assert rel(sdf, sdf_r) <= rel(sdf_r, sdf64) + tol
 
 
 @pytest.mark.parametrize("kind", ["sphere", "ellipsoid", "cube", "roundcube", "capsule", "octahedron",
