@@ -79,7 +79,7 @@ int n3ds_stroke_backward(float* grad_shape_params, float* grad_color_params, flo
                          int inv_scale_radius, int grad_mode, void* workspace,
                          size_t workspace_bytes, n3ds_stream_t stream);
 
-/* Replaces compose_forward (compositing.cu:159-204; declared compositing.h:10-14).
+/* Replaces compose_forward (compositing.cu:159-204; declared compositing.h:11-15).
  * density_out [P], color_out [P,C], alphas [P,S], colors [P,S,C], density_params [S];
  * C in {1, 3}. */
 int n3ds_compose_forward(float* density_out, float* color_out, const float* alphas,
@@ -90,7 +90,7 @@ int n3ds_compose_forward(float* density_out, float* color_out, const float* alph
  * transmittance in front of every stroke), 0 in compat mode. */
 size_t n3ds_compose_workspace_bytes(int64_t n_points, int64_t n_strokes, int grad_mode);
 
-/* Replaces compose_backward (compositing.cu:206-262; declared compositing.h:24-31).
+/* Replaces compose_backward (compositing.cu:206-263; declared compositing.h:25-32).
  * Accumulates into grad_alphas [P,S], grad_colors [P,S,C], grad_density_params [S].
  * grad_density_out [P] and grad_color_out [P,C] may be NULL (treated as zero).
  * Exact mode is division-free (a top-down and a bottom-up sweep) and needs

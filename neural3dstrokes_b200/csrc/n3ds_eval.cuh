@@ -15,22 +15,28 @@ __device__ __forceinline__ float soft_alpha(int mode, float m) {
   return 0.f;  // STEP_HARD handled by the caller from the sign of the SDF
 }
 
+// Local-frame sample p = M (x - t) (three 128-bit loads). The translation is
+// subtracted first: folding it into an offset c = -M t cancels catastrophically for
+// small strokes far from the origin.
 __device__ __forceinline__ V3 prim_local(const float* rec, V3 x) {
-  V3 u = x - ld3(rec + R_T);
-  return {dot(ld3(rec + R_M), u), dot(ld3(rec + R_M + 3), u), dot(ld3(rec + R_M + 6), u)};
+  const float4 m0 = rec4(rec)[R_M / 4], m1 = rec4(rec)[R_M / 4 + 1], m2 = rec4(rec)[R_M / 4 + 2];
+  const V3 d = {x.x - m0.w, x.y - m1.w, x.z - m2.w};
+  return {fmaf(m0.x, d.x, fmaf(m0.y, d.y, m0.z * d.z)), fmaf(m1.x, d.x, fmaf(m1.y, d.y, m1.z * d.z)),
+          fmaf(m2.x, d.x, fmaf(m2.y, d.y, m2.z * d.z))};
 }
 
 // Forward alpha of one stroke record at world sample x; rinv = 1 / sample radius.
 // Optionally returns the SDF value.
 __device__ __forceinline__ float pair_alpha(const float* rec, V3 x, float rinv, float* sdf_out = nullptr) {
-  int kind = __float_as_int(rec[R_KIND]);
-  int base = kind & 15;
-  int mode = (kind >> 8) & 3;
+  const float4 h = rec4(rec)[0];
+  const int kind = __float_as_int(h.x);
+  const int base = kind & 15;
+  const int mode = (kind >> 8) & 3;
   float sdf, f = 1.f;
   if (base <= B_TETRAHEDRON) {
     V3 p = prim_local(rec, x);
     sdf = prim_sdf(base, p, rec[R_BP]);
-    if (kind & K_S3FAC) f = s3_factor(base, p, ld3(rec + R_S));
+    if (kind & K_S3FAC) f = s3_factor(base, p, xyz(rec4(rec)[R_S / 4]));
   } else if (base == B_QUAD_BEZIER) {
     QuadFwd q;
     sdf = quad_eval(rec, x, q);
@@ -40,7 +46,7 @@ __device__ __forceinline__ float pair_alpha(const float* rec, V3 x, float rinv, 
   }
   if (sdf_out) *sdf_out = sdf;
   if (mode == STEP_HARD) return sdf <= 0.f ? 1.f : 0.f;
-  float k = rec[R_KFIX] * f * rinv;
+  float k = h.y * f * rinv;
   return soft_alpha(mode, -sdf * k);
 }
 
@@ -76,7 +82,7 @@ __device__ __forceinline__ V3 prim_backprop(const float* rec, int kind, V3 p, fl
   float gbpu;
   V3 gp = prim_grad(base, p, rec[R_BP], &gbpu, compat) * dsdf;
   v[G_BP] += gbpu * dsdf;
-  V3 s = ld3(rec + R_S), si = ld3(rec + R_SINV);
+  V3 s = xyz(rec4(rec)[R_S / 4]), si = xyz(rec4(rec)[R_SINV / 4]);
   V3 q = s * p;
   float kfac = compat ? 0.f : K;
   if ((kind & K_S3FAC) && !compat && base == B_SPHERE) {
@@ -105,7 +111,7 @@ __device__ __forceinline__ V3 prim_backprop(const float* rec, int kind, V3 p, fl
   v[G_GP + 1] += gp.y;
   v[G_GP + 2] += gp.z;
   // dL/dx = M^T gp
-  return ld3(rec + R_M) * gp.x + ld3(rec + R_M + 3) * gp.y + ld3(rec + R_M + 6) * gp.z;
+  return xyz(rec4(rec)[R_M / 4]) * gp.x + xyz(rec4(rec)[R_M / 4 + 1]) * gp.y + xyz(rec4(rec)[R_M / 4 + 2]) * gp.z;
 }
 
 // Warp transpose-reduction of NV per-lane values: after it, lane l holds the warp

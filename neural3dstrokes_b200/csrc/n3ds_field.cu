@@ -247,11 +247,12 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_con
             if (lane == 0) atomicAdd(&s_kcount[__float_as_int(rec[R_KIND]) & 15], (unsigned long long)nact);
             const float a = pair_alpha(rec, c.x, c.rinv);
             const float w = a * T;
+            const float4 col = rec4(rec)[R_COLOR / 4];
             T *= (1.0f - a);
             sig += rec[R_DENSITY] * w;
-            cr += rec[R_COLOR] * w;
-            cg += rec[R_COLOR + 1] * w;
-            cb += rec[R_COLOR + 2] * w;
+            cr += col.x * w;
+            cg += col.y * w;
+            cb += col.z * w;
           }
         }
         if (c.active) {
@@ -295,7 +296,8 @@ struct CompAdj {
 __device__ __forceinline__ float compose_step(const float* rec, float a, float m, int mode, CompAdj& s,
                                               float* v, int compat) {
   const float d = rec[R_DENSITY];
-  const float c0 = rec[R_COLOR], c1 = rec[R_COLOR + 1], c2 = rec[R_COLOR + 2];
+  const float4 col = rec4(rec)[R_COLOR / 4];
+  const float c0 = col.x, c1 = col.y, c2 = col.z;
   const float w = a * s.T;
   const float T1 = s.T * (1.0f - a);
   s.Ps += d * w;
@@ -412,7 +414,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
             const int sl = hi - b;
             const float* rec = S.recs + size_t(sl) * REC_FLOATS;
             float* row = S.gacc + size_t(sl) * GRAD_SLOTS;
-            const int kind = __float_as_int(rec[R_KIND]);
+            const float4 h = rec4(rec)[0];
+            const int kind = __float_as_int(h.x);
             const int base = kind & 15;
             const int mode = (kind >> 8) & 3;
             if (base <= B_TETRAHEDRON) {
@@ -421,8 +424,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
               for (int j = 0; j < 16; j++) v[j] = 0.f;
               const V3 p = prim_local(rec, c.x);
               const float sdf = prim_sdf(base, p, rec[R_BP]);
-              const float f = (kind & K_S3FAC) ? s3_factor(base, p, ld3(rec + R_S)) : 1.f;
-              const float kk = rec[R_KFIX] * f * c.rinv;
+              const float f = (kind & K_S3FAC) ? s3_factor(base, p, xyz(rec4(rec)[R_S / 4])) : 1.f;
+              const float kk = h.y * f * c.rinv;
               const float m = -sdf * kk;
               const float a = mode == STEP_HARD ? (sdf <= 0.f ? 1.f : 0.f) : soft_alpha(mode, m);
               const float dm = compose_step(rec, a, m, mode, s, v, compat);
@@ -436,7 +439,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
               for (int j = 0; j < 16; j++) v[j] = 0.f;
               QuadFwd qf;
               const float sdf = quad_eval(rec, c.x, qf);
-              const float kk = rec[R_KFIX] * c.rinv;
+              const float kk = h.y * c.rinv;
               const float m = -sdf * kk;
               const float a = mode == STEP_HARD ? (sdf <= 0.f ? 1.f : 0.f) : soft_alpha(mode, m);
               const float dm = compose_step(rec, a, m, mode, s, v, compat);
@@ -449,7 +452,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
               for (int j = 0; j < 32; j++) v[j] = 0.f;
               CubicFwd cf;
               const float sdf = cubic_eval(rec, c.x, cf);
-              const float kk = rec[R_KFIX] * c.rinv;
+              const float kk = h.y * c.rinv;
               const float m = -sdf * kk;
               const float a = mode == STEP_HARD ? (sdf <= 0.f ? 1.f : 0.f) : soft_alpha(mode, m);
               const float dm = compose_step(rec, a, m, mode, s, v, compat);
@@ -681,9 +684,9 @@ __global__ void prep_kernel(const PrepLaunch P) {
     // sample that meets it NaN (the culling sphere is infinite) so that the error
     // cannot pass silently.
     atomicOr(P.status, ST_BAD_KIND);
+    for (int j = 0; j < REC_FLOATS; j++) rec[j] = 0.f;
     rec[R_KIND] = __int_as_float(B_CAPPED_TORUS | (STEP_LAPLACE << 8));
     rec[R_KFIX] = __int_as_float(0x7fc00000);
-    for (int j = R_COLOR; j < R_CULL_R; j++) rec[j] = 0.f;
     P.cull_a[4 * s] = 0.f; P.cull_a[4 * s + 1] = 0.f; P.cull_a[4 * s + 2] = 0.f;
     P.cull_a[4 * s + 3] = __int_as_float(0x7f800000);
     P.cull_b[s] = 0.f;
@@ -705,6 +708,7 @@ __global__ void prep_kernel(const PrepLaunch P) {
   const bool s3f = s3 && P.inv_scale_radius;
   if (s1k) kind |= K_S1K;
   if (s3f) kind |= K_S3FAC;
+  for (int j = 0; j < REC_FLOATS; j++) rec[j] = 0.f;
   rec[R_KIND] = __int_as_float(kind);
   const float* col = P.color_params + s * (long long)P.color_stride;
   rec[R_COLOR] = col[0];
@@ -719,11 +723,15 @@ __global__ void prep_kernel(const PrepLaunch P) {
   V3 cw = t;
   float Rb;
   if (base <= B_TETRAHEDRON) {
-    // M = S^-1 R^T: row i is column i of R divided by s_i
-    rec[R_M + 0] = R.r0.x / sc.x; rec[R_M + 1] = R.r1.x / sc.x; rec[R_M + 2] = R.r2.x / sc.x;
-    rec[R_M + 3] = R.r0.y / sc.y; rec[R_M + 4] = R.r1.y / sc.y; rec[R_M + 5] = R.r2.y / sc.y;
-    rec[R_M + 6] = R.r0.z / sc.z; rec[R_M + 7] = R.r1.z / sc.z; rec[R_M + 8] = R.r2.z / sc.z;
-    rec[R_T] = t.x; rec[R_T + 1] = t.y; rec[R_T + 2] = t.z;
+    // M = S^-1 R^T: row i is column i of R divided by s_i; the row's w holds t_i
+    const V3 mr[3] = {v3(R.r0.x, R.r1.x, R.r2.x) * (1.f / sc.x), v3(R.r0.y, R.r1.y, R.r2.y) * (1.f / sc.y),
+                      v3(R.r0.z, R.r1.z, R.r2.z) * (1.f / sc.z)};
+    for (int i = 0; i < 3; i++) {
+      rec[R_M + 4 * i] = mr[i].x;
+      rec[R_M + 4 * i + 1] = mr[i].y;
+      rec[R_M + 4 * i + 2] = mr[i].z;
+    }
+    rec[R_M + 3] = t.x; rec[R_M + 7] = t.y; rec[R_M + 11] = t.z;
     rec[R_S] = sc.x; rec[R_S + 1] = sc.y; rec[R_S + 2] = sc.z;
     rec[R_SINV] = 1.f / sc.x; rec[R_SINV + 1] = 1.f / sc.y; rec[R_SINV + 2] = 1.f / sc.z;
     const float bp = base_param_count(base) > 0 ? prm[0] : 0.f;
@@ -744,7 +752,7 @@ __global__ void prep_kernel(const PrepLaunch P) {
     V3 b = (A - B * 2.0f) + C;
     V3 c = a * 2.0f;
     for (int j = 0; j < 3; j++) {
-      rec[R_QA + j] = (&A.x)[j]; rec[R_QB + j] = (&B.x)[j]; rec[R_QC + j] = (&C.x)[j];
+      rec[R_QA + j] = (&A.x)[j];
       rec[R_Qa + j] = (&a.x)[j]; rec[R_Qb + j] = (&b.x)[j]; rec[R_Qc + j] = (&c.x)[j];
     }
     rec[R_QR1] = prm[9];
@@ -762,7 +770,7 @@ __global__ void prep_kernel(const PrepLaunch P) {
     V3 P4[4];
     for (int k = 0; k < 4; k++) {
       P4[k] = v3(prm[3 * k], prm[3 * k + 1], prm[3 * k + 2]);
-      rec[R_CA + 3 * k] = P4[k].x; rec[R_CA + 3 * k + 1] = P4[k].y; rec[R_CA + 3 * k + 2] = P4[k].z;
+      rec[R_CA + 4 * k] = P4[k].x; rec[R_CA + 4 * k + 1] = P4[k].y; rec[R_CA + 4 * k + 2] = P4[k].z;
     }
     rec[R_CR1] = prm[12];
     rec[R_CR2] = prm[13];
@@ -801,12 +809,9 @@ __global__ void prep_kernel(const PrepLaunch P) {
     }
   }
   if (!cull) Rb = __int_as_float(0x7f800000);
-  rec[R_CULL_R] = Rb * 1.0001f + 1e-6f;
-  rec[R_CULL_C] = cw.x; rec[R_CULL_C + 1] = cw.y; rec[R_CULL_C + 2] = cw.z;
-  rec[R_CULL_M] = cm * 1.0001f;
   P.cull_a[4 * s] = cw.x; P.cull_a[4 * s + 1] = cw.y; P.cull_a[4 * s + 2] = cw.z;
-  P.cull_a[4 * s + 3] = rec[R_CULL_R];
-  P.cull_b[s] = rec[R_CULL_M];
+  P.cull_a[4 * s + 3] = Rb * 1.0001f + 1e-6f;
+  P.cull_b[s] = cm * 1.0001f;
 }
 
 __device__ void prim_param_grads(const FinalizeLaunch& F, long long s, int base, int flags, const float* g,
@@ -868,7 +873,7 @@ __device__ void prim_param_grads(const FinalizeLaunch& F, long long s, int base,
     // dL/dt = -M^T sum g_p
     const float gx = g[G_GP], gy = g[G_GP + 1], gz = g[G_GP + 2];
     for (int j = 0; j < 3; j++)
-      out[off + j] = -(rec[R_M + j] * gx + rec[R_M + 3 + j] * gy + rec[R_M + 6 + j] * gz);
+      out[off + j] = -(rec[R_M + j] * gx + rec[R_M + 4 + j] * gy + rec[R_M + 8 + j] * gz);
   }
 }
 

@@ -56,32 +56,36 @@ __host__ __device__ __forceinline__ int sdf_id_param_count(int sdf_id) {
   return n;
 }
 
-// ---- record field offsets
+// ---- record field offsets (floats). Hot fields sit in 16-byte groups so the inner
+// loops read them with 128-bit shared-memory loads (rec4(rec)[k]).
+// q0: kind word, soft-step slope, density, softness
 constexpr int R_KIND = 0;      // int bits
-constexpr int R_COLOR = 1;     // 3
-constexpr int R_DENSITY = 4;
-constexpr int R_KFIX = 5;      // kappa/delta (times s for single-scale with inv_scale_radius)
-constexpr int R_DELTA = 6;
-constexpr int R_CULL_R = 7;    // culling sphere radius (world)
-constexpr int R_CULL_C = 8;    // 3, culling sphere centre (world)
-constexpr int R_CULL_M = 11;   // culling margin per unit sample radius
+constexpr int R_KFIX = 1;      // kappa/delta (times s for single-scale with inv_scale_radius)
+constexpr int R_DENSITY = 2;
+constexpr int R_DELTA = 3;
+// q1: colour, base parameter (round-cube radius / capsule half-length)
+constexpr int R_COLOR = 4;     // 3
+constexpr int R_BP = 7;
 // primitives
-constexpr int R_M = 12;        // 9, rows of M = S^-1 R^T
-constexpr int R_T = 21;        // 3, translation
-constexpr int R_S = 24;        // 3, scale per axis
-constexpr int R_SINV = 27;     // 3, 1/scale per axis
-constexpr int R_BP = 30;       // base parameter (round-cube radius / capsule half-length)
+constexpr int R_M = 8;         // q2..q4: rows (m_i0, m_i1, m_i2, t_i), p = M (x - t),
+                               // M = S^-1 R^T (t is subtracted first: M x - M t cancels)
+constexpr int R_S = 20;        // q5: scale per axis
+constexpr int R_SINV = 24;     // q6: 1/scale per axis
 // quadratic Bezier
-constexpr int R_QA = 12, R_QB = 15, R_QC = 18;     // control points
-constexpr int R_Qa = 21, R_Qb = 24, R_Qc = 27;     // a = B-A, b = A-2B+C, c = 2a
-constexpr int R_QR1 = 30, R_QR2 = 31;
-constexpr int R_QKK = 32, R_QKX = 33, R_QAA2 = 34; // 1/|b|^2, kk*(a.b), 2|a|^2
-constexpr int R_QAB = 35;                          // a.b
+constexpr int R_QA = 8, R_QKK = 11;    // q2: A, 1/|b|^2
+constexpr int R_Qa = 12, R_QKX = 15;   // q3: a = B - A, kk (a.b)
+constexpr int R_Qb = 16, R_QAA2 = 19;  // q4: b = A - 2B + C, 2 |a|^2
+constexpr int R_Qc = 20, R_QAB = 23;   // q5: c = 2a, a.b
+constexpr int R_QR1 = 24, R_QR2 = 25;  // q6: radii
 // cubic Bezier
-constexpr int R_CA = 12, R_CB = 15, R_CC = 18, R_CD = 21;
-constexpr int R_CR1 = 24, R_CR2 = 25;
-constexpr int R_CV = 26;       // 11 polyline vertices, 33 floats (26..58)
+constexpr int R_CA = 8, R_CR1 = 11;    // q2: A, r1
+constexpr int R_CB = 12, R_CR2 = 15;   // q3: B, r2
+constexpr int R_CC = 16, R_CD = 20;    // q4, q5: C, D
+constexpr int R_CV = 24;       // 11 polyline vertices, 33 floats (24..56), read as 9 float4
 constexpr int CUBIC_SEGMENTS = 10;
+
+__device__ __forceinline__ const float4* rec4(const float* rec) { return reinterpret_cast<const float4*>(rec); }
+__device__ __forceinline__ V3 xyz(float4 v) { return {v.x, v.y, v.z}; }
 
 // ---- per-stroke reduced-gradient slots (GRAD_SLOTS floats per stroke)
 constexpr int GRAD_SLOTS = 32;

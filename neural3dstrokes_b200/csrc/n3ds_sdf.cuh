@@ -147,10 +147,12 @@ __device__ __forceinline__ float quad_newton(float s, float pt, float q) {
 }
 
 __device__ __forceinline__ float quad_eval(const float* rec, V3 pos, QuadFwd& s) {
-  V3 A = ld3(rec + R_QA), a = ld3(rec + R_Qa), b = ld3(rec + R_Qb), c = ld3(rec + R_Qc);
-  float kk = rec[R_QKK], kx = rec[R_QKX];
+  const float4 qA = rec4(rec)[R_QA / 4], qa = rec4(rec)[R_Qa / 4], qb = rec4(rec)[R_Qb / 4],
+               qc = rec4(rec)[R_Qc / 4];
+  V3 A = xyz(qA), a = xyz(qa), b = xyz(qb), c = xyz(qc);
+  float kk = qA.w, kx = qa.w;
   V3 d = A - pos;
-  float ky = kk * (rec[R_QAA2] + dot(d, b)) / 3.0f;
+  float ky = kk * (qb.w + dot(d, b)) / 3.0f;
   float kz = kk * dot(d, a);
   float p = ky - kx * kx;
   float p3 = p * p * p;
@@ -201,8 +203,10 @@ __device__ __forceinline__ float quad_eval(const float* rec, V3 pos, QuadFwd& s)
 // Reverse mode of quad_eval for upstream w = dL/dSDF.
 // Returns dL/dpos; g[0..8] += dL/d(A,B,C), g[9], g[10] += dL/d(r1, r2).
 __device__ __forceinline__ V3 quad_adjoint(const float* rec, const QuadFwd& s, float w, float* g) {
-  V3 a = ld3(rec + R_Qa), b = ld3(rec + R_Qb), c = ld3(rec + R_Qc);
-  float kk = rec[R_QKK];
+  const float4 qA = rec4(rec)[R_QA / 4], qa = rec4(rec)[R_Qa / 4], qb = rec4(rec)[R_Qb / 4],
+               qc = rec4(rec)[R_Qc / 4];
+  V3 a = xyz(qa), b = xyz(qb), c = xyz(qc);
+  float kk = qA.w;
   float r1 = rec[R_QR1], r2 = rec[R_QR2];
   float t = s.t;
   V3 ge = s.e * (w / s.dist);           // dL/de
@@ -262,7 +266,7 @@ __device__ __forceinline__ V3 quad_adjoint(const float* rec, const QuadFwd& s, f
   }
   // ky = kk (aa2 + d.b) / 3 ; kz = kk (d.a)
   float db = dot(s.d, b), da = dot(s.d, a);
-  float gkk = gky * (rec[R_QAA2] + db) / 3.f + gkz * da;
+  float gkk = gky * (qb.w + db) / 3.f + gkz * da;
   float gaa2 = gky * kk / 3.f;
   float gdb = gky * kk / 3.f;
   float gda = gkz * kk;
@@ -270,7 +274,7 @@ __device__ __forceinline__ V3 quad_adjoint(const float* rec, const QuadFwd& s, f
   gb += s.d * gdb;
   V3 ga = s.d * gda;
   // stroke constants: kx = kk (a.b), kk = 1/(b.b), aa2 = 2 a.a, c = 2 a
-  gkk += gkx * rec[R_QAB];
+  gkk += gkx * qc.w;
   ga += b * (gkx * kk);
   gb += a * (gkx * kk);
   gb += b * (-2.f * kk * kk * gkk);
@@ -307,11 +311,17 @@ __device__ __forceinline__ float cubic_eval(const float* rec, V3 pos, CubicFwd& 
   float best = 1e18f, t_min = 0.f, tau_best = 0.f, tau_raw_best = 0.f;
   int seg = 0;
   float t_start = 0.f;
-  V3 s0 = ld3(rec + R_CV);
+  float vtx[36];
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    const float4 q = rec4(rec)[R_CV / 4 + k];
+    vtx[4 * k] = q.x; vtx[4 * k + 1] = q.y; vtx[4 * k + 2] = q.z; vtx[4 * k + 3] = q.w;
+  }
+  V3 s0 = v3(vtx[0], vtx[1], vtx[2]);
 #pragma unroll
   for (int i = 1; i <= CUBIC_SEGMENTS; i++) {
     float t_end = i * step;
-    V3 s1 = ld3(rec + R_CV + 3 * i);
+    V3 s1 = v3(vtx[3 * i], vtx[3 * i + 1], vtx[3 * i + 2]);
     V3 ab = s1 - s0;
     float tr = dot(pos - s0, ab) / dot(ab, ab);
     float tt = clampf(tr, 0.f, 1.f);
@@ -329,11 +339,13 @@ __device__ __forceinline__ float cubic_eval(const float* rec, V3 pos, CubicFwd& 
   }
   float w[4];
   cubic_weights(t_min, w);
-  V3 P = ld3(rec + R_CA) * w[0] + ld3(rec + R_CB) * w[1] + ld3(rec + R_CC) * w[2] + ld3(rec + R_CD) * w[3];
+  const float4 cA = rec4(rec)[R_CA / 4], cB = rec4(rec)[R_CB / 4], cC = rec4(rec)[R_CC / 4],
+               cD = rec4(rec)[R_CD / 4];
+  V3 P = xyz(cA) * w[0] + xyz(cB) * w[1] + xyz(cC) * w[2] + xyz(cD) * w[3];
   V3 v = P - pos;
   float dist = sqrtf(dot(v, v));
   s.t = t_min; s.tau = tau_best; s.tau_raw = tau_raw_best; s.seg = seg; s.v = v; s.dist = dist;
-  float r1 = rec[R_CR1], r2 = rec[R_CR2];
+  float r1 = cA.w, r2 = cB.w;
   return dist - (r1 + t_min * (r2 - r1));
 }
 
@@ -345,7 +357,9 @@ __device__ __forceinline__ float cubic_eval(const float* rec, V3 pos, CubicFwd& 
 __device__ __forceinline__ V3 cubic_adjoint(const float* rec, V3 pos, const CubicFwd& s, float w,
                                             float* g, int compat) {
   constexpr float step = 1.0f / CUBIC_SEGMENTS;
-  float r1 = rec[R_CR1], r2 = rec[R_CR2];
+  const float4 cA = rec4(rec)[R_CA / 4], cB = rec4(rec)[R_CB / 4], cC = rec4(rec)[R_CC / 4],
+               cD = rec4(rec)[R_CD / 4];
+  float r1 = cA.w, r2 = cB.w;
   float t = s.t;
   float bw[4];
   cubic_weights(t, bw);
@@ -361,7 +375,7 @@ __device__ __forceinline__ V3 cubic_adjoint(const float* rec, V3 pos, const Cubi
     }
     return -gv;
   }
-  V3 A = ld3(rec + R_CA), B = ld3(rec + R_CB), C = ld3(rec + R_CC), D = ld3(rec + R_CD);
+  V3 A = xyz(cA), B = xyz(cB), C = xyz(cC), D = xyz(cD);
   V3 gv = s.v * (w / s.dist);
   float u = 1.f - t;
   V3 dB = (B - A) * (3.f * u * u) + (C - B) * (6.f * u * t) + (D - C) * (3.f * t * t);

@@ -22,7 +22,7 @@ namespace n3ds {
 constexpr int UF_WARPS = 4;
 
 __global__ void __launch_bounds__(UF_WARPS * 32) uf_stroke_fwd_kernel(const UfStroke L) {
-  __shared__ float recs[32 * REC_FLOATS];
+  __shared__ __align__(16) float recs[32 * REC_FLOATS];
   __shared__ float ta[UF_WARPS][32][33];
   __shared__ float tsd[UF_WARPS][32][33];
   const int s0 = blockIdx.y * 32;
@@ -58,8 +58,10 @@ __global__ void __launch_bounds__(UF_WARPS * 32) uf_stroke_fwd_kernel(const UfSt
 
 template <int NV>
 __global__ void __launch_bounds__(UF_WARPS * 32) uf_stroke_bwd_kernel(const UfStroke L) {
-  constexpr int RS = REC_FLOATS + 1;  // padded stride: lane-indexed record reads hit distinct banks
-  __shared__ float recs[32 * RS];
+  // padded stride (17 float4): rows stay 16-byte aligned and lane-indexed 128-bit
+  // record loads of a quarter warp hit distinct banks
+  constexpr int RS = REC_FLOATS + 4;
+  __shared__ __align__(16) float recs[32 * RS];
   const int s0 = blockIdx.y * 32;
   const int ns = min(32, L.n_strokes - s0);
   for (int i = threadIdx.x; i < ns * REC_FLOATS; i += blockDim.x)
@@ -94,7 +96,7 @@ __global__ void __launch_bounds__(UF_WARPS * 32) uf_stroke_bwd_kernel(const UfSt
     if (base <= B_TETRAHEDRON) {
       pl = prim_local(rec, x);
       sdf = prim_sdf(base, pl, rec[R_BP]);
-      if (kind & K_S3FAC) f = s3_factor(base, pl, ld3(rec + R_S));
+      if (kind & K_S3FAC) f = s3_factor(base, pl, xyz(rec4(rec)[R_S / 4]));
     } else if (base == B_QUAD_BEZIER) {
       sdf = quad_eval(rec, x, qf);
     } else {
