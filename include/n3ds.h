@@ -101,6 +101,28 @@ int n3ds_compose_backward(float* grad_alphas, float* grad_colors, float* grad_de
                           int64_t n_points, int64_t n_strokes, int64_t color_dim, int grad_mode,
                           void* workspace, size_t workspace_bytes, n3ds_stream_t stream);
 
+/* Maximum n_strokes of n3ds_stroke_forward_static. */
+#define N3DS_STATIC_MAX_STROKES 4096
+
+/* n3ds_stroke_forward without a workspace argument (no counterpart in the reference):
+ * for callers that hold no device allocator of their own (a C or FFI host that only
+ * passes through tensors it was given) or must not allocate once running (cudaMalloc
+ * synchronises the device and can fail under a fixed memory budget). Its scratch, the
+ * prepared records of up to N3DS_STATIC_MAX_STROKES strokes (1.7 MB), is one
+ * file-scope device array per device; more strokes return N3DS_ERR_INVALID. Nothing
+ * in the scratch has to start at zero. Two calls in flight on the same device at once
+ * race on that scratch; calls on one stream are ordered. The first call on a device
+ * (with that device current) looks the array's address up with cudaGetSymbolAddress;
+ * a caller that records the call into a stream capture makes one call on that device
+ * before capturing. Same arguments, outputs and errors as n3ds_stroke_forward. */
+int n3ds_stroke_forward_static(float* alpha_out, float* color_out, float* sdf_out, int64_t n_texcoord,
+                               const float* x, const float* radius, const float* viewdir,
+                               const float* shape_params, const float* color_params, int64_t n_points,
+                               int64_t n_viewdirs, int64_t n_strokes, int64_t n_shape_params,
+                               int64_t n_color_params, uint32_t sdf_id, uint32_t color_id,
+                               float sdf_delta, int use_laplace_transform, int inv_scale_radius,
+                               n3ds_stream_t stream);
+
 /* ------------------------------------------------------------------------------
  * Layer 2: fused stroke field
  * (StrokeField.predict_density models.py:660-711 + compute_alpha_weights /

@@ -199,6 +199,11 @@ int run_seg_passes(bool backward, const n3ds_batch_t* b, const Resolved& rv, n3d
 
 }  // namespace
 
+namespace n3ds {
+// Error reporting for entry points defined in other translation units.
+int report_error(int code, const std::string& msg) { return fail(code, msg); }
+}  // namespace n3ds
+
 extern "C" {
 
 const char* n3ds_last_error(void) { return g_last_error.c_str(); }
