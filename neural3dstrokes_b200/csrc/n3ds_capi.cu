@@ -55,7 +55,10 @@ constexpr size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 struct WsLayout {
   size_t recs, cull_a, cull_b, state, seeds, bstate, gslots, counters, status, stats, total;
 };
-constexpr int N_COUNTERS = 128;
+// Ray counters: one block of MAX_SCENES_PER_LAUNCH per segment-kernel launch, the
+// first half for forward launches, the second for backward launches.
+constexpr int N_LAUNCH_SLOTS = 64;
+constexpr int N_COUNTERS = N_LAUNCH_SLOTS * n3ds::MAX_SCENES_PER_LAUNCH;
 
 WsLayout ws_layout(long long total_rays, int N, long long S) {
   WsLayout w{};
@@ -152,7 +155,7 @@ int run_seg_passes(bool backward, const n3ds_batch_t* b, const Resolved& rv, n3d
   }
   const DevInfo di = dev_info();
   const size_t smem = backward ? n3ds::seg_bwd_smem(cap) : n3ds::seg_fwd_smem(cap);
-  int counter = counter_base;
+  int counter = 0;
   for (int pass = 0; pass < passes; pass++) {
     std::vector<int> scenes;
     for (int i = 0; i < b->n_scenes; i++)
@@ -164,6 +167,8 @@ int run_seg_passes(bool backward, const n3ds_batch_t* b, const Resolved& rv, n3d
       L.segs_per_tile = rv.segs_per_tile;
       L.n_scenes = 0;
       int tiles = 0;
+      double work_total = 0.0;
+      std::vector<double> work;
       for (size_t k = g; k < scenes.size() && k < g + n3ds::MAX_SCENES_PER_LAUNCH; k++) {
         const int i = scenes[k];
         n3ds::SceneDesc& d = L.sc[L.n_scenes++];
@@ -177,18 +182,28 @@ int run_seg_passes(bool backward, const n3ds_batch_t* b, const Resolved& rv, n3d
         d.chunk_n = std::max(0, hi - lo);
         d.first_pass = pass == 0;
         d.last_pass = pass == nch[i] - 1;
-        d.tile_begin = tiles;  // work items are rays: this scene's first ray in the launch
         tiles += d.n_rays;
+        // cost model: per ray, a fixed part (loads, segment setup) worth ~16 strokes
+        // plus the culling and evaluation of the chunk
+        work.push_back(double(d.n_rays) * double(d.chunk_n + 16));
+        work_total += work.back();
       }
       if (tiles == 0) continue;
-      if (counter >= N_COUNTERS) return fail(N3DS_ERR_INVALID, "batch needs too many launches (raise chunk size or split the batch)");
+      if (counter >= N_LAUNCH_SLOTS / 2)
+        return fail(N3DS_ERR_INVALID, "batch needs too many launches (raise chunk size or split the batch)");
       if (launch_count) {  // planning only
         ++*launch_count;
         continue;
       }
       L.tiles_total = tiles;
-      L.tile_counter = base.tile_counter + counter++;
+      L.tile_counter = base.tile_counter + (counter_base + counter++) * n3ds::MAX_SCENES_PER_LAUNCH;
       const int grid = std::min(tiles, di.sms);
+      // scene affinity: scene k's home CTAs start at its work prefix x grid
+      double prefix = 0.0;
+      for (int k = 0; k < L.n_scenes; k++) {
+        L.sc[k].home_lo = (int)std::lround(prefix / work_total * grid);
+        prefix += work[k];
+      }
       cudaError_t e = backward ? n3ds::launch_seg_bwd(L, grid, rv.warps, smem, st)
                                : n3ds::launch_seg_fwd(L, grid, rv.warps, smem, st);
       if (e != cudaSuccess) return fail(N3DS_ERR_CUDA, std::string("segment kernel launch: ") + cudaGetErrorString(e));
@@ -364,7 +379,7 @@ int n3ds_field_backward(const n3ds_batch_t* batch, const n3ds_rays_t* rays, cons
   SL.grad_x = grad_x;
   SL.stats = nullptr;
   record_event(rv, 2, st);
-  rc = run_seg_passes(true, batch, rv, SL, N_COUNTERS / 2, st);
+  rc = run_seg_passes(true, batch, rv, SL, N_LAUNCH_SLOTS / 2, st);
   if (rc) return rc;
   record_event(rv, 3, st);
   if (S > 0) {

@@ -11,10 +11,12 @@
 // strokes for its own sample; the stroke (and so the SDF type) is warp-uniform, so
 // mixed-type scenes run without divergence.
 //
-// Persistent CTAs (one per SM); each warp takes whole rays (all their segments) from a
-// global counter and keeps the next one it took in shared memory. The CTA synchronises
-// only when the smallest ray held by its warps belongs to another scene: then it
-// restages that scene's records, and warps whose ray belongs to it carry on.
+// Persistent CTAs (one per SM) with scene affinity: the host gives every scene of a
+// launch a share of the CTAs proportional to its work (rays x strokes in the chunk),
+// and each CTA stages its home scene once. Its warps take whole rays (all their
+// segments) from that scene's counter; when the scene runs dry the CTA synchronises
+// once and moves to the scene with the most rays left, restaging its records. So a
+// CTA waits for its slowest warp only at a scene change, a few times per launch.
 // Scenes with more strokes than one stage holds run in several passes (one launch
 // each), carrying the per-sample composite state through HBM.
 //
@@ -91,11 +93,25 @@ __device__ __forceinline__ V3 shfl3(V3 v, int src) {
           __shfl_sync(0xffffffffu, v.z, src)};
 }
 
-__device__ __forceinline__ int find_scene(const SegLaunch& L, int tile) {
-  int lo = 0;
+// Home scene of this CTA: the last scene whose CTA range starts at or before it.
+__device__ __forceinline__ int home_scene(const SegLaunch& L) {
+  int h = 0;
   for (int i = 1; i < L.n_scenes; i++)
-    if (L.sc[i].tile_begin <= tile) lo = i;
-  return lo;
+    if (L.sc[i].home_lo <= (int)blockIdx.x) h = i;
+  return h;
+}
+
+// Scene with the most rays left to take, or -1 when every scene is taken (thread 0).
+__device__ __forceinline__ int next_scene(const SegLaunch& L) {
+  int best = -1, most = 0;
+  for (int i = 0; i < L.n_scenes; i++) {
+    const int left = L.sc[i].n_rays - *reinterpret_cast<volatile int*>(L.tile_counter + i);
+    if (left > most) {
+      most = left;
+      best = i;
+    }
+  }
+  return best;
 }
 
 __host__ __device__ constexpr size_t align16(size_t v) { return (v + 15) & ~size_t(15); }
@@ -192,42 +208,29 @@ template <int WARPS>
 __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_constant__ SegLaunch L) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t bar;
-  __shared__ int s_hold[WARPS];
   __shared__ int s_scene, s_fail;
   __shared__ unsigned long long s_kcount[16];  // evaluated (sample, stroke) pairs per base
   const Stage S = carve(smem, L.chunk_cap, false);
   const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
   if (threadIdx.x == 0) {
     mbar_init(&bar, 1);
     s_fail = 0;
   }
   if (threadIdx.x < 16) s_kcount[threadIdx.x] = 0ull;
-  if (lane == 0) s_hold[warp] = atomicAdd(L.tile_counter, 1);
   uint32_t phase = 0;
-  int staged = -1;
-  while (true) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int best = 0x7fffffff;
-      for (int w = 0; w < WARPS; w++) best = min(best, s_hold[w]);
-      s_scene = best < L.tiles_total ? find_scene(L, best) : -1;
-    }
-    __syncthreads();
-    const int sci = s_scene;
-    if (sci < 0) break;
-    if (sci != staged) {
-      if (!stage_chunk(L, L.sc[sci], S, &bar, phase, &s_fail)) {
-        if (threadIdx.x == 0) atomicOr(L.status, ST_WAIT_TIMEOUT);
-        return;
-      }
-      staged = sci;
+  int sci = home_scene(L);
+  while (sci >= 0) {
+    if (!stage_chunk(L, L.sc[sci], S, &bar, phase, &s_fail)) {
+      if (threadIdx.x == 0) atomicOr(L.status, ST_WAIT_TIMEOUT);
+      return;
     }
     const SceneDesc& sc = L.sc[sci];
-    const int item_end = sc.tile_begin + sc.n_rays;
-    int item = s_hold[warp];
-    while (item >= sc.tile_begin && item < item_end) {
-      const int ray_local = item - sc.tile_begin;
+    int* counter = L.tile_counter + sci;
+    int item = 0;
+    if (lane == 0) item = atomicAdd(counter, 1);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    while (item < sc.n_rays) {
+      const int ray_local = item;
       for (int g = 0; g < L.segs_per_ray; g++) {
         SegCtx c = seg_setup(L, sc, ray_local * L.segs_per_ray + g, lane);
         float T, sig, cr, cg, cb;
@@ -260,12 +263,14 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_con
           st[0] = T; st[1] = sig; st[2] = cr; st[3] = cg; st[4] = cb;
         }
       }
-      if (lane == 0) item = atomicAdd(L.tile_counter, 1);
+      if (lane == 0) item = atomicAdd(counter, 1);
       item = __shfl_sync(0xffffffffu, item, 0);
     }
-    if (lane == 0) s_hold[warp] = item;
+    __syncthreads();  // every warp is done with the staged chunk
+    if (threadIdx.x == 0) s_scene = next_scene(L);
+    __syncthreads();
+    sci = s_scene;
   }
-  __syncthreads();
   if (L.stats && threadIdx.x < 16 && s_kcount[threadIdx.x]) {
     atomicAdd(L.stats, s_kcount[threadIdx.x]);
     atomicAdd(L.stats + 1 + threadIdx.x, s_kcount[threadIdx.x]);
@@ -330,11 +335,9 @@ template <int WARPS>
 __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_constant__ SegLaunch L) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t bar;
-  __shared__ int s_hold[WARPS];
   __shared__ int s_scene, s_fail;
   const Stage S = carve(smem, L.chunk_cap, true);
   const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
   const int nthr = blockDim.x;
   if (threadIdx.x == 0) {
     mbar_init(&bar, 1);
@@ -343,7 +346,6 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
   for (int i = threadIdx.x; i < L.chunk_cap * GRAD_SLOTS; i += nthr) S.gacc[i] = 0.f;
   __syncthreads();
   uint32_t phase = 0;
-  int staged = -1;
   const int compat = L.compat;
 
   auto flush = [&](int sci) {
@@ -358,33 +360,19 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
     }
   };
 
-  if (lane == 0) s_hold[warp] = atomicAdd(L.tile_counter, 1);
-  while (true) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int best = 0x7fffffff;
-      for (int w = 0; w < WARPS; w++) best = min(best, s_hold[w]);
-      s_scene = best < L.tiles_total ? find_scene(L, best) : -1;
-    }
-    __syncthreads();
-    const int sci = s_scene;
-    if (sci < 0) break;
-    if (sci != staged) {
-      if (staged >= 0) {
-        flush(staged);
-        __syncthreads();
-      }
-      if (!stage_chunk(L, L.sc[sci], S, &bar, phase, &s_fail)) {
-        if (threadIdx.x == 0) atomicOr(L.status, ST_WAIT_TIMEOUT);
-        return;
-      }
-      staged = sci;
+  int sci = home_scene(L);
+  while (sci >= 0) {
+    if (!stage_chunk(L, L.sc[sci], S, &bar, phase, &s_fail)) {
+      if (threadIdx.x == 0) atomicOr(L.status, ST_WAIT_TIMEOUT);
+      return;
     }
     const SceneDesc& sc = L.sc[sci];
-    const int item_end = sc.tile_begin + sc.n_rays;
-    int item = s_hold[warp];
-    while (item >= sc.tile_begin && item < item_end) {
-      const int ray_local = item - sc.tile_begin;
+    int* counter = L.tile_counter + sci;
+    int item = 0;
+    if (lane == 0) item = atomicAdd(counter, 1);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    while (item < sc.n_rays) {
+      const int ray_local = item;
       for (int g = 0; g < L.segs_per_ray; g++) {
         SegCtx c = seg_setup(L, sc, ray_local * L.segs_per_ray + g, lane);
         CompAdj s;
@@ -479,13 +467,15 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
           }
         }
       }
-      if (lane == 0) item = atomicAdd(L.tile_counter, 1);
+      if (lane == 0) item = atomicAdd(counter, 1);
       item = __shfl_sync(0xffffffffu, item, 0);
     }
-    if (lane == 0) s_hold[warp] = item;
+    __syncthreads();  // every warp is done with the staged chunk
+    flush(sci);
+    if (threadIdx.x == 0) s_scene = next_scene(L);
+    __syncthreads();
+    sci = s_scene;
   }
-  __syncthreads();
-  if (staged >= 0) flush(staged);
 }
 
 // ============================================================== ray kernels

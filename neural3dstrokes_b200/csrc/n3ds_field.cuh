@@ -15,7 +15,7 @@ struct SceneDesc {
   int n_rays;
   int stroke_begin;      // first stroke (global)
   int n_strokes;
-  int tile_begin;        // first work item (ray) of this scene in the current launch
+  int home_lo;           // first CTA whose home is this scene (CTAs home_lo .. next scene's home_lo - 1)
   int chunk_lo;          // stroke range of the current pass, scene-local
   int chunk_n;
   int first_pass;        // 1: composite state starts fresh
@@ -40,7 +40,7 @@ struct SegLaunch {
   int tiles_total;         // work items (rays) in the launch
   int segs_per_tile;       // unused (kept for layout stability)
   int chunk_cap;           // strokes per shared-memory stage
-  int* tile_counter;
+  int* tile_counter;       // [n_scenes] next ray of each scene (zeroed before the launch)
   int* status;
   unsigned long long* stats;  // [0] evaluated (sample, stroke) pairs
   SceneDesc sc[MAX_SCENES_PER_LAUNCH];

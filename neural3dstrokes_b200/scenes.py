@@ -169,22 +169,23 @@ def config(idx, seed=0, scale=1.0):
     """Workload of benchmark configuration ``idx`` (0..4). ``scale`` < 1 shrinks the
     ray counts (tests); stroke counts and distributions are kept."""
     g = torch.Generator().manual_seed(seed + 1000 * idx)
+    gr = torch.Generator().manual_seed(seed + 1000 * idx + 1)  # rays: own stream, so scale keeps the strokes
     R = lambda n: max(32, int(n * scale))
     if idx == 0:
         sc = make_strokes(["ellipsoid"] * 64, g)
-        return Workload("cfg0: 64 ellipsoids, 4096 rays x 64 samples, forward", [sc], [make_rays(R(4096), 64, g)])
+        return Workload("cfg0: 64 ellipsoids, 4096 rays x 64 samples, forward", [sc], [make_rays(R(4096), 64, gr)])
     if idx == 1:
         kinds = [MIXED_PRIMS[int(i)] for i in torch.randint(0, 6, (500,), generator=g)]
         sc = make_strokes(kinds, g)
         return Workload("cfg1: 500 mixed primitives, 65536 rays x 128 samples, fwd+bwd", [sc],
-                        [make_rays(R(65536), 128, g)])
+                        [make_rays(R(65536), 128, gr)])
     if idx == 2:
         kinds = ["quadratic_bezier"] * 1000 + ["cubic_bezier"] * 1000
         perm = torch.randperm(2000, generator=g)
         kinds = [kinds[int(i)] for i in perm]
         sc = make_strokes(kinds, g)
         return Workload("cfg2: 2000 Bezier tubes, 262144 rays x 64 samples, fwd+bwd", [sc],
-                        [make_rays(R(262144), 64, g)])
+                        [make_rays(R(262144), 64, gr)])
     if idx == 3:
         scenes, rays = [], []
         for _ in range(16):
@@ -192,7 +193,7 @@ def config(idx, seed=0, scale=1.0):
             Rn = int(round(float(_logu(1, 4096, 65536, g))))
             kinds = [MIXED_PRIMS[int(i)] for i in torch.randint(0, 6, (S,), generator=g)]
             scenes.append(make_strokes(kinds, g))
-            rays.append(make_rays(R(Rn), 64, g))
+            rays.append(make_rays(R(Rn), 64, gr))
         return Workload("cfg3: 16 uneven scenes (S~logU[50,2000], R~logU[4096,65536]) x 64 samples, "
                         "batched fwd+bwd", scenes, rays)
     if idx == 4:
@@ -200,7 +201,7 @@ def config(idx, seed=0, scale=1.0):
         for _ in range(4):
             kinds = [ALL_KINDS[int(i)] for i in torch.randint(0, 8, (2000,), generator=g)]
             scenes.append(make_strokes(kinds, g))
-            rays.append(make_rays(R(131072), 96, g))
+            rays.append(make_rays(R(131072), 96, gr))
             kt = [ALL_KINDS[int(i)] for i in torch.randint(0, 8, (2000,), generator=g)]
             targets.append(make_strokes(kt, g))
         w = Workload("cfg4: 4 scenes x 2000 mixed strokes, 131072 rays x 96 samples, graphed training step",
