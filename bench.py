@@ -280,6 +280,59 @@ def plain_op_gpu(w, args, max_seconds=60.0):
                     "group, ray-chunked (P_chunk*S < 2^29), torch autograd for render.py, grad_x requested"}
 
 
+def loss_curves(args):
+    """Config 4's training comparison: the graphed step (forward, MSE, exact or compat
+    adjoint, Adam + clamp in one CUDA graph) against the reference op trained as the
+    reference trains (plain_op_train), K steps each from the same parameters."""
+    from neural3dstrokes_b200 import scenes
+    from neural3dstrokes_b200.field import FieldOptions
+    from neural3dstrokes_b200.train import BatchedField, GraphedTrainer
+    from oracle import cpu_port
+    dev = torch.device("cuda", 0)
+    w = scenes.config(4, scale=args.scale)
+    ref = cpu_port.reference_extension()
+    grad_mode = "compat"
+    tf = BatchedField(w.target_scenes, w.rays, w.sdf_delta, w.use_laplace, w.inv_scale_radius, device=dev,
+                      need_grad_x=False)
+    tf.forward()
+    target = tf.rgb.clone()
+    del tf
+    field = BatchedField(w.scenes, w.rays, w.sdf_delta, w.use_laplace, w.inv_scale_radius,
+                         options=FieldOptions(grad_mode=grad_mode), device=dev, need_grad_x=False)
+    trainer = GraphedTrainer(field, target, lr=1e-3)
+    ours = []
+    t0 = time.time()
+    for _ in range(args.loss_curve):
+        trainer.step()
+        ours.append(float(trainer.loss))
+    t_ours = time.time() - t0
+    line = {"mode": "loss_curve", "config": w.name, "scale": args.scale, "steps": args.loss_curve,
+            "grad_mode": grad_mode, "ours": ours, "ours_s": t_ours}
+    if ref is None:
+        line["plain_op"] = "unavailable: oracle/_ref holds no reference extension"
+    else:
+        n0 = 0
+        targets = []
+        for r in w.rays:
+            targets.append(target[n0:n0 + r.n_rays])
+            n0 += r.n_rays
+        ranges = []
+        for sc in w.scenes:
+            lo, hi = zip(*[scenes.param_ranges(k) for k in sc.kinds])
+            ranges.append((torch.tensor(lo, device=dev), torch.tensor(hi, device=dev)))
+        t0 = time.time()
+        theirs, _ = cpu_port.plain_op_train(ref, [s.to(dev) for s in w.scenes], [r.to(dev) for r in w.rays],
+                                            targets, args.loss_curve, lr=1e-3, delta=w.sdf_delta,
+                                            laplace=w.use_laplace, inv=w.inv_scale_radius, ranges=ranges)
+        line["plain_op"] = theirs
+        line["plain_op_s"] = time.time() - t0
+        line["max_rel_diff"] = max(abs(a - b) / max(abs(b), 1e-30) for a, b in zip(ours, theirs))
+    print(json.dumps(line), flush=True)
+    if args.curve_out:
+        with open(args.curve_out, "w") as f:
+            json.dump(line, f)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -292,8 +345,21 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain-op", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--schedule", default="auto", choices=["auto", "runs", "segments"],
+                    help="field kernel work decomposition (auto: the autotuner picks)")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (library defaults)")
+    ap.add_argument("--loss-curve", type=int, default=0, metavar="K",
+                    help="config 4 only: train K steps with the graphed step and with the plain reference op "
+                         "from the same start, print both loss curves (not a throughput run)")
+    ap.add_argument("--curve-out", default="", help="write the loss curves as JSON to this file")
     args = ap.parse_args()
     world, rank, local = dist_setup(args.gpus)
+    if args.loss_curve:
+        if rank == 0:
+            loss_curves(args)
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
     if args.impl == "reference":
         run_reference(args, world, rank)
         if world > 1:
@@ -301,11 +367,13 @@ def main():
         return
 
     from neural3dstrokes_b200 import scenes
+    from neural3dstrokes_b200.field import FieldOptions
     from neural3dstrokes_b200.train import BatchedField, GraphedTrainer, capture
 
     dev = torch.device("cuda", local)
     w = scenes.config(args.config, scale=args.scale)
-    field = BatchedField(w.scenes, w.rays, w.sdf_delta, w.use_laplace, w.inv_scale_radius, device=dev)
+    field = BatchedField(w.scenes, w.rays, w.sdf_delta, w.use_laplace, w.inv_scale_radius,
+                         options=FieldOptions(schedule=args.schedule), device=dev)
     g_rgb, g_acc, g_depth = workload_upstream(field)
     trainer = None
     if args.config == 4:
@@ -322,6 +390,13 @@ def main():
         field.g_depth.copy_(g_depth)
         step_fn = field.step
     pairs = field.nominal_pairs
+
+    # launch configuration: the autotuner times the candidates on this workload (not timed)
+    tuned = None
+    if args.schedule == "auto" and not args.no_tune:
+        from neural3dstrokes_b200 import autotune
+        tuned = autotune.tune(field, reps=2, use_cache=False)
+    segments = field.options.schedule != "runs"
 
     # statistics pass (not timed): evaluated pairs per primitive type, status word
     field.forward()
@@ -368,11 +443,13 @@ def main():
     fwd_flops = sum(per_base[b] * bf.get(b, 0.0) for b in range(16))
     bwd_flops = BWD_FACTOR * fwd_flops
     peak = fp32_peak(dev)
-    roofline = {"bound": "fp32", "kernel": "seg_bwd_kernel (segment adjoint)", "achieved": bwd_flops / t_bwd / 1e12,
+    kname = ("seg_bwd_kernel (segment adjoint)" if segments else "run_bwd_kernel (sample-run adjoint)")
+    roofline = {"bound": "fp32", "kernel": kname, "achieved": bwd_flops / t_bwd / 1e12,
                 "peak": peak, "unit": "TFLOP/s", "frac": bwd_flops / t_bwd / 1e12 / peak, "traffic": None,
                 "peak_source": "measured: FP32 FMA probe kernel on this GPU (no FP32 figure in the peaks file)",
                 "flops_per_launch": bwd_flops, "launch_ms": t_bwd * 1e3,
-                "seg_fwd": {"achieved": fwd_flops / t_fwd / 1e12, "launch_ms": t_fwd * 1e3,
+                "forward_kernel": {"name": "seg_fwd_kernel" if segments else "run_fwd_kernel",
+                                   "achieved": fwd_flops / t_fwd / 1e12, "launch_ms": t_fwd * 1e3,
                             "frac": fwd_flops / t_fwd / 1e12 / peak}}
 
     # end to end through the public API with host buffers: H2D of the step's inputs,
@@ -424,7 +501,10 @@ def main():
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "l2": "inputs larger than L2 (x alone %.0f MB)" % (field.x.numel() * 4 / 1e6),
                        "graph": "forward+backward captured in one CUDA graph" if trainer is None
-                       else "forward+MSE+backward+Adam captured in one CUDA graph"},
+                       else "forward+MSE+backward+Adam captured in one CUDA graph",
+                       "launch": {"schedule": "segments" if segments else "runs", "warps": field.options.warps,
+                                  "chunk_fwd": field.options.chunk_fwd, "chunk_bwd": field.options.chunk_bwd,
+                                  "picked_by": "autotuner" if tuned is not None else "flags"}},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
             "gpu_launches": launches_per_step * args.steps,
             "gpu_launches_per_step": launches_per_step,

@@ -35,6 +35,12 @@ typedef struct CUstream_st* n3ds_stream_t; /* = cudaStream_t */
 #define N3DS_ERR_WORKSPACE 4   /* workspace too small */
 #define N3DS_ERR_DEVICE 5      /* a kernel reported a device-side error status */
 
+/* Work decomposition of the fused field kernels: a warp per 32-sample segment with
+ * every lane evaluating each surviving stroke, or a warp per 64-sample unit with the
+ * (sample, stroke) pairs inside each stroke's reach packed densely into lanes. */
+#define N3DS_SCHEDULE_SEGMENTS 1
+#define N3DS_SCHEDULE_RUNS 2
+
 #define N3DS_GRAD_EXACT 0  /* exact adjoint of the forward (checked against float64 finite differences) */
 #define N3DS_GRAD_COMPAT 1 /* the reference's hand-written backward formulas */
 
@@ -164,7 +170,7 @@ typedef struct n3ds_options {
   int32_t chunk_fwd;  /* strokes per shared-memory stage, forward (0 = auto) */
   int32_t chunk_bwd;  /* strokes per shared-memory stage, backward (0 = auto) */
   int32_t warps;      /* warps per CTA: 4, 8 or 16 (0 = auto) */
-  int32_t segs_per_tile; /* 32-sample segments per CTA work tile (0 = auto) */
+  int32_t schedule;   /* N3DS_SCHEDULE_* (0 = auto: segments) */
   int32_t grad_mode;  /* N3DS_GRAD_EXACT or N3DS_GRAD_COMPAT */
   /* optional: 4 cudaEvent_t recorded on the stream around the segment kernels
    * (forward begin/end, backward begin/end), or NULL */
@@ -173,6 +179,10 @@ typedef struct n3ds_options {
 
 /* Fill *opt with the defaults. */
 void n3ds_default_options(n3ds_options_t* opt);
+
+/* The launch configuration the library uses for *opt on the current device: auto
+ * (0) stage sizes, warps and schedule replaced by their resolved values. */
+int n3ds_field_resolve_options(const n3ds_options_t* opt, n3ds_options_t* out);
 
 /* Workspace bytes for a batch (forward checkpoint, backward seeds and state,
  * prepared records, reduction slots, counters). total_strokes = sum of n_strokes. */

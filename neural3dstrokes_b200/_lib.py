@@ -44,7 +44,7 @@ class Strokes(ctypes.Structure):
 
 class Options(ctypes.Structure):
     _fields_ = [("cull_alpha", ctypes.c_float), ("chunk_fwd", c_i32), ("chunk_bwd", c_i32),
-                ("warps", c_i32), ("segs_per_tile", c_i32), ("grad_mode", c_i32),
+                ("warps", c_i32), ("schedule", c_i32), ("grad_mode", c_i32),
                 ("timing_events", ctypes.POINTER(ctypes.c_void_p))]
 
 
@@ -77,6 +77,7 @@ _SIGS = {
     "n3ds_field_read_pair_counts": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64), _P]),
     "n3ds_field_launch_count": (ctypes.c_int, [ctypes.POINTER(Batch), ctypes.POINTER(Options),
                                                ctypes.POINTER(c_i32), ctypes.POINTER(c_i32)]),
+    "n3ds_field_resolve_options": (ctypes.c_int, [ctypes.POINTER(Options), ctypes.POINTER(Options)]),
     "n3ds_stroke_forward_static": (ctypes.c_int, [_P, _P, _P, c_i64, _P, _P, _P, _P, _P, c_i64, c_i64, c_i64,
                                                   c_i64, c_i64, c_u32, c_u32, ctypes.c_float, ctypes.c_int,
                                                   ctypes.c_int, _P]),

@@ -85,8 +85,9 @@ WsLayout ws_layout(long long total_rays, int N, long long S) {
 }
 
 struct Resolved {
-  float cull_m;
-  int chunk_fwd, chunk_bwd, warps, segs_per_tile, grad_mode;
+  float cull_m, cull_alpha;
+  int chunk_fwd, chunk_bwd, warps, schedule, grad_mode;
+  int warps_fwd, warps_bwd;  // per direction (the forward segment kernel runs 24 warps by default)
   void* const* events;
 };
 
@@ -103,13 +104,24 @@ Resolved resolve(const n3ds_options_t* o) {
   r.cull_m = o->cull_alpha > 0.f ? -logf(2.f * o->cull_alpha) : -1.f;
   if (o->cull_alpha > 0.f && r.cull_m < 0.f) r.cull_m = 0.f;
   const DevInfo di = dev_info();
+  r.cull_alpha = o->cull_alpha > 0.f ? o->cull_alpha : 0.f;
   r.warps = o->warps > 0 ? o->warps : 16;
-  r.segs_per_tile = o->segs_per_tile > 0 ? o->segs_per_tile : 4 * r.warps;
-  const size_t budget = size_t(di.smem_optin) - 64;
-  int cf = o->chunk_fwd > 0 ? o->chunk_fwd : 768;
-  int cb = o->chunk_bwd > 0 ? o->chunk_bwd : 512;
-  while (cf > 32 && n3ds::seg_fwd_smem(cf) > budget) cf -= 32;
-  while (cb > 32 && n3ds::seg_bwd_smem(cb) > budget) cb -= 32;
+  r.schedule = o->schedule == N3DS_SCHEDULE_RUNS ? N3DS_SCHEDULE_RUNS : N3DS_SCHEDULE_SEGMENTS;
+  const bool runs = r.schedule == N3DS_SCHEDULE_RUNS;
+  // 24 warps only for the forward segment kernel (76 registers); the others hold
+  // 100+ registers per thread and run at most 16
+  auto pick = [](int w, bool allow24) { return allow24 && w >= 24 ? 24 : w >= 16 ? 16 : w >= 8 ? 8 : 4; };
+  r.warps_fwd = pick(o->warps > 0 ? o->warps : 24, !runs);
+  r.warps_bwd = pick(o->warps > 0 ? o->warps : 16, false);
+  r.warps = r.warps_bwd;
+  const size_t budget = size_t(di.smem_optin) - 256;  // room for static shared memory
+  // default stages: the largest multiple of 32 strokes that fits the shared memory
+  int cf = o->chunk_fwd > 0 ? o->chunk_fwd : 1024;
+  int cb = o->chunk_bwd > 0 ? o->chunk_bwd : 1024;
+  auto fwd_smem = [&](int c) { return runs ? n3ds::run_fwd_smem(c, r.warps_fwd) : n3ds::seg_fwd_smem(c); };
+  auto bwd_smem = [&](int c) { return runs ? n3ds::run_bwd_smem(c, r.warps_bwd) : n3ds::seg_bwd_smem(c); };
+  while (cf > 32 && fwd_smem(cf) > budget) cf -= 32;
+  while (cb > 32 && bwd_smem(cb) > budget) cb -= 32;
   r.chunk_fwd = cf;
   r.chunk_bwd = cb;
   r.grad_mode = o->grad_mode;
@@ -141,6 +153,9 @@ int run_seg_passes(bool backward, const n3ds_batch_t* b, const Resolved& rv, n3d
                    int counter_base, cudaStream_t st, int* launch_count = nullptr) {
   const int cap = backward ? rv.chunk_bwd : rv.chunk_fwd;
   const int spr = (b->n_samples + 31) / 32;
+  const bool runs = rv.schedule == N3DS_SCHEDULE_RUNS;
+  // work items per ray: the whole ray (segments) or 64-sample units (runs)
+  const int ipr = runs ? (b->n_samples + n3ds::RUN_UNIT_SAMPLES - 1) / n3ds::RUN_UNIT_SAMPLES : 1;
   std::vector<long long> ray_begin(b->n_scenes), stroke_begin(b->n_scenes);
   std::vector<int> nch(b->n_scenes);
   long long r0 = 0, s0 = 0;
@@ -154,7 +169,9 @@ int run_seg_passes(bool backward, const n3ds_batch_t* b, const Resolved& rv, n3d
     passes = std::max(passes, nch[i]);
   }
   const DevInfo di = dev_info();
-  const size_t smem = backward ? n3ds::seg_bwd_smem(cap) : n3ds::seg_fwd_smem(cap);
+  const int warps = backward ? rv.warps_bwd : rv.warps_fwd;
+  const size_t smem = runs ? (backward ? n3ds::run_bwd_smem(cap, warps) : n3ds::run_fwd_smem(cap, warps))
+                           : (backward ? n3ds::seg_bwd_smem(cap) : n3ds::seg_fwd_smem(cap));
   int counter = 0;
   for (int pass = 0; pass < passes; pass++) {
     std::vector<int> scenes;
@@ -164,9 +181,9 @@ int run_seg_passes(bool backward, const n3ds_batch_t* b, const Resolved& rv, n3d
       n3ds::SegLaunch L = base;
       L.chunk_cap = cap;
       L.segs_per_ray = spr;
-      L.segs_per_tile = rv.segs_per_tile;
+      L.schedule = rv.schedule;
       L.n_scenes = 0;
-      int tiles = 0;
+      long long tiles = 0;
       double work_total = 0.0;
       std::vector<double> work;
       for (size_t k = g; k < scenes.size() && k < g + n3ds::MAX_SCENES_PER_LAUNCH; k++) {
@@ -182,7 +199,9 @@ int run_seg_passes(bool backward, const n3ds_batch_t* b, const Resolved& rv, n3d
         d.chunk_n = std::max(0, hi - lo);
         d.first_pass = pass == 0;
         d.last_pass = pass == nch[i] - 1;
-        tiles += d.n_rays;
+        if ((long long)d.n_rays * ipr > 0x7fffffffLL)
+          return fail(N3DS_ERR_INVALID, "too many rays in one scene for 32-bit work counters");
+        tiles += (long long)d.n_rays * ipr;
         // cost model: per ray, a fixed part (loads, segment setup) worth ~16 strokes
         // plus the culling and evaluation of the chunk
         work.push_back(double(d.n_rays) * double(d.chunk_n + 16));
@@ -195,17 +214,19 @@ int run_seg_passes(bool backward, const n3ds_batch_t* b, const Resolved& rv, n3d
         ++*launch_count;
         continue;
       }
-      L.tiles_total = tiles;
+      L.tiles_total = (int)std::min<long long>(tiles, 0x7fffffffLL);
       L.tile_counter = base.tile_counter + (counter_base + counter++) * n3ds::MAX_SCENES_PER_LAUNCH;
-      const int grid = std::min(tiles, di.sms);
+      const int grid = (int)std::min<long long>(tiles, di.sms);
       // scene affinity: scene k's home CTAs start at its work prefix x grid
       double prefix = 0.0;
       for (int k = 0; k < L.n_scenes; k++) {
         L.sc[k].home_lo = (int)std::lround(prefix / work_total * grid);
         prefix += work[k];
       }
-      cudaError_t e = backward ? n3ds::launch_seg_bwd(L, grid, rv.warps, smem, st)
-                               : n3ds::launch_seg_fwd(L, grid, rv.warps, smem, st);
+      cudaError_t e = runs ? (backward ? n3ds::launch_run_bwd(L, grid, warps, smem, st)
+                                       : n3ds::launch_run_fwd(L, grid, warps, smem, st))
+                           : (backward ? n3ds::launch_seg_bwd(L, grid, warps, smem, st)
+                                       : n3ds::launch_seg_fwd(L, grid, warps, smem, st));
       if (e != cudaSuccess) return fail(N3DS_ERR_CUDA, std::string("segment kernel launch: ") + cudaGetErrorString(e));
     }
   }
@@ -230,7 +251,7 @@ void n3ds_default_options(n3ds_options_t* opt) {
   opt->chunk_fwd = 0;
   opt->chunk_bwd = 0;
   opt->warps = 0;
-  opt->segs_per_tile = 0;
+  opt->schedule = 0;
   opt->grad_mode = N3DS_GRAD_EXACT;
   opt->timing_events = nullptr;
 }
@@ -378,6 +399,7 @@ int n3ds_field_backward(const n3ds_batch_t* batch, const n3ds_rays_t* rays, cons
   n3ds::SegLaunch SL = make_seg(batch, rays, ws, lay, compat);
   SL.grad_x = grad_x;
   SL.stats = nullptr;
+  SL.skip_alpha = rv.cull_alpha;
   record_event(rv, 2, st);
   rc = run_seg_passes(true, batch, rv, SL, N_LAUNCH_SLOTS / 2, st);
   if (rc) return rc;
@@ -401,6 +423,21 @@ int n3ds_field_backward(const n3ds_batch_t* batch, const n3ds_rays_t* rays, cons
     n3ds::launch_finalize(F, st);
     N3DS_CUDA_TRY(cudaGetLastError());
   }
+  return N3DS_OK;
+}
+
+int n3ds_field_resolve_options(const n3ds_options_t* opt, n3ds_options_t* out) {
+  if (!out) return fail(N3DS_ERR_INVALID, "out is required");
+  n3ds_options_t d;
+  n3ds_default_options(&d);
+  const n3ds_options_t* o = opt ? opt : &d;
+  const Resolved rv = resolve(o);
+  *out = *o;
+  out->chunk_fwd = rv.chunk_fwd;
+  out->chunk_bwd = rv.chunk_bwd;
+  out->warps = o->warps;  // 0 (auto) stays: the directions differ (24 / 16 warps)
+  out->schedule = rv.schedule;
+  out->grad_mode = rv.grad_mode;
   return N3DS_OK;
 }
 

@@ -36,9 +36,11 @@ struct SegLaunch {
   float* grad_x;           // [P*3] or null
   float* gslots;           // [S*32] reduced per-stroke gradient slots
   int compat;              // reference gradient formulas
+  float skip_alpha;        // backward: skip the adjoint of a stroke whose alpha is below this at
+                           // every sample of a segment (the culling threshold; 0 never skips)
   int n_scenes;
   int tiles_total;         // work items (rays) in the launch
-  int segs_per_tile;       // unused (kept for layout stability)
+  int schedule;            // N3DS_SCHEDULE_SEGMENTS or N3DS_SCHEDULE_RUNS
   int chunk_cap;           // strokes per shared-memory stage
   int* tile_counter;       // [n_scenes] next ray of each scene (zeroed before the launch)
   int* status;
@@ -122,5 +124,13 @@ void launch_finalize(const FinalizeLaunch& L, cudaStream_t st);
 
 size_t seg_fwd_smem(int chunk_cap);
 size_t seg_bwd_smem(int chunk_cap);
+
+// sample-run kernels (n3ds_runs.cu): same launch descriptor, work items are units of
+// up to 64 samples of a ray
+constexpr int RUN_UNIT_SAMPLES = 64;
+cudaError_t launch_run_fwd(const SegLaunch& L, int grid, int warps, size_t smem, cudaStream_t st);
+cudaError_t launch_run_bwd(const SegLaunch& L, int grid, int warps, size_t smem, cudaStream_t st);
+size_t run_fwd_smem(int chunk_cap, int warps);
+size_t run_bwd_smem(int chunk_cap, int warps);
 
 }  // namespace n3ds

@@ -24,7 +24,7 @@ class FieldOptions:
     chunk_fwd: int = 0         # strokes per shared-memory stage (0: auto)
     chunk_bwd: int = 0
     warps: int = 0             # warps per CTA: 4, 8, 16 (0: auto)
-    segs_per_tile: int = 0     # 32-sample segments per CTA work tile (0: auto)
+    schedule: str = "auto"     # 'segments' (auto): lane = sample; 'runs': packed (sample, stroke) pairs
     grad_mode: str = "exact"   # 'exact' or 'compat'
 
     def c(self, events=None):
@@ -39,7 +39,7 @@ class FieldOptions:
             ev = ctypes.cast(arr, ctypes.POINTER(ctypes.c_void_p))
             self._ev_keepalive = arr
         return _lib.Options(float(self.cull_alpha), int(self.chunk_fwd), int(self.chunk_bwd), int(self.warps),
-                            int(self.segs_per_tile),
+                            {"auto": 0, "segments": 1, "runs": 2}[self.schedule],
                             _lib.N3DS_GRAD_COMPAT if self.grad_mode == "compat" else _lib.N3DS_GRAD_EXACT, ev)
 
 

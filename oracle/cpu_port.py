@@ -143,3 +143,53 @@ def plain_op_step(ref, scene, x, radius, tdist, dirs, g_rgb, g_acc, g_depth, del
             grad_shape[idx, :ps.shape[1]] += gs
             grad_color[idx] += gcol
     return rgb, acc, depth, grad_shape, grad_color, grad_density
+
+
+def plain_op_train(ref, scenes, rays, targets, steps, lr=1e-3, betas=(0.9, 0.99), eps=1e-15, delta=0.02,
+                   laplace=True, inv=True, ranges=None):
+    """MSE training of the stroke parameters through the reference CUDA op, as the
+    reference trains the stroke field: per step and scene, forward and backward of
+    the op chain (plain_op_step), then torch Adam (utils/training.py:119-136) over
+    shape, colour and density, then the parameter clamp of StrokeField.clip_params
+    (models.py:576-584). ``scenes``/``rays``/``targets`` on the GPU; ``ranges``: per
+    scene (lo, hi) tensors of the shape parameters. Returns the loss of every step
+    (before that step's update) and the trained scenes."""
+    import copy
+    scenes = [copy.copy(s) for s in scenes]
+    params = []
+    for s in scenes:
+        s.shape_params = s.shape_params.clone().requires_grad_(True)
+        s.color_params = s.color_params.clone().requires_grad_(True)
+        s.density = s.density.clone().requires_grad_(True)
+        params += [s.shape_params, s.color_params, s.density]
+    opt = torch.optim.Adam(params, lr=lr, betas=betas, eps=eps)
+    n_total = sum(t.numel() for t in targets)
+    losses = []
+    for _ in range(steps):
+        loss = 0.0
+        grads = []
+        with torch.no_grad():
+            for s, r, t in zip(scenes, rays, targets):
+                det = copy.copy(s)
+                det.shape_params, det.color_params, det.density = (s.shape_params.detach(), s.color_params.detach(),
+                                                                  s.density.detach())
+                zr = torch.zeros(r.n_rays, 3, device=t.device)
+                z = torch.zeros(r.n_rays, device=t.device)
+                rgb = plain_op_step(ref, det, r.x, r.radius, r.tdist, r.dirs, zr, z, z, delta, laplace, inv)[0]
+                diff = rgb - t
+                loss += float((diff * diff).sum())
+                g_rgb = diff * (2.0 / n_total)
+                _, _, _, gs, gc, gd = plain_op_step(ref, det, r.x, r.radius, r.tdist, r.dirs, g_rgb, z, z, delta,
+                                                    laplace, inv)
+                grads += [gs, gc, gd]
+        losses.append(loss / n_total)
+        for p, g in zip(params, grads):
+            p.grad = torch.nan_to_num(g)
+        opt.step()
+        with torch.no_grad():
+            for i, s in enumerate(scenes):
+                lo, hi = ranges[i]
+                s.shape_params.copy_(torch.minimum(torch.maximum(s.shape_params, lo), hi))
+                s.color_params.clamp_(0.0, 1.0)
+                s.density.clamp_(min=0.0)
+    return losses, scenes

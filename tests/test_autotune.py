@@ -1,0 +1,74 @@
+"""Autotuner: option resolution on the host (CPU) and a tuning pass on a small batch
+(GPU) that must leave the results unchanged. Tolerance: forward 1e-5 (helpers)."""
+import dataclasses
+import json
+
+import pytest
+import torch
+
+from helpers import FWD_TOL, rel
+from neural3dstrokes_b200 import autotune, scenes
+from neural3dstrokes_b200.field import FieldOptions
+
+
+def test_resolved_options_fill_in_auto_values():
+    for schedule in ("segments", "runs"):
+        r = autotune.resolved(FieldOptions(schedule=schedule))
+        assert r.schedule == schedule
+        assert r.chunk_fwd >= 32 and r.chunk_fwd % 32 == 0
+        assert r.chunk_bwd >= 32 and r.chunk_bwd % 32 == 0
+    assert autotune.resolved(FieldOptions()).schedule == "segments"
+    # explicit stages are kept
+    r = autotune.resolved(FieldOptions(chunk_fwd=64, chunk_bwd=96))
+    assert (r.chunk_fwd, r.chunk_bwd) == (64, 96)
+
+
+def test_candidate_set_covers_schedules_warps_and_stages():
+    c = autotune.candidates()
+    assert {o.schedule for o in c} == {"segments", "runs"}
+    assert {o.warps for o in c} == {0, 8}
+    assert {o.chunk_fwd for o in c} == {0, -1}
+
+
+class _FakeField:
+    """Stands in for BatchedField in the cache logic (no device work)."""
+
+    def __init__(self):
+        self.kinds = ["cube", "sphere"]
+        self.scene_rays = [1000, 70]
+        self.scene_strokes = [2, 0]
+        self.n_samples = 64
+        self.laplace = True
+        self.inv_scale = True
+        self.options = FieldOptions()
+        self.binds = 0
+
+    def _bind(self):
+        self.binds += 1
+
+
+def test_signature_rounds_ray_counts_and_cache_file(tmp_path, monkeypatch):
+    f = _FakeField()
+    key = autotune.signature(f)
+    assert json.loads(key)["rays"] == [1024, 64]
+    path = tmp_path / "tune.json"
+    best = FieldOptions(schedule="runs", chunk_fwd=64, chunk_bwd=32)
+    path.write_text(json.dumps({key: {"options": dataclasses.asdict(best), "ms": 1.0, "tried": 8}}))
+    monkeypatch.setenv("N3DS_TUNE_CACHE", str(path))
+    got = autotune.tune(f)
+    assert got == best and f.options == best and f.binds == 1
+
+
+@pytest.mark.gpu
+def test_tuning_keeps_results(cuda):
+    from neural3dstrokes_b200.train import BatchedField
+    w = scenes.config(3, scale=0.02)
+    field = BatchedField(w.scenes[:4], w.rays[:4], device=cuda)
+    field.forward()
+    torch.cuda.synchronize()
+    ref = field.rgb.clone()
+    best = autotune.tune(field, reps=1, use_cache=False)
+    assert field.options == best
+    field.forward()
+    torch.cuda.synchronize()
+    assert rel(field.rgb, ref) < FWD_TOL

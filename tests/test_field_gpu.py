@@ -28,10 +28,14 @@ def run_field(sc, rays, dev, delta=0.02, laplace=True, inv=True, bg=1.0, opaque=
     return out, (x, sp, col, den, dl)
 
 
+SCHEDULES = ["runs", "segments"]
+
+
+@pytest.mark.parametrize("schedule", SCHEDULES)
 @pytest.mark.parametrize("kind", KINDS)
-def test_forward_matches_oracle(cuda, kind):
+def test_forward_matches_oracle(cuda, kind, schedule):
     sc, rays = small_workload(kind)
-    (rgb, acc, depth), _ = run_field(sc, rays, cuda)
+    (rgb, acc, depth), _ = run_field(sc, rays, cuda, opts=FieldOptions(schedule=schedule))
     rgb_r, acc_r, depth_r = oracle_forward(sc, rays)
     assert rel(rgb, rgb_r) < FWD_TOL
     assert rel(acc, acc_r) < FWD_TOL
@@ -39,14 +43,16 @@ def test_forward_matches_oracle(cuda, kind):
     assert e1 < FWD_TOL and e2 < FWD_TOL
 
 
+@pytest.mark.parametrize("schedule", SCHEDULES)
 @pytest.mark.parametrize("kind", KINDS)
-def test_backward_matches_float64_autograd(cuda, kind):
+def test_backward_matches_float64_autograd(cuda, kind, schedule):
     sc, rays = small_workload(kind, n_strokes=16, n_rays=64, n_samples=40, seed=3)
     g = torch.Generator().manual_seed(7)
     g_rgb = torch.randn(rays.n_rays, 3, generator=g)
     g_acc = torch.randn(rays.n_rays, generator=g)
     g_depth = depth_upstream(sc, rays, g)
-    (rgb, acc, depth), (x, sp, col, den, dl) = run_field(sc, rays, cuda, requires_grad=True)
+    (rgb, acc, depth), (x, sp, col, den, dl) = run_field(sc, rays, cuda, requires_grad=True,
+                                                         opts=FieldOptions(schedule=schedule))
     L = (rgb * g_rgb.to(cuda)).sum() + (acc * g_acc.to(cuda)).sum() + (depth * g_depth.to(cuda)).sum()
     L.backward()
     ref = oracle_grads(sc, rays, g_rgb, g_acc, g_depth)
@@ -73,23 +79,47 @@ def test_config0_forward(cuda):
     assert e1 < FWD_TOL and e2 < FWD_TOL
 
 
-def test_culling_is_invisible(cuda):
+@pytest.mark.parametrize("schedule", SCHEDULES)
+def test_culling_is_invisible(cuda, schedule):
     sc, rays = small_workload("mixed", n_strokes=64, n_rays=256, n_samples=64, seed=11)
-    (a, acc_a, _), _ = run_field(sc, rays, cuda, opts=FieldOptions(cull_alpha=1e-9))
-    (b, acc_b, _), _ = run_field(sc, rays, cuda, opts=FieldOptions(cull_alpha=0.0))
+    (a, acc_a, _), _ = run_field(sc, rays, cuda, opts=FieldOptions(cull_alpha=1e-9, schedule=schedule))
+    (b, acc_b, _), _ = run_field(sc, rays, cuda, opts=FieldOptions(cull_alpha=0.0, schedule=schedule))
     assert rel(a, b) < 1e-6 and rel(acc_a, acc_b) < 1e-6
+
+
+@pytest.mark.parametrize("n_samples,shuffle", [(100, False), (64, True), (1, False), (33, True), (200, False)])
+def test_schedules_agree(cuda, n_samples, shuffle):
+    """Sample runs and 32-sample segments give the same outputs and gradients, also
+    for partial 64-sample units, single-sample rays and samples out of ray order
+    (which the run schedule must not cull by chord intervals)."""
+    sc, rays = small_workload("mixed", n_strokes=150, n_rays=40, n_samples=n_samples, seed=21)
+    if shuffle:
+        perm = torch.randperm(n_samples, generator=torch.Generator().manual_seed(4))
+        rays = scenes.RaySet(rays.origins, rays.dirs, rays.tdist, rays.x[:, perm].contiguous(),
+                             rays.radius[:, perm].contiguous())
+    g_rgb = torch.randn(rays.n_rays, 3, generator=torch.Generator().manual_seed(1)).to(cuda)
+    outs = []
+    for schedule in SCHEDULES:
+        (rgb, acc, depth), (x, sp, col, den, dl) = run_field(sc, rays, cuda, requires_grad=True,
+                                                             opts=FieldOptions(schedule=schedule))
+        ((rgb * g_rgb).sum() + acc.sum()).backward()
+        outs.append((rgb.detach(), acc.detach(), x.grad, sp.grad, col.grad, den.grad, dl.grad))
+    for a, b in zip(*outs):
+        assert rel(a, b) < 1e-5
 
 
 def test_multipass_matches_single_pass(cuda):
     sc, rays = small_workload("mixed", n_strokes=100, n_rays=96, n_samples=70, seed=5)
     g_rgb = torch.randn(rays.n_rays, 3, generator=torch.Generator().manual_seed(1)).to(cuda)
     outs = []
-    for opts in (FieldOptions(), FieldOptions(chunk_fwd=32, chunk_bwd=32)):
+    for opts in (FieldOptions(), FieldOptions(chunk_fwd=32, chunk_bwd=32),
+                 FieldOptions(chunk_fwd=32, chunk_bwd=32, schedule="segments")):
         (rgb, acc, depth), (x, sp, col, den, dl) = run_field(sc, rays, cuda, opts=opts, requires_grad=True)
         (rgb * g_rgb).sum().backward()
         outs.append((rgb.detach(), x.grad, sp.grad, col.grad, den.grad, dl.grad))
-    for a, b in zip(*outs):
-        assert rel(a, b) < 1e-5
+    for other in outs[1:]:
+        for a, b in zip(other, outs[0]):
+            assert rel(a, b) < 1e-5
 
 
 def test_batched_scenes_match_individual(cuda):
