@@ -208,7 +208,8 @@ def run_reference(args, world, rank):
     threads = os.cpu_count() or 1
     torch.set_num_threads(threads)
     g = torch.Generator().manual_seed(5)
-    # one step = a bounded ray sample of every scene (sized for ~2-4 s of CPU work)
+    # one step = a bounded ray sample of every scene, sized by the first (warm-up) step
+    # to ~3 s of CPU work
     n = 4 if args.config in (3, 4) else 16
     rates = []
     for it in range(args.warmup + args.steps):
@@ -225,8 +226,8 @@ def run_reference(args, world, rank):
         dt = time.perf_counter() - t0
         if it >= args.warmup:
             rates.append(pairs / dt)
-        if it == 0 and dt > 20 and n > 1:
-            n = max(1, n // 4)
+        if it == 0:
+            n = max(1, min(max(r.n_rays for r in w.rays), int(n * 3.0 / max(dt, 1e-3))))
     value = statistics.mean(rates)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,

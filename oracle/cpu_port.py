@@ -168,20 +168,21 @@ def plain_op_train(ref, scenes, rays, targets, steps, lr=1e-3, betas=(0.9, 0.99)
     for _ in range(steps):
         loss = 0.0
         grads = []
-        with torch.no_grad():
-            for s, r, t in zip(scenes, rays, targets):
-                det = copy.copy(s)
-                det.shape_params, det.color_params, det.density = (s.shape_params.detach(), s.color_params.detach(),
-                                                                  s.density.detach())
-                zr = torch.zeros(r.n_rays, 3, device=t.device)
-                z = torch.zeros(r.n_rays, device=t.device)
-                rgb = plain_op_step(ref, det, r.x, r.radius, r.tdist, r.dirs, zr, z, z, delta, laplace, inv)[0]
-                diff = rgb - t
-                loss += float((diff * diff).sum())
-                g_rgb = diff * (2.0 / n_total)
-                _, _, _, gs, gc, gd = plain_op_step(ref, det, r.x, r.radius, r.tdist, r.dirs, g_rgb, z, z, delta,
-                                                    laplace, inv)
-                grads += [gs, gc, gd]
+        # plain_op_step differentiates the render math with torch autograd itself; the
+        # stroke parameters go in detached (their gradients come from the reference op)
+        for s, r, t in zip(scenes, rays, targets):
+            det = copy.copy(s)
+            det.shape_params, det.color_params, det.density = (s.shape_params.detach(), s.color_params.detach(),
+                                                              s.density.detach())
+            zr = torch.zeros(r.n_rays, 3, device=t.device)
+            z = torch.zeros(r.n_rays, device=t.device)
+            rgb = plain_op_step(ref, det, r.x, r.radius, r.tdist, r.dirs, zr, z, z, delta, laplace, inv)[0]
+            diff = rgb - t
+            loss += float((diff * diff).sum())
+            g_rgb = diff * (2.0 / n_total)
+            _, _, _, gs, gc, gd = plain_op_step(ref, det, r.x, r.radius, r.tdist, r.dirs, g_rgb, z, z, delta,
+                                                laplace, inv)
+            grads += [gs, gc, gd]
         losses.append(loss / n_total)
         for p, g in zip(params, grads):
             p.grad = torch.nan_to_num(g)
