@@ -5,8 +5,8 @@ on its own data for each candidate launch configuration and keeps the fastest:
 
 * work decomposition (``schedule``): 32-sample segments with every lane evaluating
   each surviving stroke, or 64-sample units with packed (sample, stroke) pairs;
-* warps per CTA (rays in flight per SM): the defaults (24 forward / 16 backward for
-  segments, 16 for runs) or 8;
+* warps per CTA (rays in flight per SM), forward and backward separately (the
+  segment kernels fit 32 / 24 warps, the run kernels 16);
 * strokes per shared-memory stage: the largest that fits, or half of it (more passes,
   less shared memory per CTA).
 
@@ -29,6 +29,7 @@ from .field import FieldOptions
 
 _lock = threading.Lock()
 _memo: Dict[str, dict] = {}
+last_results: List[tuple] = []  # (milliseconds, options) of the last tuning pass
 
 
 def signature(field) -> str:
@@ -42,13 +43,15 @@ def signature(field) -> str:
 
 def candidates(grad_mode: str = "exact", cull_alpha: float = 1e-9) -> List[FieldOptions]:
     out = []
-    for schedule in ("segments", "runs"):
-        for warps in (0, 8):  # 0: 24 forward / 16 backward warps (segments), 16 (runs)
-            for half in (False, True):
-                # chunk 0 = the largest stage that fits; the halved stage is set below
-                out.append(FieldOptions(cull_alpha=cull_alpha, warps=warps, schedule=schedule,
-                                        grad_mode=grad_mode, chunk_fwd=-1 if half else 0,
-                                        chunk_bwd=-1 if half else 0))
+    # (schedule, forward warps, backward warps): the segment kernels' register use
+    # allows up to 32 / 24 warps per CTA, the run kernels 16
+    shapes = [("segments", 32, 24), ("segments", 32, 20), ("segments", 24, 16), ("segments", 16, 16),
+              ("runs", 16, 16)]
+    for schedule, wf, wb in shapes:
+        for half in (False, True):
+            # chunk 0 = the largest stage that fits; the halved stage (-1) is resolved later
+            out.append(FieldOptions(cull_alpha=cull_alpha, warps=wf, warps_bwd=wb, schedule=schedule,
+                                    grad_mode=grad_mode, chunk_fwd=-1 if half else 0, chunk_bwd=-1 if half else 0))
     return out
 
 
@@ -121,8 +124,10 @@ def tune(field, reps: int = 3, cands: Optional[List[FieldOptions]] = None, use_c
         ms = _time_step(field, reps)
         results.append((ms, opt))
         if verbose:
-            print(f"autotune {opt.schedule:8s} warps={opt.warps:2d} chunk={opt.chunk_fwd}/{opt.chunk_bwd}: "
+            print(f"autotune {opt.schedule:8s} warps={opt.warps:2d}/{opt.warps_bwd:2d} "
+                  f"chunk={opt.chunk_fwd}/{opt.chunk_bwd}: "
                   f"{ms:.3f} ms", flush=True)
+    last_results[:] = results
     ms, best = min(results, key=lambda t: t[0])
     field.options = best
     field._bind()

@@ -2,6 +2,7 @@
 // planning and kernel dispatch. Allocates nothing; every launch goes to the caller's
 // stream; no host synchronisation except in n3ds_field_read_status.
 #include <algorithm>
+#include <initializer_list>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -110,9 +111,20 @@ Resolved resolve(const n3ds_options_t* o) {
   const bool runs = r.schedule == N3DS_SCHEDULE_RUNS;
   // 24 warps only for the forward segment kernel (76 registers); the others hold
   // 100+ registers per thread and run at most 16
-  auto pick = [](int w, bool allow24) { return allow24 && w >= 24 ? 24 : w >= 16 ? 16 : w >= 8 ? 8 : 4; };
-  r.warps_fwd = pick(o->warps > 0 ? o->warps : 24, !runs);
-  r.warps_bwd = pick(o->warps > 0 ? o->warps : 16, false);
+  // instantiated CTA sizes: segment forward 4-32 warps (64 registers), segment backward
+  // 4-24 (94 registers at 20 warps, 80 with a small spill at 24), run kernels 4-16
+  // largest instantiated CTA size not above the request
+  auto pick = [](int w, std::initializer_list<int> sizes) {
+    int best = 4;
+    for (int s : sizes)
+      if (s <= w && s > best) best = s;
+    return best;
+  };
+  // defaults: the fastest measured on the benchmark workloads (32 / 24 for segments)
+  const int wf = o->warps > 0 ? o->warps : (runs ? 16 : 32);
+  const int wb = o->warps_bwd > 0 ? o->warps_bwd : (runs ? 16 : 24);
+  r.warps_fwd = runs ? pick(wf, {4, 8, 16}) : pick(wf, {4, 8, 16, 24, 32});
+  r.warps_bwd = runs ? pick(wb, {4, 8, 16}) : pick(wb, {4, 8, 16, 20, 24});
   r.warps = r.warps_bwd;
   const size_t budget = size_t(di.smem_optin) - 256;  // room for static shared memory
   // default stages: the largest multiple of 32 strokes that fits the shared memory
@@ -254,6 +266,7 @@ void n3ds_default_options(n3ds_options_t* opt) {
   opt->schedule = 0;
   opt->grad_mode = N3DS_GRAD_EXACT;
   opt->timing_events = nullptr;
+  opt->warps_bwd = 0;
 }
 
 size_t n3ds_field_workspace_bytes(const n3ds_batch_t* batch, const n3ds_options_t* opt) {
@@ -435,7 +448,8 @@ int n3ds_field_resolve_options(const n3ds_options_t* opt, n3ds_options_t* out) {
   *out = *o;
   out->chunk_fwd = rv.chunk_fwd;
   out->chunk_bwd = rv.chunk_bwd;
-  out->warps = o->warps;  // 0 (auto) stays: the directions differ (24 / 16 warps)
+  out->warps = rv.warps_fwd;
+  out->warps_bwd = rv.warps_bwd;
   out->schedule = rv.schedule;
   out->grad_mode = rv.grad_mode;
   return N3DS_OK;

@@ -86,14 +86,13 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_con
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t bar;
   __shared__ int s_scene, s_fail;
-  __shared__ unsigned long long s_kcount[16];  // evaluated (sample, stroke) pairs per base
   const Stage S = carve(smem, L.chunk_cap, false);
   const int lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     mbar_init(&bar, 1);
     s_fail = 0;
   }
-  if (threadIdx.x < 16) s_kcount[threadIdx.x] = 0ull;
+  unsigned long long kcount = 0;  // lane k: evaluated (sample, stroke) pairs of base k
   uint32_t phase = 0;
   int sci = home_scene(L);
   while (sci >= 0) {
@@ -124,8 +123,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_con
             const int b = __ffs(mask) - 1;
             mask &= mask - 1;
             const float* rec = S.recs + size_t(hi - b) * REC_FLOATS;
-            if (lane == 0) atomicAdd(&s_kcount[__float_as_int(rec[R_KIND]) & 15], (unsigned long long)nact);
             const float a = pair_alpha(rec, c.x, c.rinv);
+            if (lane == (__float_as_int(rec[R_KIND]) & 15)) kcount += nact;
             const float w = a * T;
             const float4 col = rec4(rec)[R_COLOR / 4];
             T *= (1.0f - a);
@@ -148,9 +147,9 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_con
     __syncthreads();
     sci = s_scene;
   }
-  if (L.stats && threadIdx.x < 16 && s_kcount[threadIdx.x]) {
-    atomicAdd(L.stats, s_kcount[threadIdx.x]);
-    atomicAdd(L.stats + 1 + threadIdx.x, s_kcount[threadIdx.x]);
+  if (L.stats && lane < 16 && kcount) {
+    atomicAdd(L.stats, kcount);
+    atomicAdd(L.stats + 1 + lane, kcount);
   }
 }
 
@@ -801,6 +800,7 @@ cudaError_t launch_seg_fwd(const SegLaunch& L, int grid, int warps, size_t smem,
     case 8: return launch_fwd_w<8>(L, grid, smem, st);
     case 16: return launch_fwd_w<16>(L, grid, smem, st);
     case 24: return launch_fwd_w<24>(L, grid, smem, st);
+    case 32: return launch_fwd_w<32>(L, grid, smem, st);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -809,6 +809,8 @@ cudaError_t launch_seg_bwd(const SegLaunch& L, int grid, int warps, size_t smem,
     case 4: return launch_bwd_w<4>(L, grid, smem, st);
     case 8: return launch_bwd_w<8>(L, grid, smem, st);
     case 16: return launch_bwd_w<16>(L, grid, smem, st);
+    case 20: return launch_bwd_w<20>(L, grid, smem, st);
+    case 24: return launch_bwd_w<24>(L, grid, smem, st);
     default: return cudaErrorInvalidValue;
   }
 }

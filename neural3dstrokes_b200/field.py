@@ -23,7 +23,8 @@ class FieldOptions:
     cull_alpha: float = 1e-9   # strokes whose alpha provably stays below this are skipped; 0 disables
     chunk_fwd: int = 0         # strokes per shared-memory stage (0: auto)
     chunk_bwd: int = 0
-    warps: int = 0             # warps per CTA: 4, 8, 16 (0: auto)
+    warps: int = 0             # warps per CTA, forward: 4, 8, 16, 24, 32 (0: auto)
+    warps_bwd: int = 0         # warps per CTA, backward: 4, 8, 16, 20, 24 (0: auto)
     schedule: str = "auto"     # 'segments' (auto): lane = sample; 'runs': packed (sample, stroke) pairs
     grad_mode: str = "exact"   # 'exact' or 'compat'
 
@@ -40,7 +41,8 @@ class FieldOptions:
             self._ev_keepalive = arr
         return _lib.Options(float(self.cull_alpha), int(self.chunk_fwd), int(self.chunk_bwd), int(self.warps),
                             {"auto": 0, "segments": 1, "runs": 2}[self.schedule],
-                            _lib.N3DS_GRAD_COMPAT if self.grad_mode == "compat" else _lib.N3DS_GRAD_EXACT, ev)
+                            _lib.N3DS_GRAD_COMPAT if self.grad_mode == "compat" else _lib.N3DS_GRAD_EXACT, ev,
+                            int(self.warps_bwd))
 
 
 class _Native:

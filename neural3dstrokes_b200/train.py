@@ -188,3 +188,77 @@ class GraphedTrainer:
         if self.graph is None:
             self.capture()
         self.graph.replay()
+
+
+class HostPipeline:
+    """Run a captured step on batches that live in pinned host memory, overlapping the
+    copies with the compute of the neighbouring steps.
+
+    ``inputs`` / ``outputs``: the device tensors the captured step reads / writes
+    (for a BatchedField: rays, upstream gradients, parameters / rgb, acc, depth,
+    parameter gradients). A copy stream uploads step i+1's host inputs into one of two
+    device staging sets while step i computes; the compute stream copies the staged
+    inputs into the step's own buffers (device to device), replays the step and copies
+    the results into an output staging set, which the copy stream downloads to the
+    host. Events order every hand-over. Usage::
+
+        pipe.upload(0, host_in)
+        for i in range(n):
+            if i + 1 < n:
+                pipe.upload(i + 1, host_in_next)
+            pipe.run(i, host_out)
+        pipe.synchronize()
+    """
+
+    def __init__(self, graph, inputs, outputs, device):
+        self.graph = graph
+        self.inputs = list(inputs)
+        self.outputs = list(outputs)
+        self.device = torch.device(device)
+        self.compute = torch.cuda.current_stream(self.device)
+        self.copy = torch.cuda.Stream(self.device)
+        self.stage_in = [[torch.empty_like(t) for t in self.inputs] for _ in range(2)]
+        self.stage_out = [[torch.empty_like(t) for t in self.outputs] for _ in range(2)]
+        self.loaded = [torch.cuda.Event() for _ in range(2)]   # upload into input stage k done
+        self.taken = [torch.cuda.Event() for _ in range(2)]    # input stage k copied into the step buffers
+        self.stored = [torch.cuda.Event() for _ in range(2)]   # results copied into output stage k
+        self.fetched = [torch.cuda.Event() for _ in range(2)]  # output stage k downloaded
+        self.taken_used = [False, False]
+        self.fetched_used = [False, False]
+
+    def upload(self, step, host_inputs):
+        """Queue the upload of step ``step``'s inputs (before ``run(step)``, after
+        ``run(step - 2)``)."""
+        k = step % 2
+        if self.taken_used[k]:
+            self.copy.wait_event(self.taken[k])
+        with torch.cuda.stream(self.copy):
+            for d, h in zip(self.stage_in[k], host_inputs):
+                d.copy_(h, non_blocking=True)
+        self.loaded[k].record(self.copy)
+
+    def run(self, step, host_outputs):
+        """Queue step ``step`` on its uploaded inputs and the download of its results."""
+        k = step % 2
+        c = self.compute
+        c.wait_event(self.loaded[k])
+        for d, s in zip(self.inputs, self.stage_in[k]):
+            d.copy_(s, non_blocking=True)
+        self.taken[k].record(c)
+        self.taken_used[k] = True
+        self.graph.replay()
+        if self.fetched_used[k]:
+            c.wait_event(self.fetched[k])
+        for s, d in zip(self.stage_out[k], self.outputs):
+            s.copy_(d, non_blocking=True)
+        self.stored[k].record(c)
+        self.copy.wait_event(self.stored[k])
+        with torch.cuda.stream(self.copy):
+            for h, s in zip(host_outputs, self.stage_out[k]):
+                h.copy_(s, non_blocking=True)
+        self.fetched[k].record(self.copy)
+        self.fetched_used[k] = True
+
+    def synchronize(self):
+        self.copy.synchronize()
+        self.compute.synchronize()
