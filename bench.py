@@ -35,17 +35,22 @@ METRIC = "fwd+bwd stroke√ósample evals/s on 1 B200: batched+graph vs plain op @‚
 UNIT = "evals/s"
 
 # Algorithmic FP32 flops per evaluated (sample, stroke) pair, forward: inverse
-# transform + SDF + 15 (soft step 4 + over-composite 11); sphere transform is 6
-# (translate + scale only), the Beziers have none. Backward = 2.5 x forward
-# (recompute, adjoint of each step, reduction share). Survey 8(d) table.
+# transform + SDF + 15 (soft step 4 + over-composite 11); transforms without rotation
+# (sphere, aacube, aabb) are 6, the curves have none; a per-axis scale under
+# inv_scale_radius adds 10 for the radius factor. Backward = 2.5 x forward
+# (recompute, adjoint of each step, reduction share). Survey 8(d) table; capped
+# torus, line and triangular prism counted the same way from their SDFs (16, 17, 10).
 FWD_FLOPS_BY_KIND = {
-    "sphere": 6 + 6 + 15, "ellipsoid": 21 + 6 + 10 + 15, "cube": 21 + 14 + 15, "roundcube": 21 + 16 + 15,
-    "capsule": 21 + 9 + 15, "octahedron": 21 + 6 + 15, "tetrahedron": 21 + 8 + 15,
-    "quadratic_bezier": 75 + 15, "cubic_bezier": 190 + 15,
+    "sphere": 6 + 6 + 15, "ellipsoid": 21 + 6 + 10 + 15, "aacube": 6 + 14 + 15, "cube": 21 + 14 + 15,
+    "aabb": 6 + 14 + 10 + 15, "obb": 21 + 14 + 10 + 15, "roundcube": 21 + 16 + 15, "roundbox": 21 + 16 + 10 + 15,
+    "cappedtorus": 21 + 16 + 15, "capsule": 21 + 9 + 15, "scapsule": 21 + 9 + 10 + 15, "line": 21 + 17 + 15,
+    "triprism": 21 + 10 + 15, "octahedron": 21 + 6 + 15, "tetrahedron": 21 + 8 + 15,
+    "quadratic_bezier": 75 + 15, "cubic_bezier": 190 + 15, "catmull_rom": 190 + 15,
 }
 BWD_FACTOR = 2.5
-KIND_BASE = {"sphere": 0, "ellipsoid": 0, "cube": 1, "roundcube": 2, "capsule": 4, "octahedron": 7,
-             "tetrahedron": 8, "quadratic_bezier": 9, "cubic_bezier": 10}
+KIND_BASE = {"sphere": 0, "ellipsoid": 0, "aacube": 1, "cube": 1, "aabb": 1, "obb": 1, "roundcube": 2,
+             "roundbox": 2, "cappedtorus": 3, "capsule": 4, "scapsule": 4, "line": 5, "triprism": 6,
+             "octahedron": 7, "tetrahedron": 8, "quadratic_bezier": 9, "cubic_bezier": 10, "catmull_rom": 11}
 CLOCK_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")

@@ -30,7 +30,7 @@ typedef struct CUstream_st* n3ds_stream_t; /* = cudaStream_t */
 
 #define N3DS_OK 0
 #define N3DS_ERR_INVALID 1     /* bad argument (shape, null pointer, size) */
-#define N3DS_ERR_UNSUPPORTED 2 /* sdf_id / colour type outside the implemented set */
+#define N3DS_ERR_UNSUPPORTED 2 /* colour type or output outside the implemented set */
 #define N3DS_ERR_CUDA 3        /* a CUDA call failed */
 #define N3DS_ERR_WORKSPACE 4   /* workspace too small */
 #define N3DS_ERR_DEVICE 5      /* a kernel reported a device-side error status */
@@ -169,12 +169,13 @@ typedef struct n3ds_options {
   float cull_alpha;   /* drop a stroke where its alpha provably stays below this; <= 0: no culling */
   int32_t chunk_fwd;  /* strokes per shared-memory stage, forward (0 = auto) */
   int32_t chunk_bwd;  /* strokes per shared-memory stage, backward (0 = auto) */
-  int32_t warps;      /* warps per CTA: 4, 8 or 16 (0 = auto) */
+  int32_t warps;      /* warps per CTA, forward: 4, 8, 16, 24, 32 (0 = auto) */
   int32_t schedule;   /* N3DS_SCHEDULE_* (0 = auto: segments) */
   int32_t grad_mode;  /* N3DS_GRAD_EXACT or N3DS_GRAD_COMPAT */
   /* optional: 4 cudaEvent_t recorded on the stream around the segment kernels
    * (forward begin/end, backward begin/end), or NULL */
   void* const* timing_events;
+  int32_t warps_bwd;  /* warps per CTA, backward: 4, 8, 16, 20, 24 (0 = auto) */
 } n3ds_options_t;
 
 /* Fill *opt with the defaults. */

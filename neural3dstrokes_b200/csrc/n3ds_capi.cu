@@ -534,9 +534,7 @@ int check_stroke_args(uint32_t sdf_id, uint32_t color_id, int64_t n_points, int6
   if (color_id != 0) return fail(N3DS_ERR_UNSUPPORTED, "only color_id 0 (constant_rgb) is implemented");
   const int base = (int)(sdf_id >> 4);
   if (!n3ds::base_supported(base))
-    return fail(N3DS_ERR_UNSUPPORTED, "sdf base " + std::to_string(base) +
-                                          " is outside the implemented set (sphere, cube, round cube, capsule, "
-                                          "octahedron, tetrahedron, quadratic and cubic Bezier)");
+    return fail(N3DS_ERR_INVALID, "sdf base " + std::to_string(base) + " does not exist (bases 0-11)");
   if (base > n3ds::B_TETRAHEDRON && (sdf_id & 15u))
     return fail(N3DS_ERR_UNSUPPORTED, "Bezier strokes take no transform flags");
   if (n_texcoord != 0) return fail(N3DS_ERR_UNSUPPORTED, "texcoord output is not implemented");

@@ -35,14 +35,14 @@ __device__ __forceinline__ float pair_alpha(const float* rec, V3 x, float rinv, 
   float sdf, f = 1.f;
   if (base <= B_TETRAHEDRON) {
     V3 p = prim_local(rec, x);
-    sdf = prim_sdf(base, p, rec[R_BP]);
-    if (kind & K_S3FAC) f = s3_factor(base, p, xyz(rec4(rec)[R_S / 4]));
+    sdf = prim_sdf(base, p, rec);
+    if (kind & K_S3FAC) f = s3_factor(base, p, xyz(rec4(rec)[R_S / 4]), rec);
   } else if (base == B_QUAD_BEZIER) {
     QuadFwd q;
     sdf = quad_eval(rec, x, q);
   } else {
     CubicFwd c;
-    sdf = cubic_eval(rec, x, c);
+    sdf = cubic_eval(rec, x, c, base == B_CATMULL_ROM);
   }
   if (sdf_out) *sdf_out = sdf;
   if (mode == STEP_HARD) return sdf <= 0.f ? 1.f : 0.f;
@@ -79,20 +79,39 @@ __device__ __forceinline__ V3 prim_backprop(const float* rec, int kind, V3 p, fl
                                             float* v, int compat) {
   int base = kind & 15;
   int flags = (kind >> 4) & 15;
-  float gbpu;
-  V3 gp = prim_grad(base, p, rec[R_BP], &gbpu, compat) * dsdf;
-  v[G_BP] += gbpu * dsdf;
+  float gbp[2];
+  V3 gp = prim_grad(base, p, rec, gbp, compat) * dsdf;
+  v[G_BP] += gbp[0] * dsdf;
+  v[G_BP2] += gbp[1] * dsdf;
   V3 s = xyz(rec4(rec)[R_S / 4]), si = xyz(rec4(rec)[R_SINV / 4]);
   V3 q = s * p;
   float kfac = compat ? 0.f : K;
-  if ((kind & K_S3FAC) && !compat && base == B_SPHERE) {
-    // f = |q|/|p|: dL/dp += K (s^2 p/|q|^2 - p/|p|^2); dL/ds_i += K p_i^2 s_i/|q|^2
-    float pp = dot(p, p), qq = dot(q, q);
-    gp += (s * q) * (K / qq) + p * (-K / pp);
-    V3 hs = (p * q) * (K / qq);
-    v[G_SCALE + 0] += hs.x;
-    v[G_SCALE + 1] += hs.y;
-    v[G_SCALE + 2] += hs.z;
+  if ((kind & K_S3FAC) && !compat) {
+    if (base == B_SPHERE) {
+      // f = |q|/|p|: dL/dp += K (s^2 p/|q|^2 - p/|p|^2); dL/ds_i += K p_i^2 s_i/|q|^2
+      float pp = dot(p, p), qq = dot(q, q);
+      gp += (s * q) * (K / qq) + p * (-K / pp);
+      V3 hs = (p * q) * (K / qq);
+      v[G_SCALE + 0] += hs.x;
+      v[G_SCALE + 1] += hs.y;
+      v[G_SCALE + 2] += hs.z;
+    } else {
+      // f = |s g| / |g| with g the reference gradient (s3_factor): d ln f / ds_i =
+      // s_i g_i^2 / |s g|^2, d ln f / dg = s^2 g / |s g|^2 - g / |g|^2
+      float unused[2];
+      const V3 g = prim_grad(base, p, rec, unused, 1);
+      const V3 s2g = s * s * g;
+      const float ff = dot(s2g, g), gg = dot(g, g);
+      if (ff > 0.f && gg > 0.f) {
+        const V3 hs = (s * g * g) * (K / ff);
+        v[G_SCALE + 0] += hs.x;
+        v[G_SCALE + 1] += hs.y;
+        v[G_SCALE + 2] += hs.z;
+        float gb0;
+        gp += s3_dir_adjoint(base, p, rec, s2g * (1.f / ff) - g * (1.f / gg), &gb0) * K;
+        v[G_BP] += gb0 * K;
+      }
+    }
   }
   if (flags & F_S1) {
     v[G_SCALE] += (-dot(gp, p) + ((kind & K_S1K) ? kfac : 0.f)) * si.x;

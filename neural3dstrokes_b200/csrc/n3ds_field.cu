@@ -302,8 +302,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
   #pragma unroll
               for (int j = 0; j < 16; j++) v[j] = 0.f;
               const V3 p = prim_local(rec, c.x);
-              const float sdf = prim_sdf(base, p, rec[R_BP]);
-              const float f = (kind & K_S3FAC) ? s3_factor(base, p, xyz(rec4(rec)[R_S / 4])) : 1.f;
+              const float sdf = prim_sdf(base, p, rec);
+              const float f = (kind & K_S3FAC) ? s3_factor(base, p, xyz(rec4(rec)[R_S / 4]), rec) : 1.f;
               const float kk = h.y * f * c.rinv;
               const float m = -sdf * kk;
               const float a = mode == STEP_HARD ? (sdf <= 0.f ? 1.f : 0.f) : soft_alpha(mode, m);
@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
   #pragma unroll
               for (int j = 0; j < 32; j++) v[j] = 0.f;
               CubicFwd cf;
-              const float sdf = cubic_eval(rec, c.x, cf);
+              const float sdf = cubic_eval(rec, c.x, cf, base == B_CATMULL_ROM);
               const float kk = h.y * c.rinv;
               const float m = -sdf * kk;
               const float a = mode == STEP_HARD ? (sdf <= 0.f ? 1.f : 0.f) : soft_alpha(mode, m);
@@ -349,7 +349,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
               const float dm = compose_step(rec, a, m, mode, s, v, compat);
               const float dsdf = -kk * dm;
               v[G_K] += m * dm;
-              V3 g = cubic_adjoint(rec, c.x, cf, dsdf, v + G_CTRL, compat);
+              V3 g = cubic_adjoint(rec, c.x, cf, dsdf, v + G_CTRL, compat, base == B_CATMULL_ROM);
               if (compat) g = g * dsdf;  // the reference multiplies by dL/dSDF again
               gx += g;
               reduce_into<32>(v, row, lane);
@@ -615,6 +615,7 @@ __global__ void prep_kernel(const PrepLaunch P) {
   float rho0 = 1.f, Lg = 1.f, smax = fmaxf(sc.x, fmaxf(sc.y, sc.z)), smin = fminf(sc.x, fminf(sc.y, sc.z));
   V3 cw = t;
   float Rb;
+  bool bound_ok = true;  // false: no finite culling bound (the stroke is never culled)
   if (base <= B_TETRAHEDRON) {
     // M = S^-1 R^T: row i is column i of R divided by s_i; the row's w holds t_i
     const V3 mr[3] = {v3(R.r0.x, R.r1.x, R.r2.x) * (1.f / sc.x), v3(R.r0.y, R.r1.y, R.r2.y) * (1.f / sc.y),
@@ -628,12 +629,30 @@ __global__ void prep_kernel(const PrepLaunch P) {
     rec[R_S] = sc.x; rec[R_S + 1] = sc.y; rec[R_S + 2] = sc.z;
     rec[R_SINV] = 1.f / sc.x; rec[R_SINV + 1] = 1.f / sc.y; rec[R_SINV + 2] = 1.f / sc.z;
     const float bp = base_param_count(base) > 0 ? prm[0] : 0.f;
+    const float bp2 = base_param_count(base) > 1 ? prm[1] : 0.f;
     rec[R_BP] = bp;
+    rec[R_BP2] = bp2;
+    if (base == B_CAPPED_TORUS) {
+      rec[R_TSIN] = sinf(bp);
+      rec[R_TCOS] = cosf(bp);
+    }
+    // bounds sdf_local >= Lg (|p| - rho0): exact distances (Lg = 1) minus the largest
+    // radius; for the polytopes, the facet-distance maximum over the gauge of the body
+    // (inradius / circumradius)
     switch (base) {
       case B_SPHERE: rho0 = 1.f; Lg = 1.f; break;
       case B_CUBE: rho0 = 1.7320509f; Lg = 1.f; break;
       case B_ROUND_CUBE: rho0 = fmaxf(1.7320509f + bp, 0.f); Lg = 1.f; break;
+      case B_CAPPED_TORUS: rho0 = 1.f + fmaxf(bp2, 0.f); Lg = 1.f; break;
       case B_CAPSULE: rho0 = 1.f + fabsf(bp); Lg = 1.f; break;
+      case B_LINE: rho0 = fabsf(bp) + 1.f + fabsf(bp2); Lg = 1.f; break;
+      case B_TRIPRISM: {
+        const float rc = sqrtf(1.f + bp * bp);  // vertices (x, z) = (0, 1), (+-0.866, -0.5), |y| = h
+        rho0 = rc;
+        Lg = fminf(bp, 0.5f) / rc * 0.9999f;
+        bound_ok = bp > 0.f;
+        break;
+      }
       case B_OCTAHEDRON: rho0 = 1.f; Lg = 0.5773502f; break;
       case B_TETRAHEDRON: rho0 = 1.7320511f; Lg = 0.3333333f; break;
       default: break;
@@ -660,9 +679,31 @@ __global__ void prep_kernel(const PrepLaunch P) {
     Rb = rc + fmaxf(prm[9], prm[10]);
     smax = smin = 1.f;
   } else {
-    V3 P4[4];
+    // cubic Bezier: the control points; Catmull-Rom: its power-basis coefficients
+    // (A, B, C, D of t^3, t^2, t, 1, strokes_sdf.h:1340-1349). hull[] holds Bezier
+    // control points of the same curve for the culling bound (convex-hull property).
+    const bool power = base == B_CATMULL_ROM;
+    V3 P4[4], hull[4];
+    for (int k = 0; k < 4; k++) P4[k] = v3(prm[3 * k], prm[3 * k + 1], prm[3 * k + 2]);
+    if (power) {
+      const V3 p0 = P4[0], p1 = P4[1], p2 = P4[2], p3 = P4[3];
+      const float t01 = sqrtf(sqrtf(dot(p0 - p1, p0 - p1)) + 1e-8f);
+      const float t12 = sqrtf(sqrtf(dot(p1 - p2, p1 - p2)) + 1e-8f);
+      const float t23 = sqrtf(sqrtf(dot(p2 - p3, p2 - p3)) + 1e-8f);
+      const V3 m1 = (p2 - p1) + ((p1 - p0) / t01 - (p2 - p0) / (t01 + t12)) * t12;
+      const V3 m2 = (p2 - p1) + ((p3 - p2) / t23 - (p3 - p1) / (t12 + t23)) * t12;
+      P4[0] = (p1 - p2) * 2.0f + m1 + m2;
+      P4[1] = (p2 - p1) * 3.0f - m1 * 2.0f - m2;
+      P4[2] = m1;
+      P4[3] = p1;
+      hull[0] = p1;
+      hull[1] = p1 + m1 * (1.f / 3.f);
+      hull[2] = p2 - m2 * (1.f / 3.f);
+      hull[3] = p2;
+    } else {
+      for (int k = 0; k < 4; k++) hull[k] = P4[k];
+    }
     for (int k = 0; k < 4; k++) {
-      P4[k] = v3(prm[3 * k], prm[3 * k + 1], prm[3 * k + 2]);
       rec[R_CA + 4 * k] = P4[k].x; rec[R_CA + 4 * k + 1] = P4[k].y; rec[R_CA + 4 * k + 2] = P4[k].z;
     }
     rec[R_CR1] = prm[12];
@@ -671,14 +712,15 @@ __global__ void prep_kernel(const PrepLaunch P) {
     for (int i = 0; i <= CUBIC_SEGMENTS; i++) {
       const float ti = i * step;
       float w[4];
-      cubic_weights(ti, w);
+      curve_weights(ti, w, power);
       V3 v = P4[0] * w[0] + P4[1] * w[1] + P4[2] * w[2] + P4[3] * w[3];
       rec[R_CV + 3 * i] = v.x; rec[R_CV + 3 * i + 1] = v.y; rec[R_CV + 3 * i + 2] = v.z;
     }
-    cw = (P4[0] + P4[1] + P4[2] + P4[3]) * 0.25f;
+    cw = (hull[0] + hull[1] + hull[2] + hull[3]) * 0.25f;
     float rc = 0.f;
-    for (int k = 0; k < 4; k++) rc = fmaxf(rc, sqrtf(dot(P4[k] - cw, P4[k] - cw)));
-    Rb = rc + fmaxf(prm[12], prm[13]);
+    for (int k = 0; k < 4; k++) rc = fmaxf(rc, sqrtf(dot(hull[k] - cw, hull[k] - cw)));
+    // the polyline vertices are on the curve, inside the hull; the margin covers rounding
+    Rb = rc * 1.0001f + fmaxf(prm[12], prm[13]);
     smax = smin = 1.f;
   }
   // margin per unit sample radius: the soft-step argument m = sdf * k exceeds the
@@ -701,7 +743,7 @@ __global__ void prep_kernel(const PrepLaunch P) {
       cm = mcut * delta / (kappa * Lg);
     }
   }
-  if (!cull) Rb = __int_as_float(0x7f800000);
+  if (!cull || !bound_ok) Rb = __int_as_float(0x7f800000);
   P.cull_a[4 * s] = cw.x; P.cull_a[4 * s + 1] = cw.y; P.cull_a[4 * s + 2] = cw.z;
   P.cull_a[4 * s + 3] = Rb * 1.0001f + 1e-6f;
   P.cull_b[s] = cm * 1.0001f;
@@ -709,6 +751,7 @@ __global__ void prep_kernel(const PrepLaunch P) {
 
 __device__ void prim_param_grads(const FinalizeLaunch& F, long long s, int base, int flags, const float* g,
                                  const float* rec, float* out);
+__device__ void catmull_param_grads(const float* prm, const float* gc, int compat, float* out);
 
 // Convert reduced slots into gradients of the raw reference-layout parameters.
 __global__ void finalize_kernel(const FinalizeLaunch F) {
@@ -735,6 +778,8 @@ __global__ void finalize_kernel(const FinalizeLaunch F) {
     for (int j = 0; j < 11; j++) o[j] = g[G_CTRL + j];
   } else if (base == B_CUBIC_BEZIER) {
     for (int j = 0; j < 14; j++) o[j] = g[G_CTRL + j];
+  } else if (base == B_CATMULL_ROM) {
+    catmull_param_grads(F.shape_params + s * (long long)F.param_stride, g + G_CTRL, F.compat, o);
   } else if (base <= B_TETRAHEDRON) {
     prim_param_grads(F, s, base, flags, g, rec, o);
   }
@@ -749,6 +794,7 @@ __device__ void prim_param_grads(const FinalizeLaunch& F, long long s, int base,
   int off = 0;
   const int nb = base_param_count(base);
   if (nb > 0) out[0] = g[G_BP];
+  if (nb > 1) out[1] = g[G_BP2];
   off = nb;
   if (s1) { out[off] = g[G_SCALE]; off += 1; }
   else if (s3) { out[off] = g[G_SCALE]; out[off + 1] = g[G_SCALE + 1]; out[off + 2] = g[G_SCALE + 2]; off += 3; }
@@ -768,6 +814,88 @@ __device__ void prim_param_grads(const FinalizeLaunch& F, long long s, int base,
     for (int j = 0; j < 3; j++)
       out[off + j] = -(rec[R_M + j] * gx + rec[R_M + 4 + j] * gy + rec[R_M + 8 + j] * gz);
   }
+}
+
+// Catmull-Rom: gradients of the power-basis coefficients (gc[0..11] = dL/dA, B, C, D;
+// gc[12], gc[13] = dL/dr1, r2) -> gradients of the raw control points p0..p3 and radii.
+// Exact: reverse mode through A = 2(p1 - p2) + m1 + m2, B = 3(p2 - p1) - 2 m1 - m2,
+// C = m1, D = p1 and the centripetal tangents m1, m2 with knot gaps
+// t_ij = sqrt(|p_i - p_j| + 1e-8). compat: the reference's formulas
+// (strokes_sdf.h:1404-1437), which chain the knot gaps element-wise.
+__device__ void catmull_param_grads(const float* prm, const float* gc, int compat, float* out) {
+  const V3 p0 = ld3(prm), p1 = ld3(prm + 3), p2 = ld3(prm + 6), p3 = ld3(prm + 9);
+  const V3 gA = ld3(gc), gB = ld3(gc + 3), gC = ld3(gc + 6), gD = ld3(gc + 9);
+  const V3 d01 = p0 - p1, d12 = p1 - p2, d23 = p2 - p3;
+  const float l01 = sqrtf(dot(d01, d01)), l12 = sqrtf(dot(d12, d12)), l23 = sqrtf(dot(d23, d23));
+  const float t01 = sqrtf(l01 + 1e-8f), t12 = sqrtf(l12 + 1e-8f), t23 = sqrtf(l23 + 1e-8f);
+  V3 g0, g1 = gA * 2.f - gB * 3.f + gD, g2 = gB * 3.f - gA * 2.f, g3;
+  const V3 gm1 = gA - gB * 2.f + gC, gm2 = gA - gB;
+  if (compat) {
+    const float dm1_dp0 = t12 / (t01 + t12) - t12 / t01, dm1_dp1 = -1.f + t12 / t01,
+                dm1_dp2 = 1.f - t12 / (t01 + t12), dm2_dp1 = -1.f + t12 / (t12 + t23),
+                dm2_dp2 = 1.f - t12 / t23, dm2_dp3 = t12 / t23 - t12 / (t12 + t23);
+    const V3 dm1_dt01 = ((p2 - p0) / ((t01 + t12) * (t01 + t12)) - (p1 - p0) / (t01 * t01)) * t12;
+    const V3 dm1_dt12 = (p1 - p0) / t01 + (p2 - p0) * (t12 / ((t01 + t12) * (t01 + t12))) - (p2 - p0) / (t01 + t12);
+    const V3 dm2_dt12 = (p2 - p1) / t23 + (p3 - p1) * (t12 / ((t12 + t23) * (t12 + t23))) - (p3 - p1) / (t12 + t23);
+    const V3 dm2_dt23 = ((p2 - p3) / (t23 * t23) + (p3 - p1) / ((t12 + t23) * (t12 + t23))) * t12;
+    const V3 dt01 = d01 / (2.f * powf(dot(d01, d01) + 1e-8f, 0.75f));
+    const V3 dt12 = d12 / (2.f * powf(dot(d12, d12) + 1e-8f, 0.75f));
+    const V3 dt23 = d23 / (2.f * powf(dot(d23, d23) + 1e-8f, 0.75f));
+    g0 = gm1 * (dm1_dt01 * dt01 + dm1_dp0);
+    g1 += gm1 * (dm1_dt12 * dt12 - dm1_dt01 * dt01 + dm1_dp1) + gm2 * (dm2_dt12 * dt12 + dm2_dp1);
+    g2 += gm1 * (dm1_dp2 - dm1_dt12 * dt12) + gm2 * (dm2_dt23 * dt23 - dm2_dt12 * dt12 + dm2_dp2);
+    g3 = gm2 * (dm2_dp3 - dm2_dt23 * dt23);
+  } else {
+    g0 = v3(0.f, 0.f, 0.f);
+    g3 = v3(0.f, 0.f, 0.f);
+    float gt01 = 0.f, gt12 = 0.f, gt23 = 0.f;
+    // m1 = p2 - p1 + t12 (u - v), u = (p1 - p0) / t01, v = (p2 - p0) / (t01 + t12)
+    {
+      const V3 u = (p1 - p0) / t01, v = (p2 - p0) / (t01 + t12);
+      g2 += gm1;
+      g1 -= gm1;
+      gt12 += dot(gm1, u - v);
+      const V3 gu = gm1 * t12;
+      g1 += gu / t01;
+      g0 -= gu / t01;
+      gt01 -= dot(gu, p1 - p0) / (t01 * t01);
+      const float S = t01 + t12;
+      g2 -= gu / S;
+      g0 += gu / S;
+      const float gS = dot(gu, p2 - p0) / (S * S);
+      gt01 += gS;
+      gt12 += gS;
+    }
+    // m2 = p2 - p1 + t12 (u2 - v2), u2 = (p3 - p2) / t23, v2 = (p3 - p1) / (t12 + t23)
+    {
+      const V3 u = (p3 - p2) / t23, v = (p3 - p1) / (t12 + t23);
+      g2 += gm2;
+      g1 -= gm2;
+      gt12 += dot(gm2, u - v);
+      const V3 gu = gm2 * t12;
+      g3 += gu / t23;
+      g2 -= gu / t23;
+      gt23 -= dot(gu, p3 - p2) / (t23 * t23);
+      const float S = t12 + t23;
+      g3 -= gu / S;
+      g1 += gu / S;
+      const float gS = dot(gu, p3 - p1) / (S * S);
+      gt12 += gS;
+      gt23 += gS;
+    }
+    // t_ij = sqrt(|d_ij| + 1e-8), d_ij = p_i - p_j
+    if (l01 > 0.f) { const V3 q = d01 * (gt01 / (2.f * t01 * l01)); g0 += q; g1 -= q; }
+    if (l12 > 0.f) { const V3 q = d12 * (gt12 / (2.f * t12 * l12)); g1 += q; g2 -= q; }
+    if (l23 > 0.f) { const V3 q = d23 * (gt23 / (2.f * t23 * l23)); g2 += q; g3 -= q; }
+  }
+  const V3 gs[4] = {g0, g1, g2, g3};
+  for (int k = 0; k < 4; k++) {
+    out[3 * k] = gs[k].x;
+    out[3 * k + 1] = gs[k].y;
+    out[3 * k + 2] = gs[k].z;
+  }
+  out[12] = gc[12];
+  out[13] = gc[13];
 }
 
 // ================================================================ launchers

@@ -40,10 +40,11 @@ __host__ __device__ __forceinline__ int base_param_count(int base) {
     default: return 0;
   }
 }
-__host__ __device__ __forceinline__ bool base_supported(int base) {
-  return base == B_SPHERE || base == B_CUBE || base == B_ROUND_CUBE || base == B_CAPSULE ||
-         base == B_OCTAHEDRON || base == B_TETRAHEDRON || base == B_QUAD_BEZIER ||
-         base == B_CUBIC_BEZIER;
+__host__ __device__ __forceinline__ bool base_supported(int base) { return base >= 0 && base <= B_CATMULL_ROM; }
+// Curves evaluated through the polyline machinery (power-basis coefficients for
+// Catmull-Rom, Bernstein control points for the cubic Bezier).
+__host__ __device__ __forceinline__ bool base_is_cubic_curve(int base) {
+  return base == B_CUBIC_BEZIER || base == B_CATMULL_ROM;
 }
 // Shape-parameter count of a reference sdf_id (strokes.py:227-252).
 __host__ __device__ __forceinline__ int sdf_id_param_count(int sdf_id) {
@@ -65,19 +66,24 @@ constexpr int R_DENSITY = 2;
 constexpr int R_DELTA = 3;
 // q1: colour, base parameter (round-cube radius / capsule half-length)
 constexpr int R_COLOR = 4;     // 3
-constexpr int R_BP = 7;
+constexpr int R_BP = 7;        // first base parameter (round-cube radius, capsule / line half-length,
+                               // torus cap angle, prism half-height)
 // primitives
 constexpr int R_M = 8;         // q2..q4: rows (m_i0, m_i1, m_i2, t_i), p = M (x - t),
                                // M = S^-1 R^T (t is subtracted first: M x - M t cancels)
 constexpr int R_S = 20;        // q5: scale per axis
 constexpr int R_SINV = 24;     // q6: 1/scale per axis
+// second base parameter and derived constants (primitives; q7)
+constexpr int R_BP2 = 28;      // torus tube radius, line radius change
+constexpr int R_TSIN = 29, R_TCOS = 30;  // sin, cos of the torus cap angle
 // quadratic Bezier
 constexpr int R_QA = 8, R_QKK = 11;    // q2: A, 1/|b|^2
 constexpr int R_Qa = 12, R_QKX = 15;   // q3: a = B - A, kk (a.b)
 constexpr int R_Qb = 16, R_QAA2 = 19;  // q4: b = A - 2B + C, 2 |a|^2
 constexpr int R_Qc = 20, R_QAB = 23;   // q5: c = 2a, a.b
 constexpr int R_QR1 = 24, R_QR2 = 25;  // q6: radii
-// cubic Bezier
+// cubic Bezier (Bernstein control points A..D) / Catmull-Rom (power-basis
+// coefficients of t^3, t^2, t, 1, strokes_sdf.h:1333-1349)
 constexpr int R_CA = 8, R_CR1 = 11;    // q2: A, r1
 constexpr int R_CB = 12, R_CR2 = 15;   // q3: B, r2
 constexpr int R_CC = 16, R_CD = 20;    // q4, q5: C, D
@@ -96,10 +102,10 @@ constexpr int G_K = 4;         // sum dL/dk * k  (softness and scale-through-wid
 constexpr int G_GP = 5;        // 3: sum of dL/dp (local frame)
 constexpr int G_TORQUE = 8;    // 3: sum (S^-1 g_p) x (S p)
 constexpr int G_SCALE = 11;    // 3: per-axis scale gradient (S1 uses the first)
-constexpr int G_BP = 14;       // base parameter
-constexpr int G_PRIM_USED = 15;
+constexpr int G_BP = 14;       // first base parameter
+constexpr int G_BP2 = 15;      // second base parameter
 // Beziers: raw control-point and radius gradients
-constexpr int G_CTRL = 5;      // quad: 9 + r1, r2 (5..15); cubic: 12 + r1, r2 (5..18)
+constexpr int G_CTRL = 5;      // quad: 9 + r1, r2 (5..15); cubic / Catmull-Rom: 12 + r1, r2 (5..18)
 
 __device__ __forceinline__ V3 ld3(const float* p) { return v3(p[0], p[1], p[2]); }
 

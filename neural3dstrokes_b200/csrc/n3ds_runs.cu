@@ -559,8 +559,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) run_bwd_kernel(const __grid_con
             V3 g;
             if (bse <= B_TETRAHEDRON) {
               const V3 pl = prim_local(rec, x);
-              const float sdf = prim_sdf(bse, pl, rec[R_BP]);
-              const float f = (kind & K_S3FAC) ? s3_factor(bse, pl, xyz(rec4(rec)[R_S / 4])) : 1.f;
+              const float sdf = prim_sdf(bse, pl, rec);
+              const float f = (kind & K_S3FAC) ? s3_factor(bse, pl, xyz(rec4(rec)[R_S / 4]), rec) : 1.f;
               const float kk = h.y * f * rinv;
               const float m = -sdf * kk;
               const float K = m * dm;
@@ -574,11 +574,11 @@ __global__ void __launch_bounds__(WARPS * 32, 1) run_bwd_kernel(const __grid_con
               g = quad_adjoint(rec, qf, -kk * dm, v + G_CTRL);
             } else {
               CubicFwd cf;
-              const float sdf = cubic_eval(rec, x, cf);
+              const float sdf = cubic_eval(rec, x, cf, bse == B_CATMULL_ROM);
               const float kk = h.y * rinv;
               const float dsdf = -kk * dm;
               v[G_K] = -sdf * kk * dm;
-              g = cubic_adjoint(rec, x, cf, dsdf, v + G_CTRL, compat);
+              g = cubic_adjoint(rec, x, cf, dsdf, v + G_CTRL, compat, bse == B_CATMULL_ROM);
               if (compat) g = g * dsdf;  // the reference multiplies by dL/dSDF again
             }
             atomicAdd(gxb + 3 * j, g.x);

@@ -25,9 +25,31 @@ __device__ __forceinline__ V3 cube_inside_axis(V3 q, V3 sg) {
 }
 
 // ------------------------------------------------------------------ primitives
-// p is the local-frame sample, bp the base parameter.
+// p is the local-frame sample; base parameters are read from the record.
 
-__device__ __forceinline__ float prim_sdf(int base, V3 p, float bp) {
+constexpr float PRISM_C = 0.866025f;  // strokes_sdf.h:530
+
+// Capped torus term k (strokes_sdf.h:379-381): the cap test selects the projection on
+// the cap direction (sin a, cos a) or the distance to the axis.
+__device__ __forceinline__ bool torus_cap(float px, float py, float s, float c) { return px * c - py * s > 0.f; }
+
+// |p|^2 + 1 - 2k of the capped torus (strokes_sdf.h:382) without its cancellation near
+// the tube: (px - sin a)^2 + (py - cos a)^2 + pz^2 on the cap (sin^2 + cos^2 = 1), and
+// (k - 1)^2 + pz^2 - 1e-8 off it (k^2 = px^2 + py^2 + 1e-8); the same function, evaluated
+// to float32 accuracy where the reference's float32 form loses digits.
+__device__ __forceinline__ float torus_q(float px, float py, float pz, float s, float c, float* k) {
+  if (torus_cap(px, py, s, c)) {
+    *k = px * s + py * c;
+    const float dx = px - s, dy = py - c;
+    return dx * dx + dy * dy + pz * pz;
+  }
+  *k = sqrtf(px * px + py * py + 1e-8f);
+  const float d = *k - 1.f;
+  return d * d + pz * pz - 1e-8f;
+}
+
+__device__ __forceinline__ float prim_sdf(int base, V3 p, const float* rec) {
+  const float bp = rec[R_BP];
   switch (base) {
     case B_SPHERE:  // strokes_sdf.h:245-249
       return sqrtf(dot(p, p) + 1e-8f) - 1.f;
@@ -41,9 +63,25 @@ __device__ __forceinline__ float prim_sdf(int base, V3 p, float bp) {
       V3 qp = vmax0(q);
       return sqrtf(dot(qp, qp) + 1e-8f) + fminf(max3(q), 0.f) - bp;
     }
+    case B_CAPPED_TORUS: {  // 376-383
+      float k;
+      const float q = torus_q(fabsf(p.x), p.y, p.z, rec[R_TSIN], rec[R_TCOS], &k);
+      return sqrtf(q + 1e-8f) - rec[R_BP2];
+    }
     case B_CAPSULE: {  // 434-440
       p.y -= clampf(p.y, -bp, bp);
       return sqrtf(dot(p, p) + 1e-8f) - 1.f;
+    }
+    case B_LINE: {  // 473-482
+      const float rd = rec[R_BP2];
+      const float t = clampf((p.y + bp) / (2.0f * bp), 0.f, 1.f);
+      const float r = (1.f - rd) + t * ((1.f + rd) - (1.f - rd));
+      p.y -= clampf(p.y, -bp, bp);
+      return sqrtf(dot(p, p) + 1e-8f) - r;
+    }
+    case B_TRIPRISM: {  // 527-531
+      const V3 q = vabs(p);
+      return fmaxf(q.y - bp, fmaxf(q.x * PRISM_C + p.z * 0.5f, -p.z) - 0.5f);
     }
     case B_OCTAHEDRON:  // 584-588
       return (fabsf(p.x) + fabsf(p.y) + fabsf(p.z) - 1.f) * OCTA_K;
@@ -54,11 +92,15 @@ __device__ __forceinline__ float prim_sdf(int base, V3 p, float bp) {
   }
 }
 
-// Exact dSDF/dp of prim_sdf; *gbp receives dSDF/d(base parameter).
-// compat != 0 reproduces the reference's cube exterior formula 2*max(q,0)
-// (strokes_sdf.h:289) instead of the normalised one.
-__device__ __forceinline__ V3 prim_grad(int base, V3 p, float bp, float* gbp, int compat) {
-  *gbp = 0.f;
+// Exact dSDF/dp of prim_sdf; gbp[0], gbp[1] receive dSDF/d(base parameters).
+// compat != 0 reproduces the reference's own formulas where they differ: the cube
+// exterior 2*max(q,0) (strokes_sdf.h:289) and the capped torus, whose branch follows
+// k > 0 and whose distance-branch and angle terms are written differently there
+// (strokes_sdf.h:385-422).
+__device__ __forceinline__ V3 prim_grad(int base, V3 p, const float* rec, float* gbp, int compat) {
+  const float bp = rec[R_BP];
+  gbp[0] = 0.f;
+  gbp[1] = 0.f;
   switch (base) {
     case B_SPHERE: {
       float inv = rsqrtf(dot(p, p) + 1e-8f);
@@ -78,15 +120,62 @@ __device__ __forceinline__ V3 prim_grad(int base, V3 p, float bp, float* gbp, in
       V3 qp = vmax0(q);
       V3 g = sg * (qp * rsqrtf(dot(qp, qp) + 1e-8f));
       if (max3(q) < 0.f) g += cube_inside_axis(q, sg);
-      *gbp = -1.f;
+      gbp[0] = -1.f;
       return g;
+    }
+    case B_CAPPED_TORUS: {
+      const float px = fabsf(p.x), s = rec[R_TSIN], c = rec[R_TCOS];
+      gbp[1] = -1.f;
+      float k;
+      const float inv = rsqrtf(torus_q(px, p.y, p.z, s, c, &k) + 1e-8f);
+      if (compat) {
+        if (k > 0.f) {
+          gbp[0] = -(px * c + p.y * s);
+          return V3{p.x - sgn(p.x) * s, p.y - c, p.z} * inv;
+        }
+        return V3{2.f * p.x, 2.f * p.y, p.z} * inv;
+      }
+      float kx, ky, ka;
+      if (torus_cap(px, p.y, s, c)) {
+        kx = s; ky = c; ka = px * c - p.y * s;
+      } else {
+        kx = px / k; ky = p.y / k; ka = 0.f;
+      }
+      gbp[0] = -ka * inv;
+      return V3{p.x - sgn(p.x) * kx, p.y - ky, p.z} * inv;
     }
     case B_CAPSULE: {
       float y = p.y;
       p.y -= clampf(y, -bp, bp);
       float inv = rsqrtf(dot(p, p) + 1e-8f);
-      *gbp = -sgn(y) * p.y * inv;  // p.y == 0 on the straight part
+      gbp[0] = -sgn(y) * p.y * inv;  // p.y == 0 on the straight part
       return p * inv;
+    }
+    case B_LINE: {  // the reference formulas (strokes_sdf.h:484-508) are exact here
+      const float rd = rec[R_BP2];
+      const float y = p.y;
+      const float t = clampf((y + bp) / (2.0f * bp), 0.f, 1.f);
+      p.y -= clampf(y, -bp, bp);
+      V3 g = p * rsqrtf(dot(p, p) + 1e-8f);
+      if (-bp <= y && y <= bp) {
+        g.y = -rd / bp;
+        gbp[0] = y * rd / (bp * bp);
+      } else {
+        gbp[0] = g.y * (y > 0.f ? -1.f : 1.f);
+      }
+      gbp[1] = 1.f - 2.f * t;
+      return g;
+    }
+    case B_TRIPRISM: {  // strokes_sdf.h:533-569
+      const V3 q = vabs(p);
+      const float a = q.x * PRISM_C + p.z * 0.5f;
+      const bool first = a > -p.z;
+      const bool ytop = first ? (q.y - bp > a - 0.5f) : (q.y - bp > -p.z - 0.5f);
+      if (ytop) {
+        gbp[0] = -1.f;
+        return {0.f, sgn(p.y), 0.f};
+      }
+      return first ? V3{PRISM_C * sgn(p.x), 0.f, 0.5f} : V3{0.f, 0.f, -1.f};
     }
     case B_OCTAHEDRON:
       return vsgn(p) * OCTA_K;
@@ -107,16 +196,59 @@ __device__ __forceinline__ V3 prim_grad(int base, V3 p, float bp, float* gbp, in
 // Radius factor f of a multi-scale transform under inv_scale_radius
 // (strokes_forward.cu:74-81): f = |g*s| / |g| with g the SDF gradient direction.
 // For the sphere base g is parallel to p, so f = |s*p| / |p|.
-__device__ __forceinline__ float s3_factor(int base, V3 p, V3 s) {
+__device__ __forceinline__ float s3_factor(int base, V3 p, V3 s, const float* rec) {
   V3 g;
   if (base == B_SPHERE) {
     g = p;
   } else {
-    float unused;
-    g = prim_grad(base, p, 0.f, &unused, 0);
+    float unused[2];
+    g = prim_grad(base, p, rec, unused, 1);  // the reference's own gradient formulas
   }
   V3 gs = g * s;
   return sqrtf(dot(gs, gs)) / sqrtf(dot(g, g));
+}
+
+// (dg/dp)^T w for the unnormalised reference gradient g of s3_factor (compat
+// prim_grad), for the bases whose gradient direction varies with p; zero where g is
+// piecewise constant (cube and round-cube interiors, octahedron, tetrahedron, prism).
+// *gb0 receives w . dg/d(first base parameter) (the capsule half-length).
+// The capped torus and the line, which the reference never combines with a per-axis
+// scale, are treated as constant here.
+__device__ __forceinline__ V3 s3_dir_adjoint(int base, V3 p, const float* rec, V3 w, float* gb0) {
+  *gb0 = 0.f;
+  switch (base) {
+    case B_CUBE: {  // g = sgn(p) * 2 max(q, 0)
+      const V3 q = sub1(vabs(p), 1.f);
+      if (max3(q) <= 0.f) return {0.f, 0.f, 0.f};
+      return {q.x > 0.f ? 2.f * w.x : 0.f, q.y > 0.f ? 2.f * w.y : 0.f, q.z > 0.f ? 2.f * w.z : 0.f};
+    }
+    case B_ROUND_CUBE: {  // g = sgn(p) * qp / n outside
+      const V3 q = sub1(vabs(p), 1.f);
+      if (max3(q) < 0.f) return {0.f, 0.f, 0.f};
+      const V3 qp = vmax0(q), sg = vsgn(p);
+      const float inv = rsqrtf(dot(qp, qp) + 1e-8f);
+      const V3 u = qp * inv, sw = sg * w;
+      const V3 r = (sw - u * dot(u, sw)) * inv;
+      return {q.x > 0.f ? sg.x * r.x : 0.f, q.y > 0.f ? sg.y * r.y : 0.f, q.z > 0.f ? sg.z * r.z : 0.f};
+    }
+    case B_CAPSULE: {  // g = q / n with q = p - (0, clamp(y, -h, h), 0)
+      const float h = rec[R_BP];
+      const bool out = !(-h <= p.y && p.y <= h);
+      V3 q = p;
+      q.y -= clampf(p.y, -h, h);
+      const float inv = rsqrtf(dot(q, q) + 1e-8f);
+      const V3 u = q * inv;
+      V3 r = (w - u * dot(u, w)) * inv;
+      if (!out) {
+        r.y = 0.f;
+      } else {
+        *gb0 = -sgn(p.y) * r.y;  // q_y = y - sgn(y) h
+      }
+      return r;
+    }
+    default:
+      return {0.f, 0.f, 0.f};
+  }
 }
 
 // ---------------------------------------------------------- quadratic Bezier
@@ -300,13 +432,28 @@ __device__ __forceinline__ void cubic_weights(float t, float w[4]) {
   w[3] = t * t * t;
 }
 
+// Curve weights of the four stored vectors at t: Bernstein (cubic Bezier control
+// points) or the power basis t^3, t^2, t, 1 (Catmull-Rom coefficients A, B, C, D,
+// strokes_sdf.h:1333-1338).
+__device__ __forceinline__ void curve_weights(float t, float w[4], bool power) {
+  if (power) {
+    const float t2 = t * t;
+    w[0] = t2 * t;
+    w[1] = t2;
+    w[2] = t;
+    w[3] = 1.f;
+  } else {
+    cubic_weights(t, w);
+  }
+}
+
 struct CubicFwd {
   float t, tau, tau_raw, dist;
   int seg;  // winning segment 1..10, 0 when none
   V3 v;     // B(t) - pos
 };
 
-__device__ __forceinline__ float cubic_eval(const float* rec, V3 pos, CubicFwd& s) {
+__device__ __forceinline__ float cubic_eval(const float* rec, V3 pos, CubicFwd& s, bool power) {
   constexpr float step = 1.0f / CUBIC_SEGMENTS;
   float best = 1e18f, t_min = 0.f, tau_best = 0.f, tau_raw_best = 0.f;
   int seg = 0;
@@ -338,7 +485,7 @@ __device__ __forceinline__ float cubic_eval(const float* rec, V3 pos, CubicFwd& 
     s0 = s1;
   }
   float w[4];
-  cubic_weights(t_min, w);
+  curve_weights(t_min, w, power);
   const float4 cA = rec4(rec)[R_CA / 4], cB = rec4(rec)[R_CB / 4], cC = rec4(rec)[R_CC / 4],
                cD = rec4(rec)[R_CD / 4];
   V3 P = xyz(cA) * w[0] + xyz(cB) * w[1] + xyz(cC) * w[2] + xyz(cD) * w[3];
@@ -353,16 +500,17 @@ __device__ __forceinline__ float cubic_eval(const float* rec, V3 pos, CubicFwd& 
 // (strokes_sdf.h:1296-1322): -w*2v for position, 2w v * weights for control points,
 // no dependence of t on the inputs. Returns dL/dpos (before the reference's second
 // multiplication by dL/dSDF, which the caller applies in compat mode).
-// g[0..11] += dL/d(A,B,C,D); g[12], g[13] += dL/d(r1, r2).
+// g[0..11] += dL/d(A,B,C,D); g[12], g[13] += dL/d(r1, r2). power: the stored
+// vectors are Catmull-Rom power-basis coefficients (same adjoint, other weights).
 __device__ __forceinline__ V3 cubic_adjoint(const float* rec, V3 pos, const CubicFwd& s, float w,
-                                            float* g, int compat) {
+                                            float* g, int compat, bool power) {
   constexpr float step = 1.0f / CUBIC_SEGMENTS;
   const float4 cA = rec4(rec)[R_CA / 4], cB = rec4(rec)[R_CB / 4], cC = rec4(rec)[R_CC / 4],
                cD = rec4(rec)[R_CD / 4];
   float r1 = cA.w, r2 = cB.w;
   float t = s.t;
   float bw[4];
-  cubic_weights(t, bw);
+  curve_weights(t, bw, power);
   g[12] += -w * (1.f - t);
   g[13] += -w * t;
   if (compat) {
@@ -378,7 +526,8 @@ __device__ __forceinline__ V3 cubic_adjoint(const float* rec, V3 pos, const Cubi
   V3 A = xyz(cA), B = xyz(cB), C = xyz(cC), D = xyz(cD);
   V3 gv = s.v * (w / s.dist);
   float u = 1.f - t;
-  V3 dB = (B - A) * (3.f * u * u) + (C - B) * (6.f * u * t) + (D - C) * (3.f * t * t);
+  V3 dB = power ? A * (3.f * t * t) + B * (2.f * t) + C
+                : (B - A) * (3.f * u * u) + (C - B) * (6.f * u * t) + (D - C) * (3.f * t * t);
   float gt = -w * (r2 - r1) + dot(gv, dB);
 #pragma unroll
   for (int k = 0; k < 4; k++) {
@@ -398,8 +547,8 @@ __device__ __forceinline__ V3 cubic_adjoint(const float* rec, V3 pos, const Cubi
     V3 g0 = (ab * (2.f * s.tau - 1.f) - wv) * (gtau * inv);
     V3 g1 = (wv - ab * (2.f * s.tau)) * (gtau * inv);
     float w0[4], w1[4];
-    cubic_weights(t0, w0);
-    cubic_weights(t1, w1);
+    curve_weights(t0, w0, power);
+    curve_weights(t1, w1, power);
 #pragma unroll
     for (int k = 0; k < 4; k++) {
       g[3 * k + 0] += g0.x * w0[k] + g1.x * w1[k];

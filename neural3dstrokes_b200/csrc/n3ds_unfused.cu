@@ -95,12 +95,12 @@ __global__ void __launch_bounds__(UF_WARPS * 32) uf_stroke_bwd_kernel(const UfSt
     CubicFwd cf;
     if (base <= B_TETRAHEDRON) {
       pl = prim_local(rec, x);
-      sdf = prim_sdf(base, pl, rec[R_BP]);
-      if (kind & K_S3FAC) f = s3_factor(base, pl, xyz(rec4(rec)[R_S / 4]));
+      sdf = prim_sdf(base, pl, rec);
+      if (kind & K_S3FAC) f = s3_factor(base, pl, xyz(rec4(rec)[R_S / 4]), rec);
     } else if (base == B_QUAD_BEZIER) {
       sdf = quad_eval(rec, x, qf);
     } else {
-      sdf = cubic_eval(rec, x, cf);
+      sdf = cubic_eval(rec, x, cf, base == B_CATMULL_ROM);
     }
     const float kk = rec[R_KFIX] * f * rinv;
     const float m = -sdf * kk;
@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(UF_WARPS * 32) uf_stroke_bwd_kernel(const UfSt
     } else if (base == B_QUAD_BEZIER) {
       gx = quad_adjoint(rec, qf, dsdf, v + G_CTRL);
     } else {
-      gx = cubic_adjoint(rec, x, cf, dsdf, v + G_CTRL, L.compat);
+      gx = cubic_adjoint(rec, x, cf, dsdf, v + G_CTRL, L.compat, base == B_CATMULL_ROM);
       if (L.compat) gx = gx * dsdf;  // the reference multiplies by dL/dSDF again
     }
     if (L.grad_x) {
@@ -397,7 +397,7 @@ cudaError_t launch_uf_stroke_bwd(const UfStroke& L, int base, cudaStream_t st) {
   if (want > cap) want = cap;
   if (want < 1) want = 1;
   dim3 grid((unsigned)want, sblocks);
-  if (base == B_CUBIC_BEZIER)
+  if (base_is_cubic_curve(base))
     uf_stroke_bwd_kernel<32><<<grid, UF_WARPS * 32, 0, st>>>(L);
   else
     uf_stroke_bwd_kernel<16><<<grid, UF_WARPS * 32, 0, st>>>(L);

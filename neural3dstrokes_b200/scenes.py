@@ -18,14 +18,19 @@ import torch
 
 # reference sdf_ids (strokes.py:40-82, 95-106)
 SDF_ID = {
-    "sphere": 0x05, "ellipsoid": 0x0B, "cube": 0x17, "roundcube": 0x27, "capsule": 0x47,
-    "octahedron": 0x77, "tetrahedron": 0x87, "quadratic_bezier": 0x90, "cubic_bezier": 0xA0,
+    "sphere": 0x05, "ellipsoid": 0x0B, "aacube": 0x15, "cube": 0x17, "aabb": 0x19, "obb": 0x1B,
+    "roundcube": 0x27, "roundbox": 0x2B, "cappedtorus": 0x37, "capsule": 0x47, "scapsule": 0x4B, "line": 0x57,
+    "triprism": 0x67, "octahedron": 0x77, "tetrahedron": 0x87, "quadratic_bezier": 0x90, "cubic_bezier": 0xA0,
+    "catmull_rom": 0xB0,
 }
-N_PARAMS = {"sphere": 4, "ellipsoid": 9, "cube": 7, "roundcube": 8, "capsule": 8, "octahedron": 7,
-            "tetrahedron": 7, "quadratic_bezier": 11, "cubic_bezier": 14}
+N_PARAMS = {"sphere": 4, "ellipsoid": 9, "aacube": 4, "cube": 7, "aabb": 6, "obb": 9, "roundcube": 8,
+            "roundbox": 10, "cappedtorus": 9, "capsule": 8, "scapsule": 10, "line": 9, "triprism": 8,
+            "octahedron": 7, "tetrahedron": 7, "quadratic_bezier": 11, "cubic_bezier": 14, "catmull_rom": 14}
 PARAM_STRIDE = 16
 MIXED_PRIMS = ["sphere", "cube", "roundcube", "tetrahedron", "octahedron", "capsule"]
 ALL_KINDS = MIXED_PRIMS + ["quadratic_bezier", "cubic_bezier"]
+# every shape type of the reference's get_stroke (strokes.py:40-82)
+EVERY_KIND = list(SDF_ID)
 
 
 @dataclass
@@ -104,6 +109,8 @@ def make_strokes(kinds, g, density=10.0, ctrl_sigma=0.15):
     cap_half = _logu(S, 0.05, 0.3, g)
     ctrl = centre[:, None, :] + torch.randn(S, 4, 3, generator=g) * ctrl_sigma
     radii = torch.rand(S, 2, generator=g) * 0.05 + 0.01
+    if any(k in ("cappedtorus", "line", "triprism") for k in kinds):
+        extra = torch.rand(S, 2, generator=g)  # drawn only when needed: earlier scenes keep their streams
     for i, k in enumerate(kinds):
         if k == "sphere":
             row = [scale1[i:i + 1], centre[i]]
@@ -116,9 +123,27 @@ def make_strokes(kinds, g, density=10.0, ctrl_sigma=0.15):
         elif k == "capsule":
             h = torch.clamp(cap_half[i] / cap_r[i], min=0.25)
             row = [h.reshape(1), cap_r[i:i + 1], euler[i], centre[i]]
+        elif k == "aacube":
+            row = [scale1[i:i + 1], centre[i]]
+        elif k == "aabb":
+            row = [scale3[i], centre[i]]
+        elif k == "obb":
+            row = [scale3[i], euler[i], centre[i]]
+        elif k == "roundbox":
+            row = [rround[i:i + 1], scale3[i], euler[i], centre[i]]
+        elif k == "scapsule":
+            row = [(cap_half[i] / scale3[i, 0]).clamp(min=0.25).reshape(1), scale3[i], euler[i], centre[i]]
+        elif k == "cappedtorus":  # cap angle in [0.3, 2.8] rad, tube radius in [0.1, 0.5]
+            row = [(0.3 + 2.5 * extra[i, 0]).reshape(1), (0.1 + 0.4 * extra[i, 1]).reshape(1), scale1[i:i + 1],
+                   euler[i], centre[i]]
+        elif k == "line":  # half-length in [0.25, 1.25], radius change in [-0.5, 0.5]
+            row = [(0.25 + extra[i, 0]).reshape(1), (extra[i, 1] - 0.5).reshape(1), scale1[i:i + 1], euler[i],
+                   centre[i]]
+        elif k == "triprism":  # half-height in [0.2, 1.0]
+            row = [(0.2 + 0.8 * extra[i, 0]).reshape(1), scale1[i:i + 1], euler[i], centre[i]]
         elif k == "quadratic_bezier":
             row = [ctrl[i, :3].reshape(-1), radii[i]]
-        elif k == "cubic_bezier":
+        elif k in ("cubic_bezier", "catmull_rom"):
             row = [ctrl[i].reshape(-1), radii[i]]
         else:
             raise ValueError(k)
@@ -217,19 +242,31 @@ def param_ranges(kind):
     scale = (0.01, 0.5)
     rot = (-math.pi, math.pi)
     tr = (-1.0, 1.0)
-    if kind == "sphere":
+    if kind in ("sphere", "aacube"):
         r = [scale] + [tr] * 3
-    elif kind == "ellipsoid":
+    elif kind == "aabb":
+        r = [scale] * 3 + [tr] * 3
+    elif kind in ("ellipsoid", "obb"):
         r = [scale] * 3 + [rot] * 3 + [tr] * 3
     elif kind in ("cube", "octahedron", "tetrahedron"):
         r = [scale] + [rot] * 3 + [tr] * 3
     elif kind == "roundcube":
         r = [(0.0, 1.0), scale] + [rot] * 3 + [tr] * 3
+    elif kind == "roundbox":
+        r = [(0.0, 1.0)] + [scale] * 3 + [rot] * 3 + [tr] * 3
     elif kind == "capsule":
         r = [(0.25, inf), scale] + [rot] * 3 + [tr] * 3
+    elif kind == "scapsule":
+        r = [(0.25, inf)] + [scale] * 3 + [rot] * 3 + [tr] * 3
+    elif kind == "cappedtorus":
+        r = [(0.0, float(torch.acos(torch.tensor(0.0))) * 2), (0.0, inf), scale] + [rot] * 3 + [tr] * 3
+    elif kind == "line":
+        r = [(0.25, inf), (-0.8, 0.8), scale] + [rot] * 3 + [tr] * 3
+    elif kind == "triprism":
+        r = [(0.0, inf), scale] + [rot] * 3 + [tr] * 3
     elif kind == "quadratic_bezier":
         r = [(-1.0, 1.0)] * 9 + [(0.001, 0.2)] * 2
-    elif kind == "cubic_bezier":
+    elif kind in ("cubic_bezier", "catmull_rom"):
         r = [(-1.0, 1.0)] * 12 + [(0.001, 0.2)] * 2
     else:
         raise ValueError(kind)

@@ -22,7 +22,7 @@ from . import strokelib as _backend
 _BASE = {"unit_sphere": 0, "unit_cube": 1, "unit_round_cube": 2, "unit_capped_torus": 3, "unit_capsule": 4,
          "unit_line": 5, "unit_triprism": 6, "unit_octahedron": 7, "unit_tetrahedron": 8,
          "quadratic_bezier": 9, "cubic_bezier": 10, "catmull_rom": 11}
-_IMPLEMENTED_BASES = {0, 1, 2, 4, 7, 8, 9, 10}
+_IMPLEMENTED_BASES = set(range(12))
 
 _PI = math.pi
 

@@ -33,7 +33,7 @@ BASE_SDF = {
 # number of leading base parameters per base SDF (strokes.py:40-82)
 N_BASE_PARAMS = {0: 0, 1: 0, 2: 1, 3: 2, 4: 1, 5: 2, 6: 1, 7: 0, 8: 0, 9: 11, 10: 14, 11: 14}
 # the bases this build implements (the stroke-field hot path's primitive set)
-SUPPORTED_BASES = (0, 1, 2, 4, 7, 8, 9, 10)
+SUPPORTED_BASES = (0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11)
 INV_SQRT3 = 0.57735027  # strokes_sdf.h:587,612
 # the linear soft step's upper clamp 0.9999f (strokes_forward.cu:88) as float32 rounds it
 ALPHA_MAX = float(torch.tensor(0.9999, dtype=torch.float32))
@@ -184,6 +184,30 @@ def sdf_tetrahedron(p, bp):  # strokes_sdf.h:610-613
     return (torch.fmax((x + y).abs() - z, (x - y).abs() + z) - 1.0) * INV_SQRT3
 
 
+def sdf_capped_torus(p, bp):  # strokes_sdf.h:376-383
+    ang, rb = bp[None, :, 0], bp[None, :, 1]
+    px, py, pz = p[..., 0].abs(), p[..., 1], p[..., 2]
+    s, c = torch.sin(ang), torch.cos(ang)
+    cap = px * c - py * s > 0  # cross((px, py, 0), (s, c, 0)).z > 0
+    k = torch.where(cap, px * s + py * c, torch.sqrt(px * px + py * py + 1e-8))
+    return torch.sqrt(px * px + py * py + pz * pz + 1.0 - 2.0 * k + 1e-8) - rb
+
+
+def sdf_line(p, bp):  # strokes_sdf.h:473-482
+    h, rd = bp[None, :, 0], bp[None, :, 1]
+    y = p[..., 1]
+    t = cu_clamp((y + h) / (2.0 * h), 0.0, 1.0)
+    r = (1.0 - rd) + t * ((1.0 + rd) - (1.0 - rd))  # helper_math lerp
+    q = torch.stack([p[..., 0], y - cu_clamp(y, -h, h), p[..., 2]], -1)
+    return torch.sqrt(_len_sq(q) + 1e-8) - r
+
+
+def sdf_triprism(p, bp):  # strokes_sdf.h:527-531
+    h = bp[None, :, 0]
+    q = p.abs()
+    return torch.fmax(q[..., 1] - h, torch.fmax(q[..., 0] * 0.866025 + p[..., 2] * 0.5, -p[..., 2]) - 0.5)
+
+
 def _dot(a, b):
     return (a * b).sum(-1)
 
@@ -283,6 +307,59 @@ def cubic_bezier_closest(pos, A, B, C, D, num_segments=10):
     return t_min
 
 
+def catmull_rom_coeffs(p0, p1, p2, p3):
+    """Power-basis coefficients (A, B, C, D) of the centripetal Catmull-Rom segment
+    between p1 and p2 (strokes_sdf.h:1340-1349): tangents m1, m2 from the knot gaps
+    t_ij = sqrt(|p_i - p_j| + 1e-8)."""
+    t01 = torch.sqrt(torch.sqrt(_dot(p0 - p1, p0 - p1)) + 1e-8)[..., None]
+    t12 = torch.sqrt(torch.sqrt(_dot(p1 - p2, p1 - p2)) + 1e-8)[..., None]
+    t23 = torch.sqrt(torch.sqrt(_dot(p2 - p3, p2 - p3)) + 1e-8)[..., None]
+    m1 = p2 - p1 + t12 * ((p1 - p0) / t01 - (p2 - p0) / (t01 + t12))
+    m2 = p2 - p1 + t12 * ((p3 - p2) / t23 - (p3 - p1) / (t12 + t23))
+    A = 2.0 * (p1 - p2) + m1 + m2
+    B = 3.0 * (p2 - p1) - 2.0 * m1 - m2
+    return A, B, m1, p1
+
+
+def _catmull_point(t, A, B, C, D):  # strokes_sdf.h:1333-1338
+    t2 = t * t
+    return (t2 * t)[..., None] * A + t2[..., None] * B + t[..., None] * C + D
+
+
+def _polyline_closest(pos, point_fn, num_segments=10):
+    """argmin-t over a num_segments polyline of the curve point_fn(t) [1,S,3]
+    (strokes_sdf.h:1255-1270 / 1352-1367). Returns t_min [P,S]."""
+    dt = pos.dtype
+    S = pos.shape[1]
+    step = 1.0 / num_segments
+    dist_min = torch.full(pos.shape[:-1], 1e9, dtype=dt)
+    t_min = torch.zeros(pos.shape[:-1], dtype=dt)
+    t_start = torch.zeros((), dtype=dt)
+    seg_start = point_fn(t_start.expand(1, S))
+    for i in range(1, num_segments + 1):
+        t_end = torch.tensor(i * step, dtype=dt)
+        seg_end = point_fn(t_end.expand(1, S))
+        ab = seg_end - seg_start
+        tt = cu_clamp(_dot(pos - seg_start, ab) / _dot(ab, ab), 0.0, 1.0)
+        P = seg_start + tt[..., None] * ab
+        dist = torch.sqrt(_dot(pos - P, pos - P))
+        better = dist < dist_min
+        dist_min = torch.where(better, dist, dist_min)
+        t_min = torch.where(better, t_start * (1.0 - tt) + t_end * tt, t_min)
+        t_start = t_end
+        seg_start = seg_end
+    return t_min
+
+
+def sdf_catmull_rom(p, bp):  # strokes_sdf.h:1340-1385
+    A, B, C, D = catmull_rom_coeffs(bp[:, 0:3], bp[:, 3:6], bp[:, 6:9], bp[:, 9:12])
+    r1, r2 = bp[None, :, 12], bp[None, :, 13]
+    t = _polyline_closest(p, lambda tt: _catmull_point(tt, A[None], B[None], C[None], D[None]))
+    P = _catmull_point(t, A[None], B[None], C[None], D[None])
+    dist = torch.sqrt(_dot(P - p, P - p))
+    return dist - (r1 + t * (r2 - r1))
+
+
 def sdf_cubic_bezier(p, bp):  # strokes_sdf.h:1241-1294
     A, B, C, D = bp[:, 0:3], bp[:, 3:6], bp[:, 6:9], bp[:, 9:12]
     r1, r2 = bp[None, :, 12], bp[None, :, 13]
@@ -292,8 +369,9 @@ def sdf_cubic_bezier(p, bp):  # strokes_sdf.h:1241-1294
     return dist - (r1 + t * (r2 - r1))
 
 
-SDF_FN = {0: sdf_sphere, 1: sdf_cube, 2: sdf_round_cube, 4: sdf_capsule,
-          7: sdf_octahedron, 8: sdf_tetrahedron, 9: sdf_quadratic_bezier, 10: sdf_cubic_bezier}
+SDF_FN = {0: sdf_sphere, 1: sdf_cube, 2: sdf_round_cube, 3: sdf_capped_torus, 4: sdf_capsule, 5: sdf_line,
+          6: sdf_triprism, 7: sdf_octahedron, 8: sdf_tetrahedron, 9: sdf_quadratic_bezier, 10: sdf_cubic_bezier,
+          11: sdf_catmull_rom}
 
 
 # ------------------------------------------------- reference grad_sdf (compat formulas)
@@ -354,6 +432,53 @@ def grad_sdf_compat(base, p, bp, grad_sdf_upstream=None):
             gb = torch.where(inside, zero, grad_sdf_upstream * g[..., 1] *
                              torch.where(y > 0, -one, one))[..., None]
         return g, gb
+    if base == 3:  # 385-422: the branch follows k > 0, not the cap test of the forward
+        ang, rb = bp[None, :, 0], bp[None, :, 1]
+        x, y, z = p.unbind(-1)
+        px = x.abs()
+        s, c = torch.sin(ang), torch.cos(ang)
+        cap = px * c - y * s > 0
+        k = torch.where(cap, px * s + y * c, torch.sqrt(px * px + y * y))
+        inv = torch.rsqrt(px * px + y * y + z * z + 1.0 - 2.0 * k + 1e-8)
+        kpos = k > 0
+        ga = torch.stack([x - _sgn(x) * s, y - c, z], -1) * inv[..., None]
+        gb_ = torch.stack([2.0 * x, 2.0 * y, z], -1) * inv[..., None]
+        g = torch.where(kpos[..., None], ga, gb_)
+        gb = None
+        if grad_sdf_upstream is not None:
+            up = grad_sdf_upstream
+            g0 = torch.where(kpos, -up * (px * c + y * s), zero)
+            gb = torch.stack([g0, -up], -1)
+        return g, gb
+    if base == 5:  # 484-508
+        h, rd = bp[None, :, 0], bp[None, :, 1]
+        y = p[..., 1]
+        t = cu_clamp((y + h) / (2.0 * h), 0.0, 1.0)
+        q = torch.stack([p[..., 0], y - cu_clamp(y, -h, h), p[..., 2]], -1)
+        gp = q * torch.rsqrt(_len_sq(q) + 1e-8)[..., None]
+        inside = (-h <= y) & (y <= h)
+        g = torch.stack([gp[..., 0], torch.where(inside, -rd / h * one, gp[..., 1]), gp[..., 2]], -1)
+        gb = None
+        if grad_sdf_upstream is not None:
+            up = grad_sdf_upstream
+            g0 = torch.where(inside, y * rd / (h * h), gp[..., 1] * torch.where(y > 0, -one, one))
+            gb = torch.stack([up * g0, up * (1.0 - 2.0 * t)], -1)
+        return g, gb
+    if base == 6:  # 533-569
+        h = bp[None, :, 0]
+        q = p.abs()
+        x, y, z = p.unbind(-1)
+        a = q[..., 0] * 0.866025 + z * 0.5
+        first = a > -z
+        ytop = torch.where(first, q[..., 1] - h > a - 0.5, q[..., 1] - h > -z - 0.5)
+        gy = torch.stack([zero, _sgn(y), zero], -1)
+        gface = torch.where(first[..., None], torch.stack([0.866025 * _sgn(x), zero, 0.5 * one], -1),
+                            torch.stack([zero, zero, -one], -1))
+        g = torch.where(ytop[..., None], gy, gface)
+        gb = None
+        if grad_sdf_upstream is not None:
+            gb = torch.where(ytop, -grad_sdf_upstream, zero)[..., None]
+        return g, gb
     if base == 7:  # 590-596
         return torch.stack([_sgn(p[..., 0]), _sgn(p[..., 1]), _sgn(p[..., 2])], -1) * INV_SQRT3, None
     if base == 8:  # 615-632
@@ -380,6 +505,45 @@ def grad_sdf_compat(base, p, bp, grad_sdf_upstream=None):
             gb = torch.cat([gv * (u * u * u)[..., None], gv * (3.0 * u * u * t)[..., None],
                             gv * (3.0 * u * t * t)[..., None], gv * (t * t * t)[..., None],
                             (-gs * u)[..., None], (-gs * t)[..., None]], -1)
+        return -gv, gb
+    if base == 11:  # 1387-1447: the knot-gap chain is taken element-wise, as written there
+        p0, p1, p2, p3 = bp[:, 0:3], bp[:, 3:6], bp[:, 6:9], bp[:, 9:12]
+        A, B, C, D = catmull_rom_coeffs(p0, p1, p2, p3)
+        t = _polyline_closest(p, lambda tt: _catmull_point(tt, A[None], B[None], C[None], D[None]))
+        P = _catmull_point(t, A[None], B[None], C[None], D[None])
+        v = P - p
+        gs = grad_sdf_upstream if grad_sdf_upstream is not None else zero
+        gv = gs[..., None] * 2.0 * v
+        gb = None
+        if grad_sdf_upstream is not None:
+            p0p1, p1p2, p2p3 = p0 - p1, p1 - p2, p2 - p3
+            t01 = torch.sqrt(torch.sqrt(_dot(p0p1, p0p1)) + 1e-8)[:, None]
+            t12 = torch.sqrt(torch.sqrt(_dot(p1p2, p1p2)) + 1e-8)[:, None]
+            t23 = torch.sqrt(torch.sqrt(_dot(p2p3, p2p3)) + 1e-8)[:, None]
+            tt = t[..., None]
+            gA, gB, gC, gD = gv * tt ** 3, gv * tt * tt, gv * tt, gv
+            gm1 = gA - gB * 2.0 + gC
+            gm2 = gA - gB
+            dm1_dp0 = t12 / (t01 + t12) - t12 / t01
+            dm1_dp1 = -1.0 + t12 / t01
+            dm1_dp2 = 1.0 - t12 / (t01 + t12)
+            dm2_dp1 = -1.0 + t12 / (t12 + t23)
+            dm2_dp2 = 1.0 - t12 / t23
+            dm2_dp3 = t12 / t23 - t12 / (t12 + t23)
+            dm1_dt01 = t12 * ((p2 - p0) / ((t01 + t12) * (t01 + t12)) - (p1 - p0) / (t01 * t01))
+            dm1_dt12 = (p1 - p0) / t01 + t12 * (p2 - p0) / ((t01 + t12) * (t01 + t12)) - (p2 - p0) / (t01 + t12)
+            dm2_dt12 = (p2 - p1) / t23 + t12 * (p3 - p1) / ((t12 + t23) * (t12 + t23)) - (p3 - p1) / (t12 + t23)
+            dm2_dt23 = t12 * ((p2 - p3) / (t23 * t23) + (p3 - p1) / ((t12 + t23) * (t12 + t23)))
+            dt01 = p0p1 / (2.0 * torch.pow(_dot(p0p1, p0p1) + 1e-8, 0.75))[:, None]
+            dt12 = p1p2 / (2.0 * torch.pow(_dot(p1p2, p1p2) + 1e-8, 0.75))[:, None]
+            dt23 = p2p3 / (2.0 * torch.pow(_dot(p2p3, p2p3) + 1e-8, 0.75))[:, None]
+            g0 = gm1 * (dm1_dp0 + dm1_dt01 * dt01)
+            g1 = gA * 2.0 + gB * -3.0 + gD + gm1 * (dm1_dp1 - dm1_dt01 * dt01 + dm1_dt12 * dt12) + \
+                gm2 * (dm2_dp1 + dm2_dt12 * dt12)
+            g2 = gA * -2.0 + gB * 3.0 + gm1 * (dm1_dp2 - dm1_dt12 * dt12) + \
+                gm2 * (dm2_dp2 - dm2_dt12 * dt12 + dm2_dt23 * dt23)
+            g3 = gm2 * (dm2_dp3 - dm2_dt23 * dt23)
+            gb = torch.cat([g0, g1, g2, g3, (-gs * (1.0 - t))[..., None], (-gs * t)[..., None]], -1)
         return -gv, gb
     raise NotImplementedError(f"grad_sdf_compat: base {base}")
 

@@ -85,8 +85,8 @@ def make_render(ref_root, out):
     print("render golden written")
 
 
-KINDS = ["sphere", "ellipsoid", "cube", "roundcube", "capsule", "octahedron", "tetrahedron",
-         "quadratic_bezier", "cubic_bezier"]
+KINDS = ["sphere", "ellipsoid", "aacube", "cube", "aabb", "obb", "roundcube", "roundbox", "cappedtorus", "capsule",
+         "scapsule", "line", "triprism", "octahedron", "tetrahedron", "quadratic_bezier", "cubic_bezier", "catmull_rom"]
 
 
 def make_strokelib(out):

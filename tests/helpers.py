@@ -29,6 +29,9 @@ def small_workload(kind, n_strokes=24, n_rays=128, n_samples=48, seed=0):
     g = torch.Generator().manual_seed(seed)
     if kind == "mixed":
         kinds = [scenes.ALL_KINDS[int(i)] for i in torch.randint(0, 8, (n_strokes,), generator=g)]
+    elif kind == "every":
+        n = len(scenes.EVERY_KIND)
+        kinds = [scenes.EVERY_KIND[int(i)] for i in torch.randint(0, n, (n_strokes,), generator=g)]
     else:
         kinds = [kind] * n_strokes
     sc = scenes.make_strokes(kinds, g)

@@ -12,8 +12,7 @@ from neural3dstrokes_b200.field import FieldOptions, render_strokes
 
 pytestmark = pytest.mark.gpu
 
-KINDS = ["sphere", "ellipsoid", "cube", "roundcube", "capsule", "octahedron", "tetrahedron",
-         "quadratic_bezier", "cubic_bezier", "mixed"]
+KINDS = scenes.EVERY_KIND + ["mixed", "every"]
 
 
 def run_field(sc, rays, dev, delta=0.02, laplace=True, inv=True, bg=1.0, opaque=False, opts=None,

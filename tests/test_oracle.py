@@ -60,8 +60,7 @@ def test_render_restatement_matches_reference_render():
 
 
 STROKELIB = os.path.join(GOLDEN, "strokelib_golden.npz")
-KINDS = ["sphere", "ellipsoid", "cube", "roundcube", "capsule", "octahedron", "tetrahedron",
-         "quadratic_bezier", "cubic_bezier"]
+KINDS = scenes.EVERY_KIND  # every shape type of the reference get_stroke
 
 
 @pytest.mark.skipif(not os.path.exists(STROKELIB), reason="strokelib golden not recorded yet")
@@ -78,7 +77,7 @@ def test_port_matches_reference_strokelib(kind, mode):
     # CPU port and the CUDA op (and from float64) at rare near-tie / near-degenerate
     # samples; the linear soft step (slope 0.5 / (delta r) = 25) amplifies that, so
     # their alpha and SDF values are held to 1e-4
-    tol = 1e-4 if "bezier" in kind else 1e-5
+    tol = 1e-4 if kind in ("quadratic_bezier", "cubic_bezier", "catmull_rom") else 1e-5
     a, c, sdf = sf.stroke_forward(g("x"), g("radius"), g("shape"), g("color"), sid, delta, lap, inv, return_sdf=True)
     assert rel(a, g("alpha")) < tol and rel(c, g("colors")) == 0.0 and rel(sdf, g("sdf")) < tol
     a64, _, sdf64 = sf.stroke_forward(g("x").double(), g("radius").double(), g("shape").double(),

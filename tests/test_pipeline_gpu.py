@@ -1,9 +1,12 @@
 """HostPipeline: batches uploaded from pinned host memory on a copy stream, overlapped
 with the compute of the neighbouring steps, give the same results as running each
-step directly (bit-identical: same kernels, same inputs)."""
+step directly: rgb and grad_x bit-identical (per-sample arithmetic in a fixed order),
+the stroke-parameter gradients within 1e-6 (their per-CTA partial sums meet in
+floating-point atomics, whose order varies from run to run)."""
 import pytest
 import torch
 
+from helpers import rel
 from neural3dstrokes_b200 import scenes
 from neural3dstrokes_b200.train import BatchedField, HostPipeline, capture
 
@@ -37,5 +40,7 @@ def test_pipelined_steps_match_direct_steps(cuda):
             d.copy_(h)
         graph.replay()
         torch.cuda.synchronize()
-        for h, d in zip(host_out[i], outs):
-            assert torch.equal(h, d.cpu()), i
+        rgb, gshape, gx = (t.cpu() for t in outs)
+        assert torch.equal(host_out[i][0], rgb), i
+        assert torch.equal(host_out[i][2], gx), i
+        assert rel(host_out[i][1], gshape) < 1e-6, i

@@ -20,8 +20,8 @@ from oracle import strokefield as sf
 
 pytestmark = pytest.mark.gpu
 
-SDF_KINDS = ["sphere", "ellipsoid", "cube", "roundcube", "capsule", "octahedron", "tetrahedron",
-             "quadratic_bezier", "cubic_bezier"]
+SDF_KINDS = scenes.EVERY_KIND  # every shape type of the reference get_stroke
+CURVES = ("quadratic_bezier", "cubic_bezier", "catmull_rom")
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
@@ -69,7 +69,7 @@ def test_stroke_forward_matches_oracle(cuda, kind, lap, inv):
     # Bezier SDF values: the float32 closest-point solve (closed-form cubic roots,
     # polyline argmin) is ill-conditioned at rare near-degenerate / near-tie samples,
     # so the raw SDF (not a rendered output) is held to 1e-4; alpha above stays 1e-5
-    assert rel(sdf, sdf_r) < (1e-4 if "bezier" in kind else FWD_TOL)
+    assert rel(sdf, sdf_r) < (1e-4 if kind in CURVES else FWD_TOL)
 
 
 @pytest.mark.parametrize("kind", SDF_KINDS)
@@ -177,8 +177,11 @@ def test_errors_are_runtime_errors(cuda):
     with pytest.raises(RuntimeError, match="must be a CUDA tensor"):
         sl.stroke_forward(torch.empty(60, 4), torch.empty(60, 4, 3), torch.empty(0), torch.empty(0), x, r, vd, ps,
                           col, sid, 0, 0.02, True, True)
-    with pytest.raises(RuntimeError, match="implemented set"):
-        run_forward(sl, 0x37, torch.zeros(4, 9), col, x, r, vd, 0.02, True, True, cuda)  # capped torus
+    with pytest.raises(RuntimeError, match="constant_rgb"):  # gradient_rgb colour field
+        sl.stroke_forward(torch.empty(60, 4, device=cuda), torch.empty(60, 4, 3, device=cuda),
+                          torch.empty(0, device=cuda), torch.empty(0, device=cuda), x.to(cuda), r.to(cuda),
+                          vd.to(cuda), ps.to(cuda),
+                          torch.rand(4, 12, device=cuda), sid, 1, 0.02, True, True)
     with pytest.raises(RuntimeError, match="fn_id"):
         run_forward(sl, 0xc0, ps, col, x, r, vd, 0.02, True, True, cuda)
     with pytest.raises(RuntimeError, match="Unsupported color dimension"):
@@ -195,7 +198,7 @@ def test_forward_matches_reference_op(cuda, kind):
     if ref is None:
         pytest.skip("reference extension not built (oracle/_ref)")
     sid, ps, col, x, r, vd, _ = group(kind, n_points=2000, seed=8)
-    tol = 1e-4 if "bezier" in kind else FWD_TOL
+    tol = 1e-4 if kind in CURVES else FWD_TOL
     for lap, inv in [(True, True), (False, False)]:
         a, c, sdf = run_forward(sl, sid, ps, col, x, r, vd, 0.02, lap, inv, cuda)
         a_r, c_r, sdf_r = run_forward(ref, sid, ps, col, x, r, vd, 0.02, lap, inv, cuda)
@@ -210,8 +213,7 @@ def test_forward_matches_reference_op(cuda, kind):
         assert rel(sdf, sdf_r) <= rel(sdf_r, sdf64) + tol
 
 
-@pytest.mark.parametrize("kind", ["sphere", "ellipsoid", "cube", "roundcube", "capsule", "octahedron",
-                                  "tetrahedron", "cubic_bezier"])
+@pytest.mark.parametrize("kind", [k for k in scenes.EVERY_KIND if k != "quadratic_bezier"])
 def test_compat_backward_matches_reference_op(cuda, kind):
     ref = ref_ext()
     if ref is None:
