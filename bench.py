@@ -48,6 +48,11 @@ FWD_FLOPS_BY_KIND = {
     "quadratic_bezier": 75 + 15, "cubic_bezier": 190 + 15, "catmull_rom": 190 + 15,
 }
 BWD_FACTOR = 2.5
+# DRAM bytes per step of the backward segment kernel on the batched uneven-scene
+# workload (config 3), from one ncu capture at a quarter of its rays (all passes of
+# one step, dram__bytes_read.sum + dram__bytes_write.sum; launch-list summary in
+# profiles/launches_cfg3_quarter.md); traffic grows with the ray count.
+SEG_BWD_TRAFFIC_CFG3_QUARTER = 553.6e6
 KIND_BASE = {"sphere": 0, "ellipsoid": 0, "aacube": 1, "cube": 1, "aabb": 1, "obb": 1, "roundcube": 2,
              "roundbox": 2, "cappedtorus": 3, "capsule": 4, "scapsule": 4, "line": 5, "triprism": 6,
              "octahedron": 7, "tetrahedron": 8, "quadratic_bezier": 9, "cubic_bezier": 10, "catmull_rom": 11}
@@ -453,8 +458,11 @@ def main():
     bwd_flops = BWD_FACTOR * fwd_flops
     peak = fp32_peak(dev)
     kname = ("seg_bwd_kernel (segment adjoint)" if segments else "run_bwd_kernel (sample-run adjoint)")
+    traffic = SEG_BWD_TRAFFIC_CFG3_QUARTER * args.scale / 0.25 if (args.config == 3 and segments) else None
     roofline = {"bound": "fp32", "kernel": kname, "achieved": bwd_flops / t_bwd / 1e12,
-                "peak": peak, "unit": "TFLOP/s", "frac": bwd_flops / t_bwd / 1e12 / peak, "traffic": None,
+                "peak": peak, "unit": "TFLOP/s", "frac": bwd_flops / t_bwd / 1e12 / peak, "traffic": traffic,
+                "traffic_note": "DRAM bytes per step over the backward launches, ncu at 1/4 of the rays, scaled"
+                                if traffic else None,
                 "peak_source": "measured: FP32 FMA probe kernel on this GPU (no FP32 figure in the peaks file)",
                 "flops_per_launch": bwd_flops, "launch_ms": t_bwd * 1e3,
                 "forward_kernel": {"name": "seg_fwd_kernel" if segments else "run_fwd_kernel",
