@@ -107,6 +107,29 @@ int n3ds_compose_backward(float* grad_alphas, float* grad_colors, float* grad_de
                           int64_t n_points, int64_t n_strokes, int64_t color_dim, int grad_mode,
                           void* workspace, size_t workspace_bytes, n3ds_stream_t stream);
 
+/* Composition modes of compose_strokes other than 'over' (strokes.py:390-417). */
+#define N3DS_COMPOSE_MAX 1
+#define N3DS_COMPOSE_MAX_DENSITY_WEIGHTED 2
+#define N3DS_COMPOSE_SOFTMAX 3
+#define N3DS_COMPOSE_SOFTMAX_DENSITY_WEIGHTED 4
+
+/* Replaces the torch code of compose_strokes for the modes above (strokes.py:390-417;
+ * the reference has no native kernel for them). density_out [P], color_out [P,C]
+ * (written), alphas [P,S], colors [P,S,C], density_params [S]; C in {1, 3}. max modes
+ * pick the first maximum (NaN counts as the largest), as torch.argmax. */
+int n3ds_compose_mode_forward(int mode, float* density_out, float* color_out, const float* alphas,
+                              const float* colors, const float* density_params, int64_t n_points,
+                              int64_t n_strokes, int64_t color_dim, n3ds_stream_t stream);
+
+/* Backward of n3ds_compose_mode_forward: writes (overwrites) grad_alphas [P,S] and
+ * grad_colors [P,S,C]; accumulates into grad_density_params [S] (caller-zeroed).
+ * grad_density_out [P] and grad_color_out [P,C] may be NULL (zero). */
+int n3ds_compose_mode_backward(int mode, float* grad_alphas, float* grad_colors, float* grad_density_params,
+                               const float* grad_density_out, const float* grad_color_out,
+                               const float* alphas, const float* colors, const float* density_params,
+                               int64_t n_points, int64_t n_strokes, int64_t color_dim,
+                               n3ds_stream_t stream);
+
 /* Maximum n_strokes of n3ds_stroke_forward_static. */
 #define N3DS_STATIC_MAX_STROKES 4096
 

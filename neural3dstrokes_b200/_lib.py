@@ -78,6 +78,9 @@ _SIGS = {
     "n3ds_field_launch_count": (ctypes.c_int, [ctypes.POINTER(Batch), ctypes.POINTER(Options),
                                                ctypes.POINTER(c_i32), ctypes.POINTER(c_i32)]),
     "n3ds_field_resolve_options": (ctypes.c_int, [ctypes.POINTER(Options), ctypes.POINTER(Options)]),
+    "n3ds_compose_mode_forward": (ctypes.c_int, [ctypes.c_int, _P, _P, _P, _P, _P, c_i64, c_i64, c_i64, _P]),
+    "n3ds_compose_mode_backward": (ctypes.c_int, [ctypes.c_int, _P, _P, _P, _P, _P, _P, _P, _P, c_i64, c_i64,
+                                                  c_i64, _P]),
     "n3ds_stroke_forward_static": (ctypes.c_int, [_P, _P, _P, c_i64, _P, _P, _P, _P, _P, c_i64, c_i64, c_i64,
                                                   c_i64, c_i64, c_u32, c_u32, ctypes.c_float, ctypes.c_int,
                                                   ctypes.c_int, _P]),

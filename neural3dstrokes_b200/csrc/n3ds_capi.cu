@@ -439,6 +439,38 @@ int n3ds_field_backward(const n3ds_batch_t* batch, const n3ds_rays_t* rays, cons
   return N3DS_OK;
 }
 
+int n3ds_compose_mode_forward(int mode, float* density_out, float* color_out, const float* alphas,
+                              const float* colors, const float* density_params, int64_t n_points,
+                              int64_t n_strokes, int64_t color_dim, n3ds_stream_t stream) {
+  if (mode < N3DS_COMPOSE_MAX || mode > N3DS_COMPOSE_SOFTMAX_DENSITY_WEIGHTED)
+    return fail(N3DS_ERR_INVALID, "unknown composition mode " + std::to_string(mode));
+  if (color_dim != 1 && color_dim != 3) return fail(N3DS_ERR_INVALID, "Unsupported color dimension");
+  if (n_points < 0 || n_strokes < 0) return fail(N3DS_ERR_INVALID, "negative size");
+  if (n_points == 0) return N3DS_OK;
+  if (!density_out || !color_out || (n_strokes > 0 && (!alphas || !colors || !density_params)))
+    return fail(N3DS_ERR_INVALID, "null tensor pointer");
+  N3DS_CUDA_TRY(n3ds::launch_compose_mode_fwd(mode, density_out, color_out, alphas, colors, density_params, n_points,
+                                              n_strokes, (int)color_dim, reinterpret_cast<cudaStream_t>(stream)));
+  return N3DS_OK;
+}
+
+int n3ds_compose_mode_backward(int mode, float* grad_alphas, float* grad_colors, float* grad_density_params,
+                               const float* grad_density_out, const float* grad_color_out, const float* alphas,
+                               const float* colors, const float* density_params, int64_t n_points,
+                               int64_t n_strokes, int64_t color_dim, n3ds_stream_t stream) {
+  if (mode < N3DS_COMPOSE_MAX || mode > N3DS_COMPOSE_SOFTMAX_DENSITY_WEIGHTED)
+    return fail(N3DS_ERR_INVALID, "unknown composition mode " + std::to_string(mode));
+  if (color_dim != 1 && color_dim != 3) return fail(N3DS_ERR_INVALID, "Unsupported color dimension");
+  if (n_points < 0 || n_strokes < 0) return fail(N3DS_ERR_INVALID, "negative size");
+  if (n_points == 0 || n_strokes == 0) return N3DS_OK;
+  if (!grad_alphas || !grad_colors || !grad_density_params || !alphas || !colors || !density_params)
+    return fail(N3DS_ERR_INVALID, "null tensor pointer");
+  N3DS_CUDA_TRY(n3ds::launch_compose_mode_bwd(mode, grad_alphas, grad_colors, grad_density_params, grad_density_out,
+                                              grad_color_out, alphas, colors, density_params, n_points, n_strokes,
+                                              (int)color_dim, reinterpret_cast<cudaStream_t>(stream)));
+  return N3DS_OK;
+}
+
 int n3ds_field_resolve_options(const n3ds_options_t* opt, n3ds_options_t* out) {
   if (!out) return fail(N3DS_ERR_INVALID, "out is required");
   n3ds_options_t d;

@@ -48,4 +48,11 @@ cudaError_t launch_uf_stroke_bwd(const UfStroke& L, int base, cudaStream_t st);
 cudaError_t launch_uf_compose_fwd(const UfCompose& L, cudaStream_t st);
 cudaError_t launch_uf_compose_bwd(const UfCompose& L, cudaStream_t st);
 
+// non-'over' composition modes (n3ds_compose_modes.cu)
+cudaError_t launch_compose_mode_fwd(int mode, float* density, float* color, const float* alphas, const float* colors,
+                                    const float* dp, long long P, long long S, int C, cudaStream_t st);
+cudaError_t launch_compose_mode_bwd(int mode, float* g_alpha, float* g_colors, float* g_dp, const float* g_dens,
+                                    const float* g_col, const float* alphas, const float* colors, const float* dp,
+                                    long long P, long long S, int C, cudaStream_t st);
+
 }  // namespace n3ds

@@ -9,14 +9,16 @@ operators of ``neural3dstrokes_b200.strokelib``.
 
 Differences, all deliberate: the shape/colour tables are this module's own; calling
 get_stroke repeatedly does not grow the range lists (the reference mutates them in
-place, strokes.py:245-252); the shape types and colour types outside the implemented
-set raise ``NotImplementedError`` instead of compiling a kernel for them.
+place, strokes.py:245-252); colour types other than constant_rgb raise
+``NotImplementedError``; the non-'over' composition modes run on their own CUDA
+kernels (torch ops in the reference).
 """
 import math
 
 import torch
 from torch.autograd.function import once_differentiable
 
+from . import _lib
 from . import strokelib as _backend
 
 _BASE = {"unit_sphere": 0, "unit_cube": 1, "unit_round_cube": 2, "unit_capped_torus": 3, "unit_capsule": 4,
@@ -214,8 +216,57 @@ class _ComposeFn(torch.autograd.Function):
         return ga.reshape(*ctx.pre, S), gcs.reshape(*ctx.pre, S, c.shape[-1]), gdp
 
 
+_COMPOSE_MODES = {"max": 1, "max_density_weighted": 2, "softmax": 3, "softmax_density_weighted": 4}
+
+
+class _ComposeModeFn(torch.autograd.Function):
+    """max / max_density_weighted / softmax / softmax_density_weighted compositing
+    (reference strokes.py:390-417, torch ops there; one CUDA kernel per direction here)."""
+
+    @staticmethod
+    def forward(ctx, alphas, colors, density_params, mode):
+        if density_params.dim() != 1 or alphas.shape[:-1] != colors.shape[:-2] or \
+                alphas.shape[-1] != colors.shape[-2] or alphas.shape[-1] != density_params.shape[0]:
+            raise ValueError("expected alphas [..., S], colors [..., S, C], density_params [S]")
+        pre = alphas.shape[:-1]
+        S = density_params.shape[0]
+        C = colors.shape[-1]
+        a = alphas.contiguous().reshape(-1, S).float()
+        c = colors.contiguous().reshape(-1, S, C).float()
+        d = density_params.contiguous().float()
+        dens = torch.empty(a.shape[0], device=a.device)
+        col = torch.empty(a.shape[0], C, device=a.device)
+        lib = _lib.load()
+        with torch.cuda.device(a.device):
+            _lib.check(lib.n3ds_compose_mode_forward(mode, _lib.ptr(dens), _lib.ptr(col), _lib.ptr(a), _lib.ptr(c),
+                                                     _lib.ptr(d), a.shape[0], S, C, _lib.stream_ptr()))
+        ctx.save_for_backward(a, c, d)
+        ctx.pre, ctx.mode = pre, mode
+        return dens.reshape(*pre), col.reshape(*pre, C)
+
+    @staticmethod
+    @once_differentiable
+    def backward(ctx, g_dens, g_col):
+        a, c, d = ctx.saved_tensors
+        S, C = d.shape[0], c.shape[-1]
+        gd = None if g_dens is None else g_dens.contiguous().float().reshape(-1)
+        gc = None if g_col is None else g_col.contiguous().float().reshape(-1, C)
+        ga, gcs, gdp = torch.empty_like(a), torch.empty_like(c), torch.zeros_like(d)
+        lib = _lib.load()
+        with torch.cuda.device(a.device):
+            _lib.check(lib.n3ds_compose_mode_backward(ctx.mode, _lib.ptr(ga), _lib.ptr(gcs), _lib.ptr(gdp),
+                                                      _lib.ptr(gd), _lib.ptr(gc), _lib.ptr(a), _lib.ptr(c),
+                                                      _lib.ptr(d), a.shape[0], S, C, _lib.stream_ptr()))
+        return ga.reshape(*ctx.pre, S), gcs.reshape(*ctx.pre, S, C), gdp, None
+
+
 def compose_strokes(alphas, colors, density_params, composition_type: str):
-    """Composite strokes (reference strokes.py:376-419); 'over' is implemented."""
+    """Composite strokes (reference strokes.py:376-419): 'over' through the drop-in
+    _strokelib operators, the other modes through their own kernels."""
     if composition_type == "over":
         return _ComposeFn.apply(alphas, colors, density_params)
-    raise NotImplementedError(f"composition type {composition_type} is not implemented ('over' is)")
+    if composition_type in _COMPOSE_MODES:
+        if not alphas.is_cuda:
+            raise RuntimeError("alphas must be a CUDA tensor")
+        return _ComposeModeFn.apply(alphas, colors, density_params, _COMPOSE_MODES[composition_type])
+    raise ValueError(f"Unknown composition type {composition_type}")

@@ -712,6 +712,25 @@ def compose_backward_compat(grad_density, grad_color, alphas, colors, density_pa
     return g_alpha, g_colors, g_dp
 
 
+def compose_mode(alphas, colors, density_params, composition_type):
+    """The torch compositing modes of compose_strokes (strokes.py:390-417), restated."""
+    d = torch.broadcast_to(density_params, alphas.shape)
+    if composition_type in ("max", "max_density_weighted"):
+        key = alphas if composition_type == "max" else alphas * d
+        idx = torch.argmax(key, dim=-1, keepdim=True)
+        a = torch.take_along_dim(alphas, idx, dim=-1).squeeze(-1)
+        density = a * density_params[idx].squeeze(-1)
+        color = torch.take_along_dim(colors, idx[..., None], dim=-2).squeeze(-2)
+        return density, color
+    if composition_type in ("softmax", "softmax_density_weighted"):
+        key = alphas if composition_type == "softmax" else alphas * d
+        w = torch.softmax(key * (1.0 / 0.05), dim=-1)
+        density = torch.einsum("...s,...s->...", w, alphas * d)
+        color = torch.einsum("...s,...sc->...c", w, colors)
+        return density, color
+    raise ValueError(composition_type)
+
+
 # ------------------------------------------------------- stroke backward (compat)
 
 def stroke_backward_compat(grad_alpha, grad_color, x, radius, alpha, shape_params,

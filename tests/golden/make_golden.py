@@ -10,6 +10,10 @@ Three sources, each a seeded, small input set:
             source/utils/render.py and runs compute_alpha_weights (plain and opaque
             background) and volumetric_rendering in float64 on seeded inputs.
             -> render_golden.npz
+--compose   (CPU, needs the reference checkout): imports the reference strokes.py with a
+            stub ``_strokelib`` and runs its torch compositing modes (max,
+            max_density_weighted, softmax, softmax_density_weighted,
+            strokes.py:390-417) in float64 with autograd. -> compose_modes_golden.npz
 --strokelib (GPU, needs oracle/_ref built from the reference sources by
             oracle/build_ref.py): runs the reference CUDA operators stroke_forward,
             stroke_backward, compose_forward, compose_backward on seeded inputs for
@@ -58,6 +62,34 @@ def make_layouts(ref_root, out):
     with open(os.path.join(out, "layouts.json"), "w") as f:
         json.dump(res, f, indent=1, sort_keys=True)
     print("layouts:", len(res), "shape types")
+
+
+def make_compose_modes(ref_root, out):
+    sys.modules["_strokelib"] = types.ModuleType("_strokelib")  # stub backend: 'over' is not called
+    path = os.path.join(ref_root, "source", "strokelib", "strokes.py")
+    spec = importlib.util.spec_from_file_location("ref_strokes_compose", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    g = torch.Generator().manual_seed(77)
+    arrays = {}
+    for C in (1, 3):
+        a = torch.rand(2, 16, 23, generator=g, dtype=torch.float64) ** 2
+        c = torch.rand(2, 16, 23, C, generator=g, dtype=torch.float64)
+        d = torch.rand(23, generator=g, dtype=torch.float64) * 10
+        gd = torch.randn(2, 16, generator=g, dtype=torch.float64)
+        gc = torch.randn(2, 16, C, generator=g, dtype=torch.float64)
+        for k, v in dict(alphas=a, colors=c, density_params=d, g_density=gd, g_color=gc).items():
+            arrays[f"c{C}/{k}"] = v.numpy()
+        for mode in ("max", "max_density_weighted", "softmax", "softmax_density_weighted"):
+            ta, tc, td = (t.clone().requires_grad_(True) for t in (a, c, d))
+            dens, col = mod.compose_strokes(ta, tc, td, mode)
+            ((dens * gd).sum() + (col * gc).sum()).backward()
+            for k, v in dict(density=dens, color=col, grad_alphas=ta.grad, grad_colors=tc.grad,
+                             grad_density_params=td.grad).items():
+                arrays[f"c{C}/{mode}/{k}"] = v.detach().numpy()
+    del sys.modules["_strokelib"]
+    np.savez_compressed(os.path.join(out, "compose_modes_golden.npz"), **arrays)
+    print("compose modes golden written:", len(arrays), "arrays")
 
 
 def make_render(ref_root, out):
@@ -159,6 +191,7 @@ if __name__ == "__main__":
     ap.add_argument("--layouts", action="store_true")
     ap.add_argument("--render", action="store_true")
     ap.add_argument("--strokelib", action="store_true")
+    ap.add_argument("--compose", action="store_true")
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--out", default=HERE)
     a = ap.parse_args()
@@ -169,3 +202,5 @@ if __name__ == "__main__":
         make_render(a.ref, a.out)
     if a.strokelib:
         make_strokelib(a.out)
+    if a.compose:
+        make_compose_modes(a.ref, a.out)

@@ -191,3 +191,20 @@ def test_known_divergences_of_reference_backward():
     _, c = sf.compose_forward(alg, co, dp)
     ga_ex, = torch.autograd.grad((c * gc).sum(), [alg])
     assert rel(ga_ref, ga_ex) > 1e-3                     # colour -> alpha approximation
+
+
+def test_compose_modes_restatement_matches_reference_torch():
+    """oracle.compose_mode against the reference's own torch compositing modes
+    (strokes.py:390-417), run in float64 by tests/golden/make_golden.py --compose."""
+    z = np.load(os.path.join(GOLDEN, "compose_modes_golden.npz"))
+    for C in (1, 3):
+        t = {k: torch.from_numpy(z[f"c{C}/{k}"]) for k in ("alphas", "colors", "density_params", "g_density",
+                                                         "g_color")}
+        for mode in ("max", "max_density_weighted", "softmax", "softmax_density_weighted"):
+            a, c, d = (t[k].clone().requires_grad_(True) for k in ("alphas", "colors", "density_params"))
+            dens, col = sf.compose_mode(a, c, d, mode)
+            ((dens * t["g_density"]).sum() + (col * t["g_color"]).sum()).backward()
+            ref = lambda k: torch.from_numpy(z[f"c{C}/{mode}/{k}"])
+            assert rel(dens, ref("density")) < 1e-12 and rel(col, ref("color")) < 1e-12, mode
+            assert rel(a.grad, ref("grad_alphas")) < 1e-12 and rel(c.grad, ref("grad_colors")) < 1e-12, mode
+            assert rel(d.grad, ref("grad_density_params")) < 1e-12, mode
