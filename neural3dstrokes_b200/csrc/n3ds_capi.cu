@@ -563,7 +563,7 @@ int check_stroke_args(uint32_t sdf_id, uint32_t color_id, int64_t n_points, int6
                       int64_t n_shape_params, int64_t n_color_params, int64_t n_texcoord, void* ws, size_t ws_bytes) {
   // fn_id bound as strokes_forward.cu:202-204, then this build's implemented subset
   if (sdf_id * 4u + color_id >= 12u * 16u * 4u) return fail(N3DS_ERR_INVALID, "fn_id must be in [0, num_fn_ids]");
-  if (color_id != 0) return fail(N3DS_ERR_UNSUPPORTED, "only color_id 0 (constant_rgb) is implemented");
+  if (color_id > 3) return fail(N3DS_ERR_INVALID, "color_id must be 0-3");
   const int base = (int)(sdf_id >> 4);
   if (!n3ds::base_supported(base))
     return fail(N3DS_ERR_INVALID, "sdf base " + std::to_string(base) + " does not exist (bases 0-11)");
@@ -575,7 +575,12 @@ int check_stroke_args(uint32_t sdf_id, uint32_t color_id, int64_t n_points, int6
   if (n_strokes > 0 && n_shape_params < n3ds::sdf_id_param_count((int)sdf_id))
     return fail(N3DS_ERR_INVALID, "shape_params has " + std::to_string(n_shape_params) + " columns, sdf_id needs " +
                                       std::to_string(n3ds::sdf_id_param_count((int)sdf_id)));
-  if (n_strokes > 0 && n_color_params < 3) return fail(N3DS_ERR_INVALID, "color_params needs 3 columns");
+  const int64_t need_c = color_id == 0 ? 3 : (color_id == 3 ? 27 : 12);
+  if (n_strokes > 0 && n_color_params < need_c)
+    return fail(N3DS_ERR_INVALID, "color_params needs " + std::to_string(need_c) + " columns for color_id " +
+                                      std::to_string(color_id));
+  if (color_id >= 2 && n_viewdirs > 0 && n_points % n_viewdirs != 0)
+    return fail(N3DS_ERR_INVALID, "the points must be a whole number of samples per view direction");
   if (n_strokes > 65535LL * 32) return fail(N3DS_ERR_INVALID, "too many strokes");
   if (!ws || ws_bytes < n3ds_stroke_workspace_bytes(n_strokes))
     return fail(N3DS_ERR_WORKSPACE, "workspace too small: need " + std::to_string(n3ds_stroke_workspace_bytes(n_strokes)));
@@ -610,6 +615,21 @@ n3ds::PrepLaunch uniform_prep(const StrokeWs& w, const float* shape_params, int6
   p.stats = nullptr;
   return p;
 }
+n3ds::UfColor color_launch(const float* x, const float* viewdir, const float* recs, const float* color_params,
+                           int64_t n_color_params, uint32_t color_id, int64_t P, int64_t n_viewdirs, int64_t S) {
+  n3ds::UfColor C{};
+  C.x = x;
+  C.viewdir = viewdir;
+  C.recs = recs;
+  C.color_params = color_params;
+  C.color_stride = (int)n_color_params;
+  C.color_id = (int)color_id;
+  C.n_points = P;
+  C.spr = n_viewdirs > 0 ? std::max<int64_t>(1, P / n_viewdirs) : 1;
+  C.n_strokes = (int)S;
+  return C;
+}
+
 }  // namespace
 
 int n3ds_stroke_forward(float* alpha_out, float* color_out, float* sdf_out, int64_t n_texcoord, const float* x,
@@ -618,7 +638,6 @@ int n3ds_stroke_forward(float* alpha_out, float* color_out, float* sdf_out, int6
                         int64_t n_shape_params, int64_t n_color_params, uint32_t sdf_id, uint32_t color_id,
                         float sdf_delta, int use_laplace_transform, int inv_scale_radius, void* workspace,
                         size_t workspace_bytes, n3ds_stream_t stream) {
-  (void)viewdir;
   int rc = check_stroke_args(sdf_id, color_id, n_points, n_viewdirs, n_strokes, n_shape_params, n_color_params,
                              n_texcoord, workspace, workspace_bytes);
   if (rc) return rc;
@@ -640,7 +659,15 @@ int n3ds_stroke_forward(float* alpha_out, float* color_out, float* sdf_out, int6
   L.alpha = alpha_out;
   L.color = color_out;
   L.sdf = sdf_out;
+  L.color_const = color_id == 0;
   N3DS_CUDA_TRY(n3ds::launch_uf_stroke_fwd(L, (int)(sdf_id >> 4), st));
+  if (color_id != 0) {
+    if (color_id >= 2 && !viewdir) return fail(N3DS_ERR_INVALID, "viewdir is required by the SH colour fields");
+    n3ds::UfColor C = color_launch(x, viewdir, w.recs, color_params, n_color_params, color_id, n_points, n_viewdirs,
+                                   n_strokes);
+    C.color = color_out;
+    N3DS_CUDA_TRY(n3ds::launch_uf_color_fwd(C, st));
+  }
   return N3DS_OK;
 }
 
@@ -651,7 +678,6 @@ int n3ds_stroke_backward(float* grad_shape_params, float* grad_color_params, flo
                          int64_t n_shape_params, int64_t n_color_params, uint32_t sdf_id, uint32_t color_id,
                          float sdf_delta, int use_laplace_transform, int inv_scale_radius, int grad_mode,
                          void* workspace, size_t workspace_bytes, n3ds_stream_t stream) {
-  (void)viewdir;
   int rc = check_stroke_args(sdf_id, color_id, n_points, n_viewdirs, n_strokes, n_shape_params, n_color_params, 0,
                              workspace, workspace_bytes);
   if (rc) return rc;
@@ -680,7 +706,19 @@ int n3ds_stroke_backward(float* grad_shape_params, float* grad_color_params, flo
     L.grad_x = grad_x;
     L.gslots = w.gslots;
     L.compat = compat;
+    L.color_const = color_id == 0;
     N3DS_CUDA_TRY(n3ds::launch_uf_stroke_bwd(L, (int)(sdf_id >> 4), st));
+    if (color_id != 0) {
+      if (color_id >= 2 && !viewdir) return fail(N3DS_ERR_INVALID, "viewdir is required by the SH colour fields");
+      n3ds::UfColor C = color_launch(x, viewdir, w.recs, color_params, n_color_params, color_id, n_points,
+                                     n_viewdirs, n_strokes);
+      C.g_color = grad_color;
+      C.grad_color_params = grad_color_params;
+      C.gslots = w.gslots;
+      C.grad_x = grad_x;
+      C.compat = compat;
+      N3DS_CUDA_TRY(n3ds::launch_uf_color_bwd(C, st));
+    }
   }
   n3ds::FinalizeLaunch F{};
   F.sdf_ids = nullptr;

@@ -50,7 +50,8 @@ __global__ void __launch_bounds__(UF_WARPS * 32) uf_stroke_fwd_kernel(const UfSt
         L.alpha[row + lane] = ta[warp][rr][lane];
         if (L.sdf) L.sdf[row + lane] = tsd[warp][rr][lane];
       }
-      for (int e = lane; e < 3 * ns; e += 32) L.color[row * 3 + e] = recs[(e / 3) * REC_FLOATS + R_COLOR + e % 3];
+      if (L.color_const)
+        for (int e = lane; e < 3 * ns; e += 32) L.color[row * 3 + e] = recs[(e / 3) * REC_FLOATS + R_COLOR + e % 3];
     }
     __syncwarp();
   }
@@ -84,7 +85,7 @@ __global__ void __launch_bounds__(UF_WARPS * 32) uf_stroke_bwd_kernel(const UfSt
     const float ga = active ? L.g_alpha[pi] : 0.f;
     const float a = active ? L.alpha_in[pi] : 0.f;
     const float gs = (active && L.g_sdf) ? L.g_sdf[pi] : 0.f;
-    if (active) {
+    if (active && L.color_const) {
       v[G_COLOR] += L.g_color[3 * pi];
       v[G_COLOR + 1] += L.g_color[3 * pi + 1];
       v[G_COLOR + 2] += L.g_color[3 * pi + 2];

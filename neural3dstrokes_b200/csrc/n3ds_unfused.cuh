@@ -23,7 +23,29 @@ struct UfStroke {
   float* grad_x;           // [P*3] or null (accumulated)
   float* gslots;           // [S*32] reduced slots
   int compat;
+  int color_const;         // 1: constant rgb colour (written / reduced here); else a colour field kernel runs
 };
+
+// Colour fields (n3ds_colors.cu): gradient rgb (color_id 1), SH2 (2), SH3 (3).
+struct UfColor {
+  const float* x;              // [P*3]
+  const float* viewdir;        // [R*3]
+  const float* recs;           // [S*64] prepared records
+  const float* color_params;   // [S*color_stride]
+  int color_stride;
+  int color_id;
+  long long n_points;
+  long long spr;               // points per view direction
+  int n_strokes;
+  float* color;                // forward: [P*S*3]
+  const float* g_color;        // backward: [P*S*3]
+  float* grad_color_params;    // backward: [S*color_stride], accumulated
+  float* gslots;               // backward, exact mode: position term into the transform slots
+  float* grad_x;               // backward, exact mode: [P*3] or null, accumulated
+  int compat;
+};
+cudaError_t launch_uf_color_fwd(const UfColor& L, cudaStream_t st);
+cudaError_t launch_uf_color_bwd(const UfColor& L, cudaStream_t st);
 
 struct UfCompose {
   const float* alphas;     // [P*S]

@@ -9,9 +9,8 @@ operators of ``neural3dstrokes_b200.strokelib``.
 
 Differences, all deliberate: the shape/colour tables are this module's own; calling
 get_stroke repeatedly does not grow the range lists (the reference mutates them in
-place, strokes.py:245-252); colour types other than constant_rgb raise
-``NotImplementedError``; the non-'over' composition modes run on their own CUDA
-kernels (torch ops in the reference).
+place, strokes.py:245-252); texture coordinates are not produced; the non-'over'
+composition modes run on their own CUDA kernels (torch ops in the reference).
 """
 import math
 
@@ -61,7 +60,13 @@ _SHAPES = {
     "catmull_rom": ("catmull_rom", [(-1, 1)] * 12 + [(0.001, 0.2)] * 2, _spline_sampler(4, 2), 0, 0, 0, 0),
 }
 
-_COLORS = {"constant_rgb": (0, [(0, 1)] * 3, lambda: torch.rand(3))}
+# name -> (color_id, parameter ranges, sampler) (strokes.py:84-91)
+_COLORS = {
+    "constant_rgb": (0, [(0, 1)] * 3, lambda: torch.rand(3)),
+    "gradient_rgb": (1, [(-1, 1)] * 6 + [(0, 1)] * 6, lambda: torch.cat([torch.rand(6) - 0.5, torch.rand(6)], dim=-1)),
+    "constant_sh2": (2, [(None, None)] * 12, lambda: torch.randn(12)),
+    "constant_sh3": (3, [(None, None)] * 27, lambda: torch.randn(27)),
+}
 _COLOR_DIM = 3
 
 
@@ -126,7 +131,7 @@ def get_stroke(shape_type: str, color_type: str, init_type: str):
     if shape_type not in _SHAPES:
         raise KeyError(shape_type)
     if color_type not in _COLORS:
-        raise NotImplementedError(f"colour type {color_type} is not implemented (constant_rgb is)")
+        raise KeyError(color_type)
     base, base_ranges, base_sampler, t, r, s1, s3 = _SHAPES[shape_type]
     if _BASE[base] not in _IMPLEMENTED_BASES:
         raise NotImplementedError(f"shape type {shape_type} is outside the implemented set")

@@ -597,10 +597,90 @@ def soft_step(sdf, radius_eff, sdf_delta, use_laplace):
     return torch.where(pos, soft, hard)
 
 
+# ------------------------------------------------------------- colour fields
+
+def sh_weights(degree, d):
+    """Real spherical-harmonic basis up to ``degree`` (2: 4 terms, 3: 9 terms) of the
+    directions d [..., 3], the polynomial forms of sh.h:9-28 (tiny-cuda-nn's
+    convention: Y_1 = -c1 y, c1 z, -c1 x; Y_2 terms with c2 = sqrt(15)/(2 sqrt(pi)))."""
+    x, y, z = d.unbind(-1)
+    pi = math.pi
+    c0 = 1.0 / (2.0 * math.sqrt(pi))
+    c1 = math.sqrt(3.0) / (2.0 * math.sqrt(pi))
+    w = [torch.full_like(x, c0), -c1 * y, c1 * z, -c1 * x]
+    if degree >= 3:
+        c2 = math.sqrt(15.0) / (2.0 * math.sqrt(pi))
+        c20 = math.sqrt(5.0) / (4.0 * math.sqrt(pi))
+        c22 = math.sqrt(15.0) / (4.0 * math.sqrt(pi))
+        w += [c2 * x * y, -c2 * y * z, c20 * (3.0 * z * z - 1.0), -c2 * x * z, c22 * (x * x - y * y)]
+    return torch.stack(w, -1)
+
+
+def color_field(color_id, p_local, x, viewdir_per_point, color_params):
+    """Colour per (sample, stroke) [P,S,3] (strokes_color.h:34-171): constant rgb;
+    gradient rgb between two points of the unit (local) frame; degree-2 / degree-3
+    spherical harmonics of the world view direction through a sigmoid."""
+    P, S = p_local.shape[0], p_local.shape[1]
+    if color_id == 0:
+        return color_params[None, :, :3].expand(P, -1, -1)
+    if color_id == 1:
+        pos0, pos1 = color_params[None, :, 0:3], color_params[None, :, 3:6]
+        c0, c1 = color_params[None, :, 6:9], color_params[None, :, 9:12]
+        v0 = p_local - pos0
+        v1 = pos1 - pos0
+        t = torch.sigmoid(_dot(v0, v1) / _dot(v1, v1) * 5.0 - 2.5)[..., None]
+        return c0 * (1.0 - t) + c1 * t
+    if color_id in (2, 3):
+        n = 4 if color_id == 2 else 9
+        w = sh_weights(color_id, viewdir_per_point)  # [P, n]
+        coef = color_params[:, :3 * n].reshape(S, n, 3)
+        return torch.sigmoid(torch.einsum("pn,snc->psc", w, coef))
+    raise ValueError(color_id)
+
+
+def color_param_grads(color_id, p_local, viewdir_per_point, color_params, grad_color):
+    """dL/d(colour params) [S, Pc] from dL/dcolour [P,S,3], the reference's formulas
+    (strokes_color.h:70-97, 115-131, 153-169): exact in the parameters, no position
+    gradient."""
+    S = color_params.shape[0]
+    if color_id == 0:
+        return grad_color.sum(0)
+    if color_id == 1:
+        pos0, pos1 = color_params[None, :, 0:3], color_params[None, :, 3:6]
+        c0, c1 = color_params[None, :, 6:9], color_params[None, :, 9:12]
+        v0 = p_local - pos0
+        v1 = pos1 - pos0
+        d0, d1 = _dot(v0, v1), _dot(v1, v1)
+        t = torch.sigmoid(d0 / d1 * 5.0 - 2.5)
+        gt = _dot(grad_color, c1 - c0)
+        gtr = 5.0 * t * (1.0 - t) * gt
+        gd0 = gtr / d1
+        gd1 = -gtr * d0 / (d1 * d1)
+        gv1 = gd0[..., None] * v0 + (gd1 * 2.0)[..., None] * v1
+        gv0 = gd0[..., None] * v1
+        return torch.cat([(-gv0 - gv1).sum(0), gv1.sum(0), (grad_color * (1.0 - t)[..., None]).sum(0),
+                          (grad_color * t[..., None]).sum(0)], -1)
+    n = 4 if color_id == 2 else 9
+    w = sh_weights(color_id, viewdir_per_point)
+    coef = color_params[:, :3 * n].reshape(S, n, 3)
+    rgb = torch.sigmoid(torch.einsum("pn,snc->psc", w, coef))
+    grgb = grad_color * rgb * (1.0 - rgb)
+    return torch.einsum("psc,pn->snc", grgb, w).reshape(S, 3 * n)
+
+
+def viewdir_per_point(viewdir, n_points):
+    """The view direction of each point: viewdir[p // (P / n_viewdirs)]
+    (strokes_forward.cu:47-48, 195-197)."""
+    if viewdir is None or viewdir.numel() == 0:
+        return None
+    spr = n_points // viewdir.shape[0]
+    return viewdir.repeat_interleave(spr, dim=0)
+
+
 def stroke_forward(x, radius, shape_params, color_params, sdf_id, sdf_delta,
-                   use_laplace=False, inv_scale_radius=False, return_sdf=False):
-    """alpha [P,S], color [P,S,3] for one sdf_id group, constant_rgb colour
-    (strokes_forward.cu:17-109; ColorField<CONSTANT_RGB> strokes_color.h:34-48)."""
+                   use_laplace=False, inv_scale_radius=False, return_sdf=False, color_id=0, viewdir=None):
+    """alpha [P,S], color [P,S,3] for one sdf_id group and colour type
+    (strokes_forward.cu:17-109; ColorField strokes_color.h:34-171)."""
     base = decode_sdf_id(sdf_id)[0]
     if base not in SDF_FN:
         raise NotImplementedError(f"base sdf {base} is outside the implemented set")
@@ -614,7 +694,7 @@ def stroke_forward(x, radius, shape_params, color_params, sdf_id, sdf_delta,
         if f is not None:
             r = r / f
     alpha = soft_step(sdf, r, sdf_delta, use_laplace)
-    color = color_params[None, :, :3].expand(x.shape[0], -1, -1)
+    color = color_field(color_id, p, x, viewdir_per_point(viewdir, x.shape[0]), color_params)
     if return_sdf:
         return alpha, color, sdf
     return alpha, color
@@ -735,7 +815,7 @@ def compose_mode(alphas, colors, density_params, composition_type):
 
 def stroke_backward_compat(grad_alpha, grad_color, x, radius, alpha, shape_params,
                            color_params, sdf_id, sdf_delta, use_laplace=False,
-                           inv_scale_radius=False, grad_sdf=None, need_grad_x=True):
+                           inv_scale_radius=False, grad_sdf=None, need_grad_x=True, color_id=0, viewdir=None):
     """The reference stroke adjoint (strokes_backward.cu:17-157) for one sdf_id group.
 
     dAlpha/dSDF is taken from the saved alpha; the soft-step width is treated as a
@@ -763,7 +843,7 @@ def stroke_backward_compat(grad_alpha, grad_color, x, radius, alpha, shape_param
     dl_dsdf = grad_alpha * dadsdf
     if grad_sdf is not None:
         dl_dsdf = dl_dsdf + grad_sdf
-    g_color = grad_color.sum(0)
+    g_color = color_param_grads(color_id, p, viewdir_per_point(viewdir, x.shape[0]), color_params, grad_color)
     if base == 9:
         # The reference quadratic-Bezier adjoint (strokes_sdf.h:709-1172) is not
         # restated: its comma-operator and sign slips make it a different function.

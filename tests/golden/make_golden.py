@@ -164,6 +164,39 @@ def make_strokelib(out):
                 arrays[f"{tag}/{k}"] = v.detach().cpu().numpy()
             arrays[f"{tag}/sdf_id"] = np.array(sid)
             arrays[f"{tag}/delta"] = np.array(delta)
+    # colour fields: gradient rgb (unit-frame positions), SH2, SH3 (view directions)
+    for kind in ("sphere", "obb", "capsule", "cubic_bezier"):
+        for cid, npc in ((1, 12), (2, 12), (3, 27)):
+            g = torch.Generator().manual_seed(700 + 10 * cid + len(kind))
+            sc = scenes.make_strokes([kind] * 9, g)
+            rays = scenes.make_rays(16, 12, g)
+            sid = scenes.SDF_ID[kind]
+            ps = sc.shape_params[:, :sf.num_shape_params(sid)].contiguous()
+            if cid == 1:
+                cp = torch.cat([torch.rand(9, 6, generator=g) * 2 - 1, torch.rand(9, 6, generator=g)], -1)
+            else:
+                cp = torch.randn(9, npc, generator=g)
+            x = rays.x.reshape(-1, 3).contiguous()
+            r = rays.radius.reshape(-1).contiguous()
+            vd = (rays.dirs / rays.dirs.norm(dim=-1, keepdim=True)).contiguous()
+            P, S = x.shape[0], ps.shape[0]
+            tag = f"{kind}_c{cid}"
+            a = torch.empty(P, S, device=dev)
+            c = torch.empty(P, S, 3, device=dev)
+            ref.stroke_forward(a, c, torch.empty(0, device=dev), torch.empty(0, device=dev), x.to(dev), r.to(dev),
+                               vd.to(dev), ps.to(dev), cp.to(dev), sid, cid, 0.02, True, True)
+            ga = torch.randn(P, S, generator=g)
+            gc = torch.randn(P, S, 3, generator=g)
+            gps = torch.zeros_like(ps, device=dev)
+            gcol = torch.zeros_like(cp, device=dev)
+            gx = torch.zeros(P, 3, device=dev)
+            ref.stroke_backward(gps, gcol, gx, ga.to(dev), gc.to(dev), torch.empty(0, device=dev), x.to(dev),
+                                r.to(dev), vd.to(dev), a, ps.to(dev), cp.to(dev), sid, cid, 0.02, True, True)
+            for k, v in dict(x=x, radius=r, viewdir=vd, shape=ps, color=cp, alpha=a, colors=c, g_alpha=ga,
+                             g_color=gc, grad_shape=gps, grad_color=gcol, grad_x=gx).items():
+                arrays[f"{tag}/{k}"] = v.detach().cpu().numpy()
+            arrays[f"{tag}/sdf_id"] = np.array(sid)
+            arrays[f"{tag}/color_id"] = np.array(cid)
     g = torch.Generator().manual_seed(99)
     P, S = 300, 37
     al = torch.rand(P, S, generator=g) ** 3

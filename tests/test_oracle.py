@@ -208,3 +208,24 @@ def test_compose_modes_restatement_matches_reference_torch():
             assert rel(dens, ref("density")) < 1e-12 and rel(col, ref("color")) < 1e-12, mode
             assert rel(a.grad, ref("grad_alphas")) < 1e-12 and rel(c.grad, ref("grad_colors")) < 1e-12, mode
             assert rel(d.grad, ref("grad_density_params")) < 1e-12, mode
+
+
+@pytest.mark.skipif(not os.path.exists(STROKELIB), reason="strokelib golden not recorded yet")
+@pytest.mark.parametrize("kind", ["sphere", "obb", "capsule", "cubic_bezier"])
+@pytest.mark.parametrize("cid", [1, 2, 3])
+def test_color_fields_match_reference_strokelib(kind, cid):
+    """Colour fields (gradient rgb, SH2, SH3) of the restatement against the reference op:
+    colours and the colour-parameter gradients (the reference formulas)."""
+    z = np.load(STROKELIB)
+    tag = f"{kind}_c{cid}"
+    if f"{tag}/alpha" not in z.files:
+        pytest.skip("colour-field golden vectors not recorded")
+    g = lambda k: torch.from_numpy(z[f"{tag}/{k}"]).double()
+    sid = int(z[f"{tag}/sdf_id"])
+    a, c = sf.stroke_forward(g("x"), g("radius"), g("shape"), g("color"), sid, 0.02, True, True, color_id=cid,
+                             viewdir=g("viewdir"))
+    assert rel(c, g("colors")) < 1e-5 and rel(a, g("alpha")) < 1e-4
+    gs, gc, gx = sf.stroke_backward_compat(g("g_alpha"), g("g_color"), g("x"), g("radius"), g("alpha"), g("shape"),
+                                           g("color"), sid, 0.02, True, True, color_id=cid, viewdir=g("viewdir"))
+    assert rel(gc, g("grad_color")) < 1e-5, rel(gc, g("grad_color"))
+    assert rel(gs, g("grad_shape")) < 1e-4 and rel(gx, g("grad_x")) < 1e-4
