@@ -58,12 +58,13 @@ int n3ds_version(void);
 size_t n3ds_stroke_workspace_bytes(int64_t n_strokes);
 
 /* Replaces stroke_forward (strokes_forward.cu:170-225; declared strokes.h:14-27).
- * alpha_out [P,S], color_out [P,S,3], sdf_out [P,S] or NULL; texcoord output is not
- * implemented (pass n_texcoord = 0). x [P,3], radius [P], viewdir [R,3] (unused by
- * constant_rgb; only its count n_viewdirs is checked: P must be a multiple),
- * shape_params [S,Ps], color_params [S,Pc]. sdf_id / color_id as produced by the
- * reference get_stroke (strokes.py:95-106); color_id must be 0 (constant_rgb). */
-int n3ds_stroke_forward(float* alpha_out, float* color_out, float* sdf_out, int64_t n_texcoord,
+ * alpha_out [P,S], color_out [P,S,3], sdf_out [P,S] or NULL, texcoord_out [P,S,2] with
+ * n_texcoord its float count (0 and NULL: not produced). x [P,3], radius [P], viewdir
+ * [R,3] (the SH colour fields read viewdir[p / (P / R)]), shape_params [S,Ps],
+ * color_params [S,Pc]. sdf_id / color_id as produced by the reference get_stroke
+ * (strokes.py:95-106): every base SDF; colour 0 constant rgb, 1 gradient rgb (12
+ * params), 2 SH2 (12), 3 SH3 (27). */
+int n3ds_stroke_forward(float* alpha_out, float* color_out, float* sdf_out, float* texcoord_out, int64_t n_texcoord,
                         const float* x, const float* radius, const float* viewdir,
                         const float* shape_params, const float* color_params, int64_t n_points,
                         int64_t n_viewdirs, int64_t n_strokes, int64_t n_shape_params,
@@ -144,7 +145,8 @@ int n3ds_compose_mode_backward(int mode, float* grad_alphas, float* grad_colors,
  * (with that device current) looks the array's address up with cudaGetSymbolAddress;
  * a caller that records the call into a stream capture makes one call on that device
  * before capturing. Same arguments, outputs and errors as n3ds_stroke_forward. */
-int n3ds_stroke_forward_static(float* alpha_out, float* color_out, float* sdf_out, int64_t n_texcoord,
+int n3ds_stroke_forward_static(float* alpha_out, float* color_out, float* sdf_out, float* texcoord_out,
+                               int64_t n_texcoord,
                                const float* x, const float* radius, const float* viewdir,
                                const float* shape_params, const float* color_params, int64_t n_points,
                                int64_t n_viewdirs, int64_t n_strokes, int64_t n_shape_params,

@@ -53,7 +53,7 @@ _SIGS = {
     "n3ds_last_error": (ctypes.c_char_p, []),
     "n3ds_version": (ctypes.c_int, []),
     "n3ds_stroke_workspace_bytes": (c_size_t, [c_i64]),
-    "n3ds_stroke_forward": (ctypes.c_int, [_P, _P, _P, c_i64, _P, _P, _P, _P, _P, c_i64, c_i64, c_i64, c_i64,
+    "n3ds_stroke_forward": (ctypes.c_int, [_P, _P, _P, _P, c_i64, _P, _P, _P, _P, _P, c_i64, c_i64, c_i64, c_i64,
                                            c_i64, c_u32, c_u32, ctypes.c_float, ctypes.c_int, ctypes.c_int,
                                            _P, c_size_t, _P]),
     "n3ds_stroke_backward": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, c_i64, c_i64,
@@ -81,7 +81,7 @@ _SIGS = {
     "n3ds_compose_mode_forward": (ctypes.c_int, [ctypes.c_int, _P, _P, _P, _P, _P, c_i64, c_i64, c_i64, _P]),
     "n3ds_compose_mode_backward": (ctypes.c_int, [ctypes.c_int, _P, _P, _P, _P, _P, _P, _P, _P, c_i64, c_i64,
                                                   c_i64, _P]),
-    "n3ds_stroke_forward_static": (ctypes.c_int, [_P, _P, _P, c_i64, _P, _P, _P, _P, _P, c_i64, c_i64, c_i64,
+    "n3ds_stroke_forward_static": (ctypes.c_int, [_P, _P, _P, _P, c_i64, _P, _P, _P, _P, _P, c_i64, c_i64, c_i64,
                                                   c_i64, c_i64, c_u32, c_u32, ctypes.c_float, ctypes.c_int,
                                                   ctypes.c_int, _P]),
 }

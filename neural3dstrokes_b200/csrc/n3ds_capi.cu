@@ -569,7 +569,8 @@ int check_stroke_args(uint32_t sdf_id, uint32_t color_id, int64_t n_points, int6
     return fail(N3DS_ERR_INVALID, "sdf base " + std::to_string(base) + " does not exist (bases 0-11)");
   if (base > n3ds::B_TETRAHEDRON && (sdf_id & 15u))
     return fail(N3DS_ERR_UNSUPPORTED, "Bezier strokes take no transform flags");
-  if (n_texcoord != 0) return fail(N3DS_ERR_UNSUPPORTED, "texcoord output is not implemented");
+  if (n_texcoord != 0 && n_texcoord < 2 * n_points * n_strokes)
+    return fail(N3DS_ERR_INVALID, "texcoord_output must hold [P, S, 2] floats");
   if (n_points < 0 || n_strokes < 0) return fail(N3DS_ERR_INVALID, "negative sizes");
   if (n_viewdirs <= 0 && n_points > 0) return fail(N3DS_ERR_INVALID, "viewdir must have at least one row");
   if (n_strokes > 0 && n_shape_params < n3ds::sdf_id_param_count((int)sdf_id))
@@ -632,7 +633,8 @@ n3ds::UfColor color_launch(const float* x, const float* viewdir, const float* re
 
 }  // namespace
 
-int n3ds_stroke_forward(float* alpha_out, float* color_out, float* sdf_out, int64_t n_texcoord, const float* x,
+int n3ds_stroke_forward(float* alpha_out, float* color_out, float* sdf_out, float* texcoord_out, int64_t n_texcoord,
+                        const float* x,
                         const float* radius, const float* viewdir, const float* shape_params,
                         const float* color_params, int64_t n_points, int64_t n_viewdirs, int64_t n_strokes,
                         int64_t n_shape_params, int64_t n_color_params, uint32_t sdf_id, uint32_t color_id,
@@ -667,6 +669,12 @@ int n3ds_stroke_forward(float* alpha_out, float* color_out, float* sdf_out, int6
                                    n_strokes);
     C.color = color_out;
     N3DS_CUDA_TRY(n3ds::launch_uf_color_fwd(C, st));
+  }
+  if (n_texcoord != 0) {
+    if (!texcoord_out) return fail(N3DS_ERR_INVALID, "texcoord_out is null");
+    n3ds::UfColor C = color_launch(x, viewdir, w.recs, color_params, n_color_params, color_id, n_points, n_viewdirs,
+                                   n_strokes);
+    N3DS_CUDA_TRY(n3ds::launch_uf_texcoord(C, texcoord_out, st));
   }
   return N3DS_OK;
 }

@@ -232,6 +232,76 @@ __global__ void __launch_bounds__(COL_WARPS * 32) uf_color_bwd_kernel(const UfCo
   }
 }
 
+// Orders the axes of d by the values sc (permute_multiscale_axis, strokes_sdf.h:212-222).
+__device__ __forceinline__ V3 permute_by(V3 d, V3 sc) {
+  if (sc.x > sc.y) {
+    if (sc.y > sc.z) return d;
+    return sc.x > sc.z ? V3{d.x, d.z, d.y} : V3{d.z, d.x, d.y};
+  }
+  if (sc.z > sc.y) return V3{d.z, d.y, d.x};
+  return sc.x > sc.z ? V3{d.y, d.x, d.z} : V3{d.y, d.z, d.x};
+}
+
+// Texture coordinates of the local sample (BaseSDF::texcoord: sphere strokes_sdf.h:259-267,
+// cube and round cube 302-310 / 359-367, capsule 455-467, line 510-522; (0, 0) for the
+// other bases). The per-axis permutation reads three values at the offset each base
+// uses there: the scales, or for the round cube its radius and two scales.
+__device__ __forceinline__ float2 prim_texcoord(const float* rec, int kind, V3 p) {
+  constexpr float PI_F = 3.14159265358979323846f;
+  const int base = kind & 15;
+  const bool s3 = ((kind >> 4) & F_S3) && !((kind >> 4) & F_S1);
+  const V3 s = xyz(rec4(rec)[R_S / 4]);
+  switch (base) {
+    case B_SPHERE: {
+      V3 d = p * rsqrtf(dot(p, p));
+      if (s3) d = permute_by(d, s);
+      return make_float2(asinf(clampf(d.x, -1.f, 1.f)) / PI_F + 0.5f, atan2f(d.z, d.y) / (2.0f * PI_F) + 0.5f);
+    }
+    case B_CUBE:
+    case B_ROUND_CUBE: {
+      V3 uvt = p * 0.5f + 0.5f;
+      if (s3) uvt = permute_by(uvt, base == B_CUBE ? s : V3{rec[R_BP], s.x, s.y});
+      return make_float2(clampf(uvt.x, 0.f, 1.f), clampf(uvt.y, 0.f, 1.f));
+    }
+    case B_CAPSULE:
+    case B_LINE: {
+      const float h = rec[R_BP];
+      const float u = base == B_CAPSULE ? clampf((p.y / (h + 1.0f)) * 0.5f + 0.5f, 0.f, 1.f)
+                                        : clampf((p.y + h + 1.0f - rec[R_BP2]) / (2.0f * h + 2.0f), 0.f, 1.f);
+      // the capsule reads its scales after the half-length; the line (single-scale in
+      // every reference shape) would read its radius change first
+      const V3 sc = base == B_CAPSULE ? s : V3{rec[R_BP2], s.x, s.y};
+      if (s3 && sc.z > sc.x) p = V3{p.z, p.y, p.x};
+      return make_float2(u, atan2f(p.z, p.x) / (2.0f * PI_F) + 0.5f);
+    }
+    default:
+      return make_float2(0.f, 0.f);
+  }
+}
+
+__global__ void __launch_bounds__(COL_WARPS * 32) uf_texcoord_kernel(const UfColor L, float* texcoord) {
+  __shared__ __align__(16) float recs[32 * COL_RS];
+  const int s0 = blockIdx.y * 32;
+  const int ns = min(32, L.n_strokes - s0);
+  for (int i = threadIdx.x; i < ns * REC_FLOATS; i += blockDim.x)
+    recs[(i / REC_FLOATS) * COL_RS + (i % REC_FLOATS)] = L.recs[(long long)s0 * REC_FLOATS + i];
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const bool active = lane < ns;
+  const long long s = s0 + (active ? lane : 0);
+  const float* rec = recs + (active ? lane : 0) * COL_RS;
+  const int kind = __float_as_int(rec[R_KIND]);
+  const long long S = L.n_strokes;
+  for (long long p = (long long)blockIdx.x * COL_WARPS + warp; p < L.n_points; p += (long long)gridDim.x * COL_WARPS) {
+    const V3 x = v3(L.x[3 * p], L.x[3 * p + 1], L.x[3 * p + 2]);
+    const float2 uv = prim_texcoord(rec, kind, unit_pos(rec, kind & 15, x));
+    if (active) {
+      texcoord[(p * S + s) * 2] = uv.x;
+      texcoord[(p * S + s) * 2 + 1] = uv.y;
+    }
+  }
+}
+
 dim3 color_grid(const UfColor& L) {
   const int sblocks = (L.n_strokes + 31) / 32;
   long long want = (148LL * 8 + sblocks - 1) / sblocks;
@@ -251,6 +321,11 @@ cudaError_t launch_uf_color_fwd(const UfColor& L, cudaStream_t st) {
     case 3: uf_color_fwd_kernel<3><<<grid, COL_WARPS * 32, 0, st>>>(L); break;
     default: return cudaErrorInvalidValue;
   }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_uf_texcoord(const UfColor& L, float* texcoord, cudaStream_t st) {
+  uf_texcoord_kernel<<<color_grid(L), COL_WARPS * 32, 0, st>>>(L, texcoord);
   return cudaGetLastError();
 }
 

@@ -65,7 +65,8 @@ int scratch_address(void** out) {
 
 }  // namespace
 
-extern "C" int n3ds_stroke_forward_static(float* alpha_out, float* color_out, float* sdf_out, int64_t n_texcoord,
+extern "C" int n3ds_stroke_forward_static(float* alpha_out, float* color_out, float* sdf_out, float* texcoord_out,
+                                          int64_t n_texcoord,
                                           const float* x, const float* radius, const float* viewdir,
                                           const float* shape_params, const float* color_params, int64_t n_points,
                                           int64_t n_viewdirs, int64_t n_strokes, int64_t n_shape_params,
@@ -82,7 +83,7 @@ extern "C" int n3ds_stroke_forward_static(float* alpha_out, float* color_out, fl
   void* scratch = nullptr;
   int rc = scratch_address(&scratch);
   if (rc) return rc;
-  return n3ds_stroke_forward(alpha_out, color_out, sdf_out, n_texcoord, x, radius, viewdir, shape_params,
+  return n3ds_stroke_forward(alpha_out, color_out, sdf_out, texcoord_out, n_texcoord, x, radius, viewdir, shape_params,
                              color_params, n_points, n_viewdirs, n_strokes, n_shape_params, n_color_params, sdf_id,
                              color_id, sdf_delta, use_laplace_transform, inv_scale_radius, scratch, kScratchBytes,
                              stream);

@@ -46,6 +46,8 @@ struct UfColor {
 };
 cudaError_t launch_uf_color_fwd(const UfColor& L, cudaStream_t st);
 cudaError_t launch_uf_color_bwd(const UfColor& L, cudaStream_t st);
+// texture coordinates [P*S*2] of the local samples (uses x, recs, n_points, n_strokes)
+cudaError_t launch_uf_texcoord(const UfColor& L, float* texcoord, cudaStream_t st);
 
 struct UfCompose {
   const float* alphas;     // [P*S]

@@ -75,7 +75,8 @@ def stroke_forward(alpha_output, color_output, sdf_output, texcoord_output, x, r
         ws_bytes = lib.n3ds_stroke_workspace_bytes(S)
         ws = _lib.workspace(ws_bytes, x.device)
         rc = lib.n3ds_stroke_forward(
-            _lib.ptr(alpha_output), _lib.ptr(color_output), _lib.ptr(sdf_output), texcoord_output.numel(),
+            _lib.ptr(alpha_output), _lib.ptr(color_output), _lib.ptr(sdf_output), _lib.ptr(texcoord_output),
+            texcoord_output.numel(),
             _lib.ptr(x), _lib.ptr(radius), _lib.ptr(viewdir), _lib.ptr(shape_params), _lib.ptr(color_params),
             P, viewdir.size(0), S, shape_params.size(1) if shape_params.dim() == 2 else 0,
             color_params.size(1) if color_params.dim() == 2 else 0, int(sdf_id), int(color_id),

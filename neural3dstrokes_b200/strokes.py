@@ -9,8 +9,8 @@ operators of ``neural3dstrokes_b200.strokelib``.
 
 Differences, all deliberate: the shape/colour tables are this module's own; calling
 get_stroke repeatedly does not grow the range lists (the reference mutates them in
-place, strokes.py:245-252); texture coordinates are not produced; the non-'over'
-composition modes run on their own CUDA kernels (torch ops in the reference).
+place, strokes.py:245-252); the non-'over' composition modes run on their own CUDA
+kernels (torch ops in the reference).
 """
 import math
 
@@ -86,8 +86,6 @@ class _StrokeFn(torch.autograd.Function):
             raise ValueError("x must have shape [..., num_samples, 3]")
         if shape_params.dim() != 2 or color_params.dim() != 2 or shape_params.shape[0] != color_params.shape[0]:
             raise ValueError("shape_params / color_params must be [num_strokes, n] with equal num_strokes")
-        if return_texcoord:
-            raise NotImplementedError("texcoord output is not implemented")
         pre = x.shape[:-1]
         x = x.contiguous().reshape(-1, 3).float()
         radius = radius.contiguous().reshape(-1).float()
@@ -98,13 +96,15 @@ class _StrokeFn(torch.autograd.Function):
         alpha = torch.empty(x.shape[0], S, device=x.device)
         color = torch.empty(x.shape[0], S, _COLOR_DIM, device=x.device)
         sdf = torch.empty(0 if no_sdf else (x.shape[0], S), device=x.device)
-        _backend.stroke_forward(alpha, color, sdf, torch.empty(0, device=x.device), x, radius, viewdir,
-                                shape_params, color_params, sdf_id, color_id, sdf_delta, use_laplace_transform,
-                                inv_scale_radius)
+        tex = torch.empty((x.shape[0], S, 2) if return_texcoord else 0, device=x.device)
+        _backend.stroke_forward(alpha, color, sdf, tex, x, radius, viewdir, shape_params, color_params, sdf_id,
+                                color_id, sdf_delta, use_laplace_transform, inv_scale_radius)
         ctx.save_for_backward(x, radius, viewdir, alpha, shape_params, color_params)
         ctx.args = (sdf_id, color_id, sdf_delta, use_laplace_transform, inv_scale_radius, pre)
+        if return_texcoord:
+            ctx.mark_non_differentiable(tex)
         return (alpha.reshape(*pre, S), color.reshape(*pre, S, _COLOR_DIM),
-                None if no_sdf else sdf.reshape(*pre, S), None)
+                None if no_sdf else sdf.reshape(*pre, S), tex.reshape(*pre, S, 2) if return_texcoord else None)
 
     @staticmethod
     @once_differentiable

@@ -668,6 +668,63 @@ def color_param_grads(color_id, p_local, viewdir_per_point, color_params, grad_c
     return torch.einsum("psc,pn->snc", grgb, w).reshape(S, 3 * n)
 
 
+# ---------------------------------------------------------- texture coordinates
+
+def _permute_by_scale(d, sc):
+    """permute_multiscale_axis (strokes_sdf.h:212-222): order the axes by the three
+    values sc [S,3] (the per-axis scale, read at the base's offset)."""
+    sx, sy, sz = (sc[None, :, k] for k in range(3))
+    x, y, z = d.unbind(-1)
+    c1 = sx > sy
+    c2 = sy > sz
+    c3 = sx > sz
+    c4 = sz > sy
+    out_x = torch.where(c1, torch.where(c2, x, torch.where(c3, x, z)), torch.where(c4, z, torch.where(c3, y, y)))
+    out_y = torch.where(c1, torch.where(c2, y, torch.where(c3, z, x)), torch.where(c4, y, torch.where(c3, x, z)))
+    out_z = torch.where(c1, torch.where(c2, z, torch.where(c3, y, y)), torch.where(c4, x, torch.where(c3, z, x)))
+    return torch.stack([out_x, out_y, out_z], -1)
+
+
+def texcoord(p, shape_params, sdf_id):
+    """Surface texture coordinates (u, v) [P,S,2] of the local sample (BaseSDF::texcoord,
+    strokes_sdf.h: sphere 259-267, cube / round cube 302-310 / 359-367, capsule 455-467,
+    line 510-522; (0, 0) for the others). The per-axis permutation reads three values
+    at the offset each base uses there (the round cube's reads its radius and two
+    scales)."""
+    base, t, r, s1, s3 = decode_sdf_id(sdf_id)
+    P, S = p.shape[0], p.shape[1]
+    zero = torch.zeros(P, S, dtype=p.dtype)
+    pi = 3.14159265358979323846
+    if base == 0:
+        d = p * torch.rsqrt(_len_sq(p))[..., None]
+        if s3:
+            d = _permute_by_scale(d, shape_params[:, 0:3])
+        u = torch.asin(cu_clamp(d[..., 0], -1.0, 1.0)) / pi + 0.5
+        v = torch.atan2(d[..., 2], d[..., 1]) / (2.0 * pi) + 0.5
+        return torch.stack([u, v], -1)
+    if base in (1, 2):
+        uvt = p * 0.5 + 0.5
+        if s3:
+            uvt = _permute_by_scale(uvt, shape_params[:, 0:3])
+        return torch.stack([cu_clamp(uvt[..., 0], 0.0, 1.0), cu_clamp(uvt[..., 1], 0.0, 1.0)], -1)
+    if base in (4, 5):
+        h = shape_params[None, :, 0]
+        y = p[..., 1]
+        if base == 4:
+            u = cu_clamp((y / (h + 1.0)) * 0.5 + 0.5, 0.0, 1.0)
+        else:
+            rd = shape_params[None, :, 1]
+            u = cu_clamp((y + h + 1.0 - rd) / (2.0 * h + 2.0), 0.0, 1.0)
+        px, pz = p[..., 0], p[..., 2]
+        if s3:
+            sc = shape_params[:, 1:4]
+            swap = (sc[None, :, 2] > sc[None, :, 0])
+            px, pz = torch.where(swap, p[..., 2], p[..., 0]), torch.where(swap, p[..., 0], p[..., 2])
+        v = torch.atan2(pz, px) / (2.0 * pi) + 0.5
+        return torch.stack([u, v], -1)
+    return torch.stack([zero, zero], -1)
+
+
 def viewdir_per_point(viewdir, n_points):
     """The view direction of each point: viewdir[p // (P / n_viewdirs)]
     (strokes_forward.cu:47-48, 195-197)."""
@@ -678,7 +735,8 @@ def viewdir_per_point(viewdir, n_points):
 
 
 def stroke_forward(x, radius, shape_params, color_params, sdf_id, sdf_delta,
-                   use_laplace=False, inv_scale_radius=False, return_sdf=False, color_id=0, viewdir=None):
+                   use_laplace=False, inv_scale_radius=False, return_sdf=False, color_id=0, viewdir=None,
+                   return_texcoord=False):
     """alpha [P,S], color [P,S,3] for one sdf_id group and colour type
     (strokes_forward.cu:17-109; ColorField strokes_color.h:34-171)."""
     base = decode_sdf_id(sdf_id)[0]
@@ -695,6 +753,8 @@ def stroke_forward(x, radius, shape_params, color_params, sdf_id, sdf_delta,
             r = r / f
     alpha = soft_step(sdf, r, sdf_delta, use_laplace)
     color = color_field(color_id, p, x, viewdir_per_point(viewdir, x.shape[0]), color_params)
+    if return_texcoord:
+        return alpha, color, sdf, texcoord(p, shape_params, sdf_id)
     if return_sdf:
         return alpha, color, sdf
     return alpha, color

@@ -197,6 +197,26 @@ def make_strokelib(out):
                 arrays[f"{tag}/{k}"] = v.detach().cpu().numpy()
             arrays[f"{tag}/sdf_id"] = np.array(sid)
             arrays[f"{tag}/color_id"] = np.array(cid)
+    # texture coordinates (the shapes with a texcoord mapping, their per-axis-scale
+    # variants, and one without)
+    for kind in ("sphere", "ellipsoid", "cube", "aabb", "roundbox", "capsule", "scapsule", "line", "octahedron"):
+        g = torch.Generator().manual_seed(900 + len(kind))
+        sc = scenes.make_strokes([kind] * 7, g)
+        rays = scenes.make_rays(12, 10, g)
+        sid = scenes.SDF_ID[kind]
+        ps = sc.shape_params[:, :sf.num_shape_params(sid)].contiguous()
+        x = rays.x.reshape(-1, 3).contiguous()
+        r = rays.radius.reshape(-1).contiguous()
+        P, S = x.shape[0], ps.shape[0]
+        a = torch.empty(P, S, device=dev)
+        c = torch.empty(P, S, 3, device=dev)
+        tex = torch.empty(P, S, 2, device=dev)
+        ref.stroke_forward(a, c, torch.empty(0, device=dev), tex, x.to(dev), r.to(dev), rays.dirs.to(dev),
+                           ps.to(dev), sc.color_params.to(dev), sid, 0, 0.02, True, True)
+        tag = f"{kind}_tex"
+        for k, v in dict(x=x, radius=r, shape=ps, color=sc.color_params, texcoord=tex).items():
+            arrays[f"{tag}/{k}"] = v.detach().cpu().numpy()
+        arrays[f"{tag}/sdf_id"] = np.array(sid)
     g = torch.Generator().manual_seed(99)
     P, S = 300, 37
     al = torch.rand(P, S, generator=g) ** 3

@@ -102,3 +102,26 @@ def test_color_field_compat_matches_reference_op(cuda, kind, cid):
         outs.append((gps, gcp, gx))
     for m, rr in zip(*outs):
         assert rel(m, rr) < GRAD_TOL, rel(m, rr)
+
+
+@pytest.mark.parametrize("kind", ["sphere", "ellipsoid", "cube", "aabb", "roundbox", "capsule", "scapsule", "line",
+                                  "octahedron", "cubic_bezier"])
+def test_texcoord_matches_oracle(cuda, kind):
+    g = torch.Generator().manual_seed(41)
+    sc = scenes.make_strokes([kind] * 10, g)
+    rays = scenes.make_rays(30, 12, g)
+    sid = scenes.SDF_ID[kind]
+    ps = sc.shape_params[:, :sf.num_shape_params(sid)].contiguous()
+    x = rays.x.reshape(-1, 3).contiguous()
+    r = rays.radius.reshape(-1).contiguous()
+    P, S = x.shape[0], ps.shape[0]
+    a = torch.empty(P, S, device=cuda)
+    c = torch.empty(P, S, 3, device=cuda)
+    tex = torch.empty(P, S, 2, device=cuda)
+    sl.stroke_forward(a, c, torch.empty(0, device=cuda), tex, x.to(cuda), r.to(cuda), rays.dirs.to(cuda), ps.to(cuda),
+                      sc.color_params.to(cuda), sid, 0, 0.02, True, True)
+    *_, tex_r = sf.stroke_forward(x.double(), r.double(), ps.double(), sc.color_params.double(), sid, 0.02, True, True,
+                                  return_texcoord=True)
+    d = (tex.cpu().double() - tex_r).abs()
+    d = torch.minimum(d, (1.0 - d).abs())
+    assert float(d.max()) < 1e-5, float(d.max())

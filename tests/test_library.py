@@ -40,12 +40,12 @@ def test_pure_host_calls():
     bad = _lib.Batch(0, nr, ns, 64)
     assert lib.n3ds_field_workspace_bytes(ctypes.byref(bad), ctypes.byref(o)) == 0
     # argument validation happens before any device work
-    rc = lib.n3ds_stroke_forward(None, None, None, 20, None, None, None, None, None, 10, 1, 4, 9, 3, 0x37, 0,
+    rc = lib.n3ds_stroke_forward(None, None, None, None, 20, None, None, None, None, None, 10, 1, 4, 9, 3, 0x37, 0,
                                  0.02, 1, 1, None, 0, None)
-    assert rc == 2 and b"texcoord" in lib.n3ds_last_error()
-    rc = lib.n3ds_stroke_forward(None, None, None, 0, None, None, None, None, None, 10, 1, 4, 9, 3, 0x37, 3,
+    assert rc == 1 and b"texcoord" in lib.n3ds_last_error()
+    rc = lib.n3ds_stroke_forward(None, None, None, None, 0, None, None, None, None, None, 10, 1, 4, 9, 3, 0x37, 3,
                                  0.02, 1, 1, None, 0, None)
     assert rc == 1 and b"27 columns" in lib.n3ds_last_error()
-    rc = lib.n3ds_stroke_forward(None, None, None, 0, None, None, None, None, None, 10, 1, 4, 4, 3, 0xC0, 0,
+    rc = lib.n3ds_stroke_forward(None, None, None, None, 0, None, None, None, None, None, 10, 1, 4, 4, 3, 0xC0, 0,
                                  0.02, 1, 1, None, 0, None)
     assert rc in (1, 2)  # sdf base 12 does not exist

@@ -229,3 +229,23 @@ def test_color_fields_match_reference_strokelib(kind, cid):
                                            g("color"), sid, 0.02, True, True, color_id=cid, viewdir=g("viewdir"))
     assert rel(gc, g("grad_color")) < 1e-5, rel(gc, g("grad_color"))
     assert rel(gs, g("grad_shape")) < 1e-4 and rel(gx, g("grad_x")) < 1e-4
+
+
+@pytest.mark.skipif(not os.path.exists(STROKELIB), reason="strokelib golden not recorded yet")
+@pytest.mark.parametrize("kind", ["sphere", "ellipsoid", "cube", "aabb", "roundbox", "capsule", "scapsule", "line",
+                                  "octahedron"])
+def test_texcoord_matches_reference_strokelib(kind):
+    """Texture coordinates of the restatement against the reference op (away from the
+    v seam, where atan2 jumps between 0 and 1)."""
+    z = np.load(STROKELIB)
+    tag = f"{kind}_tex"
+    if f"{tag}/texcoord" not in z.files:
+        pytest.skip("texcoord golden vectors not recorded")
+    g = lambda k: torch.from_numpy(z[f"{tag}/{k}"]).double()
+    sid = int(z[f"{tag}/sdf_id"])
+    *_, tex = sf.stroke_forward(g("x"), g("radius"), g("shape"), g("color"), sid, 0.02, True, True,
+                                return_texcoord=True)
+    ref = g("texcoord")
+    d = (tex - ref).abs()
+    d = torch.minimum(d, (1.0 - d).abs())  # the seam of v
+    assert float(d.max()) < 1e-5, float(d.max())

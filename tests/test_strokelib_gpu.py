@@ -177,9 +177,9 @@ def test_errors_are_runtime_errors(cuda):
     with pytest.raises(RuntimeError, match="must be a CUDA tensor"):
         sl.stroke_forward(torch.empty(60, 4), torch.empty(60, 4, 3), torch.empty(0), torch.empty(0), x, r, vd, ps,
                           col, sid, 0, 0.02, True, True)
-    with pytest.raises(RuntimeError, match="texcoord"):  # texture coordinates are not produced
+    with pytest.raises(RuntimeError, match="texcoord"):  # texcoord output too small for [P, S, 2]
         sl.stroke_forward(torch.empty(60, 4, device=cuda), torch.empty(60, 4, 3, device=cuda),
-                          torch.empty(0, device=cuda), torch.empty(60, 4, 2, device=cuda), x.to(cuda), r.to(cuda),
+                          torch.empty(0, device=cuda), torch.empty(60, 4, 1, device=cuda), x.to(cuda), r.to(cuda),
                           vd.to(cuda), ps.to(cuda), col.to(cuda), sid, 0, 0.02, True, True)
     with pytest.raises(RuntimeError, match="27 columns"):  # SH3 needs 27 colour parameters
         sl.stroke_forward(torch.empty(60, 4, device=cuda), torch.empty(60, 4, 3, device=cuda),

@@ -39,7 +39,7 @@ def _outputs(P, S, dev):
 def _call(lib, fn, outs, sid, ps, col, x, r, vd, delta, lap, inv, ws=None):
     a, c, d = outs
     P, S = x.shape[0], ps.shape[0]
-    args = [_lib.ptr(a), _lib.ptr(c), _lib.ptr(d), 0, _lib.ptr(x), _lib.ptr(r), _lib.ptr(vd), _lib.ptr(ps),
+    args = [_lib.ptr(a), _lib.ptr(c), _lib.ptr(d), None, 0, _lib.ptr(x), _lib.ptr(r), _lib.ptr(vd), _lib.ptr(ps),
             _lib.ptr(col), P, vd.shape[0], S, ps.shape[1], col.shape[1], sid, 0, delta, int(lap), int(inv)]
     if ws is not None:
         args += [_lib.ptr(ws), ws.numel()]
