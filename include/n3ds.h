@@ -170,13 +170,17 @@ typedef struct n3ds_batch {
 } n3ds_batch_t;
 
 typedef struct n3ds_rays {
-  const float* x;      /* [R*N*3] sample positions */
-  const float* radius; /* [R*N] sample radii */
+  const float* x;      /* [R*N*3] sample positions, or NULL to cast them from the rays */
+  const float* radius; /* [R*N] sample radii (unused when x is NULL) */
   const float* tdist;  /* [R*(N+1)] fence-post distances */
   const float* dirs;   /* [R*3] ray directions (their norm scales the intervals) */
   const float* bg;     /* [R*3] background colour, or NULL to use bg_value */
   float bg_value;
   int32_t opaque_background;
+  /* with x == NULL the kernels cast the samples themselves (cast_rays, render.py:5-26):
+   * x_i = dirs * t_i + origins, radius_i = radii * t_i, t_i = (tdist_i + tdist_i+1) / 2 */
+  const float* origins; /* [R*3] */
+  const float* radii;   /* [R] base radii */
 } n3ds_rays_t;
 
 typedef struct n3ds_strokes {
@@ -232,7 +236,9 @@ int n3ds_field_backward(const n3ds_batch_t* batch, const n3ds_rays_t* rays,
                         n3ds_stream_t stream);
 
 /* Synchronously read (and clear) the device status word and the count of evaluated
- * (sample, stroke) pairs of the last forward. status 0 = fine. */
+ * (sample, stroke) pairs of the last forward. n3ds_field_forward clears the status
+ * word first, so it reports the last forward and the backwards after it: 0 = fine,
+ * bit 1 = an unsupported sdf id, bit 2 = a bounded wait gave up. */
 int n3ds_field_read_status(void* workspace, int32_t* status, uint64_t* evaluated_pairs,
                            n3ds_stream_t stream);
 

@@ -32,7 +32,7 @@ class Batch(ctypes.Structure):
 class Rays(ctypes.Structure):
     _fields_ = [("x", ctypes.c_void_p), ("radius", ctypes.c_void_p), ("tdist", ctypes.c_void_p),
                 ("dirs", ctypes.c_void_p), ("bg", ctypes.c_void_p), ("bg_value", ctypes.c_float),
-                ("opaque_background", c_i32)]
+                ("opaque_background", c_i32), ("origins", ctypes.c_void_p), ("radii", ctypes.c_void_p)]
 
 
 class Strokes(ctypes.Structure):

@@ -280,8 +280,10 @@ static int field_common(const n3ds_batch_t* batch, const n3ds_rays_t* rays, cons
                         void* ws, size_t ws_bytes, long long* R, long long* S, WsLayout* lay) {
   int rc = check_batch(batch, R, S);
   if (rc) return rc;
-  if (!rays || (*R > 0 && (!rays->x || !rays->radius || !rays->tdist || !rays->dirs)))
-    return fail(N3DS_ERR_INVALID, "rays: x, radius, tdist and dirs are required");
+  if (!rays || (*R > 0 && (!rays->tdist || !rays->dirs)))
+    return fail(N3DS_ERR_INVALID, "rays: tdist and dirs are required");
+  if (*R > 0 && !(rays->x ? rays->radius != nullptr : (rays->origins && rays->radii)))
+    return fail(N3DS_ERR_INVALID, "rays: x and radius, or origins and radii (samples cast in-kernel), are required");
   if (!strokes || (*S > 0 && (!strokes->sdf_ids || !strokes->shape_params || !strokes->color_params ||
                               !strokes->density || !strokes->sdf_delta)))
     return fail(N3DS_ERR_INVALID, "strokes: sdf_ids, shape_params, color_params, density, sdf_delta required");
@@ -326,6 +328,10 @@ static n3ds::SegLaunch make_seg(const n3ds_batch_t* b, const n3ds_rays_t* rays, 
   n3ds::SegLaunch L{};
   L.x = rays->x;
   L.radius = rays->radius;
+  L.origins = rays->origins;
+  L.dirs = rays->dirs;
+  L.tdist = rays->tdist;
+  L.radii = rays->radii;
   L.n_samples = b->n_samples;
   L.recs = reinterpret_cast<const float*>(ws + lay.recs);
   L.cull_a = reinterpret_cast<const float*>(ws + lay.cull_a);
@@ -367,6 +373,9 @@ int n3ds_field_forward(const n3ds_batch_t* batch, const n3ds_rays_t* rays, const
   const Resolved rv = resolve(opt);
   char* ws = static_cast<char*>(workspace);
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  // the status word covers one forward and the backward after it (the prep kernel
+  // sets bits of it, so it is cleared before that kernel rather than by it)
+  N3DS_CUDA_TRY(cudaMemsetAsync(ws + lay.status, 0, sizeof(int32_t), st));
   n3ds::launch_prep(make_prep(strokes, S, rv, ws, lay, false), st);
   N3DS_CUDA_TRY(cudaGetLastError());
   record_event(rv, 0, st);

@@ -55,8 +55,7 @@ __device__ __forceinline__ SegCtx seg_setup(const SegLaunch& L, const SceneDesc&
   const int cnt = min(32, L.n_samples - i0);
   c.active = lane < cnt;
   c.si = ray * L.n_samples + i0 + (c.active ? lane : 0);
-  c.x = v3(L.x[3 * c.si], L.x[3 * c.si + 1], L.x[3 * c.si + 2]);
-  c.r = L.radius[c.si];
+  load_sample(L, ray, i0 + (c.active ? lane : 0), c.si, c.x, c.r);
   c.rinv = 1.f / c.r;
   c.A = shfl3(c.x, 0);
   V3 B = shfl3(c.x, cnt - 1);

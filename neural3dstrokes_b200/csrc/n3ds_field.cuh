@@ -23,8 +23,12 @@ struct SceneDesc {
 };
 
 struct SegLaunch {
-  const float* x;          // [P*3]
+  const float* x;          // [P*3], or null: samples cast from the rays below
   const float* radius;     // [P]
+  const float* origins;    // [R*3] (cast mode)
+  const float* dirs;       // [R*3] (cast mode)
+  const float* tdist;      // [R*(N+1)] (cast mode)
+  const float* radii;      // [R] (cast mode)
   int n_samples;           // samples per ray
   int segs_per_ray;        // ceil(n_samples / 32)
   const float* recs;       // [S*64] prepared stroke records

@@ -96,8 +96,8 @@ __device__ __forceinline__ void unit_setup(const SegLaunch& L, long long si0, in
   for (int b = 0; b < 2; b++) {
     const int j = lane + 32 * b;
     const long long si = si0 + (j < cnt ? j : 0);
-    U.x[b] = v3(L.x[3 * si], L.x[3 * si + 1], L.x[3 * si + 2]);
-    U.r[b] = L.radius[si];
+    const long long ray = si / L.n_samples;
+    load_sample(L, ray, (int)(si - ray * L.n_samples), si, U.x[b], U.r[b]);
   }
   U.A = shfl3(U.x[0], 0);
   const V3 last = cnt <= 32 ? shfl3(U.x[0], cnt - 1) : shfl3(U.x[1], cnt - 33);
@@ -229,8 +229,11 @@ __device__ __forceinline__ void eval_pairs(const SegLaunch& L, const RunStage& R
       const int e = B.table[p];
       const int slot = B.run_sk[e >> 8] & 0xffff;
       const long long si = U.si0 + (e & 255);
-      const V3 x = v3(L.x[3 * si], L.x[3 * si + 1], L.x[3 * si + 2]);
-      B.val[p] = pair_alpha(R.s.recs + size_t(slot) * REC_FLOATS, x, 1.f / L.radius[si]);
+      const long long ray = si / L.n_samples;
+      V3 x;
+      float rr;
+      load_sample(L, ray, (int)(si - ray * L.n_samples), si, x, rr);
+      B.val[p] = pair_alpha(R.s.recs + size_t(slot) * REC_FLOATS, x, 1.f / rr);
     }
   }
   __syncwarp();
@@ -549,8 +552,11 @@ __global__ void __launch_bounds__(WARPS * 32, 1) run_bwd_kernel(const __grid_con
             const int j = e & 255;
             slot = B.run_sk[run] & 0xffff;
             const long long si = U.si0 + j;
-            const V3 x = v3(L.x[3 * si], L.x[3 * si + 1], L.x[3 * si + 2]);
-            const float rinv = 1.f / L.radius[si];
+            const long long ray = si / L.n_samples;
+            V3 x;
+            float rr;
+            load_sample(L, ray, (int)(si - ray * L.n_samples), si, x, rr);
+            const float rinv = 1.f / rr;
             const float dm = B.val[p];
             const float* rec = R.s.recs + size_t(slot) * REC_FLOATS;
             const float4 h = rec4(rec)[0];

@@ -130,4 +130,21 @@ __device__ __forceinline__ bool stage_chunk(const SegLaunch& L, const SceneDesc&
   return *s_fail == 0;
 }
 
+// Sample i of ray `ray` (global sample index si = ray * n_samples + i): position and
+// radius from the inputs, or cast from the ray as cast_rays does (render.py:20-25):
+// t = (t0 + t1) / 2, x = d t + o, radius = r t.
+__device__ __forceinline__ void load_sample(const SegLaunch& L, long long ray, int i, long long si, V3& x, float& r) {
+  if (L.x) {
+    x = v3(L.x[3 * si], L.x[3 * si + 1], L.x[3 * si + 2]);
+    r = L.radius[si];
+  } else {
+    const float* td = L.tdist + ray * (L.n_samples + 1);
+    const float t = (td[i] + td[i + 1]) * 0.5f;
+    x = v3(__fadd_rn(__fmul_rn(L.dirs[3 * ray], t), L.origins[3 * ray]),
+           __fadd_rn(__fmul_rn(L.dirs[3 * ray + 1], t), L.origins[3 * ray + 1]),
+           __fadd_rn(__fmul_rn(L.dirs[3 * ray + 2], t), L.origins[3 * ray + 2]));
+    r = L.radii[ray] * t;
+  }
+}
+
 }  // namespace n3ds

@@ -49,13 +49,14 @@ class _Native:
     """ctypes argument blocks for one call (kept alive for the call's duration)."""
 
     def __init__(self, scene_rays, scene_strokes, n_samples, x, radius, tdist, dirs, bg, bg_value, opaque,
-                 sdf_ids, shape_params, color_params, density, delta, laplace, inv_scale, options):
+                 sdf_ids, shape_params, color_params, density, delta, laplace, inv_scale, options, origins=None,
+                 radii=None):
         n = len(scene_rays)
         self.nr = (ctypes.c_int64 * n)(*[int(v) for v in scene_rays])
         self.ns = (ctypes.c_int32 * n)(*[int(v) for v in scene_strokes])
         self.batch = _lib.Batch(n, self.nr, self.ns, int(n_samples))
         self.rays = _lib.Rays(_lib.ptr(x), _lib.ptr(radius), _lib.ptr(tdist), _lib.ptr(dirs), _lib.ptr(bg),
-                              float(bg_value), int(bool(opaque)))
+                              float(bg_value), int(bool(opaque)), _lib.ptr(origins), _lib.ptr(radii))
         self.strokes = _lib.Strokes(_lib.ptr(sdf_ids), _lib.ptr(shape_params), int(shape_params.shape[1]),
                                     _lib.ptr(color_params), _lib.ptr(density), _lib.ptr(delta), int(bool(laplace)),
                                     int(bool(inv_scale)))
@@ -74,10 +75,13 @@ def _f32(t, name):
 class _FieldFn(torch.autograd.Function):
     @staticmethod
     def forward(ctx, x, radius, tdist, dirs, shape_params, color_params, density, delta, bg_t, sdf_ids,
-                scene_rays, scene_strokes, bg_value, opaque, laplace, inv_scale, options):
-        R, N = x.shape[0], x.shape[1]
-        x, radius, tdist, dirs = (_f32(t, n) for t, n in ((x, "x"), (radius, "radius"), (tdist, "tdist"),
-                                                           (dirs, "dirs")))
+                scene_rays, scene_strokes, bg_value, opaque, laplace, inv_scale, options, origins=None, radii=None):
+        R, N = tdist.shape[0], tdist.shape[1] - 1
+        tdist, dirs = _f32(tdist, "tdist"), _f32(dirs, "dirs")
+        if x is not None:
+            x, radius = _f32(x, "x"), _f32(radius, "radius")
+        else:  # samples cast in-kernel from the rays
+            origins, radii = _f32(origins, "origins"), _f32(radii, "radii")
         shape_params, color_params, density, delta = (
             _f32(t, n) for t, n in ((shape_params, "shape_params"), (color_params, "color_params"),
                                     (density, "density"), (delta, "sdf_delta")))
@@ -86,21 +90,23 @@ class _FieldFn(torch.autograd.Function):
         sdf_ids = sdf_ids.contiguous()
         bg_c = _f32(bg_t, "bg") if bg_t is not None else None
         nat = _Native(scene_rays, scene_strokes, N, x, radius, tdist, dirs, bg_c, bg_value, opaque, sdf_ids,
-                      shape_params, color_params, density, delta, laplace, inv_scale, options)
+                      shape_params, color_params, density, delta, laplace, inv_scale, options, origins, radii)
         lib = _lib.load()
-        with torch.cuda.device(x.device):
+        dev = tdist.device
+        with torch.cuda.device(dev):
             ws_bytes = nat.ws_bytes()
             if ws_bytes == 0:
                 raise RuntimeError("invalid batch description")
-            ws = _lib.workspace(ws_bytes, x.device)
-            rgb = torch.empty(R, 3, device=x.device)
-            acc = torch.empty(R, device=x.device)
-            depth = torch.empty(R, device=x.device)
+            ws = _lib.workspace(ws_bytes, dev)
+            rgb = torch.empty(R, 3, device=dev)
+            acc = torch.empty(R, device=dev)
+            depth = torch.empty(R, device=dev)
             rc = lib.n3ds_field_forward(ctypes.byref(nat.batch), ctypes.byref(nat.rays), ctypes.byref(nat.strokes),
                                         ctypes.byref(nat.opt), _lib.ptr(rgb), _lib.ptr(acc), _lib.ptr(depth),
                                         _lib.ptr(ws), ws_bytes, _lib.stream_ptr())
         _lib.check(rc)
-        ctx.save_for_backward(x, radius, tdist, dirs, shape_params, color_params, density, delta, sdf_ids)
+        ctx.save_for_backward(x, radius, tdist, dirs, shape_params, color_params, density, delta, sdf_ids, origins,
+                              radii)
         ctx.bg = bg_c
         ctx.ws, ctx.ws_bytes = ws, ws_bytes
         ctx.meta = (scene_rays, scene_strokes, bg_value, opaque, laplace, inv_scale, options)
@@ -108,26 +114,27 @@ class _FieldFn(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, g_rgb, g_acc, g_depth):
-        x, radius, tdist, dirs, shape_params, color_params, density, delta, sdf_ids = ctx.saved_tensors
+        x, radius, tdist, dirs, shape_params, color_params, density, delta, sdf_ids, origins, radii = \
+            ctx.saved_tensors
         scene_rays, scene_strokes, bg_value, opaque, laplace, inv_scale, options = ctx.meta
-        N = x.shape[1]
+        N = tdist.shape[1] - 1
         nat = _Native(scene_rays, scene_strokes, N, x, radius, tdist, dirs, ctx.bg, bg_value, opaque, sdf_ids,
-                      shape_params, color_params, density, delta, laplace, inv_scale, options)
-        gx = torch.empty_like(x) if ctx.needs_input_grad[0] else None
+                      shape_params, color_params, density, delta, laplace, inv_scale, options, origins, radii)
+        gx = torch.empty_like(x) if (x is not None and ctx.needs_input_grad[0]) else None
         gshape = torch.empty_like(shape_params)
         gcol = torch.empty_like(color_params)
         gden = torch.empty_like(density)
         gdel = torch.empty_like(delta)
         g = [t.contiguous().float() if t is not None else None for t in (g_rgb, g_acc, g_depth)]
         lib = _lib.load()
-        with torch.cuda.device(x.device):
+        with torch.cuda.device(tdist.device):
             rc = lib.n3ds_field_backward(ctypes.byref(nat.batch), ctypes.byref(nat.rays), ctypes.byref(nat.strokes),
                                          ctypes.byref(nat.opt), _lib.ptr(g[0]), _lib.ptr(g[1]), _lib.ptr(g[2]),
                                          _lib.ptr(gx), _lib.ptr(gshape), _lib.ptr(gcol), _lib.ptr(gden),
                                          _lib.ptr(gdel), _lib.ptr(ctx.ws), ctx.ws_bytes, _lib.stream_ptr())
         _lib.check(rc)
         return (gx, None, None, None, gshape, gcol, gden, gdel, None, None, None, None, None, None, None, None,
-                None)
+                None, None, None)
 
 
 def render_strokes(x: torch.Tensor, radius: torch.Tensor, tdist: torch.Tensor, dirs: torch.Tensor,
@@ -171,6 +178,39 @@ def render_strokes(x: torch.Tensor, radius: torch.Tensor, tdist: torch.Tensor, d
     return _FieldFn.apply(x, radius, tdist, dirs, shape_params, color_params, density, delta, bg_t, sdf_ids,
                           scene_rays, scene_strokes, bg_value, opaque_background, use_laplace_transform,
                           inv_scale_radius, opts)
+
+
+def render_rays(origins: torch.Tensor, directions: torch.Tensor, radii: torch.Tensor, tdist: torch.Tensor,
+                shape_params: torch.Tensor, sdf_ids: torch.Tensor, color_params: torch.Tensor, density: torch.Tensor,
+                sdf_delta, use_laplace_transform: bool = True, inv_scale_radius: bool = True, bg=1.0,
+                opaque_background: bool = False, options: Optional[FieldOptions] = None,
+                scene_sizes: Optional[Sequence] = None):
+    """render_strokes with the samples cast in the kernels from the rays, as
+    cast_rays does (render.py:5-26): x = directions * t + origins, radius = radii * t,
+    t the interval midpoints of tdist. origins / directions [R,3], radii [R] or [R,1],
+    tdist [R,N+1]. Gradients flow to the stroke parameters and sdf_delta (the rays are
+    data in the reference's training step, models.py:183-191)."""
+    R = int(tdist.shape[0])
+    S = int(sdf_ids.numel())
+    dev = tdist.device
+    if origins.shape != (R, 3) or directions.shape != (R, 3) or radii.numel() != R or tdist.dim() != 2:
+        raise ValueError("expected origins / directions [R,3], radii [R], tdist [R,N+1]")
+    if torch.is_tensor(sdf_delta):
+        delta = sdf_delta.to(dev, torch.float32)
+        if delta.dim() == 0:
+            delta = delta.expand(S)
+    else:
+        delta = torch.full((S,), float(sdf_delta), device=dev)
+    if scene_sizes is None:
+        scene_sizes = [(R, S)]
+    scene_rays = [int(a) for a, _ in scene_sizes]
+    scene_strokes = [int(b) for _, b in scene_sizes]
+    if sum(scene_rays) != R or sum(scene_strokes) != S:
+        raise ValueError("scene_sizes do not add up to the ray / stroke counts")
+    bg_t, bg_value = (bg, 0.0) if torch.is_tensor(bg) else (None, float(bg))
+    return _FieldFn.apply(None, None, tdist, directions, shape_params, color_params, density, delta, bg_t, sdf_ids,
+                          scene_rays, scene_strokes, bg_value, opaque_background, use_laplace_transform,
+                          inv_scale_radius, options or FieldOptions(), origins, radii.reshape(R))
 
 
 def field_status(workspace):

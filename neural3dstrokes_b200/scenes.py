@@ -12,7 +12,7 @@ sample radius 1.
 """
 import math
 from dataclasses import dataclass, field
-from typing import List
+from typing import List, Optional
 
 import torch
 
@@ -57,6 +57,7 @@ class RaySet:
     tdist: torch.Tensor    # [R, N+1]
     x: torch.Tensor        # [R, N, 3]
     radius: torch.Tensor   # [R, N]
+    radii: Optional[torch.Tensor] = None  # [R] base radii when radius = radii * t (cast_rays)
 
     @property
     def n_rays(self):
@@ -67,7 +68,8 @@ class RaySet:
         return int(self.x.shape[1])
 
     def to(self, device):
-        return RaySet(*(t.to(device) for t in (self.origins, self.dirs, self.tdist, self.x, self.radius)))
+        return RaySet(*(t.to(device) if t is not None else None
+                        for t in (self.origins, self.dirs, self.tdist, self.x, self.radius, self.radii)))
 
 
 def _unit(v):
@@ -155,7 +157,10 @@ def make_strokes(kinds, g, density=10.0, ctrl_sigma=0.15):
     return Scene(list(kinds), sdf_ids, params, colors, dens)
 
 
-def make_rays(n_rays, n_samples, g, near=2.0, far=6.0, jitter=0.5):
+def make_rays(n_rays, n_samples, g, near=2.0, far=6.0, jitter=0.5, base_radius=None):
+    """Rays through the scene box. With ``base_radius`` (a float) the rays are cones as
+    in cast_rays: per-ray base radii uniform in [0.5, 1.5] * base_radius and sample
+    radius = radii * t; without it every sample radius is 1."""
     u = _unit(torch.randn(n_rays, 3, generator=g))
     origins = 4.0 * u
     d0 = -u
@@ -170,8 +175,10 @@ def make_rays(n_rays, n_samples, g, near=2.0, far=6.0, jitter=0.5):
     tdist = near + (k[None, :] + jit) * ((far - near) / n_samples)
     t = 0.5 * (tdist[:, :-1] + tdist[:, 1:])
     x = origins[:, None, :] + dirs[:, None, :] * t[..., None]
-    radius = torch.ones(n_rays, n_samples)
-    return RaySet(origins, dirs, tdist, x, radius)
+    if base_radius is None:
+        return RaySet(origins, dirs, tdist, x, torch.ones(n_rays, n_samples))
+    radii = (torch.rand(n_rays, generator=g) + 0.5) * float(base_radius)
+    return RaySet(origins, dirs, tdist, x, radii[:, None] * t, radii)
 
 
 @dataclass

@@ -25,7 +25,10 @@ from .scenes import PARAM_STRIDE, RaySet, Scene, param_ranges
 class BatchedField:
     def __init__(self, scenes: List[Scene], rays: List[RaySet], sdf_delta=0.02, use_laplace=True,
                  inv_scale_radius=True, bg=1.0, opaque_background=False, options: Optional[FieldOptions] = None,
-                 device="cuda", need_grad_x=True):
+                 device="cuda", need_grad_x=True, cast: bool = False):
+        """``cast``: keep only the rays (origins, directions, base radii ``RaySet.radii``,
+        fence posts) on the device and let the kernels cast the samples
+        (x = d t + o, radius = radii t, as cast_rays); no position gradient then."""
         dev = torch.device(device)
         self.device = dev
         self.n_scenes = len(scenes)
@@ -35,8 +38,17 @@ class BatchedField:
         self.scene_rays = [r.n_rays for r in rays]
         self.scene_strokes = [s.n_strokes for s in scenes]
         cat = lambda ts: torch.cat(ts).to(dev).contiguous()
-        self.x = cat([r.x for r in rays])
-        self.radius = cat([r.radius for r in rays])
+        self.cast = bool(cast)
+        if self.cast:
+            if any(r.radii is None for r in rays):
+                raise ValueError("cast mode needs per-ray base radii (RaySet.radii)")
+            self.origins = cat([r.origins for r in rays])
+            self.radii = cat([r.radii for r in rays])
+            self.x = self.radius = None
+        else:
+            self.origins = self.radii = None
+            self.x = cat([r.x for r in rays])
+            self.radius = cat([r.radius for r in rays])
         self.tdist = cat([r.tdist for r in rays])
         self.dirs = cat([r.dirs for r in rays])
         self.sdf_ids = cat([s.sdf_ids for s in scenes])
@@ -45,7 +57,7 @@ class BatchedField:
         self.density = cat([s.density for s in scenes])
         self.kinds = [k for s in scenes for k in s.kinds]
         S = self.shape.shape[0]
-        R = self.x.shape[0]
+        R = self.tdist.shape[0]
         self.delta = torch.full((S,), float(sdf_delta), device=dev)
         self.rgb = torch.empty(R, 3, device=dev)
         self.acc = torch.empty(R, device=dev)
@@ -53,7 +65,7 @@ class BatchedField:
         self.g_rgb = torch.zeros(R, 3, device=dev)
         self.g_acc = torch.zeros(R, device=dev)
         self.g_depth = torch.zeros(R, device=dev)
-        self.grad_x = torch.empty_like(self.x) if need_grad_x else None
+        self.grad_x = torch.empty_like(self.x) if (need_grad_x and not self.cast) else None
         self.grad_shape = torch.empty_like(self.shape)
         self.grad_color = torch.empty_like(self.color)
         self.grad_density = torch.empty_like(self.density)
@@ -71,7 +83,7 @@ class BatchedField:
         self._ns = (ctypes.c_int32 * n)(*self.scene_strokes)
         self.c_batch = _lib.Batch(n, self._nr, self._ns, self.n_samples)
         self.c_rays = _lib.Rays(_lib.ptr(self.x), _lib.ptr(self.radius), _lib.ptr(self.tdist), _lib.ptr(self.dirs),
-                                None, self.bg_value, int(self.opaque))
+                                None, self.bg_value, int(self.opaque), _lib.ptr(self.origins), _lib.ptr(self.radii))
         self.c_strokes = _lib.Strokes(_lib.ptr(self.sdf_ids), _lib.ptr(self.shape), PARAM_STRIDE,
                                       _lib.ptr(self.color), _lib.ptr(self.density), _lib.ptr(self.delta),
                                       int(self.laplace), int(self.inv_scale))
