@@ -196,8 +196,9 @@ typedef struct n3ds_strokes {
 
 typedef struct n3ds_options {
   float cull_alpha;   /* drop a stroke where its alpha provably stays below this; <= 0: no culling */
-  int32_t chunk_fwd;  /* strokes per shared-memory stage, forward (0 = auto) */
-  int32_t chunk_bwd;  /* strokes per shared-memory stage, backward (0 = auto) */
+  int32_t chunk_fwd;  /* strokes per shared-memory stage, forward (0 = auto; else rounded
+                         down to a multiple of 32, at least 32) */
+  int32_t chunk_bwd;  /* strokes per shared-memory stage, backward (same rules) */
   int32_t warps;      /* warps per CTA, forward: 4, 8, 16, 24, 32 (0 = auto) */
   int32_t schedule;   /* N3DS_SCHEDULE_* (0 = auto: segments) */
   int32_t grad_mode;  /* N3DS_GRAD_EXACT or N3DS_GRAD_COMPAT */
@@ -205,6 +206,9 @@ typedef struct n3ds_options {
    * (forward begin/end, backward begin/end), or NULL */
   void* const* timing_events;
   int32_t warps_bwd;  /* warps per CTA, backward: 4, 8, 16, 20, 24 (0 = auto) */
+  /* 1: no backward follows this forward, so the segment kernels skip recording which
+   * strokes the backward needs (a backward after such a forward culls by itself) */
+  int32_t forward_only;
 } n3ds_options_t;
 
 /* Fill *opt with the defaults. */

@@ -41,7 +41,7 @@ def signature(field) -> str:
                       sort_keys=True)
 
 
-def candidates(grad_mode: str = "exact", cull_alpha: float = 1e-9) -> List[FieldOptions]:
+def candidates(grad_mode: str = "exact", cull_alpha: float = 1e-9, forward_only: bool = False) -> List[FieldOptions]:
     out = []
     # (schedule, forward warps, backward warps): the segment kernels' register use
     # allows up to 32 / 24 warps per CTA, the run kernels 16
@@ -51,7 +51,8 @@ def candidates(grad_mode: str = "exact", cull_alpha: float = 1e-9) -> List[Field
         for half in (False, True):
             # chunk 0 = the largest stage that fits; the halved stage (-1) is resolved later
             out.append(FieldOptions(cull_alpha=cull_alpha, warps=wf, warps_bwd=wb, schedule=schedule,
-                                    grad_mode=grad_mode, chunk_fwd=-1 if half else 0, chunk_bwd=-1 if half else 0))
+                                    grad_mode=grad_mode, chunk_fwd=-1 if half else 0, chunk_bwd=-1 if half else 0,
+                                    forward_only=forward_only))
     return out
 
 
@@ -117,7 +118,7 @@ def tune(field, reps: int = 3, cands: Optional[List[FieldOptions]] = None, use_c
         return best
     base = field.options
     results = []
-    for opt in cands or candidates(base.grad_mode, base.cull_alpha):
+    for opt in cands or candidates(base.grad_mode, base.cull_alpha, base.forward_only):
         opt = _resolve_half(field, opt)
         field.options = opt
         field._bind()

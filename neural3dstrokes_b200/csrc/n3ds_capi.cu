@@ -54,14 +54,22 @@ DevInfo dev_info() {
 constexpr size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
 struct WsLayout {
-  size_t recs, cull_a, cull_b, state, seeds, bstate, gslots, counters, status, stats, total;
+  size_t recs, cull_a, cull_b, state, seeds, bstate, gslots, counters, masks, status, stats, mask_tag, total;
 };
 // Ray counters: one block of MAX_SCENES_PER_LAUNCH per segment-kernel launch, the
 // first half for forward launches, the second for backward launches.
 constexpr int N_LAUNCH_SLOTS = 64;
 constexpr int N_COUNTERS = N_LAUNCH_SLOTS * n3ds::MAX_SCENES_PER_LAUNCH;
 
-WsLayout ws_layout(long long total_rays, int N, long long S) {
+// Stroke-block mask words of a batch: per scene, segments x ceil(strokes / 32).
+long long mask_words(const n3ds_batch_t* b) {
+  const long long spr = (b->n_samples + 31) / 32;
+  long long total = 0;
+  for (int i = 0; i < b->n_scenes; i++) total += b->n_rays[i] * spr * ((b->n_strokes[i] + 31) / 32);
+  return total;
+}
+
+WsLayout ws_layout(long long total_rays, int N, long long S, long long n_mask_words) {
   WsLayout w{};
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -70,9 +78,11 @@ WsLayout ws_layout(long long total_rays, int N, long long S) {
     return o;
   };
   const size_t P = size_t(total_rays) * size_t(N);
-  // header: int32 status at +0, uint64 evaluated pairs at +8, uint64 per-base counts at +16
+  // header: int32 status at +0, uint64 evaluated pairs at +8, uint64 per-base counts at
+  // +16, int32 stroke-block mask tag at +248
   w.status = take(256);
   w.stats = w.status + 8;
+  w.mask_tag = w.status + 248;
   w.recs = take(size_t(S) * n3ds::REC_FLOATS * 4);
   w.cull_a = take(size_t(S) * 16);
   w.cull_b = take(size_t(S + 4) * 4);
@@ -81,6 +91,7 @@ WsLayout ws_layout(long long total_rays, int N, long long S) {
   w.bstate = take(P * 8 * 4);
   w.gslots = take(size_t(S) * n3ds::GRAD_SLOTS * 4);
   w.counters = take(N_COUNTERS * 4);
+  w.masks = take(size_t(n_mask_words) * 4);
   w.total = off;
   return w;
 }
@@ -90,6 +101,7 @@ struct Resolved {
   int chunk_fwd, chunk_bwd, warps, schedule, grad_mode;
   int warps_fwd, warps_bwd;  // per direction (the forward segment kernel runs 24 warps by default)
   void* const* events;
+  int forward_only;
 };
 
 void record_event(const Resolved& rv, int i, cudaStream_t st) {
@@ -128,8 +140,10 @@ Resolved resolve(const n3ds_options_t* o) {
   r.warps = r.warps_bwd;
   const size_t budget = size_t(di.smem_optin) - 256;  // room for static shared memory
   // default stages: the largest multiple of 32 strokes that fits the shared memory
-  int cf = o->chunk_fwd > 0 ? o->chunk_fwd : 1024;
-  int cb = o->chunk_bwd > 0 ? o->chunk_bwd : 1024;
+  // (multiples of 32, so that the 32-stroke blocks of every pass line up with the
+  // stroke-block mask words in both directions)
+  int cf = o->chunk_fwd > 0 ? std::max(32, o->chunk_fwd / 32 * 32) : 1024;
+  int cb = o->chunk_bwd > 0 ? std::max(32, o->chunk_bwd / 32 * 32) : 1024;
   auto fwd_smem = [&](int c) { return runs ? n3ds::run_fwd_smem(c, r.warps_fwd) : n3ds::seg_fwd_smem(c); };
   auto bwd_smem = [&](int c) { return runs ? n3ds::run_bwd_smem(c, r.warps_bwd) : n3ds::seg_bwd_smem(c); };
   while (cf > 32 && fwd_smem(cf) > budget) cf -= 32;
@@ -137,6 +151,7 @@ Resolved resolve(const n3ds_options_t* o) {
   r.chunk_fwd = cf;
   r.chunk_bwd = cb;
   r.grad_mode = o->grad_mode;
+  r.forward_only = o->forward_only != 0;
   r.events = o->timing_events;
   return r;
 }
@@ -168,13 +183,15 @@ int run_seg_passes(bool backward, const n3ds_batch_t* b, const Resolved& rv, n3d
   const bool runs = rv.schedule == N3DS_SCHEDULE_RUNS;
   // work items per ray: the whole ray (segments) or 64-sample units (runs)
   const int ipr = runs ? (b->n_samples + n3ds::RUN_UNIT_SAMPLES - 1) / n3ds::RUN_UNIT_SAMPLES : 1;
-  std::vector<long long> ray_begin(b->n_scenes), stroke_begin(b->n_scenes);
+  std::vector<long long> ray_begin(b->n_scenes), stroke_begin(b->n_scenes), mask_begin(b->n_scenes);
   std::vector<int> nch(b->n_scenes);
-  long long r0 = 0, s0 = 0;
+  long long r0 = 0, s0 = 0, m0 = 0;
   int passes = 1;
   for (int i = 0; i < b->n_scenes; i++) {
     ray_begin[i] = r0;
     stroke_begin[i] = s0;
+    mask_begin[i] = m0;
+    m0 += b->n_rays[i] * spr * ((b->n_strokes[i] + 31) / 32);
     r0 += b->n_rays[i];
     s0 += b->n_strokes[i];
     nch[i] = std::max(1, (b->n_strokes[i] + cap - 1) / cap);
@@ -211,6 +228,8 @@ int run_seg_passes(bool backward, const n3ds_batch_t* b, const Resolved& rv, n3d
         d.chunk_n = std::max(0, hi - lo);
         d.first_pass = pass == 0;
         d.last_pass = pass == nch[i] - 1;
+        d.mask_words = (b->n_strokes[i] + 31) / 32;
+        d.mask_begin = mask_begin[i];
         if ((long long)d.n_rays * ipr > 0x7fffffffLL)
           return fail(N3DS_ERR_INVALID, "too many rays in one scene for 32-bit work counters");
         tiles += (long long)d.n_rays * ipr;
@@ -267,13 +286,14 @@ void n3ds_default_options(n3ds_options_t* opt) {
   opt->grad_mode = N3DS_GRAD_EXACT;
   opt->timing_events = nullptr;
   opt->warps_bwd = 0;
+  opt->forward_only = 0;
 }
 
 size_t n3ds_field_workspace_bytes(const n3ds_batch_t* batch, const n3ds_options_t* opt) {
   (void)opt;
   long long R = 0, S = 0;
   if (check_batch(batch, &R, &S) != N3DS_OK) return 0;
-  return ws_layout(R, batch->n_samples, S).total;
+  return ws_layout(R, batch->n_samples, S, mask_words(batch)).total;
 }
 
 static int field_common(const n3ds_batch_t* batch, const n3ds_rays_t* rays, const n3ds_strokes_t* strokes,
@@ -289,7 +309,7 @@ static int field_common(const n3ds_batch_t* batch, const n3ds_rays_t* rays, cons
     return fail(N3DS_ERR_INVALID, "strokes: sdf_ids, shape_params, color_params, density, sdf_delta required");
   if (*S > 0 && (strokes->param_stride < 1 || strokes->param_stride > 64))
     return fail(N3DS_ERR_INVALID, "strokes: param_stride must be in [1, 64]");
-  *lay = ws_layout(*R, batch->n_samples, *S);
+  *lay = ws_layout(*R, batch->n_samples, *S, mask_words(batch));
   if (!ws || ws_bytes < lay->total)
     return fail(N3DS_ERR_WORKSPACE, "workspace too small: need " + std::to_string(lay->total) + " bytes");
   if (reinterpret_cast<uintptr_t>(ws) % 256)
@@ -320,6 +340,15 @@ static n3ds::PrepLaunch make_prep(const n3ds_strokes_t* s, long long S, const Re
   p.n_counters = N_COUNTERS;
   p.gslots = zero_slots ? reinterpret_cast<float*>(ws + lay.gslots) : nullptr;
   p.stats = zero_slots ? nullptr : reinterpret_cast<unsigned long long*>(ws + lay.stats);
+  if (!zero_slots) {
+    // forward: tag the stroke-block masks the segment kernels are about to write with
+    // the skip threshold they use (the run schedule writes none)
+    p.mask_tag = reinterpret_cast<int*>(ws + lay.mask_tag);
+    float tag = rv.cull_alpha;
+    int bits;
+    std::memcpy(&bits, &tag, sizeof(bits));
+    p.mask_tag_value = (rv.schedule == N3DS_SCHEDULE_SEGMENTS && !rv.forward_only) ? bits : -1;
+  }
   return p;
 }
 
@@ -344,6 +373,8 @@ static n3ds::SegLaunch make_seg(const n3ds_batch_t* b, const n3ds_rays_t* rays, 
   L.tile_counter = reinterpret_cast<int*>(ws + lay.counters);
   L.status = reinterpret_cast<int*>(ws + lay.status);
   L.stats = reinterpret_cast<unsigned long long*>(ws + lay.stats);
+  L.block_masks = reinterpret_cast<unsigned*>(ws + lay.masks);
+  L.mask_tag = reinterpret_cast<const int*>(ws + lay.mask_tag);
   return L;
 }
 
@@ -379,7 +410,10 @@ int n3ds_field_forward(const n3ds_batch_t* batch, const n3ds_rays_t* rays, const
   n3ds::launch_prep(make_prep(strokes, S, rv, ws, lay, false), st);
   N3DS_CUDA_TRY(cudaGetLastError());
   record_event(rv, 0, st);
-  rc = run_seg_passes(false, batch, rv, make_seg(batch, rays, ws, lay, 0), 0, st);
+  n3ds::SegLaunch FL = make_seg(batch, rays, ws, lay, 0);
+  FL.skip_alpha = rv.cull_alpha;
+  if (rv.forward_only) FL.block_masks = nullptr;
+  rc = run_seg_passes(false, batch, rv, FL, 0, st);
   if (rc) return rc;
   record_event(rv, 1, st);
   if (R > 0) {

@@ -80,7 +80,8 @@ __device__ __forceinline__ unsigned cull_block(const Stage& S, const SegCtx& c, 
 
 // ================================================================== forward
 
-template <int WARPS>
+// RECORD: write the stroke-block masks (L.block_masks non-null) for the backward.
+template <int WARPS, bool RECORD>
 __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_constant__ SegLaunch L) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t bar;
@@ -116,13 +117,21 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_con
           T = st[0]; sig = st[1]; cr = st[2]; cg = st[3]; cb = st[4];
         }
         const unsigned nact = __popc(__ballot_sync(0xffffffffu, c.active));
+        unsigned* bm = RECORD ? L.block_masks + sc.mask_begin +
+                                    (long long)(ray_local * L.segs_per_ray + g) * sc.mask_words
+                              : nullptr;
+        // mask word w of the segment is held by lane w % 32 and stored 32 at a time
+        const int w0 = (sc.n_strokes - sc.chunk_lo - sc.chunk_n) >> 5;  // first word of the chunk
+        unsigned held = 0;
         for (int hi = sc.chunk_n - 1; hi >= 0; hi -= 32) {
           unsigned mask = cull_block(S, c, hi, lane);
+          unsigned kept = 0;  // this lane's strokes of the block whose adjoint the backward needs
           while (mask) {
             const int b = __ffs(mask) - 1;
             mask &= mask - 1;
             const float* rec = S.recs + size_t(hi - b) * REC_FLOATS;
             const float a = pair_alpha(rec, c.x, c.rinv);
+            if (RECORD && a >= L.skip_alpha) kept |= 1u << b;
             if (lane == (__float_as_int(rec[R_KIND]) & 15)) kcount += nact;
             const float w = a * T;
             const float4 col = rec4(rec)[R_COLOR / 4];
@@ -131,6 +140,15 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_con
             cr += col.x * w;
             cg += col.y * w;
             cb += col.z * w;
+          }
+          if (RECORD) {
+            kept = __reduce_or_sync(0xffffffffu, c.active ? kept : 0u);
+            const int w = (sc.n_strokes - 1 - (sc.chunk_lo + hi)) >> 5;
+            if (lane == (w & 31)) held = kept;
+            if ((w & 31) == 31 || hi < 32) {  // group of 32 words complete, or the chunk's last block
+              const int first = (w0 >> 5) == (w >> 5) ? (w0 & 31) : 0;
+              if (lane >= first && lane <= (w & 31)) bm[(w & ~31) + lane] = held;
+            }
           }
         }
         if (c.active) {
@@ -237,6 +255,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
   __syncthreads();
   uint32_t phase = 0;
   const int compat = L.compat;
+  const unsigned* masks = (L.block_masks && *L.mask_tag == __float_as_int(L.skip_alpha)) ? L.block_masks : nullptr;
 
   auto flush = [&](int sci) {
     const SceneDesc& o = L.sc[sci];
@@ -284,8 +303,22 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
           s.T = b[0]; s.Ps = b[1]; s.Pr = b[2]; s.Pg = b[3]; s.Pb = b[4];
           gx = v3(b[5], b[6], b[7]);
         }
+        const unsigned* bm =
+            masks ? masks + sc.mask_begin + (long long)(ray_local * L.segs_per_ray + g) * sc.mask_words : nullptr;
+        unsigned held = 0;  // mask words (w & ~31) + lane of the current group of 32
         for (int hi = sc.chunk_n - 1; hi >= 0; hi -= 32) {
-          unsigned mask = cull_block(S, c, hi, lane);
+          unsigned mask;
+          if (bm) {
+            const int w = (sc.n_strokes - 1 - (sc.chunk_lo + hi)) >> 5;
+            if (hi == sc.chunk_n - 1 || (w & 31) == 0) {
+              const int wl = (w & ~31) + lane;
+              held = wl < sc.mask_words ? bm[wl] : 0u;
+            }
+            mask = __shfl_sync(0xffffffffu, held, w & 31);
+            if (hi < 31) mask &= (2u << hi) - 1u;  // only strokes hi .. 0 exist in the last block
+          } else {
+            mask = cull_block(S, c, hi, lane);
+          }
           while (mask) {
             const int b = __ffs(mask) - 1;
             mask &= mask - 1;
@@ -555,6 +588,7 @@ __global__ void ray_bwd_kernel(const RayLaunch L) {
 __global__ void prep_kernel(const PrepLaunch P) {
   const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (s < P.n_counters) P.counters[s] = 0;
+  if (P.mask_tag && s == 0) *P.mask_tag = P.mask_tag_value;
   if (P.stats && s < 17) P.stats[s] = 0ull;
   if (s >= P.n_strokes) return;
   if (P.gslots) {
@@ -908,9 +942,10 @@ void launch_prep(const PrepLaunch& p, cudaStream_t st) {
 
 template <int W>
 static cudaError_t launch_fwd_w(const SegLaunch& L, int grid, size_t smem, cudaStream_t st) {
-  cudaError_t e = cudaFuncSetAttribute(seg_fwd_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  auto* k = L.block_masks ? seg_fwd_kernel<W, true> : seg_fwd_kernel<W, false>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  seg_fwd_kernel<W><<<grid, W * 32, smem, st>>>(L);
+  k<<<grid, W * 32, smem, st>>>(L);
   return cudaGetLastError();
 }
 template <int W>

@@ -20,6 +20,8 @@ struct SceneDesc {
   int chunk_n;
   int first_pass;        // 1: composite state starts fresh
   int last_pass;         // 1: the pass that finishes the scene
+  int mask_words;        // ceil(n_strokes / 32): stroke-block words per segment
+  long long mask_begin;  // first word of the scene's stroke-block masks (segment-major)
 };
 
 struct SegLaunch {
@@ -40,7 +42,7 @@ struct SegLaunch {
   float* grad_x;           // [P*3] or null
   float* gslots;           // [S*32] reduced per-stroke gradient slots
   int compat;              // reference gradient formulas
-  float skip_alpha;        // backward: skip the adjoint of a stroke whose alpha is below this at
+  float skip_alpha;        // forward: mask threshold; backward: skip the adjoint of a stroke whose alpha is below this at
                            // every sample of a segment (the culling threshold; 0 never skips)
   int n_scenes;
   int tiles_total;         // work items (rays) in the launch
@@ -49,6 +51,13 @@ struct SegLaunch {
   int* tile_counter;       // [n_scenes] next ray of each scene (zeroed before the launch)
   int* status;
   unsigned long long* stats;  // [0] evaluated (sample, stroke) pairs
+  // Stroke-block masks, one 32-bit word per (segment, block of 32 strokes counted
+  // from the scene's top stroke): bit b = stroke (top - b) survived culling and has
+  // alpha >= skip_alpha at some sample of the segment. The forward writes them when
+  // non-null; the backward reads them instead of culling when mask_tag holds the bits
+  // of its skip_alpha (written by the forward's prep kernel).
+  unsigned* block_masks;
+  const int* mask_tag;
   SceneDesc sc[MAX_SCENES_PER_LAUNCH];
 };
 
@@ -94,6 +103,8 @@ struct PrepLaunch {
   int n_counters;
   float* gslots;           // zeroed when non-null
   unsigned long long* stats;
+  int* mask_tag;           // set to mask_tag_value when non-null
+  int mask_tag_value;
 };
 
 struct FinalizeLaunch {

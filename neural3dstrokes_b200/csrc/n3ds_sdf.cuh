@@ -365,6 +365,11 @@ __device__ __forceinline__ V3 quad_adjoint(const float* rec, const QuadFwd& s, f
   // pt^3 = p^3 + 2.5e-9 (Cardano: u0^3 + u1^3 = -q, u0 u1 = -pt), so differentiating
   // that cubic gives the exact derivative of the regularised closed form:
   //   ds = -(3 s dpt + dq) / (3 (s^2 + pt)),  dpt/dp = p^2 / pt^2.
+  // dpt/dp has no bound where p^3 + 2.5e-9 crosses zero (the cube root's vertical
+  // tangent; pt can round to exactly 0 there): it is capped at 1e3 so that one sample
+  // in that thin shell cannot turn the stroke's gradient into inf / NaN. Likewise
+  // 1 / sqrt(1 - arg^2) of the trigonometric branch is capped at 1e4 (the bound the
+  // reference's own regulariser gives, strokes_sdf.h:1093-1095).
   float gkx = 0.f, gky = 0.f, gkz = 0.f;
   if (gtr != 0.f && (s.pos_branch || s.sigma < 0.f)) {
     // a (refined) true root: one-real-root branch, or the trig branch's -(m+n) root
@@ -373,7 +378,8 @@ __device__ __forceinline__ V3 quad_adjoint(const float* rec, const QuadFwd& s, f
     float den = 3.f * (sr * sr + pt);
     if (fabsf(den) < 1e-30f) den = copysignf(1e-30f, den);
     const float gq = -gtr / den;
-    const float gp = -3.f * sr * (s.p * s.p) / (pt * pt) * gtr / den;
+    const float dpt = fminf((s.p * s.p) / (pt * pt), 1e3f);
+    const float gp = -3.f * sr * dpt * gtr / den;
     gkx = -gtr - 2.f * s.kx * gp + gq * (6.f * s.kx * s.kx - 3.f * s.ky);
     gky = gp - 3.f * s.kx * gq;
     gkz = gq;
@@ -386,7 +392,7 @@ __device__ __forceinline__ V3 quad_adjoint(const float* rec, const QuadFwd& s, f
     float sv, cv;
     sincosf(s.v, &sv, &cv);
     const float gv = -sv * gm + BEZ_SQRT3 * cv * gn;
-    const float garg = -(gv / 3.f) * rsqrtf(fmaxf(1.f - s.arg * s.arg, 1e-30f));
+    const float garg = -(gv / 3.f) * rsqrtf(fmaxf(1.f - s.arg * s.arg, 1e-8f));
     const float gq = garg / s.den;
     const float gden = -garg * s.arg / s.den;
     float gp = 2.f * s.z * gden;

@@ -10,6 +10,7 @@ positions and every stroke parameter: shape (translation, rotation, scale, base
 parameters, Bezier control points and radii), colour, density and softness.
 """
 import ctypes
+import dataclasses
 from dataclasses import dataclass
 from typing import Optional, Sequence
 
@@ -27,6 +28,7 @@ class FieldOptions:
     warps_bwd: int = 0         # warps per CTA, backward: 4, 8, 16, 20, 24 (0: auto)
     schedule: str = "auto"     # 'segments' (auto): lane = sample; 'runs': packed (sample, stroke) pairs
     grad_mode: str = "exact"   # 'exact' or 'compat'
+    forward_only: bool = False  # no backward follows: skip the bookkeeping the backward reads
 
     def c(self, events=None):
         """ctypes options; ``events``: optional 4 torch.cuda.Event(enable_timing=True)
@@ -42,7 +44,7 @@ class FieldOptions:
         return _lib.Options(float(self.cull_alpha), int(self.chunk_fwd), int(self.chunk_bwd), int(self.warps),
                             {"auto": 0, "segments": 1, "runs": 2}[self.schedule],
                             _lib.N3DS_GRAD_COMPAT if self.grad_mode == "compat" else _lib.N3DS_GRAD_EXACT, ev,
-                            int(self.warps_bwd))
+                            int(self.warps_bwd), int(bool(self.forward_only)))
 
 
 class _Native:
@@ -89,8 +91,10 @@ class _FieldFn(torch.autograd.Function):
             raise RuntimeError("sdf_ids must be a CUDA int32 tensor")
         sdf_ids = sdf_ids.contiguous()
         bg_c = _f32(bg_t, "bg") if bg_t is not None else None
+        # without any input that needs a gradient no backward can follow
+        fwd_opts = options if any(ctx.needs_input_grad) else dataclasses.replace(options, forward_only=True)
         nat = _Native(scene_rays, scene_strokes, N, x, radius, tdist, dirs, bg_c, bg_value, opaque, sdf_ids,
-                      shape_params, color_params, density, delta, laplace, inv_scale, options, origins, radii)
+                      shape_params, color_params, density, delta, laplace, inv_scale, fwd_opts, origins, radii)
         lib = _lib.load()
         dev = tdist.device
         with torch.cuda.device(dev):

@@ -16,8 +16,8 @@ KINDS = scenes.EVERY_KIND + ["mixed", "every"]
 
 
 def run_field(sc, rays, dev, delta=0.02, laplace=True, inv=True, bg=1.0, opaque=False, opts=None,
-              requires_grad=False):
-    x = rays.x.to(dev).requires_grad_(requires_grad)
+              requires_grad=False, x_grad=True):
+    x = rays.x.to(dev).requires_grad_(requires_grad and x_grad)
     sp = sc.shape_params.to(dev).requires_grad_(requires_grad)
     col = sc.color_params.to(dev).requires_grad_(requires_grad)
     den = sc.density.to(dev).requires_grad_(requires_grad)
@@ -42,22 +42,23 @@ def test_forward_matches_oracle(cuda, kind, schedule):
     assert e1 < FWD_TOL and e2 < FWD_TOL
 
 
+@pytest.mark.parametrize("x_grad", [True, False])
 @pytest.mark.parametrize("schedule", SCHEDULES)
 @pytest.mark.parametrize("kind", KINDS)
-def test_backward_matches_float64_autograd(cuda, kind, schedule):
+def test_backward_matches_float64_autograd(cuda, kind, schedule, x_grad):
     sc, rays = small_workload(kind, n_strokes=16, n_rays=64, n_samples=40, seed=3)
     g = torch.Generator().manual_seed(7)
     g_rgb = torch.randn(rays.n_rays, 3, generator=g)
     g_acc = torch.randn(rays.n_rays, generator=g)
     g_depth = depth_upstream(sc, rays, g)
     (rgb, acc, depth), (x, sp, col, den, dl) = run_field(sc, rays, cuda, requires_grad=True,
-                                                         opts=FieldOptions(schedule=schedule))
+                                                         opts=FieldOptions(schedule=schedule), x_grad=x_grad)
     L = (rgb * g_rgb.to(cuda)).sum() + (acc * g_acc.to(cuda)).sum() + (depth * g_depth.to(cuda)).sum()
     L.backward()
     ref = oracle_grads(sc, rays, g_rgb, g_acc, g_depth)
     m = shape_param_mask(sc)
     errs = {
-        "x": rel(x.grad, ref["x"]),
+        "x": rel(x.grad, ref["x"]) if x_grad else 0.0,
         "shape": rel(sp.grad.cpu()[m], ref["shape"][m]),
         "color": rel(col.grad, ref["color"]),
         "density": rel(den.grad, ref["density"]),
@@ -107,15 +108,20 @@ def test_schedules_agree(cuda, n_samples, shuffle):
         assert rel(a, b) < 1e-5
 
 
-def test_multipass_matches_single_pass(cuda):
-    sc, rays = small_workload("mixed", n_strokes=100, n_rays=96, n_samples=70, seed=5)
+@pytest.mark.parametrize("x_grad", [True, False])
+def test_multipass_matches_single_pass(cuda, x_grad):
+    """Several shared-memory stages per scene (also stage sizes that are not multiples
+    of 32, which are rounded down) give the single-stage results."""
+    sc, rays = small_workload("every", n_strokes=100, n_rays=96, n_samples=70, seed=5)
     g_rgb = torch.randn(rays.n_rays, 3, generator=torch.Generator().manual_seed(1)).to(cuda)
     outs = []
     for opts in (FieldOptions(), FieldOptions(chunk_fwd=32, chunk_bwd=32),
-                 FieldOptions(chunk_fwd=32, chunk_bwd=32, schedule="segments")):
-        (rgb, acc, depth), (x, sp, col, den, dl) = run_field(sc, rays, cuda, opts=opts, requires_grad=True)
+                 FieldOptions(chunk_fwd=32, chunk_bwd=32, schedule="segments"),
+                 FieldOptions(chunk_fwd=100, chunk_bwd=70, schedule="segments")):
+        (rgb, acc, depth), (x, sp, col, den, dl) = run_field(sc, rays, cuda, opts=opts, requires_grad=True,
+                                                             x_grad=x_grad)
         (rgb * g_rgb).sum().backward()
-        outs.append((rgb.detach(), x.grad, sp.grad, col.grad, den.grad, dl.grad))
+        outs.append((rgb.detach(), x.grad if x_grad else rgb.detach(), sp.grad, col.grad, den.grad, dl.grad))
     for other in outs[1:]:
         for a, b in zip(other, outs[0]):
             assert rel(a, b) < 1e-5
@@ -162,3 +168,34 @@ def test_empty_scene_and_rays(cuda):
     sc2, rays2 = small_workload("sphere", n_strokes=4, n_rays=0, n_samples=32)
     (rgb2, acc2, _), _ = run_field(sc2, rays2, cuda)
     assert rgb2.shape == (0, 3) and acc2.shape == (0,)
+
+
+def test_backward_without_matching_block_masks(cuda):
+    """The backward reads the forward's stroke-block masks only when they were written
+    with its skip threshold; after a forward of the run schedule (which writes none)
+    it culls by itself and gives the same gradients."""
+    from neural3dstrokes_b200.train import BatchedField
+    sc, rays = small_workload("every", n_strokes=90, n_rays=128, n_samples=64, seed=8)
+    f = BatchedField([sc], [rays], device=cuda)
+    g = torch.Generator().manual_seed(3)
+    f.g_rgb.copy_(torch.randn(f.g_rgb.shape, generator=g))
+    f.g_acc.copy_(torch.randn(f.g_acc.shape, generator=g))
+    f.step()
+    ref = [t.clone() for t in (f.grad_x, f.grad_shape, f.grad_color, f.grad_density, f.grad_delta)]
+    for first in (FieldOptions(schedule="runs"), FieldOptions(forward_only=True)):
+        f.c_opt = first.c()
+        f.forward()
+        f.c_opt = FieldOptions(schedule="segments").c()
+        f.backward()
+        for a, b in zip((f.grad_x, f.grad_shape, f.grad_color, f.grad_density, f.grad_delta), ref):
+            assert rel(a, b) < 1e-5
+
+
+def test_forward_only_outputs_are_identical(cuda):
+    """A forward that records nothing for a backward (no input needs a gradient) gives
+    the same outputs bit for bit."""
+    sc, rays = small_workload("every", n_strokes=60, n_rays=100, n_samples=50, seed=4)
+    (a, acc_a, d_a), _ = run_field(sc, rays, cuda, requires_grad=True)
+    with torch.no_grad():
+        (b, acc_b, d_b), _ = run_field(sc, rays, cuda)
+    assert torch.equal(a.detach(), b) and torch.equal(acc_a.detach(), acc_b) and torch.equal(d_a.detach(), d_b)
