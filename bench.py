@@ -37,9 +37,10 @@ UNIT = "evals/s"
 # Algorithmic FP32 flops per evaluated (sample, stroke) pair, forward: inverse
 # transform + SDF + 15 (soft step 4 + over-composite 11); transforms without rotation
 # (sphere, aacube, aabb) are 6, the curves have none; a per-axis scale under
-# inv_scale_radius adds 10 for the radius factor. Backward = 2.5 x forward
-# (recompute, adjoint of each step, reduction share). Survey 8(d) table; capped
-# torus, line and triangular prism counted the same way from their SDFs (16, 17, 10).
+# inv_scale_radius adds 10 for the radius factor. Backward = 2.5 x forward per pair
+# it evaluates (recompute, adjoint of each step, reduction share); it evaluates only
+# the strokes the forward's block masks keep, counted on the device. Capped torus,
+# line and triangular prism counted the same way from their SDFs (16, 17, 10).
 FWD_FLOPS_BY_KIND = {
     "sphere": 6 + 6 + 15, "ellipsoid": 21 + 6 + 10 + 15, "aacube": 6 + 14 + 15, "cube": 21 + 14 + 15,
     "aabb": 6 + 14 + 10 + 15, "obb": 21 + 14 + 10 + 15, "roundcube": 21 + 16 + 15, "roundbox": 21 + 16 + 10 + 15,
@@ -52,7 +53,7 @@ BWD_FACTOR = 2.5
 # workload (config 3), from one ncu capture at a quarter of its rays (all passes of
 # one step, dram__bytes_read.sum + dram__bytes_write.sum; launch-list summary in
 # profiles/launches_cfg3_quarter.md); traffic grows with the ray count.
-SEG_BWD_TRAFFIC_CFG3_QUARTER = 553.6e6
+SEG_BWD_TRAFFIC_CFG3_QUARTER = 573.2e6
 KIND_BASE = {"sphere": 0, "ellipsoid": 0, "aacube": 1, "cube": 1, "aabb": 1, "obb": 1, "roundcube": 2,
              "roundbox": 2, "cappedtorus": 3, "capsule": 4, "scapsule": 4, "line": 5, "triprism": 6,
              "octahedron": 7, "tetrahedron": 8, "quadratic_bezier": 9, "cubic_bezier": 10, "catmull_rom": 11}
@@ -412,10 +413,13 @@ def main():
                       for ms, o in autotune.last_results]
     segments = field.options.schedule != "runs"
 
-    # statistics pass (not timed): evaluated pairs per primitive type, status word
+    # statistics pass (not timed): evaluated pairs per primitive type (forward) and
+    # in total (backward), status word
     field.forward()
+    field.backward()
     torch.cuda.synchronize(dev)
     per_base = field.pair_counts()
+    bwd_evaluated = field.backward_pairs()
     status, evaluated = field.status()
     if status != 0:
         raise SystemExit(f"device status {status}")
@@ -455,7 +459,7 @@ def main():
     t_fwd, t_bwd = statistics.mean(fwd_t), statistics.mean(bwd_t)
     bf = base_flops(field.kinds)
     fwd_flops = sum(per_base[b] * bf.get(b, 0.0) for b in range(16))
-    bwd_flops = BWD_FACTOR * fwd_flops
+    bwd_flops = BWD_FACTOR * fwd_flops * (bwd_evaluated / evaluated if (bwd_evaluated and evaluated) else 1.0)
     peak = fp32_peak(dev)
     kname = ("seg_bwd_kernel (segment adjoint)" if segments else "run_bwd_kernel (sample-run adjoint)")
     traffic = SEG_BWD_TRAFFIC_CFG3_QUARTER * args.scale / 0.25 if (args.config == 3 and segments) else None
@@ -518,7 +522,8 @@ def main():
             "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators, no dataset)",
             "config": {"workload": w.name, "scenes": len(w.scenes), "nominal_pairs_per_step": pairs,
-                       "evaluated_pairs_per_step": int(evaluated), "rays": int(field.rgb.shape[0]),
+                       "evaluated_pairs_per_step": int(evaluated),
+                       "backward_evaluated_pairs_per_step": int(bwd_evaluated), "rays": int(field.rgb.shape[0]),
                        "samples_per_ray": field.n_samples, "strokes": int(field.shape.shape[0]),
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "l2": "inputs larger than L2 (x alone %.0f MB)" % (field.x.numel() * 4 / 1e6),

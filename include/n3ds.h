@@ -255,6 +255,12 @@ int n3ds_field_launch_count(const n3ds_batch_t* batch, const n3ds_options_t* opt
  * SDF type (16 counters, indexed by sdf_id >> 4). */
 int n3ds_field_read_pair_counts(void* workspace, uint64_t* per_base, n3ds_stream_t stream);
 
+/* Synchronously read the (sample, stroke) pairs that the backwards since the last
+ * forward evaluated (segment schedule; the forward resets the count). With the
+ * stroke-block masks of its forward the backward evaluates only the strokes that
+ * reach the skip threshold somewhere in a segment, far fewer than the forward. */
+int n3ds_field_read_backward_pairs(void* workspace, uint64_t* pairs, n3ds_stream_t stream);
+
 /* Adam step fused with the reference's parameter clamp (utils/training.py:119-136,
  * models.py:576-584) over n floats: m = b1 m + (1-b1) g; v = b2 v + (1-b2) g^2;
  * p -= lr * mhat / (sqrt(vhat) + eps); then p = clamp(p, lo, hi) where lo/hi may be

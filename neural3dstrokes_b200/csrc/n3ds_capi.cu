@@ -79,7 +79,7 @@ WsLayout ws_layout(long long total_rays, int N, long long S, long long n_mask_wo
   };
   const size_t P = size_t(total_rays) * size_t(N);
   // header: int32 status at +0, uint64 evaluated pairs at +8, uint64 per-base counts at
-  // +16, int32 stroke-block mask tag at +248
+  // +16, uint64 backward-evaluated pairs at +144, int32 stroke-block mask tag at +248
   w.status = take(256);
   w.stats = w.status + 8;
   w.mask_tag = w.status + 248;
@@ -454,7 +454,7 @@ int n3ds_field_backward(const n3ds_batch_t* batch, const n3ds_rays_t* rays, cons
   }
   n3ds::SegLaunch SL = make_seg(batch, rays, ws, lay, compat);
   SL.grad_x = grad_x;
-  SL.stats = nullptr;
+  SL.stats = reinterpret_cast<unsigned long long*>(ws + lay.stats) + 17;  // backward pair count
   SL.skip_alpha = rv.cull_alpha;
   record_event(rv, 2, st);
   rc = run_seg_passes(true, batch, rv, SL, N_LAUNCH_SLOTS / 2, st);
@@ -551,6 +551,15 @@ int n3ds_field_read_pair_counts(void* workspace, uint64_t* per_base, n3ds_stream
   if (!workspace || !per_base) return fail(N3DS_ERR_INVALID, "workspace and per_base required");
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   N3DS_CUDA_TRY(cudaMemcpyAsync(per_base, static_cast<char*>(workspace) + 16, 16 * sizeof(uint64_t),
+                                cudaMemcpyDeviceToHost, st));
+  N3DS_CUDA_TRY(cudaStreamSynchronize(st));
+  return N3DS_OK;
+}
+
+int n3ds_field_read_backward_pairs(void* workspace, uint64_t* pairs, n3ds_stream_t stream) {
+  if (!workspace || !pairs) return fail(N3DS_ERR_INVALID, "workspace and pairs required");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  N3DS_CUDA_TRY(cudaMemcpyAsync(pairs, static_cast<char*>(workspace) + 8 + 17 * sizeof(uint64_t), sizeof(uint64_t),
                                 cudaMemcpyDeviceToHost, st));
   N3DS_CUDA_TRY(cudaStreamSynchronize(st));
   return N3DS_OK;

@@ -256,6 +256,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
   uint32_t phase = 0;
   const int compat = L.compat;
   const unsigned* masks = (L.block_masks && *L.mask_tag == __float_as_int(L.skip_alpha)) ? L.block_masks : nullptr;
+  unsigned long long bcount = 0;  // lane 0: evaluated (sample, stroke) pairs
 
   auto flush = [&](int sci) {
     const SceneDesc& o = L.sc[sci];
@@ -305,6 +306,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
         }
         const unsigned* bm =
             masks ? masks + sc.mask_begin + (long long)(ray_local * L.segs_per_ray + g) * sc.mask_words : nullptr;
+        const unsigned nact = __popc(__ballot_sync(0xffffffffu, c.active));
         unsigned held = 0;  // mask words (w & ~31) + lane of the current group of 32
         for (int hi = sc.chunk_n - 1; hi >= 0; hi -= 32) {
           unsigned mask;
@@ -325,6 +327,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
             const int sl = hi - b;
             const float* rec = S.recs + size_t(sl) * REC_FLOATS;
             float* row = S.gacc + size_t(sl) * GRAD_SLOTS;
+            bcount += nact;
             const float4 h = rec4(rec)[0];
             const int kind = __float_as_int(h.x);
             const int base = kind & 15;
@@ -411,6 +414,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
     __syncthreads();
     sci = s_scene;
   }
+  if (L.stats && lane == 0 && bcount) atomicAdd(L.stats, bcount);
 }
 
 // ============================================================== ray kernels
@@ -589,7 +593,7 @@ __global__ void prep_kernel(const PrepLaunch P) {
   const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (s < P.n_counters) P.counters[s] = 0;
   if (P.mask_tag && s == 0) *P.mask_tag = P.mask_tag_value;
-  if (P.stats && s < 17) P.stats[s] = 0ull;
+  if (P.stats && s < 18) P.stats[s] = 0ull;
   if (s >= P.n_strokes) return;
   if (P.gslots) {
     float* g = P.gslots + s * GRAD_SLOTS;

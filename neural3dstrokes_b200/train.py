@@ -129,6 +129,13 @@ class BatchedField:
         _lib.check(_lib.load().n3ds_field_read_pair_counts(_lib.ptr(self.ws), arr, _lib.stream_ptr(self.device)))
         return [int(v) for v in arr]
 
+    def backward_pairs(self):
+        """(sample, stroke) pairs the backwards since the last forward evaluated."""
+        v = ctypes.c_uint64(0)
+        _lib.check(_lib.load().n3ds_field_read_backward_pairs(_lib.ptr(self.ws), ctypes.byref(v),
+                                                             _lib.stream_ptr(self.device)))
+        return int(v.value)
+
     def status(self):
         st = ctypes.c_int32(0)
         pairs = ctypes.c_uint64(0)
