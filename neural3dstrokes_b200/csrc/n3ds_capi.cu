@@ -412,7 +412,12 @@ int n3ds_field_forward(const n3ds_batch_t* batch, const n3ds_rays_t* rays, const
   record_event(rv, 0, st);
   n3ds::SegLaunch FL = make_seg(batch, rays, ws, lay, 0);
   FL.skip_alpha = rv.cull_alpha;
-  if (rv.forward_only) FL.block_masks = nullptr;
+  if (rv.forward_only || rv.schedule != N3DS_SCHEDULE_SEGMENTS) {
+    FL.block_masks = nullptr;
+  } else if (lay.masks < lay.total) {
+    // the segment kernels store only non-empty mask words
+    N3DS_CUDA_TRY(cudaMemsetAsync(ws + lay.masks, 0, lay.total - lay.masks, st));
+  }
   rc = run_seg_passes(false, batch, rv, FL, 0, st);
   if (rc) return rc;
   record_event(rv, 1, st);

@@ -120,11 +120,9 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_con
         unsigned* bm = RECORD ? L.block_masks + sc.mask_begin +
                                     (long long)(ray_local * L.segs_per_ray + g) * sc.mask_words
                               : nullptr;
-        // mask word w of the segment is held by lane w % 32 and stored 32 at a time
-        const int w0 = (sc.n_strokes - sc.chunk_lo - sc.chunk_n) >> 5;  // first word of the chunk
-        unsigned held = 0;
         for (int hi = sc.chunk_n - 1; hi >= 0; hi -= 32) {
           unsigned mask = cull_block(S, c, hi, lane);
+          const bool any = mask != 0;
           unsigned kept = 0;  // this lane's strokes of the block whose adjoint the backward needs
           while (mask) {
             const int b = __ffs(mask) - 1;
@@ -141,14 +139,10 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_con
             cg += col.y * w;
             cb += col.z * w;
           }
-          if (RECORD) {
+          // the words start at zero (cleared before the launch): store the non-empty ones
+          if (RECORD && any) {
             kept = __reduce_or_sync(0xffffffffu, c.active ? kept : 0u);
-            const int w = (sc.n_strokes - 1 - (sc.chunk_lo + hi)) >> 5;
-            if (lane == (w & 31)) held = kept;
-            if ((w & 31) == 31 || hi < 32) {  // group of 32 words complete, or the chunk's last block
-              const int first = (w0 >> 5) == (w >> 5) ? (w0 & 31) : 0;
-              if (lane >= first && lane <= (w & 31)) bm[(w & ~31) + lane] = held;
-            }
+            if (lane == 0 && kept) bm[(sc.n_strokes - 1 - (sc.chunk_lo + hi)) >> 5] = kept;
           }
         }
         if (c.active) {

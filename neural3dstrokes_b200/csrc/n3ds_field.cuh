@@ -53,9 +53,10 @@ struct SegLaunch {
   unsigned long long* stats;  // [0] evaluated (sample, stroke) pairs
   // Stroke-block masks, one 32-bit word per (segment, block of 32 strokes counted
   // from the scene's top stroke): bit b = stroke (top - b) survived culling and has
-  // alpha >= skip_alpha at some sample of the segment. The forward writes them when
-  // non-null; the backward reads them instead of culling when mask_tag holds the bits
-  // of its skip_alpha (written by the forward's prep kernel).
+  // alpha >= skip_alpha at some sample of the segment. The forward stores the non-zero
+  // words when non-null (the host clears the array first); the backward reads them
+  // instead of culling when mask_tag holds the bits of its skip_alpha (written by the
+  // forward's prep kernel).
   unsigned* block_masks;
   const int* mask_tag;
   SceneDesc sc[MAX_SCENES_PER_LAUNCH];
