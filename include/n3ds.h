@@ -255,6 +255,26 @@ int n3ds_field_launch_count(const n3ds_batch_t* batch, const n3ds_options_t* opt
  * SDF type (16 counters, indexed by sdf_id >> 4). */
 int n3ds_field_read_pair_counts(void* workspace, uint64_t* per_base, n3ds_stream_t stream);
 
+/* Image texture of stroke colours and alphas (ImageTexture, source/textures.py:36-83,
+ * applied between stroke_fn and compose_strokes at models.py:704-706), over n
+ * (sample, stroke) pairs: tint = bilinear sample of image [channels, height, width]
+ * at texcoords [n,2] as F.grid_sample(image, texcoords * 2 - 1, align_corners=True)
+ * with zero padding; color_out [n,3] = (colors * tint_ratio + 1 - tint_ratio) * tint
+ * (a 1-channel tint broadcasts); alpha_out [n] = alphas * mean(tint) when
+ * modulate_alpha, else alphas (alpha_out may be NULL). channels must be 1 or 3. */
+int n3ds_texture_forward(float* color_out, float* alpha_out, const float* texcoords, const float* colors,
+                         const float* alphas, int64_t n, const float* image, int32_t channels, int32_t height,
+                         int32_t width, float tint_ratio, int32_t modulate_alpha, n3ds_stream_t stream);
+
+/* Backward of n3ds_texture_forward: writes (overwrites) grad_colors [n,3] =
+ * grad_color_out * tint * tint_ratio and grad_alphas [n] = grad_alpha_out * mean(tint)
+ * (modulate_alpha) or grad_alpha_out; NULL upstream grads count as zero, NULL outputs
+ * are skipped. No gradient for texcoords or the image (none in the reference). */
+int n3ds_texture_backward(float* grad_colors, float* grad_alphas, const float* grad_color_out,
+                          const float* grad_alpha_out, const float* texcoords, int64_t n, const float* image,
+                          int32_t channels, int32_t height, int32_t width, float tint_ratio,
+                          int32_t modulate_alpha, n3ds_stream_t stream);
+
 /* Synchronously read the (sample, stroke) pairs that the backwards since the last
  * forward evaluated (segment schedule; the forward resets the count). With the
  * stroke-block masks of its forward the backward evaluates only the strokes that

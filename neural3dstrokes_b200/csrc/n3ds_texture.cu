@@ -1,0 +1,147 @@
+// Image texture modulation of stroke colours and alphas (the reference's ImageTexture,
+// source/textures.py:36-83), one thread per (sample, stroke) pair:
+//   tint    = bilinear sample of the texture [C, H, W] at texcoord (u, v), as
+//             F.grid_sample(image, (u, v) * 2 - 1, align_corners=True) with zero
+//             padding outside the image (textures.py:58-60);
+//   colour' = (colour * tint_ratio + (1 - tint_ratio)) * tint   (C = 1 broadcasts)
+//   alpha'  = alpha * mean(tint) when modulate_alpha, else alpha  (textures.py:77-81).
+// The backward gives dL/dcolour = dL/dcolour' * tint * tint_ratio and dL/dalpha =
+// dL/dalpha' * mean(tint) (or the identity); the texture is a buffer and texcoords
+// carry no gradient in the reference, so neither gets one here.
+//
+// Traffic: texcoord 8 B, colour 12 B, alpha 4 B in, colour 12 B and alpha 4 B out per
+// pair (40 B); the texture itself (256 x 256 x 3 floats = 768 KB by default) stays in
+// L2 / L1 after the first touches.
+#include <algorithm>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "../../include/n3ds.h"
+
+namespace n3ds {
+int report_error(int code, const std::string& msg);  // sets n3ds_last_error (n3ds_capi.cu)
+}
+
+namespace {
+
+struct Tex {
+  const float* image;  // [C, H, W]
+  int C, H, W;
+};
+
+// Bilinear tap of channel c at unnormalised pixel coordinates (ix, iy), corners
+// outside the image read as zero.
+__device__ __forceinline__ float tex_value(const Tex& t, int c, int x, int y) {
+  if (x < 0 || y < 0 || x >= t.W || y >= t.H) return 0.f;
+  return __ldg(t.image + ((size_t)c * t.H + y) * t.W + x);
+}
+
+// tint[0..C-1] at texcoord (u, v), with grid_sample's unnormalisation for
+// align_corners=True: ix = ((g + 1) / 2) (W - 1), g = u * 2 - 1.
+__device__ __forceinline__ void sample_tint(const Tex& t, float u, float v, float* tint) {
+  const float gx = u * 2.f - 1.f, gy = v * 2.f - 1.f;
+  // beyond one pixel outside the image every corner reads zero, so clamping there
+  // changes nothing and keeps the integer conversion in range
+  const float ix = fminf(fmaxf(((gx + 1.f) / 2.f) * (float)(t.W - 1), -2.f), (float)t.W + 1.f);
+  const float iy = fminf(fmaxf(((gy + 1.f) / 2.f) * (float)(t.H - 1), -2.f), (float)t.H + 1.f);
+  const float fx = floorf(ix), fy = floorf(iy);
+  const int x0 = (int)fx, y0 = (int)fy;
+  const float wx1 = ix - fx, wx0 = (fx + 1.f) - ix;
+  const float wy1 = iy - fy, wy0 = (fy + 1.f) - iy;
+  for (int c = 0; c < t.C; c++) {
+    tint[c] = tex_value(t, c, x0, y0) * (wx0 * wy0) + tex_value(t, c, x0 + 1, y0) * (wx1 * wy0) +
+              tex_value(t, c, x0, y0 + 1) * (wx0 * wy1) + tex_value(t, c, x0 + 1, y0 + 1) * (wx1 * wy1);
+  }
+}
+
+// Non-finite coordinates give a zero tint (no pixel is read).
+__device__ __forceinline__ bool coords_ok(float u, float v) { return isfinite(u) && isfinite(v); }
+
+__global__ void texture_fwd_kernel(float* color_out, float* alpha_out, const float* texcoords, const float* colors,
+                                   const float* alphas, long long n, Tex t, float tint_ratio, int modulate) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float u = texcoords[2 * i], v = texcoords[2 * i + 1];
+    float tint[3] = {0.f, 0.f, 0.f};
+    if (coords_ok(u, v)) sample_tint(t, u, v, tint);
+    if (t.C == 1) tint[1] = tint[2] = tint[0];
+    const float base = 1.f - tint_ratio;
+    color_out[3 * i] = (colors[3 * i] * tint_ratio + base) * tint[0];
+    color_out[3 * i + 1] = (colors[3 * i + 1] * tint_ratio + base) * tint[1];
+    color_out[3 * i + 2] = (colors[3 * i + 2] * tint_ratio + base) * tint[2];
+    if (alpha_out) {
+      const float a = alphas[i];
+      alpha_out[i] = modulate ? a * (t.C == 1 ? tint[0] : (tint[0] + tint[1] + tint[2]) / 3.f) : a;
+    }
+  }
+}
+
+__global__ void texture_bwd_kernel(float* grad_colors, float* grad_alphas, const float* g_color,
+                                   const float* g_alpha, const float* texcoords, long long n, Tex t,
+                                   float tint_ratio, int modulate) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float u = texcoords[2 * i], v = texcoords[2 * i + 1];
+    float tint[3] = {0.f, 0.f, 0.f};
+    if (coords_ok(u, v)) sample_tint(t, u, v, tint);
+    if (t.C == 1) tint[1] = tint[2] = tint[0];
+    if (grad_colors) {
+      for (int k = 0; k < 3; k++) grad_colors[3 * i + k] = g_color ? g_color[3 * i + k] * tint[k] * tint_ratio : 0.f;
+    }
+    if (grad_alphas) {
+      const float g = g_alpha ? g_alpha[i] : 0.f;
+      grad_alphas[i] = modulate ? g * (t.C == 1 ? tint[0] : (tint[0] + tint[1] + tint[2]) / 3.f) : g;
+    }
+  }
+}
+
+int check_texture(int64_t n, const float* texcoords, const float* image, int32_t channels, int32_t height,
+                  int32_t width) {
+  if (n < 0) return n3ds::report_error(N3DS_ERR_INVALID, "texture: n must be >= 0");
+  if (channels != 1 && channels != 3)
+    return n3ds::report_error(N3DS_ERR_INVALID, "texture: the image must have 1 (grayscale) or 3 (RGB) channels, got " +
+                                                    std::to_string(channels));
+  if (height < 1 || width < 1) return n3ds::report_error(N3DS_ERR_INVALID, "texture: image height and width must be >= 1");
+  if (n > 0 && (!texcoords || !image)) return n3ds::report_error(N3DS_ERR_INVALID, "texture: texcoords and image required");
+  return N3DS_OK;
+}
+
+unsigned grid_for(long long n) {
+  const long long blocks = (n + 255) / 256;
+  return (unsigned)std::max<long long>(1, std::min<long long>(blocks, 148LL * 16));
+}
+
+}  // namespace
+
+extern "C" int n3ds_texture_forward(float* color_out, float* alpha_out, const float* texcoords, const float* colors,
+                                    const float* alphas, int64_t n, const float* image, int32_t channels,
+                                    int32_t height, int32_t width, float tint_ratio, int32_t modulate_alpha,
+                                    n3ds_stream_t stream) {
+  int rc = check_texture(n, texcoords, image, channels, height, width);
+  if (rc) return rc;
+  if (n > 0 && (!color_out || !colors)) return n3ds::report_error(N3DS_ERR_INVALID, "texture: colors and color_out required");
+  if (n > 0 && alpha_out && !alphas) return n3ds::report_error(N3DS_ERR_INVALID, "texture: alpha_out needs alphas");
+  if (n == 0) return N3DS_OK;
+  Tex t{image, channels, height, width};
+  texture_fwd_kernel<<<grid_for(n), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+      color_out, alpha_out, texcoords, colors, alphas, n, t, tint_ratio, modulate_alpha != 0);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return n3ds::report_error(N3DS_ERR_CUDA, std::string("texture forward: ") + cudaGetErrorString(e));
+  return N3DS_OK;
+}
+
+extern "C" int n3ds_texture_backward(float* grad_colors, float* grad_alphas, const float* grad_color_out,
+                                     const float* grad_alpha_out, const float* texcoords, int64_t n,
+                                     const float* image, int32_t channels, int32_t height, int32_t width,
+                                     float tint_ratio, int32_t modulate_alpha, n3ds_stream_t stream) {
+  int rc = check_texture(n, texcoords, image, channels, height, width);
+  if (rc) return rc;
+  if (n == 0 || (!grad_colors && !grad_alphas)) return N3DS_OK;
+  Tex t{image, channels, height, width};
+  texture_bwd_kernel<<<grid_for(n), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+      grad_colors, grad_alphas, grad_color_out, grad_alpha_out, texcoords, n, t, tint_ratio, modulate_alpha != 0);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return n3ds::report_error(N3DS_ERR_CUDA, std::string("texture backward: ") + cudaGetErrorString(e));
+  return N3DS_OK;
+}

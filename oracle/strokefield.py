@@ -941,3 +941,17 @@ def stroke_backward_compat(grad_alpha, grad_color, x, radius, alpha, shape_param
     grad_shape = torch.cat(grads, -1) if grads else torch.zeros_like(shape_params)
     grad_x = g.sum(1) if need_grad_x else None
     return grad_shape, g_color, grad_x
+
+
+def image_texture(texcoords, colors, alphas, image, tint_ratio=1.0, modulate_alpha=False):
+    """ImageTexture.forward (textures.py:58-83): tint = F.grid_sample of image [C,H,W]
+    at texcoords [N,2] * 2 - 1 (bilinear, align_corners=True, zero padding);
+    colours (colors * tint_ratio + 1 - tint_ratio) * tint; alphas * mean(tint) when
+    modulate_alpha. Differentiable in colors and alphas (the texture is a buffer)."""
+    import torch.nn.functional as F
+    uvs = texcoords.reshape(1, 1, -1, 2) * 2 - 1
+    tint = F.grid_sample(image.unsqueeze(0), uvs, align_corners=True)[0, :, 0, :].permute(1, 0)
+    colors = (colors * tint_ratio + (1.0 - tint_ratio)) * tint
+    if modulate_alpha:
+        alphas = alphas * tint.mean(-1)
+    return colors, alphas
