@@ -275,6 +275,34 @@ int n3ds_texture_backward(float* grad_colors, float* grad_alphas, const float* g
                           int32_t channels, int32_t height, int32_t width, float tint_ratio,
                           int32_t modulate_alpha, n3ds_stream_t stream);
 
+/* Proposal resampling of ray intervals (source/utils/stepfun.py; the step that makes
+ * the stroke level's fence posts, models.py:147-185). One warp per ray; n_bins <= 2048.
+ *
+ * n3ds_max_dilate_weights: stepfun.max_dilate_weights (stepfun.py:136-147) of the step
+ * functions t [R, n_bins+1], w [R, n_bins] into t_out [R, 3 n_bins + 1] and
+ * w_out [R, 3 n_bins]. */
+int n3ds_max_dilate_weights(float* t_out, float* w_out, const float* t, const float* w, int64_t n_rays,
+                            int32_t n_bins, float dilation, float domain_lo, float domain_hi, int32_t renormalize,
+                            n3ds_stream_t stream);
+
+/* stepfun.sample_intervals (stepfun.py:280-317): n_samples intervals [R, n_samples+1]
+ * from t [R, n_bins+1] and w_logits [R, n_bins]. jitter: NULL for the deterministic
+ * centred samples (rand=False), else the uniform [0,1) draws of the reference's
+ * torch.rand, [R] when single_jitter or [R, n_samples]. n_samples >= 2. */
+int n3ds_sample_intervals(float* s_out, const float* t, const float* w_logits, int64_t n_rays, int32_t n_bins,
+                          int32_t n_samples, const float* jitter, int32_t single_jitter, float domain_lo,
+                          float domain_hi, n3ds_stream_t stream);
+
+/* One proposal level fused (models.py:156-185): if dilation > 0, max_dilate_weights
+ * with renormalisation and the [1:-1] slice; logits where(s[1:] > s[:-1],
+ * log(w + resample_padding), -inf); sample_intervals; and tdist = s * far + (1 - s) *
+ * near (the identity ray-distance warp). Outputs s_out and/or t_out [R, n_samples+1]
+ * (t_out needs near, far [R]). */
+int n3ds_resample_intervals(float* s_out, float* t_out, const float* sdist, const float* weights, int64_t n_rays,
+                            int32_t n_bins, int32_t n_samples, float dilation, float resample_padding,
+                            const float* jitter, int32_t single_jitter, float domain_lo, float domain_hi,
+                            const float* near, const float* far, n3ds_stream_t stream);
+
 /* Synchronously read the (sample, stroke) pairs that the backwards since the last
  * forward evaluated (segment schedule; the forward resets the count). With the
  * stroke-block masks of its forward the backward evaluates only the strokes that

@@ -77,6 +77,13 @@ _SIGS = {
     "n3ds_fp32_probe": (ctypes.c_int, [_P, c_i32, c_i32, _P]),
     "n3ds_field_read_pair_counts": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64), _P]),
     "n3ds_field_read_backward_pairs": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64), _P]),
+    "n3ds_max_dilate_weights": (ctypes.c_int, [_P, _P, _P, _P, c_i64, c_i32, ctypes.c_float, ctypes.c_float,
+                                               ctypes.c_float, c_i32, _P]),
+    "n3ds_sample_intervals": (ctypes.c_int, [_P, _P, _P, c_i64, c_i32, c_i32, _P, c_i32, ctypes.c_float,
+                                             ctypes.c_float, _P]),
+    "n3ds_resample_intervals": (ctypes.c_int, [_P, _P, _P, _P, c_i64, c_i32, c_i32, ctypes.c_float,
+                                               ctypes.c_float, _P, c_i32, ctypes.c_float, ctypes.c_float, _P, _P,
+                                               _P]),
     "n3ds_texture_forward": (ctypes.c_int, [_P, _P, _P, _P, _P, c_i64, _P, c_i32, c_i32, c_i32, ctypes.c_float,
                                             c_i32, _P]),
     "n3ds_texture_backward": (ctypes.c_int, [_P, _P, _P, _P, _P, c_i64, _P, c_i32, c_i32, c_i32, ctypes.c_float,

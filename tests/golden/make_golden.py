@@ -14,12 +14,18 @@ Three sources, each a seeded, small input set:
             stub ``_strokelib`` and runs its torch compositing modes (max,
             max_density_weighted, softmax, softmax_density_weighted,
             strokes.py:390-417) in float64 with autograd. -> compose_modes_golden.npz
+--stepfun   (CPU, needs the reference checkout): imports the reference
+            source/utils/stepfun.py and coord.py and runs, in float32, max_dilate_weights,
+            sample_intervals (deterministic, single and per-sample jitter; the jitter
+            draws are recorded by re-seeding) and the proposal-level chain of
+            models.py:147-185 (dilate, slice, logits, sample, s_to_t).
+            -> stepfun_golden.npz
 --strokelib (GPU, needs oracle/_ref built from the reference sources by
             oracle/build_ref.py): runs the reference CUDA operators stroke_forward,
             stroke_backward, compose_forward, compose_backward on seeded inputs for
             every implemented primitive. -> strokelib_golden.npz
 
-Usage: python tests/golden/make_golden.py [--layouts] [--render] [--strokelib]
+Usage: python tests/golden/make_golden.py [--layouts] [--render] [--compose] [--stepfun] [--strokelib]
        [--ref /root/reference] [--out tests/golden]
 """
 import argparse
@@ -115,6 +121,50 @@ def make_render(ref_root, out):
                         depth=rend["depth"].numpy(), acc=rend["acc"].numpy(), rgb_opaque=rend1["rgb"].numpy(),
                         depth_opaque=rend1["depth"].numpy(), acc_opaque=rend1["acc"].numpy())
     print("render golden written")
+
+
+def make_stepfun(ref_root, out):
+    sys.path.insert(0, ref_root)
+    from source.utils import coord as ref_coord  # noqa: E402
+    from source.utils import stepfun as ref_stepfun  # noqa: E402
+    g = torch.Generator().manual_seed(77)
+    R, M = 48, 64
+    # level-0 style posts in [0, 1] with a few zero-width bins, peaked weights with zeros
+    steps = torch.rand(R, M, generator=g) + 0.05
+    steps[torch.rand(R, M, generator=g) < 0.05] = 0.0
+    t = torch.cat([torch.zeros(R, 1), torch.cumsum(steps, -1)], -1)
+    t = t / t[:, -1:]
+    w = torch.rand(R, M, generator=g) ** 6
+    w[torch.rand(R, M, generator=g) < 0.2] = 0.0
+    w[0] = 0.0
+    w[0, 17] = 1.0  # all weight in one bin
+    w = w / w.sum(-1, keepdim=True).clamp_min(1e-12)
+    dilation = 0.0025 + 0.5 / 64
+    td, wd = ref_stepfun.max_dilate_weights(t, w, dilation, domain=(0.0, 1.0), renormalize=True)
+    sd, wsl = td[..., 1:-1], wd[..., 1:-1]
+    logits = torch.where(sd[..., 1:] > sd[..., :-1], torch.log(wsl + 0.0), torch.full_like(sd[..., :-1], -torch.inf))
+    res = {"t": t, "w": w, "dilation": np.float64(dilation), "t_dilate": td, "w_dilate": wd, "logits": logits}
+    N = 32
+    res["s_det"] = ref_stepfun.sample_intervals(False, sd, logits, N, single_jitter=True, domain=(0.0, 1.0))
+    for name, single in (("single", True), ("multi", False)):
+        torch.manual_seed(5)
+        res["s_" + name] = ref_stepfun.sample_intervals(True, sd, logits, N, single_jitter=single, domain=(0.0, 1.0))
+        torch.manual_seed(5)
+        res["jit_" + name] = torch.rand(R, 1 if single else N)
+    # the first level: one interval [0, 1] of weight 1, 64 proposal samples, then s_to_t
+    near = 2.0 + torch.rand(R, 1, generator=g)
+    far = near + 1.0 + 3 * torch.rand(R, 1, generator=g)
+    _, s_to_t = ref_coord.construct_ray_warps(None, near, far)
+    s0 = torch.cat([torch.zeros(R, 1), torch.ones(R, 1)], -1)
+    l0 = torch.log(torch.ones(R, 1) + 0.0)
+    torch.manual_seed(9)
+    s1 = ref_stepfun.sample_intervals(True, s0, l0, 64, single_jitter=True, domain=(0.0, 1.0))
+    torch.manual_seed(9)
+    res["jit_level0"] = torch.rand(R, 1)
+    res.update(near=near, far=far, s_level0=s1, t_level0=s_to_t(s1))
+    np.savez_compressed(os.path.join(out, "stepfun_golden.npz"),
+                        **{k: (v.numpy() if torch.is_tensor(v) else v) for k, v in res.items()})
+    print("stepfun golden written")
 
 
 KINDS = ["sphere", "ellipsoid", "aacube", "cube", "aabb", "obb", "roundcube", "roundbox", "cappedtorus", "capsule",
@@ -245,6 +295,7 @@ if __name__ == "__main__":
     ap.add_argument("--render", action="store_true")
     ap.add_argument("--strokelib", action="store_true")
     ap.add_argument("--compose", action="store_true")
+    ap.add_argument("--stepfun", action="store_true")
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--out", default=HERE)
     a = ap.parse_args()
@@ -257,3 +308,5 @@ if __name__ == "__main__":
         make_strokelib(a.out)
     if a.compose:
         make_compose_modes(a.ref, a.out)
+    if a.stepfun:
+        make_stepfun(a.ref, a.out)
