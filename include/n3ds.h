@@ -303,6 +303,75 @@ int n3ds_resample_intervals(float* s_out, float* t_out, const float* sdist, cons
                             const float* jitter, int32_t single_jitter, float domain_lo, float domain_hi,
                             const float* near, const float* far, n3ds_stream_t stream);
 
+/* Stroke insertion and reset on the device: StrokeField.step_update
+ * (source/models.py:586-658) with the stroke count in device memory, so a training
+ * step needs no host round trip. */
+#define N3DS_INSERT_MAX_STROKES 8192
+#define N3DS_INIT_RECON 0      /* strokes.py:258-270 */
+#define N3DS_INIT_GEN_BOX 1    /* strokes.py:271-278 */
+#define N3DS_INIT_GEN_SPHERE 2 /* strokes.py:279-289 */
+#define N3DS_BASE_SAMPLER_NONE 0
+#define N3DS_BASE_SAMPLER_ROUND 1    /* 0.8 u (round cube / box) */
+#define N3DS_BASE_SAMPLER_TORUS 2    /* u, u (capped torus) */
+#define N3DS_BASE_SAMPLER_CAPSULE 3  /* u + 0.25 */
+#define N3DS_BASE_SAMPLER_LINE 4     /* u + 0.25, u - 0.5 */
+#define N3DS_BASE_SAMPLER_UNIFORM 5  /* u (triangular prism) */
+#define N3DS_BASE_SAMPLER_SPLINE 6   /* control points around the centre + radii (strokes.py:28-37) */
+#define N3DS_COLOR_SAMPLER_UNIFORM 0  /* constant_rgb: u x n_color */
+#define N3DS_COLOR_SAMPLER_GRADIENT 1 /* gradient_rgb: u - 0.5 x 6, u x 6 */
+#define N3DS_COLOR_SAMPLER_NORMAL 2   /* constant_sh2 / sh3: N(0, 1) x n_color */
+
+typedef struct {
+  int32_t n_shape;        /* shape parameters per stroke (must match the flags below) */
+  int32_t n_color;        /* colour parameters per stroke */
+  int32_t base_sampler;   /* N3DS_BASE_SAMPLER_* */
+  int32_t spline_points;  /* spline sampler: control points (1-4) */
+  int32_t spline_radii;   /* spline sampler: radii (0-2) */
+  int32_t t, r, s1, s3;   /* translation, rotation, single / per-axis scale parameters */
+  int32_t init_type;      /* N3DS_INIT_* */
+  int32_t color_sampler;  /* N3DS_COLOR_SAMPLER_* */
+} n3ds_stroke_sampler_t;
+
+typedef struct {
+  int32_t max_num_strokes;     /* <= N3DS_INSERT_MAX_STROKES */
+  int32_t init_num_strokes;
+  float reset_density;         /* -INFINITY when the densities are not trained */
+  int32_t use_error_field;
+  int32_t use_shape_grads;
+  float shape_split_update_rate;
+  int32_t min_update_interval;
+  int32_t min_reset_interval;
+  float max_reset_frac;
+  uint64_t seed;               /* random draws: hash of (seed, training step, row, draw) */
+} n3ds_insert_config_t;
+
+/* Scratch bytes of n3ds_insert_step. */
+size_t n3ds_insert_workspace_bytes(const n3ds_insert_config_t* cfg, const n3ds_stroke_sampler_t* smp);
+
+/* One step_update: stroke_step / last_update_step are device int32 scalars (the
+ * stroke count and the training step of the last update). next_target is the host's
+ * min(int(max_num * clamp(train_frac, 0, 1)^step_power) + init_num, max_num) for
+ * cur_step (models.py:589-594); the kernel takes next = max(next_target, stroke_step).
+ * errors [n_errors] / error_coords [n_errors, 3] are the caller's error-field samples
+ * (may be NULL / 0); grad_ema [max, n_shape] the shape-gradient EMA (may be NULL).
+ * Parameters: shape_params [max, n_shape], color_params [max, n_color], density [max]
+ * rows are rewritten in place. No host synchronisation: the host passes the step's
+ * scalars (cur_step, next_target, train_frac) as arguments, everything that depends on
+ * device data (stroke count, resets, the update decision) stays on the device. */
+int n3ds_insert_step(const n3ds_insert_config_t* cfg, const n3ds_stroke_sampler_t* smp, float* shape_params,
+                     float* color_params, float* density, const float* grad_ema, int32_t* stroke_step,
+                     int32_t* last_update_step, int64_t cur_step, int32_t next_target, float train_frac,
+                     const float* errors, const float* error_coords, int64_t n_errors, void* workspace,
+                     size_t workspace_bytes, n3ds_stream_t stream);
+
+/* ema = ema * decay + grad * (1 - decay) over n floats (models.py:596-598). */
+int n3ds_ema_update(float* ema, const float* grad, int64_t n, float decay, n3ds_stream_t stream);
+
+/* Clamp each column j of x [rows, cols] to [lo[j], hi[j]] (host arrays; NaN = no bound),
+ * as StrokeField.clip_params (models.py:576-584). cols <= N3DS_CLIP_MAX_COLS. */
+#define N3DS_CLIP_MAX_COLS 32
+int n3ds_clip_columns(float* x, int64_t rows, int32_t cols, const float* lo, const float* hi, n3ds_stream_t stream);
+
 /* Synchronously read the (sample, stroke) pairs that the backwards since the last
  * forward evaluated (segment schedule; the forward resets the count). With the
  * stroke-block masks of its forward the backward evaluates only the strokes that

@@ -84,6 +84,12 @@ _SIGS = {
     "n3ds_resample_intervals": (ctypes.c_int, [_P, _P, _P, _P, c_i64, c_i32, c_i32, ctypes.c_float,
                                                ctypes.c_float, _P, c_i32, ctypes.c_float, ctypes.c_float, _P, _P,
                                                _P]),
+    "n3ds_insert_workspace_bytes": (c_size_t, [_P, _P]),
+    "n3ds_insert_step": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, c_i64, c_i32, ctypes.c_float, _P, _P, c_i64,
+                                        _P, c_size_t, _P]),
+    "n3ds_ema_update": (ctypes.c_int, [_P, _P, c_i64, ctypes.c_float, _P]),
+    "n3ds_clip_columns": (ctypes.c_int, [_P, c_i64, c_i32, ctypes.POINTER(ctypes.c_float),
+                                         ctypes.POINTER(ctypes.c_float), _P]),
     "n3ds_texture_forward": (ctypes.c_int, [_P, _P, _P, _P, _P, c_i64, _P, c_i32, c_i32, c_i32, ctypes.c_float,
                                             c_i32, _P]),
     "n3ds_texture_backward": (ctypes.c_int, [_P, _P, _P, _P, _P, c_i64, _P, c_i32, c_i32, c_i32, ctypes.c_float,
