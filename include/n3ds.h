@@ -197,7 +197,7 @@ typedef struct n3ds_strokes {
 typedef struct n3ds_options {
   float cull_alpha;   /* drop a stroke where its alpha provably stays below this; <= 0: no culling */
   int32_t chunk_fwd;  /* strokes per shared-memory stage, forward (0 = auto; else rounded
-                         down to a multiple of 32, at least 32) */
+                         down to a multiple of 32, within [32, 1024]) */
   int32_t chunk_bwd;  /* strokes per shared-memory stage, backward (same rules) */
   int32_t warps;      /* warps per CTA, forward: 4, 8, 16, 24, 32 (0 = auto) */
   int32_t schedule;   /* N3DS_SCHEDULE_* (0 = auto: segments) */

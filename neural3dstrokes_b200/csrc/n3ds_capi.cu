@@ -142,9 +142,10 @@ Resolved resolve(const n3ds_options_t* o) {
   // default stages: the largest multiple of 32 strokes that fits the shared memory
   // (multiples of 32, so that the 32-stroke blocks of every pass line up with the
   // stroke-block mask words in both directions)
-  int cf = o->chunk_fwd > 0 ? std::max(32, o->chunk_fwd / 32 * 32) : 1024;
-  int cb = o->chunk_bwd > 0 ? std::max(32, o->chunk_bwd / 32 * 32) : 1024;
-  auto fwd_smem = [&](int c) { return runs ? n3ds::run_fwd_smem(c, r.warps_fwd) : n3ds::seg_fwd_smem(c); };
+  // (at most 1024 = 32 blocks of 32: the forward keeps one block's mask per lane)
+  int cf = o->chunk_fwd > 0 ? std::min(1024, std::max(32, o->chunk_fwd / 32 * 32)) : 1024;
+  int cb = o->chunk_bwd > 0 ? std::min(1024, std::max(32, o->chunk_bwd / 32 * 32)) : 1024;
+  auto fwd_smem = [&](int c) { return runs ? n3ds::run_fwd_smem(c, r.warps_fwd) : n3ds::seg_fwd_smem(c, r.warps_fwd); };
   auto bwd_smem = [&](int c) { return runs ? n3ds::run_bwd_smem(c, r.warps_bwd) : n3ds::seg_bwd_smem(c); };
   while (cf > 32 && fwd_smem(cf) > budget) cf -= 32;
   while (cb > 32 && bwd_smem(cb) > budget) cb -= 32;
@@ -200,7 +201,7 @@ int run_seg_passes(bool backward, const n3ds_batch_t* b, const Resolved& rv, n3d
   const DevInfo di = dev_info();
   const int warps = backward ? rv.warps_bwd : rv.warps_fwd;
   const size_t smem = runs ? (backward ? n3ds::run_bwd_smem(cap, warps) : n3ds::run_fwd_smem(cap, warps))
-                           : (backward ? n3ds::seg_bwd_smem(cap) : n3ds::seg_fwd_smem(cap));
+                           : (backward ? n3ds::seg_bwd_smem(cap) : n3ds::seg_fwd_smem(cap, warps));
   int counter = 0;
   for (int pass = 0; pass < passes; pass++) {
     std::vector<int> scenes;

@@ -32,8 +32,10 @@
 
 namespace n3ds {
 
-size_t seg_fwd_smem(int cap) { return align16(cap * 16) + align16(cap * 4) + size_t(cap) * REC_FLOATS * 4; }
-size_t seg_bwd_smem(int cap) { return seg_fwd_smem(cap) + size_t(cap) * GRAD_SLOTS * 4; }
+__host__ __device__ inline size_t stage_bytes(int cap) { return align16(cap * 16) + align16(cap * 4) + size_t(cap) * REC_FLOATS * 4; }
+// forward: the stage plus, per warp, 32 words of polytope-test rejections
+size_t seg_fwd_smem(int cap, int warps) { return stage_bytes(cap) + size_t(warps) * 32 * 4; }
+size_t seg_bwd_smem(int cap) { return stage_bytes(cap) + size_t(cap) * GRAD_SLOTS * 4; }
 
 // Segment geometry shared by both directions.
 struct SegCtx {
@@ -67,14 +69,60 @@ __device__ __forceinline__ SegCtx seg_setup(const SegLaunch& L, const SceneDesc&
   return c;
 }
 
-__device__ __forceinline__ unsigned cull_block(const Stage& S, const SegCtx& c, int hi, int lane) {
+// Tetrahedron / octahedron reach test (cull_block, flagged strokes). Their SDFs are
+// (g(p) - 1) / sqrt(3) with g the largest of the diagonal forms +-x +-y +-z (four of
+// them for the tetrahedron, strokes_sdf.h:584-588, 607-613), so the samples where
+// alpha reaches the cut lie in the polytope g(p) <= 1 + sqrt(3) tau_local, tau_local
+// = R_PLANE / sqrt(3) * r. Every sample of the segment is within rho of the chord A..B,
+// so the chord, in the stroke's local frame, is clipped against the planes offset by
+// that distance (|n| = sqrt(3)); an empty interval means no sample can reach the cut.
+__device__ __forceinline__ bool polytope_reachable(const float* rec, const SegCtx& c) {
+  const float4 m0 = rec4(rec)[R_M / 4], m1 = rec4(rec)[R_M / 4 + 1], m2 = rec4(rec)[R_M / 4 + 2];
+  const V3 dA = v3(c.A.x - m0.w, c.A.y - m1.w, c.A.z - m2.w);
+  const V3 dB = dA + c.AB;
+  const V3 a = v3(fmaf(m0.x, dA.x, fmaf(m0.y, dA.y, m0.z * dA.z)), fmaf(m1.x, dA.x, fmaf(m1.y, dA.y, m1.z * dA.z)),
+                  fmaf(m2.x, dA.x, fmaf(m2.y, dA.y, m2.z * dA.z)));
+  const V3 b = v3(fmaf(m0.x, dB.x, fmaf(m0.y, dB.y, m0.z * dB.z)), fmaf(m1.x, dB.x, fmaf(m1.y, dB.y, m1.z * dB.z)),
+                  fmaf(m2.x, dB.x, fmaf(m2.y, dB.y, m2.z * dB.z)));
+  const float cc = (1.f + rec[R_PLANE] * c.rmax + 1.7320508f * c.rho * rec[R_SINV]) * 1.0001f + 1e-5f;
+  float lo = 0.f, hi = 1.f;
+  bool out = false;
+  auto plane = [&](float fa, float fb) {
+    fa -= cc;
+    fb -= cc;
+    if (fa > 0.f && fb > 0.f) out = true;
+    else if (fa > 0.f) lo = fmaxf(lo, fa / (fa - fb));
+    else if (fb > 0.f) hi = fminf(hi, fa / (fa - fb));
+  };
+  const float ua = a.x + a.y, va = a.x - a.y, ub = b.x + b.y, vb = b.x - b.y;
+  // the tetrahedron's faces: |x + y| - z and |x - y| + z
+  plane(ua - a.z, ub - b.z);
+  plane(-ua - a.z, -ub - b.z);
+  plane(va + a.z, vb + b.z);
+  plane(-va + a.z, -vb + b.z);
+  if ((__float_as_int(rec[R_KIND]) & 15) == B_OCTAHEDRON) {  // the other four
+    plane(ua + a.z, ub + b.z);
+    plane(-ua + a.z, -ub + b.z);
+    plane(va - a.z, vb - b.z);
+    plane(-va - a.z, -vb - b.z);
+  }
+  return !out && lo <= hi + 1e-6f;
+}
+
+// Sphere test of one 32-stroke block; *poly gets the survivors flagged for the
+// polytope test (the forward batches those tests, see seg_fwd_kernel).
+__device__ __forceinline__ unsigned cull_block_sphere(const Stage& S, const SegCtx& c, int hi, int lane,
+                                                      unsigned* poly) {
   const int sl = hi - lane;
-  bool cand = false;
+  bool cand = false, flagged = false;
   if (sl >= 0) {
     float4 ca = S.cull_a[sl];
     float d = seg_dist(v3(ca.x, ca.y, ca.z), c.A, c.AB, c.invL2);
-    cand = !(d - c.rho > ca.w + S.cull_b[sl] * c.rmax);
+    const float cb = S.cull_b[sl];
+    cand = !(d - c.rho > ca.w + fabsf(cb) * c.rmax);
+    flagged = cand && __float_as_int(cb) < 0;
   }
+  *poly = __ballot_sync(0xffffffffu, flagged);
   return __ballot_sync(0xffffffffu, cand);
 }
 
@@ -88,6 +136,9 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_con
   __shared__ int s_scene, s_fail;
   const Stage S = carve(smem, L.chunk_cap, false);
   const int lane = threadIdx.x & 31;
+  // this warp's 32 words of polytope-test rejections (one per block of the chunk)
+  unsigned* const kill = reinterpret_cast<unsigned*>(smem + stage_bytes(L.chunk_cap)) + (threadIdx.x >> 5) * 32;
+  kill[lane] = 0u;
   if (threadIdx.x == 0) {
     mbar_init(&bar, 1);
     s_fail = 0;
@@ -120,8 +171,59 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_con
         unsigned* bm = RECORD ? L.block_masks + sc.mask_begin +
                                     (long long)(ray_local * L.segs_per_ray + g) * sc.mask_words
                               : nullptr;
-        for (int hi = sc.chunk_n - 1; hi >= 0; hi -= 32) {
-          unsigned mask = cull_block(S, c, hi, lane);
+        // Culling in three steps. 1: the sphere test of every block of the chunk (at most
+        // 32 blocks); lane k keeps block k's survivors and its polytope-flagged subset.
+        const int nblk = (sc.chunk_n + 31) >> 5;
+        unsigned my_mask = 0u, my_poly = 0u;
+        for (int k = 0; k < nblk; k++) {
+          unsigned pm;
+          const unsigned m = cull_block_sphere(S, c, sc.chunk_n - 1 - 32 * k, lane, &pm);
+          if (lane == k) {
+            my_mask = m;
+            my_poly = pm;
+          }
+        }
+        // 2: the flagged candidates of all blocks, 32 per pass, one per lane: the owner
+        // block is the last with prefix count <= the candidate's index (5-step binary
+        // search over the lanes), the stroke its n-th flagged bit; rejections are
+        // collected in this warp's kill words.
+        if (__any_sync(0xffffffffu, my_poly != 0u)) {
+          const int cnt = __popc(my_poly);
+          int incl = cnt;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+          }
+          const int off = incl - cnt;
+          const int total = __shfl_sync(0xffffffffu, incl, 31);
+          for (int g0 = 0; g0 < total; g0 += 32) {
+            const int g = g0 + lane;
+            int kk = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1) {
+              const int o = __shfl_sync(0xffffffffu, off, (kk + step) & 31);
+              if (o <= g) kk += step;
+            }
+            const unsigned pm = __shfl_sync(0xffffffffu, my_poly, kk);
+            const int okk = __shfl_sync(0xffffffffu, off, kk);
+            if (g < total) {
+              unsigned x = pm;
+              for (int n = g - okk; n > 0; n--) x &= x - 1u;
+              const int bit = __ffs(x) - 1;
+              const int slot = sc.chunk_n - 1 - 32 * kk - bit;
+              if (!polytope_reachable(S.recs + size_t(slot) * REC_FLOATS, c)) atomicOr(kill + kk, 1u << bit);
+            }
+          }
+          __syncwarp();
+          my_mask &= ~kill[lane];
+          kill[lane] = 0u;
+          __syncwarp();
+        }
+        // 3: evaluate the survivors block by block in compositing order
+        for (int k = 0; k < nblk; k++) {
+          const int hi = sc.chunk_n - 1 - 32 * k;
+          unsigned mask = __shfl_sync(0xffffffffu, my_mask, k);
           const bool any = mask != 0;
           unsigned kept = 0;  // this lane's strokes of the block whose adjoint the backward needs
           while (mask) {
@@ -313,7 +415,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
             mask = __shfl_sync(0xffffffffu, held, w & 31);
             if (hi < 31) mask &= (2u << hi) - 1u;  // only strokes hi .. 0 exist in the last block
           } else {
-            mask = cull_block(S, c, hi, lane);
+            unsigned unused;
+            mask = cull_block_sphere(S, c, hi, lane, &unused);  // conservative: no polytope test here
           }
           while (mask) {
             const int b = __ffs(mask) - 1;
@@ -777,7 +880,17 @@ __global__ void prep_kernel(const PrepLaunch P) {
   if (!cull || !bound_ok) Rb = __int_as_float(0x7f800000);
   P.cull_a[4 * s] = cw.x; P.cull_a[4 * s + 1] = cw.y; P.cull_a[4 * s + 2] = cw.z;
   P.cull_a[4 * s + 3] = Rb * 1.0001f + 1e-6f;
-  P.cull_b[s] = cm * 1.0001f;
+  // Tetrahedra and octahedra without per-axis scale also get the exact polytope test
+  // of cull_block (flagged by the margin's sign bit): their alpha reaches the cut only
+  // where the local SDF is below tau_local = cm r Lg / s, i.e. inside the polytope
+  // {gauge(p) <= 1 + sqrt(3) tau_local}, which fills 12 % (tetrahedron) / 32 %
+  // (octahedron) of the bounding sphere.
+  // (without culling the margin is meaningless, and may be negative: store 0 so that
+  // the sign bit flags the polytope test alone)
+  const bool plane = (base == B_OCTAHEDRON || base == B_TETRAHEDRON) && !s3 && cull && bound_ok;
+  if (plane) rec[R_PLANE] = 1.7320508f * cm * Lg / sc.x;
+  const float margin = (cull && bound_ok) ? fmaxf(cm, 0.f) * 1.0001f : 0.f;
+  P.cull_b[s] = plane ? -margin : margin;
 }
 
 __device__ void prim_param_grads(const FinalizeLaunch& F, long long s, int base, int flags, const float* g,

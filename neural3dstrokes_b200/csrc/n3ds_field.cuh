@@ -138,7 +138,7 @@ void launch_ray_fwd(const RayLaunch& L, cudaStream_t st);
 void launch_ray_bwd(const RayLaunch& L, cudaStream_t st);
 void launch_finalize(const FinalizeLaunch& L, cudaStream_t st);
 
-size_t seg_fwd_smem(int chunk_cap);
+size_t seg_fwd_smem(int chunk_cap, int warps);
 size_t seg_bwd_smem(int chunk_cap);
 
 // sample-run kernels (n3ds_runs.cu): same launch descriptor, work items are units of

@@ -162,7 +162,7 @@ __device__ __forceinline__ int upper_bound_u(const float* u, int n, float v) {
 // Run of stroke sl (staged slot) for this unit: first sample and count (0: culled).
 __device__ __forceinline__ int stroke_run(const RunStage& R, const Unit& U, const RunBuf& B, int sl, int* i0) {
   const float4 ca = R.s.cull_a[sl];
-  const float Rr = ca.w + R.s.cull_b[sl] * U.rmax + U.rho;
+  const float Rr = ca.w + fabsf(R.s.cull_b[sl]) * U.rmax + U.rho;
   const V3 w = v3(ca.x, ca.y, ca.z) - U.A;
   const float uc = dot(w, U.AB) * U.invL2;
   const V3 q = w - U.AB * uc;
