@@ -53,7 +53,7 @@ BWD_FACTOR = 2.5
 # workload (config 3), from one ncu capture at a quarter of its rays (all passes of
 # one step, dram__bytes_read.sum + dram__bytes_write.sum; launch-list summary in
 # profiles/launches_cfg3_quarter.md); traffic grows with the ray count.
-SEG_BWD_TRAFFIC_CFG3_QUARTER = 573.2e6
+SEG_BWD_TRAFFIC_CFG3_QUARTER = 576.0e6
 KIND_BASE = {"sphere": 0, "ellipsoid": 0, "aacube": 1, "cube": 1, "aabb": 1, "obb": 1, "roundcube": 2,
              "roundbox": 2, "cappedtorus": 3, "capsule": 4, "scapsule": 4, "line": 5, "triprism": 6,
              "octahedron": 7, "tetrahedron": 8, "quadratic_bezier": 9, "cubic_bezier": 10, "catmull_rom": 11}
