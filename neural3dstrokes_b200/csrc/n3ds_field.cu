@@ -111,6 +111,43 @@ __device__ __forceinline__ bool polytope_reachable(const float* rec, const SegCt
 
 // Sphere test of one 32-stroke block; *poly gets the survivors flagged for the
 // polytope test (the forward batches those tests, see seg_fwd_kernel).
+// Curve reach test (the forward's batched pass, flagged curves). Every sample where
+// alpha reaches the cut is within r_max + tau of the curve (the SDF uses the distance
+// to one curve point, no less than the true distance), the curve within eps of its
+// polyline (R_CTEST = r_max + eps), each polyline piece within its half-length of its
+// midpoint, and the segment's samples within rho of the chord: the chord has to pass
+// within half-length + R_CTEST + margin r_max + rho of some piece's midpoint. The
+// pieces are visited from a lane-dependent start, so that lanes reading different
+// strokes' records fall into different shared-memory banks.
+__device__ __forceinline__ bool curve_reachable(const float* rec, const SegCtx& c, float margin, int lane) {
+  const float reach = rec[R_CTEST] + margin * c.rmax + c.rho;
+  if ((__float_as_int(rec[R_KIND]) & 15) == B_QUAD_BEZIER) {
+    const float4 qA = rec4(rec)[R_QA / 4], qa = rec4(rec)[R_Qa / 4], qb = rec4(rec)[R_Qb / 4];
+    const V3 A = xyz(qA), a2 = xyz(qa) * 2.f, b = xyz(qb);
+    auto at = [&](float t) { return A + (a2 + b * t) * t; };  // B(t) = A + 2 a t + b t^2
+    int p = lane & 7;
+    V3 v0 = at(p * 0.125f);
+    for (int k = 0; k < 8; k++) {
+      const V3 v1 = at((p + 1) * 0.125f);
+      const V3 m = (v0 + v1) * 0.5f, h = (v1 - v0) * 0.5f;
+      if (seg_dist(m, c.A, c.AB, c.invL2) <= sqrtf(dot(h, h)) + reach) return true;
+      p = (p + 1) & 7;
+      v0 = p == 0 ? A : v1;
+    }
+    return false;
+  }
+  int p = lane % CUBIC_SEGMENTS;
+  V3 v0 = v3(rec[R_CV + 3 * p], rec[R_CV + 3 * p + 1], rec[R_CV + 3 * p + 2]);
+  for (int k = 0; k < CUBIC_SEGMENTS; k++) {
+    const V3 v1 = v3(rec[R_CV + 3 * p + 3], rec[R_CV + 3 * p + 4], rec[R_CV + 3 * p + 5]);
+    const V3 m = (v0 + v1) * 0.5f, h = (v1 - v0) * 0.5f;
+    if (seg_dist(m, c.A, c.AB, c.invL2) <= sqrtf(dot(h, h)) + reach) return true;
+    p = p + 1 == CUBIC_SEGMENTS ? 0 : p + 1;
+    v0 = p == 0 ? v3(rec[R_CV], rec[R_CV + 1], rec[R_CV + 2]) : v1;
+  }
+  return false;
+}
+
 __device__ __forceinline__ unsigned cull_block_sphere(const Stage& S, const SegCtx& c, int hi, int lane,
                                                       unsigned* poly) {
   const int sl = hi - lane;
@@ -212,7 +249,11 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_con
               for (int n = g - okk; n > 0; n--) x &= x - 1u;
               const int bit = __ffs(x) - 1;
               const int slot = sc.chunk_n - 1 - 32 * kk - bit;
-              if (!polytope_reachable(S.recs + size_t(slot) * REC_FLOATS, c)) atomicOr(kill + kk, 1u << bit);
+              const float* rec = S.recs + size_t(slot) * REC_FLOATS;
+              const bool reach = (__float_as_int(rec[R_KIND]) & 15) <= B_TETRAHEDRON
+                                     ? polytope_reachable(rec, c)
+                                     : curve_reachable(rec, c, fabsf(S.cull_b[slot]), lane);
+              if (!reach) atomicOr(kill + kk, 1u << bit);
             }
           }
           __syncwarp();
@@ -812,6 +853,8 @@ __global__ void prep_kernel(const PrepLaunch P) {
     float rc = fmaxf(sqrtf(dot(A - cw, A - cw)), fmaxf(sqrtf(dot(B - cw, B - cw)), sqrtf(dot(C - cw, C - cw))));
     Rb = rc + fmaxf(prm[9], prm[10]);
     smax = smin = 1.f;
+    // 8 chords at t = k/8: curve-to-chord distance <= max|B''| dt^2 / 8 = |b| / 256
+    rec[R_CTEST] = (fmaxf(prm[9], prm[10]) + sqrtf(dot(b, b)) * (1.f / 256.f)) * 1.0001f;
   } else {
     // cubic Bezier: the control points; Catmull-Rom: its power-basis coefficients
     // (A, B, C, D of t^3, t^2, t, 1, strokes_sdf.h:1340-1349). hull[] holds Bezier
@@ -850,6 +893,13 @@ __global__ void prep_kernel(const PrepLaunch P) {
       V3 v = P4[0] * w[0] + P4[1] * w[1] + P4[2] * w[2] + P4[3] * w[3];
       rec[R_CV + 3 * i] = v.x; rec[R_CV + 3 * i + 1] = v.y; rec[R_CV + 3 * i + 2] = v.z;
     }
+    // curve-to-polyline distance <= max|B''| dt^2 / 8, |B''| <= 6 max second difference
+    // of the Bezier control points (the hull points of either curve)
+    {
+      const V3 d0 = (hull[0] - hull[1] * 2.f) + hull[2], d1 = (hull[1] - hull[2] * 2.f) + hull[3];
+      const float dd = fmaxf(sqrtf(dot(d0, d0)), sqrtf(dot(d1, d1)));
+      rec[R_CTEST] = (fmaxf(prm[12], prm[13]) + dd * (6.f * step * step / 8.f)) * 1.0001f;
+    }
     cw = (hull[0] + hull[1] + hull[2] + hull[3]) * 0.25f;
     float rc = 0.f;
     for (int k = 0; k < 4; k++) rc = fmaxf(rc, sqrtf(dot(hull[k] - cw, hull[k] - cw)));
@@ -887,8 +937,9 @@ __global__ void prep_kernel(const PrepLaunch P) {
   // (octahedron) of the bounding sphere.
   // (without culling the margin is meaningless, and may be negative: store 0 so that
   // the sign bit flags the polytope test alone)
-  const bool plane = (base == B_OCTAHEDRON || base == B_TETRAHEDRON) && !s3 && cull && bound_ok;
-  if (plane) rec[R_PLANE] = 1.7320508f * cm * Lg / sc.x;
+  const bool plane = ((base == B_OCTAHEDRON || base == B_TETRAHEDRON) && !s3 && cull && bound_ok) ||
+                     (base >= B_QUAD_BEZIER && cull && bound_ok);  // curves: the piece test
+  if (plane && base <= B_TETRAHEDRON) rec[R_PLANE] = 1.7320508f * cm * Lg / sc.x;
   const float margin = (cull && bound_ok) ? fmaxf(cm, 0.f) * 1.0001f : 0.f;
   P.cull_b[s] = plane ? -margin : margin;
 }

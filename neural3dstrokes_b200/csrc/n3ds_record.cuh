@@ -89,6 +89,9 @@ constexpr int R_CA = 8, R_CR1 = 11;    // q2: A, r1
 constexpr int R_CB = 12, R_CR2 = 15;   // q3: B, r2
 constexpr int R_CC = 16, R_CD = 20;    // q4, q5: C, D
 constexpr int R_CV = 24;       // 11 polyline vertices, 33 floats (24..56), read as 9 float4
+// every curve: culling radius of its polyline pieces beyond their half-length (the
+// largest tube radius plus the curve's distance bound to its polyline)
+constexpr int R_CTEST = 60;
 constexpr int CUBIC_SEGMENTS = 10;
 
 __device__ __forceinline__ const float4* rec4(const float* rec) { return reinterpret_cast<const float4*>(rec); }
