@@ -413,14 +413,17 @@ def main():
                       for ms, o in autotune.last_results]
     segments = field.options.schedule != "runs"
 
-    # statistics pass (not timed): evaluated pairs per primitive type (forward) and
-    # in total (backward), status word
+    # statistics pass (not timed; the only one with the pair counters on): evaluated
+    # pairs per primitive type (forward) and in total (backward), status word
+    import dataclasses
+    field.c_opt = dataclasses.replace(field.options, count_pairs=True).c()
     field.forward()
     field.backward()
     torch.cuda.synchronize(dev)
     per_base = field.pair_counts()
     bwd_evaluated = field.backward_pairs()
     status, evaluated = field.status()
+    field.c_opt = field.options.c()
     if status != 0:
         raise SystemExit(f"device status {status}")
 

@@ -209,6 +209,11 @@ typedef struct n3ds_options {
   /* 1: no backward follows this forward, so the segment kernels skip recording which
    * strokes the backward needs (a backward after such a forward culls by itself) */
   int32_t forward_only;
+  /* 1: count the evaluated (sample, stroke) pairs, per base SDF type in the forward and
+   * in total in the backward (n3ds_field_read_status, _read_pair_counts,
+   * _read_backward_pairs); 0 (default): those counters stay 0 and the kernels skip the
+   * per-candidate bookkeeping */
+  int32_t count_pairs;
 } n3ds_options_t;
 
 /* Fill *opt with the defaults. */
@@ -240,7 +245,8 @@ int n3ds_field_backward(const n3ds_batch_t* batch, const n3ds_rays_t* rays,
                         n3ds_stream_t stream);
 
 /* Synchronously read (and clear) the device status word and the count of evaluated
- * (sample, stroke) pairs of the last forward. n3ds_field_forward clears the status
+ * (sample, stroke) pairs of the last forward (with options.count_pairs; else 0).
+ * n3ds_field_forward clears the status
  * word first, so it reports the last forward and the backwards after it: 0 = fine,
  * bit 1 = an unsupported sdf id, bit 2 = a bounded wait gave up. */
 int n3ds_field_read_status(void* workspace, int32_t* status, uint64_t* evaluated_pairs,

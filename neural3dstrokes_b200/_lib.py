@@ -46,7 +46,7 @@ class Options(ctypes.Structure):
     _fields_ = [("cull_alpha", ctypes.c_float), ("chunk_fwd", c_i32), ("chunk_bwd", c_i32),
                 ("warps", c_i32), ("schedule", c_i32), ("grad_mode", c_i32),
                 ("timing_events", ctypes.POINTER(ctypes.c_void_p)), ("warps_bwd", c_i32),
-                ("forward_only", c_i32)]
+                ("forward_only", c_i32), ("count_pairs", c_i32)]
 
 
 _P = ctypes.c_void_p

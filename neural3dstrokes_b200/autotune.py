@@ -41,7 +41,8 @@ def signature(field) -> str:
                       sort_keys=True)
 
 
-def candidates(grad_mode: str = "exact", cull_alpha: float = 1e-9, forward_only: bool = False) -> List[FieldOptions]:
+def candidates(grad_mode: str = "exact", cull_alpha: float = 1e-9, forward_only: bool = False,
+               count_pairs: bool = False) -> List[FieldOptions]:
     out = []
     # (schedule, forward warps, backward warps): the segment kernels' register use
     # allows up to 32 / 24 warps per CTA, the run kernels 16
@@ -52,7 +53,7 @@ def candidates(grad_mode: str = "exact", cull_alpha: float = 1e-9, forward_only:
             # chunk 0 = the largest stage that fits; the halved stage (-1) is resolved later
             out.append(FieldOptions(cull_alpha=cull_alpha, warps=wf, warps_bwd=wb, schedule=schedule,
                                     grad_mode=grad_mode, chunk_fwd=-1 if half else 0, chunk_bwd=-1 if half else 0,
-                                    forward_only=forward_only))
+                                    forward_only=forward_only, count_pairs=count_pairs))
     return out
 
 
@@ -118,7 +119,7 @@ def tune(field, reps: int = 3, cands: Optional[List[FieldOptions]] = None, use_c
         return best
     base = field.options
     results = []
-    for opt in cands or candidates(base.grad_mode, base.cull_alpha, base.forward_only):
+    for opt in cands or candidates(base.grad_mode, base.cull_alpha, base.forward_only, base.count_pairs):
         opt = _resolve_half(field, opt)
         field.options = opt
         field._bind()

@@ -102,6 +102,7 @@ struct Resolved {
   int warps_fwd, warps_bwd;  // per direction (the forward segment kernel runs 24 warps by default)
   void* const* events;
   int forward_only;
+  int count_pairs;
 };
 
 void record_event(const Resolved& rv, int i, cudaStream_t st) {
@@ -153,6 +154,7 @@ Resolved resolve(const n3ds_options_t* o) {
   r.chunk_bwd = cb;
   r.grad_mode = o->grad_mode;
   r.forward_only = o->forward_only != 0;
+  r.count_pairs = o->count_pairs != 0;
   r.events = o->timing_events;
   return r;
 }
@@ -288,6 +290,7 @@ void n3ds_default_options(n3ds_options_t* opt) {
   opt->timing_events = nullptr;
   opt->warps_bwd = 0;
   opt->forward_only = 0;
+  opt->count_pairs = 0;
 }
 
 size_t n3ds_field_workspace_bytes(const n3ds_batch_t* batch, const n3ds_options_t* opt) {
@@ -413,6 +416,7 @@ int n3ds_field_forward(const n3ds_batch_t* batch, const n3ds_rays_t* rays, const
   record_event(rv, 0, st);
   n3ds::SegLaunch FL = make_seg(batch, rays, ws, lay, 0);
   FL.skip_alpha = rv.cull_alpha;
+  if (!rv.count_pairs) FL.stats = nullptr;
   if (rv.forward_only || rv.schedule != N3DS_SCHEDULE_SEGMENTS) {
     FL.block_masks = nullptr;
   } else if (lay.masks < lay.total) {
@@ -460,7 +464,7 @@ int n3ds_field_backward(const n3ds_batch_t* batch, const n3ds_rays_t* rays, cons
   }
   n3ds::SegLaunch SL = make_seg(batch, rays, ws, lay, compat);
   SL.grad_x = grad_x;
-  SL.stats = reinterpret_cast<unsigned long long*>(ws + lay.stats) + 17;  // backward pair count
+  SL.stats = rv.count_pairs ? reinterpret_cast<unsigned long long*>(ws + lay.stats) + 17 : nullptr;  // pairs
   SL.skip_alpha = rv.cull_alpha;
   record_event(rv, 2, st);
   rc = run_seg_passes(true, batch, rv, SL, N_LAUNCH_SLOTS / 2, st);

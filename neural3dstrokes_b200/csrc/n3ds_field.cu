@@ -166,7 +166,8 @@ __device__ __forceinline__ unsigned cull_block_sphere(const Stage& S, const SegC
 // ================================================================== forward
 
 // RECORD: write the stroke-block masks (L.block_masks non-null) for the backward.
-template <int WARPS, bool RECORD>
+// STATS: count evaluated pairs per base type into L.stats (non-null).
+template <int WARPS, bool RECORD, bool STATS>
 __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_constant__ SegLaunch L) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t bar;
@@ -273,7 +274,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_con
             const float* rec = S.recs + size_t(hi - b) * REC_FLOATS;
             const float a = pair_alpha(rec, c.x, c.rinv);
             if (RECORD && a >= L.skip_alpha) kept |= 1u << b;
-            if (lane == (__float_as_int(rec[R_KIND]) & 15)) kcount += nact;
+            if (STATS && lane == (__float_as_int(rec[R_KIND]) & 15)) kcount += nact;
             const float w = a * T;
             const float4 col = rec4(rec)[R_COLOR / 4];
             T *= (1.0f - a);
@@ -301,7 +302,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_con
     __syncthreads();
     sci = s_scene;
   }
-  if (L.stats && lane < 16 && kcount) {
+  if (STATS && lane < 16 && kcount) {
     atomicAdd(L.stats, kcount);
     atomicAdd(L.stats + 1 + lane, kcount);
   }
@@ -1104,7 +1105,8 @@ void launch_prep(const PrepLaunch& p, cudaStream_t st) {
 
 template <int W>
 static cudaError_t launch_fwd_w(const SegLaunch& L, int grid, size_t smem, cudaStream_t st) {
-  auto* k = L.block_masks ? seg_fwd_kernel<W, true> : seg_fwd_kernel<W, false>;
+  auto* k = L.block_masks ? (L.stats ? seg_fwd_kernel<W, true, true> : seg_fwd_kernel<W, true, false>)
+                          : (L.stats ? seg_fwd_kernel<W, false, true> : seg_fwd_kernel<W, false, false>);
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   k<<<grid, W * 32, smem, st>>>(L);

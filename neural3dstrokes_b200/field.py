@@ -29,6 +29,7 @@ class FieldOptions:
     schedule: str = "auto"     # 'segments' (auto): lane = sample; 'runs': packed (sample, stroke) pairs
     grad_mode: str = "exact"   # 'exact' or 'compat'
     forward_only: bool = False  # no backward follows: skip the bookkeeping the backward reads
+    count_pairs: bool = False   # count evaluated pairs (statistics; a few % of the forward's work)
 
     def c(self, events=None):
         """ctypes options; ``events``: optional 4 torch.cuda.Event(enable_timing=True)
@@ -44,7 +45,7 @@ class FieldOptions:
         return _lib.Options(float(self.cull_alpha), int(self.chunk_fwd), int(self.chunk_bwd), int(self.warps),
                             {"auto": 0, "segments": 1, "runs": 2}[self.schedule],
                             _lib.N3DS_GRAD_COMPAT if self.grad_mode == "compat" else _lib.N3DS_GRAD_EXACT, ev,
-                            int(self.warps_bwd), int(bool(self.forward_only)))
+                            int(self.warps_bwd), int(bool(self.forward_only)), int(bool(self.count_pairs)))
 
 
 class _Native:

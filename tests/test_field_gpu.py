@@ -199,3 +199,25 @@ def test_forward_only_outputs_are_identical(cuda):
     with torch.no_grad():
         (b, acc_b, d_b), _ = run_field(sc, rays, cuda)
     assert torch.equal(a.detach(), b) and torch.equal(acc_a.detach(), acc_b) and torch.equal(d_a.detach(), d_b)
+
+
+def test_pair_counters_only_when_requested(cuda):
+    """options.count_pairs fills the evaluated-pair counters (forward per base type,
+    backward total); without it they stay 0 and the outputs are the same."""
+    from neural3dstrokes_b200.train import BatchedField
+    sc, rays = small_workload("mixed", n_strokes=60, n_rays=96, n_samples=64, seed=2)
+    out = []
+    for count in (True, False):
+        f = BatchedField([sc], [rays], options=FieldOptions(count_pairs=count), device=cuda)
+        f.g_rgb.fill_(1.0)
+        f.step()
+        st, pairs = f.status()
+        per_base, bwd = f.pair_counts(), f.backward_pairs()
+        assert st == 0
+        if count:
+            assert pairs > 0 and sum(per_base) == pairs and 0 < bwd <= pairs
+        else:
+            assert pairs == 0 and sum(per_base) == 0 and bwd == 0
+        out.append((f.rgb.clone(), f.grad_shape.clone()))
+    assert torch.equal(out[0][0], out[1][0])
+    assert rel(out[0][1], out[1][1]) < 1e-5
