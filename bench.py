@@ -74,33 +74,51 @@ def base_flops(kinds):
 
 
 class ClockSampler:
-    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    """nvidia-smi sampling (every 50 ms) of SM clocks and throttle reasons. A reader
+    thread stamps each line with the host clock; ``stop(lo, hi)`` keeps the samples
+    stamped inside [lo, hi], the host times around the timed region (the GPU is busy
+    from just after ``lo`` until the synchronisation that precedes ``hi``)."""
 
     def __init__(self, gpu):
         self.gpu = gpu
         self.proc = None
+        self.lines = []
+        self.thread = None
 
     def start(self):
+        import threading
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={CLOCK_FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                          "-lms", "50", "-i", str(self.gpu)], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+            return
 
-    def stop(self):
+        def read():
+            for line in self.proc.stdout:
+                self.lines.append((time.monotonic(), line))
+        self.thread = threading.Thread(target=read, daemon=True)
+        self.thread.start()
+        t_end = time.monotonic() + 3.0  # sampling is live before the timed region starts
+        while not self.lines and time.monotonic() < t_end and self.proc.poll() is None:
+            time.sleep(0.01)
+
+    def stop(self, lo=None, hi=None):
         if self.proc is None:
             return None
-        time.sleep(0.25)
         self.proc.terminate()
         try:
-            out, _ = self.proc.communicate(timeout=5)
+            self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
-            out, _ = self.proc.communicate()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
+        stamped = list(self.lines)
+        inside = [l for t, l in stamped if (lo is None or t >= lo) and (hi is None or t <= hi)]
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in out.strip().splitlines():
+        for line in inside:
             f = [v.strip() for v in line.split(",")]
             if len(f) < 9:
                 continue
@@ -113,7 +131,8 @@ class ClockSampler:
                 if v.lower().startswith("active"):
                     reasons.add(n)
         if not sm:
-            return None
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0,
+                    "note": "no nvidia-smi sample fell inside the timed region"}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
                 "samples": len(sm)}
 
@@ -437,13 +456,15 @@ def main():
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize(dev)
     barrier(world)
+    host_lo = time.monotonic()
     t0.record()
     for _ in range(args.steps):
         graph.replay()
     t1.record()
     torch.cuda.synchronize(dev)
+    host_hi = time.monotonic()
     barrier(world)
-    clk = clocks.stop()
+    clk = clocks.stop(host_lo, host_hi)
     value, step_s = replica_throughput(t0.elapsed_time(t1) * 1e-3 / args.steps, pairs, world, dev)
 
     # dominant-kernel timing with CUDA events recorded on the launching stream
