@@ -377,7 +377,9 @@ __device__ __forceinline__ void compose_skip(const float* rec, float a, CompAdj&
   s.T *= (1.0f - a);
 }
 
-template <int WARPS>
+// GX: the sample-position gradient is wanted (L.grad_x non-null); without it the
+// kernel carries no position gradient at all.
+template <int WARPS, bool GX>
 __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_constant__ SegLaunch L) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t bar;
@@ -440,7 +442,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
         } else {
           const float* b = L.bstate + 8 * c.si;
           s.T = b[0]; s.Ps = b[1]; s.Pr = b[2]; s.Pg = b[3]; s.Pb = b[4];
-          gx = v3(b[5], b[6], b[7]);
+          gx = GX ? v3(b[5], b[6], b[7]) : v3(0.f, 0.f, 0.f);
         }
         const unsigned* bm =
             masks ? masks + sc.mask_begin + (long long)(ray_local * L.segs_per_ray + g) * sc.mask_words : nullptr;
@@ -488,7 +490,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
               const float dm = compose_step(rec, a, m, mode, s, v, compat);
               const float K = m * dm;
               v[G_K] += K;
-              gx += prim_backprop(rec, kind, p, -kk * dm, K, v, compat);
+              const V3 gp = prim_backprop(rec, kind, p, -kk * dm, K, v, compat);
+              if (GX) gx += gp;
               reduce_into<16>(v, row, lane);
             } else if (base == B_QUAD_BEZIER) {
               float v[16];
@@ -505,7 +508,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
               }
               const float dm = compose_step(rec, a, m, mode, s, v, compat);
               v[G_K] += m * dm;
-              gx += quad_adjoint(rec, qf, -kk * dm, v + G_CTRL);
+              const V3 gq = quad_adjoint(rec, qf, -kk * dm, v + G_CTRL);
+              if (GX) gx += gq;
               reduce_into<16>(v, row, lane);
             } else {
               float v[32];
@@ -525,14 +529,14 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
               v[G_K] += m * dm;
               V3 g = cubic_adjoint(rec, c.x, cf, dsdf, v + G_CTRL, compat, base == B_CATMULL_ROM);
               if (compat) g = g * dsdf;  // the reference multiplies by dL/dSDF again
-              gx += g;
+              if (GX) gx += g;
               reduce_into<32>(v, row, lane);
             }
           }
         }
         if (c.active) {
           if (sc.last_pass) {
-            if (L.grad_x) {
+            if (GX) {
               L.grad_x[3 * c.si] = gx.x;
               L.grad_x[3 * c.si + 1] = gx.y;
               L.grad_x[3 * c.si + 2] = gx.z;
@@ -540,7 +544,9 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
           } else {
             float* b = L.bstate + 8 * c.si;
             b[0] = s.T; b[1] = s.Ps; b[2] = s.Pr; b[3] = s.Pg; b[4] = s.Pb;
-            b[5] = gx.x; b[6] = gx.y; b[7] = gx.z;
+            if (GX) {
+              b[5] = gx.x; b[6] = gx.y; b[7] = gx.z;
+            }
           }
         }
       }
@@ -1114,9 +1120,10 @@ static cudaError_t launch_fwd_w(const SegLaunch& L, int grid, size_t smem, cudaS
 }
 template <int W>
 static cudaError_t launch_bwd_w(const SegLaunch& L, int grid, size_t smem, cudaStream_t st) {
-  cudaError_t e = cudaFuncSetAttribute(seg_bwd_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  auto* k = L.grad_x ? seg_bwd_kernel<W, true> : seg_bwd_kernel<W, false>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  seg_bwd_kernel<W><<<grid, W * 32, smem, st>>>(L);
+  k<<<grid, W * 32, smem, st>>>(L);
   return cudaGetLastError();
 }
 
