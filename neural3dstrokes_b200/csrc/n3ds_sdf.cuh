@@ -461,9 +461,8 @@ struct CubicFwd {
 
 __device__ __forceinline__ float cubic_eval(const float* rec, V3 pos, CubicFwd& s, bool power) {
   constexpr float step = 1.0f / CUBIC_SEGMENTS;
-  float best = 1e18f, t_min = 0.f, tau_best = 0.f, tau_raw_best = 0.f;
+  float best = 1e18f, tau_best = 0.f, tau_raw_best = 0.f;
   int seg = 0;
-  float t_start = 0.f;
   float vtx[36];
 #pragma unroll
   for (int k = 0; k < 9; k++) {
@@ -473,7 +472,6 @@ __device__ __forceinline__ float cubic_eval(const float* rec, V3 pos, CubicFwd& 
   V3 s0 = v3(vtx[0], vtx[1], vtx[2]);
 #pragma unroll
   for (int i = 1; i <= CUBIC_SEGMENTS; i++) {
-    float t_end = i * step;
     V3 s1 = v3(vtx[3 * i], vtx[3 * i + 1], vtx[3 * i + 2]);
     V3 ab = s1 - s0;
     float tr = dot(pos - s0, ab) / dot(ab, ab);
@@ -482,14 +480,15 @@ __device__ __forceinline__ float cubic_eval(const float* rec, V3 pos, CubicFwd& 
     float d2 = dot(dv, dv);
     if (d2 < best) {
       best = d2;
-      t_min = t_start * (1.0f - tt) + t_end * tt;
       tau_best = tt;
       tau_raw_best = tr;
       seg = i;
     }
-    t_start = t_end;
     s0 = s1;
   }
+  // the winning segment's t, as the reference's t_start (1 - tau) + t_end tau with
+  // t_start = (seg - 1) step, t_end = seg step (the same float values as in its loop)
+  const float t_min = seg ? ((float)(seg - 1) * step) * (1.0f - tau_best) + ((float)seg * step) * tau_best : 0.f;
   float w[4];
   curve_weights(t_min, w, power);
   const float4 cA = rec4(rec)[R_CA / 4], cB = rec4(rec)[R_CB / 4], cC = rec4(rec)[R_CC / 4],
