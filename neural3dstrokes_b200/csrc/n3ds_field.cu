@@ -4,12 +4,15 @@
 // consecutive samples; one warp owns one segment at a time (lane = sample). Stroke
 // records of the current scene are staged into shared memory by one bulk
 // (cp.async.bulk / TMA) copy per chunk of strokes, completed on an mbarrier. For each
-// segment the warp first culls the chunk: lane j tests stroke (top - j) of a
+// segment the forward warp first culls the chunk: lane j tests stroke (top - j) of a
 // 32-stroke block against the segment's bounding capsule, and a ballot gives the
 // surviving strokes in descending index order, i.e. the reference compositing order
-// (compositing.cu:34, last stroke on top). Every lane then evaluates the surviving
-// strokes for its own sample; the stroke (and so the SDF type) is warp-uniform, so
-// mixed-type scenes run without divergence.
+// (compositing.cu:34, last stroke on top); the survivors that carry an exact reach
+// test (tetrahedra, octahedra, curves) are then tested 32 at a time, one per lane.
+// Every lane then evaluates the surviving strokes for its own sample; the stroke (and
+// so the SDF type) is warp-uniform, so mixed-type scenes run without divergence. The
+// forward records, per segment and 32-stroke block, which survivors reach the alpha
+// threshold at some sample; the backward reads those words instead of culling.
 //
 // Persistent CTAs (one per SM) with scene affinity: the host gives every scene of a
 // launch a share of the CTAs proportional to its work (rays x strokes in the chunk),
@@ -27,7 +30,9 @@
 //                     + g_C . (T_{s+1} c_s - suffix_C) - g_T T_final,
 // and reduces per-stroke gradients across the warp with a transpose reduction
 // before one shared-memory atomic per value; CTAs flush to global memory once per
-// staged chunk.
+// staged chunk. Template switches compile out what a call does not need: the mask
+// recording (a forward no backward follows), the pair counters (statistics) and the
+// sample-position gradient.
 #include "n3ds_stage.cuh"
 
 namespace n3ds {
