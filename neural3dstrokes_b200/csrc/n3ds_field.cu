@@ -116,6 +116,26 @@ __device__ __forceinline__ bool polytope_reachable(const float* rec, const SegCt
 
 // Sphere test of one 32-stroke block; *poly gets the survivors flagged for the
 // polytope test (the forward batches those tests, see seg_fwd_kernel).
+// Ellipsoid reach test (flagged per-axis-scaled spheres): the chord, in the stroke's
+// local frame, must pass within 1 + R_PLANE r_max of the origin; the samples' distance
+// rho to the chord grows by at most 1 / s_min in that frame.
+__device__ __forceinline__ bool ellipsoid_reachable(const float* rec, const SegCtx& c) {
+  const float4 m0 = rec4(rec)[R_M / 4], m1 = rec4(rec)[R_M / 4 + 1], m2 = rec4(rec)[R_M / 4 + 2];
+  const V3 dA = v3(c.A.x - m0.w, c.A.y - m1.w, c.A.z - m2.w);
+  const V3 dB = dA + c.AB;
+  const V3 a = v3(fmaf(m0.x, dA.x, fmaf(m0.y, dA.y, m0.z * dA.z)), fmaf(m1.x, dA.x, fmaf(m1.y, dA.y, m1.z * dA.z)),
+                  fmaf(m2.x, dA.x, fmaf(m2.y, dA.y, m2.z * dA.z)));
+  const V3 b = v3(fmaf(m0.x, dB.x, fmaf(m0.y, dB.y, m0.z * dB.z)), fmaf(m1.x, dB.x, fmaf(m1.y, dB.y, m1.z * dB.z)),
+                  fmaf(m2.x, dB.x, fmaf(m2.y, dB.y, m2.z * dB.z)));
+  const float sinv = fmaxf(rec[R_SINV], fmaxf(rec[R_SINV + 1], rec[R_SINV + 2]));
+  const float reach = (1.f + rec[R_PLANE] * c.rmax + c.rho * sinv) * 1.0001f + 1e-5f;
+  const V3 ab = b - a;
+  const float l2 = dot(ab, ab);
+  const float u = l2 > 0.f ? clampf(-dot(a, ab) / l2, 0.f, 1.f) : 0.f;
+  const V3 q = a + ab * u;
+  return dot(q, q) <= reach * reach;
+}
+
 // Curve reach test (the forward's batched pass, flagged curves). Every sample where
 // alpha reaches the cut is within r_max + tau of the curve (the SDF uses the distance
 // to one curve point, no less than the true distance), the curve within eps of its
@@ -256,9 +276,10 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_con
               const int bit = __ffs(x) - 1;
               const int slot = sc.chunk_n - 1 - 32 * kk - bit;
               const float* rec = S.recs + size_t(slot) * REC_FLOATS;
-              const bool reach = (__float_as_int(rec[R_KIND]) & 15) <= B_TETRAHEDRON
-                                     ? polytope_reachable(rec, c)
-                                     : curve_reachable(rec, c, fabsf(S.cull_b[slot]), lane);
+              const int rb = __float_as_int(rec[R_KIND]) & 15;
+              const bool reach = rb == B_SPHERE        ? ellipsoid_reachable(rec, c)
+                                 : rb <= B_TETRAHEDRON ? polytope_reachable(rec, c)
+                                                       : curve_reachable(rec, c, fabsf(S.cull_b[slot]), lane);
               if (!reach) atomicOr(kill + kk, 1u << bit);
             }
           }
@@ -949,9 +970,17 @@ __global__ void prep_kernel(const PrepLaunch P) {
   // (octahedron) of the bounding sphere.
   // (without culling the margin is meaningless, and may be negative: store 0 so that
   // the sign bit flags the polytope test alone)
+  // Per-axis-scaled spheres (ellipsoids): alpha reaches the cut only where the local
+  // radius |p| <= 1 + tau_local, tau_local = m_cut delta r / (kappa f) with the radius
+  // factor f >= s_min under inv_scale_radius (f = 1 without it).
+  const bool ell = base == B_SPHERE && s3 && cull && bound_ok;
   const bool plane = ((base == B_OCTAHEDRON || base == B_TETRAHEDRON) && !s3 && cull && bound_ok) ||
-                     (base >= B_QUAD_BEZIER && cull && bound_ok);  // curves: the piece test
-  if (plane && base <= B_TETRAHEDRON) rec[R_PLANE] = 1.7320508f * cm * Lg / sc.x;
+                     (base >= B_QUAD_BEZIER && cull && bound_ok) || ell;  // curves: the piece test
+  if (plane && (base == B_OCTAHEDRON || base == B_TETRAHEDRON)) rec[R_PLANE] = 1.7320508f * cm * Lg / sc.x;
+  if (ell) {
+    const float mc = mode == STEP_HARD ? 0.f : (mode == STEP_LINEAR ? 0.5f : P.cull_m);
+    rec[R_PLANE] = fmaxf(mc, 0.f) * delta / kappa / (P.inv_scale_radius ? smin : 1.f);
+  }
   const float margin = (cull && bound_ok) ? fmaxf(cm, 0.f) * 1.0001f : 0.f;
   P.cull_b[s] = plane ? -margin : margin;
 }

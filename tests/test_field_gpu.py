@@ -79,9 +79,10 @@ def test_config0_forward(cuda):
     assert e1 < FWD_TOL and e2 < FWD_TOL
 
 
+@pytest.mark.parametrize("kind", ["mixed", "every", "ellipsoid"])
 @pytest.mark.parametrize("schedule", SCHEDULES)
-def test_culling_is_invisible(cuda, schedule):
-    sc, rays = small_workload("mixed", n_strokes=64, n_rays=256, n_samples=64, seed=11)
+def test_culling_is_invisible(cuda, schedule, kind):
+    sc, rays = small_workload(kind, n_strokes=64, n_rays=256, n_samples=64, seed=11)
     (a, acc_a, _), _ = run_field(sc, rays, cuda, opts=FieldOptions(cull_alpha=1e-9, schedule=schedule))
     (b, acc_b, _), _ = run_field(sc, rays, cuda, opts=FieldOptions(cull_alpha=0.0, schedule=schedule))
     assert rel(a, b) < 1e-6 and rel(acc_a, acc_b) < 1e-6
