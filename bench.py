@@ -11,8 +11,15 @@ Default workload: 16 uneven scenes (strokes log-uniform in [50, 2000], rays
 log-uniform in [4096, 65536], 64 samples each, six primitive types mixed) in one
 batched launch per pass + CUDA graph. Other workloads: --config 0..4.
 
+Second workload (--workload grid): the proposal network's multi-resolution hash-grid
+encoder (10 levels x 4 channels, 2^21 rows per fine level, 240 MB of float32 table)
+over 65,536 rays x 64 samples; one step = zero the table gradient, forward, table
+backward; value in (point, level) lookups per second; the reference's own kernels,
+built from its sources, are timed beside it when present.
+
 Usage:
   python bench.py [--gpus N] [--steps K] [--warmup W] [--config C] [--impl reference]
+  python bench.py --workload grid [--steps K] [--warmup W] [--impl reference]
 Multi-GPU (torchrun): every rank runs the same workload on its own GPU (replicas, no
 data-path collective); the value is the sum over ranks of evals divided by the
 slowest rank's time.
@@ -364,12 +371,245 @@ def loss_curves(args):
             json.dump(line, f)
 
 
+GRID_METRIC = ("grid-encoder fwd+bwd (point, level) lookups/s on 1 B200: proposal hash grid "
+               "(10 levels x 4 ch, 2^21 rows/level)")
+GRID_UNIT = "lookups/s"
+
+
+def grid_workload(dev, scale=1.0, seed=0):
+    """The proposal network's grid (models.py:305-333: 10 levels, 4 channels, base 16,
+    finest 8192, 2^21 rows) and 65,536 x scale rays of 64 samples inside the unit
+    cube, points ordered along each ray as the proposal sampler emits them."""
+    from neural3dstrokes_b200 import gridencoder as ge
+    enc = ge.GridEncoder(input_dim=3, num_levels=10, level_dim=4, base_resolution=16, desired_resolution=8192,
+                         log2_hashmap_size=21).to(dev)
+    g = torch.Generator(device=dev).manual_seed(seed)
+    with torch.no_grad():
+        enc.embeddings.uniform_(-1, 1, generator=g)
+    R, N = max(1, int(65536 * scale)), 64
+    o = torch.rand(R, 1, 3, device=dev, generator=g) * 0.5 + 0.25
+    d = torch.nn.functional.normalize(torch.randn(R, 1, 3, device=dev, generator=g), dim=-1)
+    t = torch.linspace(-0.25, 0.25, N, device=dev)[None, :, None]
+    x = (o + d * t).clamp(0, 1).reshape(R * N, 3).contiguous()
+    grad = torch.randn(enc.num_levels, R * N, 4, device=dev, generator=g)
+    return enc, x, grad
+
+
+def grid_reference_module():
+    """The reference's grid encoder extension built from its sources (oracle/_ref/grid),
+    or None."""
+    import glob
+    import importlib.machinery
+    import importlib.util
+    hits = glob.glob(os.path.join(ROOT, "oracle", "_ref", "grid", "_gridencoder*.so"))
+    if not hits:
+        return None
+    loader = importlib.machinery.ExtensionFileLoader("_gridencoder", hits[0])
+    spec = importlib.util.spec_from_file_location("_gridencoder", hits[0], loader=loader)
+    mod = importlib.util.module_from_spec(spec)
+    loader.exec_module(mod)
+    return mod
+
+
+def grid_step_fn(mod, enc, x, grad, out, gemb):
+    import numpy as np
+    B, L, C = x.shape[0], enc.num_levels, 4
+    S, H = float(np.log2(enc.per_level_scale)), enc.base_resolution
+    E, offs = enc.embeddings.data, enc.offsets
+
+    def step():
+        gemb.zero_()
+        mod.grid_encode_forward(x, E, offs, out, B, 3, C, L, S, H, None, 0, False, 0)
+        mod.grid_encode_backward(grad, x, E, offs, gemb, B, 3, C, L, S, H, None, None, 0, False, 0)
+    return step
+
+
+def grid_cpu_baseline(enc, x, grad, budget_s=15.0):
+    """The oracle's forward + table backward (float64, torch on all host threads) on a
+    bounded sample of the points, in lookups/s."""
+    import numpy as np
+    from oracle import gridencoder as og
+    table = enc.embeddings.detach().double().cpu()
+    offs = enc.offsets.cpu()
+    S, H = float(np.log2(enc.per_level_scale)), enc.base_resolution
+    n = 4096
+    xs, gs = x[:n].cpu(), grad[:, :n].cpu()
+    done, t0 = 0, time.perf_counter()
+    while True:
+        og.grid_encode_forward(xs, table, offs, S, H)
+        og.grid_encode_backward(gs, xs, table, offs, S, H)
+        done += n
+        if time.perf_counter() - t0 > budget_s / 3:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": done * enc.num_levels / dt, "unit": GRID_UNIT, "cores": torch.get_num_threads(), "kind": "port",
+            "sample": f"the first {n} points, repeated {done // n}x (oracle float64, torch on the host threads)"}
+
+
+def run_grid(args, world, rank, local):
+    from neural3dstrokes_b200.train import capture
+    dev = torch.device("cuda", local)
+    enc, x, grad = grid_workload(dev, args.scale)
+    B, L, C = x.shape[0], enc.num_levels, 4
+    lookups = B * L
+    out = torch.empty(L, B, C, device=dev)
+    gemb = torch.zeros_like(enc.embeddings.data)
+    if args.impl == "reference":
+        ref = grid_reference_module()
+        if ref is None:
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "reference grid encoder not built "
+                                  "(python oracle/build_ref.py --only grid)"}), flush=True)
+            return
+        step = grid_step_fn(ref, enc, x, grad, out, gemb)
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize(dev)
+        clocks = ClockSampler(local)
+        clocks.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        lo = time.monotonic()
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        clk = clocks.stop(lo, time.monotonic())
+        t = max_over_ranks(e0.elapsed_time(e1) * 1e-3 / args.steps, world, dev)
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "metric": GRID_METRIC, "value": lookups * world / t,
+                              "unit": GRID_UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                              "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+                              "dtype": "f32", "data": "synthetic", "clocks": clk,
+                              "config": {"workload": "proposal grid", "points": B, "levels": L},
+                              "note": "the reference's grid_encode_forward / grid_encode_backward kernels built "
+                                      "from its sources for sm_100a, eager on the default stream"}), flush=True)
+        return
+
+    from neural3dstrokes_b200 import gridencoder as ge
+    step = grid_step_fn(ge, enc, x, grad, out, gemb)
+    step()  # offsets checked once (one host read) before capture
+    graph = capture(step, dev, warmup=1)
+    for _ in range(args.warmup):
+        graph.replay()
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    lo = time.monotonic()
+    e0.record()
+    for _ in range(args.steps):
+        graph.replay()
+    e1.record()
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop(lo, time.monotonic())
+    t_step = max_over_ranks(e0.elapsed_time(e1) * 1e-3 / args.steps, world, dev)
+
+    # per-kernel durations (events on the launching stream) for the roofline
+    import numpy as np
+    S, H = float(np.log2(enc.per_level_scale)), enc.base_resolution
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    tf, tb = [], []
+    for _ in range(5):
+        gemb.zero_()
+        ev[0].record()
+        ge.grid_encode_forward(x, enc.embeddings.data, enc.offsets, out, B, 3, C, L, S, H)
+        ev[1].record()
+        ge.grid_encode_backward(grad, x, enc.embeddings.data, enc.offsets, gemb, B, 3, C, L, S, H)
+        ev[2].record()
+        torch.cuda.synchronize(dev)
+        tf.append(ev[0].elapsed_time(ev[1]) * 1e-3)
+        tb.append(ev[1].elapsed_time(ev[2]) * 1e-3)
+    t_fwd, t_bwd = statistics.mean(tf), statistics.mean(tb)
+    table_bytes = enc.embeddings.numel() * 4
+    # algorithmic bytes: points (12 B) and output rows (16 B per level) once, the
+    # table once (forward); points, upstream rows and a read + write of the gradient
+    # table (backward)
+    fwd_bytes = B * 12 + L * B * C * 4 + table_bytes
+    bwd_bytes = B * 12 + L * B * C * 4 + 2 * table_bytes
+    peak, src = hbm_peak()
+    roofline = {"bound": "hbm", "kernel": "grid_bwd_kernel (table scatter)", "achieved": bwd_bytes / t_bwd / 1e9,
+                "peak": peak, "unit": "GB/s", "frac": bwd_bytes / t_bwd / 1e9 / peak, "traffic": None,
+                "peak_source": src, "bytes_per_launch": bwd_bytes, "launch_ms": t_bwd * 1e3,
+                "forward_kernel": {"name": "grid_fwd_kernel", "achieved": fwd_bytes / t_fwd / 1e9,
+                                   "launch_ms": t_fwd * 1e3, "frac": fwd_bytes / t_fwd / 1e9 / peak}}
+
+    # plain op: the reference's kernels on the same GPU, eager (they launch on the
+    # legacy default stream, which a graph cannot capture)
+    plain = None
+    ref = grid_reference_module()
+    if ref is not None:
+        rstep = grid_step_fn(ref, enc, x, grad, out, gemb)
+        for _ in range(2):
+            rstep()
+        torch.cuda.synchronize(dev)
+        e0.record()
+        for _ in range(args.steps):
+            rstep()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        tr = e0.elapsed_time(e1) * 1e-3 / args.steps
+        plain = {"value": lookups / tr, "unit": GRID_UNIT, "ms_per_step": tr * 1e3,
+                 "speedup": tr / t_step, "what": "the reference's CUDA kernels built from its sources, eager"}
+
+    # end to end: points uploaded from pinned host memory, the step, the table
+    # gradient read back, every step
+    e2e = None
+    if not args.no_e2e:
+        hx = x.cpu().pin_memory()
+        hg = torch.empty(gemb.shape, dtype=gemb.dtype, pin_memory=True)
+        n = max(3, min(args.steps, 10))
+        torch.cuda.synchronize(dev)
+        e0.record()
+        for _ in range(n):
+            x.copy_(hx, non_blocking=True)
+            graph.replay()
+            hg.copy_(gemb, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        te = max_over_ranks(e0.elapsed_time(e1) * 1e-3 / n, world, dev)
+        e2e = {"value": lookups * world / te, "unit": GRID_UNIT, "ms_per_step": te * 1e3,
+               "h2d_bytes_per_step": hx.numel() * 4, "d2h_bytes_per_step": hg.numel() * 4}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = grid_cpu_baseline(enc, x, grad, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps({
+            "metric": GRID_METRIC, "value": lookups * world / t_step, "unit": GRID_UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded rays in the unit cube)",
+            "config": {"workload": "proposal grid, 65,536 rays x 64 samples" if args.scale == 1.0 else
+                       f"proposal grid, {B // 64} rays x 64 samples", "points": B, "levels": L, "channels": C,
+                       "table_mb": table_bytes / 1e6, "l2": "inputs larger than L2 (outputs %.0f MB, table %.0f MB)"
+                       % (L * B * C * 4 / 1e6, table_bytes / 1e6),
+                       "graph": "zero + forward + backward captured in one CUDA graph"},
+            "roofline": roofline, "plain_op": plain, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+            "gpu_launches": 3 * args.steps, "gpu_launches_per_step": 3}), flush=True)
+
+
+def hbm_peak():
+    """Measured HBM copy bandwidth (GB/s) from MEASURED_PEAKS.json, else the fallback."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            pk = json.load(f)
+        for k in ("hbm_gbs", "hbm_GBs", "hbm"):
+            if k in pk:
+                return float(pk[k]), "measured (MEASURED_PEAKS.json hbm copy)"
+    except (OSError, ValueError):
+        pass
+    return 6650.0, "fallback 6.65 TB/s"
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--config", type=int, default=3)
+    ap.add_argument("--workload", default="field", choices=["field", "grid"],
+                    help="field: the stroke field (default); grid: the proposal hash-grid encoder")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--scale", type=float, default=1.0, help="ray-count scale (profiling small cases)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -385,6 +625,11 @@ def main():
     ap.add_argument("--curve-out", default="", help="write the loss curves as JSON to this file")
     args = ap.parse_args()
     world, rank, local = dist_setup(args.gpus)
+    if args.workload == "grid":
+        run_grid(args, world, rank, local)
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
     if args.loss_curve:
         if rank == 0:
             loss_curves(args)

@@ -392,6 +392,38 @@ int n3ds_adam_step(float* param, const float* grad, float* exp_avg, float* exp_a
                    const float* lo, const float* hi, int64_t n, float lr, float beta1, float beta2,
                    float eps, const int32_t* step, n3ds_stream_t stream);
 
+/* Multi-resolution grid encoder (source/gridencoder/src/gridencoder.h:7-14, the
+ * `_gridencoder` module's grid_encode_forward / grid_encode_backward /
+ * grad_total_variation). All pointers are device pointers; embeddings, outputs,
+ * dy_dx, grad, grad_embeddings and grad_inputs have the element type `dtype`,
+ * inputs are float (the total variation's inputs have `dtype` too, as in the
+ * reference). Shapes: inputs [B, D] in [0, 1] (points outside give zeros and no
+ * gradient); embeddings [offsets[L], C]; offsets [L + 1] int32; outputs [L, B, C];
+ * dy_dx [B, L * D * C] or NULL; grad [L, B, C]. S = log2(per-level scale), H = base
+ * resolution. D in {2, 3, 4, 5}, C in {1, 2, 4, 8}. grad_embeddings (and the total
+ * variation's grad) are accumulated into (zero them first); grad_inputs is written
+ * when both it and dy_dx are given. */
+#define N3DS_DTYPE_F32 0
+#define N3DS_DTYPE_F16 1
+#define N3DS_DTYPE_F64 2
+#define N3DS_GRID_HASH 0
+#define N3DS_GRID_TILED 1
+#define N3DS_INTERP_LINEAR 0
+#define N3DS_INTERP_SMOOTHSTEP 1
+int n3ds_grid_encode_forward(const float* inputs, const void* embeddings, const int32_t* offsets, void* outputs,
+                             uint32_t B, uint32_t D, uint32_t C, uint32_t L, float S, uint32_t H, void* dy_dx,
+                             uint32_t gridtype, int32_t align_corners, uint32_t interpolation, int32_t dtype,
+                             n3ds_stream_t stream);
+int n3ds_grid_encode_backward(const void* grad, const float* inputs, const void* embeddings, const int32_t* offsets,
+                              void* grad_embeddings, uint32_t B, uint32_t D, uint32_t C, uint32_t L, float S,
+                              uint32_t H, const void* dy_dx, void* grad_inputs, uint32_t gridtype,
+                              int32_t align_corners, uint32_t interpolation, int32_t dtype, n3ds_stream_t stream);
+/* grad += the total-variation gradient at the cells of B points (random points when
+ * the caller draws them), source/gridencoder/src/gridencoder.cu:453-559. */
+int n3ds_grid_total_variation(const void* inputs, const void* embeddings, void* grad, const int32_t* offsets,
+                              float weight, uint32_t B, uint32_t D, uint32_t C, uint32_t L, float S, uint32_t H,
+                              uint32_t gridtype, int32_t align_corners, int32_t dtype, n3ds_stream_t stream);
+
 /* FP32 FMA throughput probe (no counterpart in the reference; a measurement aid for
  * the roofline of these FP32-bound kernels): one launch of `blocks` x 256 threads,
  * each doing iters x 16 fused multiply-adds, i.e. blocks*256*iters*32 flops.

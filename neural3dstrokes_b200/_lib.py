@@ -100,6 +100,12 @@ _SIGS = {
     "n3ds_compose_mode_forward": (ctypes.c_int, [ctypes.c_int, _P, _P, _P, _P, _P, c_i64, c_i64, c_i64, _P]),
     "n3ds_compose_mode_backward": (ctypes.c_int, [ctypes.c_int, _P, _P, _P, _P, _P, _P, _P, _P, c_i64, c_i64,
                                                   c_i64, _P]),
+    "n3ds_grid_encode_forward": (ctypes.c_int, [_P, _P, _P, _P, c_u32, c_u32, c_u32, c_u32, ctypes.c_float, c_u32,
+                                                _P, c_u32, c_i32, c_u32, c_i32, _P]),
+    "n3ds_grid_encode_backward": (ctypes.c_int, [_P, _P, _P, _P, _P, c_u32, c_u32, c_u32, c_u32, ctypes.c_float,
+                                                 c_u32, _P, _P, c_u32, c_i32, c_u32, c_i32, _P]),
+    "n3ds_grid_total_variation": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_float, c_u32, c_u32, c_u32, c_u32,
+                                                 ctypes.c_float, c_u32, c_u32, c_i32, c_i32, _P]),
     "n3ds_stroke_forward_static": (ctypes.c_int, [_P, _P, _P, _P, c_i64, _P, _P, _P, _P, _P, c_i64, c_i64, c_i64,
                                                   c_i64, c_i64, c_u32, c_u32, ctypes.c_float, ctypes.c_int,
                                                   ctypes.c_int, _P]),

@@ -1,4 +1,5 @@
-"""Build the reference strokelib CUDA extension, unmodified, into oracle/_ref/.
+"""Build the reference strokelib and gridencoder CUDA extensions, unmodified, into
+oracle/_ref/.
 
 TEST INFRASTRUCTURE ONLY. The product never imports or links anything under
 ``oracle/``; only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU
@@ -13,7 +14,12 @@ as backend.py:34-44 does. Objects and the resulting ``_strokelib*.so`` go to
 ``oracle/_ref/`` only. The .so is git-ignored but travels to the GPU box, where the
 GPU parity tests load it as the reference op.
 
-Usage: python oracle/build_ref.py [--ref /root/reference] [--jobs 3]
+The grid encoder (source/gridencoder/src/gridencoder.cu, bindings.cpp) is built
+the same way, as backend.py:33-39 of that package does, into ``oracle/_ref/grid/``
+as ``_gridencoder*.so``; its flags ask for C++14, which torch's headers no longer
+accept, so it is compiled as C++17 like the strokelib.
+
+Usage: python oracle/build_ref.py [--ref /root/reference] [--jobs 3] [--only strokes|grid]
 """
 import argparse
 import glob
@@ -25,10 +31,40 @@ OUT = os.path.join(HERE, "_ref")
 SOURCES = ["strokes_forward.cu", "strokes_backward.cu", "compositing.cu", "bindings.cpp"]
 
 
+GRID_OUT = os.path.join(OUT, "grid")
+GRID_SOURCES = ["gridencoder.cu", "bindings.cpp"]
+NVCC_FLAGS = ["-O3", "-std=c++17", "-U__CUDA_NO_HALF_OPERATORS__",
+              "-U__CUDA_NO_HALF_CONVERSIONS__", "-U__CUDA_NO_HALF2_OPERATORS__"]
+
+
 def built_path():
-    """Return the path of the built reference extension, or None."""
+    """Return the path of the built reference strokelib extension, or None."""
     hits = sorted(glob.glob(os.path.join(OUT, "_strokelib*.so")))
     return hits[0] if hits else None
+
+
+def grid_built_path():
+    """Return the path of the built reference gridencoder extension, or None."""
+    hits = sorted(glob.glob(os.path.join(GRID_OUT, "_gridencoder*.so")))
+    return hits[0] if hits else None
+
+
+def build_grid(ref_root="/root/reference", jobs=3, verbose=True):
+    src_dir = os.path.join(ref_root, "source", "gridencoder", "src")
+    if not os.path.isdir(src_dir):
+        raise FileNotFoundError(f"reference gridencoder sources not found at {src_dir}")
+    os.makedirs(GRID_OUT, exist_ok=True)
+    os.environ["TORCH_CUDA_ARCH_LIST"] = "10.0a"
+    os.environ.setdefault("MAX_JOBS", str(jobs))
+    from torch.utils.cpp_extension import load
+
+    load(name="_gridencoder",
+         sources=[os.path.join(src_dir, f) for f in GRID_SOURCES],
+         extra_cflags=["-O3", "-std=c++17"],
+         extra_cuda_cflags=NVCC_FLAGS,
+         build_directory=GRID_OUT,
+         verbose=verbose)
+    return grid_built_path()
 
 
 def build(ref_root="/root/reference", jobs=3, verbose=True):
@@ -40,12 +76,10 @@ def build(ref_root="/root/reference", jobs=3, verbose=True):
     os.environ.setdefault("MAX_JOBS", str(jobs))
     from torch.utils.cpp_extension import load
 
-    nvcc_flags = ["-O3", "-std=c++17", "-U__CUDA_NO_HALF_OPERATORS__",
-                  "-U__CUDA_NO_HALF_CONVERSIONS__", "-U__CUDA_NO_HALF2_OPERATORS__"]
     load(name="_strokelib",
          sources=[os.path.join(src_dir, f) for f in SOURCES],
          extra_cflags=["-O3", "-std=c++17"],
-         extra_cuda_cflags=nvcc_flags,
+         extra_cuda_cflags=NVCC_FLAGS,
          extra_include_paths=[src_dir],
          build_directory=OUT,
          verbose=verbose)
@@ -56,7 +90,15 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--jobs", type=int, default=3)
+    ap.add_argument("--only", choices=["strokes", "grid"], default=None)
     a = ap.parse_args()
-    p = build(a.ref, a.jobs)
-    print("built:", p)
-    sys.exit(0 if p else 1)
+    ok = True
+    if a.only in (None, "strokes"):
+        p = build(a.ref, a.jobs)
+        print("built:", p)
+        ok = ok and p is not None
+    if a.only in (None, "grid"):
+        p = build_grid(a.ref, a.jobs)
+        print("built:", p)
+        ok = ok and p is not None
+    sys.exit(0 if ok else 1)

@@ -24,8 +24,20 @@ Three sources, each a seeded, small input set:
             oracle/build_ref.py): runs the reference CUDA operators stroke_forward,
             stroke_backward, compose_forward, compose_backward on seeded inputs for
             every implemented primitive. -> strokelib_golden.npz
+--gridlayout (CPU, needs the reference checkout): imports the reference
+            source/gridencoder/grid.py with a stub ``_gridencoder`` module and records
+            the parameter layout (offsets, grid_sizes, per-level idx counts, n_params,
+            output_dim, per_level_scale) that GridEncoder.__init__ builds for the
+            proposal / error networks' settings (models.py:305-333, 505-509) and
+            other shapes. -> grid_layouts.json
+--grid      (GPU, needs oracle/_ref/grid built by oracle/build_ref.py): runs the
+            reference grid_encode_forward (with dy_dx), grid_encode_backward and
+            grad_total_variation kernels on seeded small tables, hash and tiled,
+            linear and smoothstep, both corner alignments, D 2 and 3, C 1 to 8, in
+            float32, float64 and float16. -> grid_golden.npz
 
 Usage: python tests/golden/make_golden.py [--layouts] [--render] [--compose] [--stepfun] [--strokelib]
+       [--gridlayout] [--grid]
        [--ref /root/reference] [--out tests/golden]
 """
 import argparse
@@ -289,6 +301,109 @@ def make_strokelib(out):
     print("strokelib golden written:", len(arrays), "arrays")
 
 
+# (name, GridEncoder kwargs): the proposal and error networks' grids and other shapes
+GRID_LAYOUTS = [
+    ("proposal", dict(input_dim=3, num_levels=10, level_dim=4, base_resolution=16, desired_resolution=8192,
+                      log2_hashmap_size=21, gridtype="hash", align_corners=False)),
+    ("error", dict(input_dim=3, num_levels=10, level_dim=2, base_resolution=16, desired_resolution=8192,
+                   log2_hashmap_size=20, gridtype="hash", align_corners=False)),
+    ("default", dict()),
+    ("fractional_scale", dict(input_dim=3, num_levels=12, level_dim=2, base_resolution=16,
+                              desired_resolution=2048, log2_hashmap_size=17)),
+    ("tiled_2d_aligned", dict(input_dim=2, num_levels=6, level_dim=8, per_level_scale=1.5, base_resolution=8,
+                              log2_hashmap_size=14, gridtype="tiled", align_corners=True)),
+    ("smooth_4d", dict(input_dim=4, num_levels=5, level_dim=1, base_resolution=4, log2_hashmap_size=12,
+                       interpolation="smoothstep")),
+]
+
+
+def _load_ref_grid(ref_root):
+    sys.modules["_gridencoder"] = types.ModuleType("_gridencoder")  # stub backend: never called
+    path = os.path.join(ref_root, "source", "gridencoder", "grid.py")
+    spec = importlib.util.spec_from_file_location("ref_grid", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def make_grid_layouts(ref_root, out):
+    mod = _load_ref_grid(ref_root)
+    res = {}
+    for name, kw in GRID_LAYOUTS:
+        enc = mod.GridEncoder(**kw)
+        res[name] = dict(kwargs=kw, offsets=enc.offsets.tolist(), grid_sizes=enc.grid_sizes.tolist(),
+                         idx_counts=torch.bincount(enc.idx, minlength=enc.num_levels).tolist(),
+                         n_params=int(enc.n_params), output_dim=int(enc.output_dim),
+                         per_level_scale=float(enc.per_level_scale), embeddings_shape=list(enc.embeddings.shape),
+                         repr=repr(enc))
+    with open(os.path.join(out, "grid_layouts.json"), "w") as f:
+        json.dump(res, f, indent=1)
+    print("grid layouts written:", list(res))
+
+
+# (tag, D, C, L, S, H, log2 rows per level, gridtype, align_corners, interp, dtype)
+GRID_CASES = [
+    ("h3c4", 3, 4, 5, 1.0, 4, 10, 0, False, 0, "float32"),
+    ("h3c2_smooth", 3, 2, 4, 0.6, 5, 9, 0, False, 1, "float32"),
+    ("t3c1_align", 3, 1, 4, 0.5, 3, 11, 1, True, 0, "float32"),
+    ("h2c8", 2, 8, 6, 0.75, 4, 8, 0, False, 0, "float32"),
+    ("t2c4_smooth_align", 2, 4, 3, 1.0, 6, 12, 1, True, 1, "float32"),
+    ("h3c4_f64", 3, 4, 4, 0.8, 4, 10, 0, False, 0, "float64"),
+    ("h3c4_f16", 3, 4, 4, 1.0, 4, 10, 0, False, 0, "float16"),
+]
+
+
+def grid_case_inputs(D, C, L, S, H, log2_rows, align, dtype, seed, B=96):
+    """Seeded inputs of one case: points mostly in [0, 1] with a few outside, a table
+    whose levels hold min(2^log2_rows, dense size) rows (rounded up to 8), grads."""
+    g = torch.Generator().manual_seed(seed)
+    offsets = [0]
+    for lv in range(L):
+        scale = 2.0 ** (lv * S) * H - 1
+        res = int(np.ceil(scale)) + 1
+        dense = (res if align else res + 1) ** D
+        offsets.append(offsets[-1] + int(np.ceil(min(2 ** log2_rows, dense) / 8) * 8))
+    x = torch.rand(B, D, generator=g)
+    x[:4] = x[:4] * 1.4 - 0.2          # some points outside [0, 1]
+    x[4] = 1.0                         # the upper boundary
+    x[5] = 0.0
+    emb = (torch.rand(offsets[-1], C, generator=g) * 2 - 1).to(getattr(torch, dtype))
+    grad = torch.randn(L, B, C, generator=g).to(getattr(torch, dtype))
+    return x, emb, torch.tensor(offsets, dtype=torch.int32), grad
+
+
+def make_grid(out):
+    hits = glob.glob(os.path.join(ROOT, "oracle", "_ref", "grid", "_gridencoder*.so"))
+    if not hits:
+        raise SystemExit("oracle/_ref/grid/_gridencoder*.so missing: run python oracle/build_ref.py --only grid")
+    loader = importlib.machinery.ExtensionFileLoader("_gridencoder", hits[0])
+    spec = importlib.util.spec_from_file_location("_gridencoder", hits[0], loader=loader)
+    ref = importlib.util.module_from_spec(spec)
+    loader.exec_module(ref)
+    dev = torch.device("cuda:0")
+    arrays = {}
+    for i, (tag, D, C, L, S, H, lr, gt, al, it, dt) in enumerate(GRID_CASES):
+        x, emb, offs, grad = grid_case_inputs(D, C, L, S, H, lr, al, dt, 1000 + i)
+        B = x.shape[0]
+        xd, ed, od = x.to(dev), emb.to(dev), offs.to(dev)
+        outp = torch.empty(L, B, C, device=dev, dtype=emb.dtype)
+        dydx = torch.empty(B, L * D * C, device=dev, dtype=emb.dtype)
+        ref.grid_encode_forward(xd, ed, od, outp, B, D, C, L, S, H, dydx, gt, al, it)
+        gemb = torch.zeros_like(ed)
+        gin = torch.zeros(B, D, device=dev, dtype=emb.dtype)
+        ref.grid_encode_backward(grad.to(dev), xd, ed, od, gemb, B, D, C, L, S, H, dydx, gin, gt, al, it)
+        tv = torch.zeros_like(ed)
+        if dt != "float16":  # the reference's TV reads inputs as the table type
+            ref.grad_total_variation(xd.to(emb.dtype), ed, tv, od, 1e-3, B, D, C, L, S, H, gt, al)
+        torch.cuda.synchronize()
+        for k, v in dict(inputs=x, embeddings=emb, offsets=offs, grad=grad, outputs=outp, dy_dx=dydx,
+                         grad_embeddings=gemb, grad_inputs=gin, tv=tv).items():
+            arrays[f"{tag}/{k}"] = v.detach().cpu().numpy()
+        arrays[f"{tag}/meta"] = np.array([D, C, L, S, H, gt, int(al), it], dtype=np.float64)
+    np.savez_compressed(os.path.join(out, "grid_golden.npz"), **arrays)
+    print("grid golden written:", len(arrays), "arrays")
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--layouts", action="store_true")
@@ -296,6 +411,8 @@ if __name__ == "__main__":
     ap.add_argument("--strokelib", action="store_true")
     ap.add_argument("--compose", action="store_true")
     ap.add_argument("--stepfun", action="store_true")
+    ap.add_argument("--gridlayout", action="store_true")
+    ap.add_argument("--grid", action="store_true")
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--out", default=HERE)
     a = ap.parse_args()
@@ -310,3 +427,7 @@ if __name__ == "__main__":
         make_compose_modes(a.ref, a.out)
     if a.stepfun:
         make_stepfun(a.ref, a.out)
+    if a.gridlayout:
+        make_grid_layouts(a.ref, a.out)
+    if a.grid:
+        make_grid(a.out)
