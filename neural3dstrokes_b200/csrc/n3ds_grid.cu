@@ -132,6 +132,74 @@ __device__ __forceinline__ void load_row(const T* __restrict__ row, bool vec, ty
   for (int k = 0; k < C; k++) v[k] = to_acc<T>(row[k]);
 }
 
+// Bytes of an aligned pair of rows (2k, 2k + 1) when one vector load can fetch it
+// (float C = 1, 2, 4: 8, 16, 32 B; half C = 2, 4: 8, 16 B), else 0.
+template <typename T, int C>
+__host__ __device__ constexpr int pair_bytes() {
+  return (std::is_same<T, float>::value && C <= 4) || (std::is_same<T, __half>::value && (C == 2 || C == 4))
+             ? 2 * C * (int)sizeof(T)
+             : 0;
+}
+
+// Rows r0 and r1 of a level. When both lie in one aligned pair (r0 >> 1 == r1 >> 1:
+// the x-neighbours of a cell with even x under the coherent hash, or of an even
+// row in a dense level) one load of the pair serves both, one L1 lookup instead of
+// two; the 32-byte case uses the sm_100 256-bit load.
+template <typename T, int C>
+__device__ __forceinline__ void load_rows2(const T* __restrict__ tab, uint32_t r0, uint32_t r1, bool vec, bool vec_pair,
+                                           typename Acc<T>::type (&v0)[C], typename Acc<T>::type (&v1)[C]) {
+  constexpr int P = pair_bytes<T, C>();
+  if constexpr (P > 0) {
+    // vec_pair: the table is aligned to the pair, the level starts on an even row and
+    // row r0 | 1 exists (offsets from the C ABI may be odd)
+    if (vec_pair && (r0 >> 1) == (r1 >> 1)) {
+      const T* base = tab + (size_t)(r0 & ~1u) * C;
+      float lo[C], hi[C];
+      if constexpr (P == 32) {
+        float a[8];
+        asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+            : "=f"(a[0]), "=f"(a[1]), "=f"(a[2]), "=f"(a[3]), "=f"(a[4]), "=f"(a[5]), "=f"(a[6]), "=f"(a[7])
+            : "l"(base));
+#pragma unroll
+        for (int k = 0; k < 4; k++) { lo[k] = a[k]; hi[k] = a[4 + k]; }
+      } else if constexpr (std::is_same<T, float>::value) {
+        if constexpr (P == 16) {
+          const float4 a = __ldg(reinterpret_cast<const float4*>(base));
+          lo[0] = a.x; lo[1] = a.y; hi[0] = a.z; hi[1] = a.w;
+        } else {
+          const float2 a = __ldg(reinterpret_cast<const float2*>(base));
+          lo[0] = a.x; hi[0] = a.y;
+        }
+      } else {  // half, 8 or 16 bytes
+        uint32_t w[4];
+        if constexpr (P == 16) {
+          const uint4 a = __ldg(reinterpret_cast<const uint4*>(base));
+          w[0] = a.x; w[1] = a.y; w[2] = a.z; w[3] = a.w;
+        } else {
+          const uint2 a = __ldg(reinterpret_cast<const uint2*>(base));
+          w[0] = a.x; w[1] = a.y;
+        }
+        float f[2 * C];
+#pragma unroll
+        for (int k = 0; k < C; k++) {
+          const float2 h = __half22float2(*reinterpret_cast<const __half2*>(&w[k]));
+          f[2 * k] = h.x; f[2 * k + 1] = h.y;
+        }
+#pragma unroll
+        for (int k = 0; k < C; k++) { lo[k] = f[k]; hi[k] = f[C + k]; }
+      }
+#pragma unroll
+      for (int k = 0; k < C; k++) {
+        v0[k] = (r0 & 1u) ? hi[k] : lo[k];
+        v1[k] = (r1 & 1u) ? hi[k] : lo[k];
+      }
+      return;
+    }
+  }
+  load_row<T, C>(tab + (size_t)r0 * C, vec, v0);
+  load_row<T, C>(tab + (size_t)r1 * C, vec, v1);
+}
+
 template <typename T, int C>
 __device__ __forceinline__ void store_row(T* __restrict__ row, bool vec, const typename Acc<T>::type (&v)[C]) {
   if constexpr (std::is_same<T, float>::value && (C == 2 || C == 4 || C == 8)) {
@@ -229,7 +297,8 @@ __global__ void __launch_bounds__(kThreads) grid_fwd_kernel(const float* __restr
                                                              const int32_t* __restrict__ offsets,
                                                              T* __restrict__ outputs, T* __restrict__ dy_dx,
                                                              uint32_t B, uint32_t L, float S, uint32_t H, bool hash,
-                                                             bool align, bool smooth, bool vec_in, bool vec_out) {
+                                                             bool align, bool smooth, bool vec_in, bool vec_pair,
+                                                             bool vec_out) {
   using A = typename Acc<T>::type;
   const uint32_t b = blockIdx.x * kThreads + threadIdx.x;
   if (b >= B) return;
@@ -256,20 +325,26 @@ __global__ void __launch_bounds__(kThreads) grid_fwd_kernel(const float* __restr
   float frac[D], deriv[D];
   locate<D>(x, lv, align, smooth, cell, frac, deriv);
 
+  const bool pair_level = vec_pair && !(lv.base & 1u);
   // corner rows kept in registers for the dy/dx differences when they fit
   constexpr bool kKeep = DYDX && (1 << D) * C <= 32;
   A rows[kKeep ? (1 << D) : 1][C];
+  // corners 2j and 2j + 1 are x-neighbours: fetched together, summed in corner order
 #pragma unroll
-  for (int corner = 0; corner < (1 << D); corner++) {
-    uint32_t cc[D];
-    const float w = corner_of<D>(corner, cell, frac, cc);
-    A v[C];
-    load_row<T, C>(tab + (size_t)cell_row<D>(cc, lv, hash, align) * C, vec_in, v);
+  for (int j = 0; j < (1 << (D - 1)); j++) {
+    uint32_t c0[D], c1[D];
+    const float w0 = corner_of<D>(2 * j, cell, frac, c0);
+    const float w1 = corner_of<D>(2 * j + 1, cell, frac, c1);
+    A v0[C], v1[C];
+    const uint32_t r0 = cell_row<D>(c0, lv, hash, align), r1 = cell_row<D>(c1, lv, hash, align);
+    load_rows2<T, C>(tab, r0, r1, vec_in, pair_level && (r0 | 1u) < lv.hsize, v0, v1);
 #pragma unroll
-    for (int k = 0; k < C; k++) res[k] += (A)w * v[k];
+    for (int k = 0; k < C; k++) res[k] += (A)w0 * v0[k];
+#pragma unroll
+    for (int k = 0; k < C; k++) res[k] += (A)w1 * v1[k];
     if constexpr (kKeep) {
 #pragma unroll
-      for (int k = 0; k < C; k++) rows[corner][k] = v[k];
+      for (int k = 0; k < C; k++) { rows[2 * j][k] = v0[k]; rows[2 * j + 1][k] = v1[k]; }
     }
   }
   store_row<T, C>(out, vec_out, res);
@@ -314,34 +389,81 @@ __global__ void __launch_bounds__(kThreads) grid_fwd_kernel(const float* __restr
 }
 
 // gridencoder.cu:247-335: grad_table[corner rows] += w * grad[level, b, :].
+// Samples along a ray sit next to each other in the batch, and at coarse levels runs
+// of them share a cell, hence all 2^D corner rows: the reference's atomics then pile
+// onto a few thousand rows (level 0 of the proposal grid has 4,920). Each warp finds
+// its runs of equal cells (a ballot of run heads), sums a run's contributions per
+// corner with a segmented shuffle scan of ceil(log2(longest run)) steps, and the
+// run's last lane issues the atomic. A warp without runs takes the plain path.
 template <typename T, int D, int C>
 __global__ void __launch_bounds__(kThreads) grid_bwd_kernel(const T* __restrict__ grad, const float* __restrict__ inputs,
                                                              const int32_t* __restrict__ offsets, T* grad_table,
                                                              uint32_t B, float S, uint32_t H, bool hash, bool align,
                                                              bool smooth, bool vec_grad, bool vec_table) {
   using A = typename Acc<T>::type;
+  constexpr unsigned kFull = 0xffffffffu;
   const uint32_t b = blockIdx.x * kThreads + threadIdx.x;
-  if (b >= B) return;
+  if (__all_sync(kFull, b >= B)) return;  // whole warp past the end (warp-uniform)
   const uint32_t level = blockIdx.y;
+  const int lane = threadIdx.x & 31;
   float x[D];
+  bool valid = b < B;
 #pragma unroll
-  for (int d = 0; d < D; d++) x[d] = __ldg(inputs + (size_t)b * D + d);
-  if (!point_in_range(x, D)) return;
+  for (int d = 0; d < D; d++) x[d] = valid ? __ldg(inputs + (size_t)b * D + d) : 0.f;
+  valid = valid && point_in_range(x, D);
   A g[C];
-  load_row<T, C>(grad + ((size_t)level * B + b) * C, vec_grad, g);
+  if (valid) {
+    load_row<T, C>(grad + ((size_t)level * B + b) * C, vec_grad, g);
+  } else {
+#pragma unroll
+    for (int k = 0; k < C; k++) g[k] = A(0);
+  }
   const Level lv = level_of(offsets, level, S, H);
   T* tab = grad_table + (size_t)lv.base * C;
   uint32_t cell[D];
   float frac[D], deriv[D];
   locate<D>(x, lv, align, smooth, cell, frac, deriv);
+
+  // every lane executes every shuffle (full mask): no shuffle inside a short-circuit
+  const int prev_valid = __shfl_up_sync(kFull, (int)valid, 1);
+  bool head = !valid || lane == 0 || !prev_valid;
+#pragma unroll
+  for (int d = 0; d < D; d++) {
+    const uint32_t prev = __shfl_up_sync(kFull, cell[d], 1);
+    head = head || prev != cell[d];
+  }
+  const unsigned heads = __ballot_sync(kFull, head);
+  if (heads == kFull) {  // no shared cells in this warp
+    if (!valid) return;
+#pragma unroll
+    for (int corner = 0; corner < (1 << D); corner++) {
+      uint32_t cc[D];
+      const float w = corner_of<D>(corner, cell, frac, cc);
+      A v[C];
+#pragma unroll
+      for (int k = 0; k < C; k++) v[k] = (A)w * g[k];
+      scatter_row<T, C>(tab + (size_t)cell_row<D>(cc, lv, hash, align) * C, vec_table, v);
+    }
+    return;
+  }
+  const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
+  const int head_lane = 31 - __clz(heads & (kFull >> (31 - lane)));
+  const unsigned longest = __reduce_max_sync(kFull, tail ? (unsigned)(lane - head_lane + 1) : 0u);
 #pragma unroll
   for (int corner = 0; corner < (1 << D); corner++) {
     uint32_t cc[D];
-    const float w = corner_of<D>(corner, cell, frac, cc);
+    const float w = valid ? corner_of<D>(corner, cell, frac, cc) : 0.f;
     A v[C];
 #pragma unroll
     for (int k = 0; k < C; k++) v[k] = (A)w * g[k];
-    scatter_row<T, C>(tab + (size_t)cell_row<D>(cc, lv, hash, align) * C, vec_table, v);
+    for (unsigned off = 1; off < longest; off <<= 1) {
+#pragma unroll
+      for (int k = 0; k < C; k++) {
+        const A t = __shfl_up_sync(kFull, v[k], off);
+        if (lane - (int)off >= head_lane) v[k] += t;
+      }
+    }
+    if (tail && valid) scatter_row<T, C>(tab + (size_t)cell_row<D>(cc, lv, hash, align) * C, vec_table, v);
   }
 }
 
@@ -419,6 +541,7 @@ __global__ void __launch_bounds__(kThreads) grid_tv_kernel(const T* __restrict__
   scatter_row<T, C>(grad + ((size_t)lv.base + row) * C, vec_table, v);
 }
 
+
 bool aligned(const void* p, size_t bytes) { return ((uintptr_t)p % bytes) == 0; }
 
 template <typename T, int C>
@@ -446,12 +569,15 @@ int fwd_typed(const float* inputs, const void* table, const int32_t* offsets, vo
               const Geo& g, cudaStream_t st) {
   const dim3 grid((g.B + kThreads - 1) / kThreads, g.L);
   const bool vi = vec_ok<T, C>(table), vo = vec_ok<T, C>(outputs) && (!dy_dx || vec_ok<T, C>(dy_dx));
+  const bool vp = pair_bytes<T, C>() > 0 && aligned(table, pair_bytes<T, C>() > 0 ? pair_bytes<T, C>() : 1);
   if (dy_dx)
     grid_fwd_kernel<T, D, C, true><<<grid, kThreads, 0, st>>>(inputs, (const T*)table, offsets, (T*)outputs, (T*)dy_dx,
-                                                               g.B, g.L, g.S, g.H, g.hash, g.align, g.smooth, vi, vo);
+                                                               g.B, g.L, g.S, g.H, g.hash, g.align, g.smooth, vi, vp,
+                                                               vo);
   else
     grid_fwd_kernel<T, D, C, false><<<grid, kThreads, 0, st>>>(inputs, (const T*)table, offsets, (T*)outputs, nullptr,
-                                                                g.B, g.L, g.S, g.H, g.hash, g.align, g.smooth, vi, vo);
+                                                                g.B, g.L, g.S, g.H, g.hash, g.align, g.smooth, vi, vp,
+                                                                vo);
   return launch_error("grid encode forward");
 }
 

@@ -319,3 +319,62 @@ def test_full_size_level_sums(cuda):
     sub = torch.randperm(B, device=cuda, generator=g)[:4096]
     o_out, _ = og.grid_encode_forward(x[sub].cpu(), enc.embeddings.detach().cpu(), enc.offsets.cpu(), S, H)
     assert rel(out[:, sub], o_out) < 1e-5
+
+
+def ray_points(R, N, seed, spread=0.2):
+    """R rays of N samples each, ray-ordered as a sampler emits them: neighbours share
+    cells at the coarse levels."""
+    g = torch.Generator().manual_seed(seed)
+    o = torch.rand(R, 1, 3, generator=g) * 0.6 + 0.2
+    d = torch.nn.functional.normalize(torch.randn(R, 1, 3, generator=g), dim=-1)
+    t = torch.linspace(-spread, spread, N)[None, :, None]
+    return (o + d * t).reshape(R * N, 3).contiguous()
+
+
+def offsets_for(D, L, S, H, log2_rows, align=False):
+    offsets = [0]
+    for lv in range(L):
+        _, res = og.level_constants(lv, S, H)
+        dense = (res if align else res + 1) ** D
+        offsets.append(offsets[-1] + int(np.ceil(min(2 ** log2_rows, dense) / 8) * 8))
+    return torch.tensor(offsets, dtype=torch.int32)
+
+
+@pytest.mark.parametrize("C,dtype", [(1, torch.float32), (2, torch.float32), (4, torch.float32), (8, torch.float32),
+                                     (4, torch.float64), (4, torch.float16)])
+def test_backward_runs_of_shared_cells(cuda, C, dtype):
+    """Ray-ordered points (the warp-run aggregation of the backward), out-of-range points
+    inside runs, a partial last warp (B = 1073)."""
+    x = ray_points(37, 29, seed=C)
+    x[::17] = 1.3
+    S, H, L = 1.0, 4, 6
+    offs = offsets_for(3, L, S, H, 12)
+    g = torch.Generator().manual_seed(40 + C)
+    emb = (torch.rand(int(offs[-1]), C, generator=g, dtype=torch.float64) * 2 - 1).to(dtype)
+    grad = torch.randn(L, x.shape[0], C, generator=g, dtype=torch.float64).to(dtype)
+    out, dydx, gemb, gin, _ = run_ours(x, emb, offs, grad, S, H, 0, False, 0, cuda)
+    o_out, o_dd = og.grid_encode_forward(x, emb, offs, S, H, True)
+    o_ge, o_gi = og.grid_encode_backward(grad, x, emb, offs, S, H, o_dd)
+    ftol, gtol = (4e-3, 2e-2) if dtype == torch.float16 else (1e-5, 1e-5)
+    assert rel(out, o_out) < ftol
+    assert rel(gemb, o_ge) < gtol
+    assert rel(gin, o_gi) < gtol
+
+
+@pytest.mark.parametrize("C,dtype", [(4, torch.float32), (2, torch.float32), (1, torch.float32),
+                                     (2, torch.float16), (4, torch.float16)])
+def test_odd_level_offsets(cuda, C, dtype):
+    """Offsets the C ABI accepts but GridEncoder never builds: odd level starts and
+    odd row counts (the paired row loads must fall back to single rows there)."""
+    offs = torch.tensor([0, 13, 40, 77, 131, 250], dtype=torch.int32)
+    g = torch.Generator().manual_seed(C)
+    x = torch.cat([torch.rand(300, 3, generator=g), ray_points(10, 40, seed=3)])
+    emb = (torch.rand(250, C, generator=g, dtype=torch.float64) * 2 - 1).to(dtype)
+    grad = torch.randn(5, x.shape[0], C, generator=g, dtype=torch.float64).to(dtype)
+    for gt in (0, 1):
+        out, dydx, gemb, gin, tv = run_ours(x, emb, offs, grad, 1.0, 3, gt, False, 0, cuda)
+        o_out, o_dd = og.grid_encode_forward(x, emb, offs, 1.0, 3, True, gt)
+        o_ge, _ = og.grid_encode_backward(grad, x, emb, offs, 1.0, 3, None, gt)
+        ftol, gtol = (4e-3, 2e-2) if dtype == torch.float16 else (1e-5, 1e-5)
+        assert rel(out, o_out) < ftol and rel(dydx, o_dd) < ftol
+        assert rel(gemb, o_ge) < gtol
