@@ -365,16 +365,18 @@ def test_backward_runs_of_shared_cells(cuda, C, dtype):
                                      (2, torch.float16), (4, torch.float16)])
 def test_odd_level_offsets(cuda, C, dtype):
     """Offsets the C ABI accepts but GridEncoder never builds: odd level starts and
-    odd row counts (the paired row loads must fall back to single rows there)."""
-    offs = torch.tensor([0, 13, 40, 77, 131, 250], dtype=torch.int32)
+    odd row counts, on levels large enough (>= 2^19 rows) for the paired row loads,
+    which must fall back to single rows at an odd start or at a level's last row;
+    and small odd levels."""
+    offs = torch.tensor([0, 524289, 1048582, 1572870, 1572883, 1572910], dtype=torch.int32)
     g = torch.Generator().manual_seed(C)
-    x = torch.cat([torch.rand(300, 3, generator=g), ray_points(10, 40, seed=3)])
-    emb = (torch.rand(250, C, generator=g, dtype=torch.float64) * 2 - 1).to(dtype)
+    x = torch.cat([torch.rand(3000, 3, generator=g), ray_points(20, 50, seed=3), torch.ones(4, 3)])
+    emb = (torch.rand(int(offs[-1]), C, generator=g, dtype=torch.float64) * 2 - 1).to(dtype)
     grad = torch.randn(5, x.shape[0], C, generator=g, dtype=torch.float64).to(dtype)
-    for gt in (0, 1):
-        out, dydx, gemb, gin, tv = run_ours(x, emb, offs, grad, 1.0, 3, gt, False, 0, cuda)
-        o_out, o_dd = og.grid_encode_forward(x, emb, offs, 1.0, 3, True, gt)
-        o_ge, _ = og.grid_encode_backward(grad, x, emb, offs, 1.0, 3, None, gt)
+    for gt, S, H in ((0, 1.0, 64), (1, 1.0, 3)):
+        out, dydx, gemb, gin, tv = run_ours(x, emb, offs, grad, S, H, gt, False, 0, cuda)
+        o_out, o_dd = og.grid_encode_forward(x, emb, offs, S, H, True, gt)
+        o_ge, _ = og.grid_encode_backward(grad, x, emb, offs, S, H, None, gt)
         ftol, gtol = (4e-3, 2e-2) if dtype == torch.float16 else (1e-5, 1e-5)
         assert rel(out, o_out) < ftol and rel(dydx, o_dd) < ftol
         assert rel(gemb, o_ge) < gtol
