@@ -136,6 +136,35 @@ __device__ __forceinline__ bool ellipsoid_reachable(const float* rec, const SegC
   return dot(q, q) <= reach * reach;
 }
 
+// Capsule reach test (flagged capsules with h > 0): the SDF is the distance to the
+// axis segment y in [-h, h] minus 1 (strokes_sdf.h:434-440), so alpha reaches the cut
+// only within 1 + tau_local of that segment (R_PLANE = tau_local per unit radius).
+// The local chord's distance to the axis segment (closest points of two segments,
+// clamped to both) must not exceed it, widened by the samples' spread about the chord.
+__device__ __forceinline__ bool capsule_reachable(const float* rec, const SegCtx& c) {
+  const float4 m0 = rec4(rec)[R_M / 4], m1 = rec4(rec)[R_M / 4 + 1], m2 = rec4(rec)[R_M / 4 + 2];
+  const V3 dA = v3(c.A.x - m0.w, c.A.y - m1.w, c.A.z - m2.w);
+  const V3 dB = dA + c.AB;
+  const V3 a = v3(fmaf(m0.x, dA.x, fmaf(m0.y, dA.y, m0.z * dA.z)), fmaf(m1.x, dA.x, fmaf(m1.y, dA.y, m1.z * dA.z)),
+                  fmaf(m2.x, dA.x, fmaf(m2.y, dA.y, m2.z * dA.z)));
+  const V3 b = v3(fmaf(m0.x, dB.x, fmaf(m0.y, dB.y, m0.z * dB.z)), fmaf(m1.x, dB.x, fmaf(m1.y, dB.y, m1.z * dB.z)),
+                  fmaf(m2.x, dB.x, fmaf(m2.y, dB.y, m2.z * dB.z)));
+  const float h = rec[R_BP];
+  const float reach = (1.f + rec[R_PLANE] * c.rmax + c.rho * rec[R_SINV]) * 1.0001f + 1e-5f;
+  // chord a + u d, u in [0, 1]; axis (0, v, 0), v in [-h, h]
+  const V3 d = b - a;
+  const float dd = dot(d, d);
+  // u minimising the distance to the axis line, then v on the clamped axis, then u again
+  float u = 0.f;
+  const float den = dd - d.y * d.y;  // |d|^2 - d_y^2: the chord's part across the axis
+  if (den > 1e-12f * fmaxf(dd, 1e-30f)) u = clampf(-(a.x * d.x + a.z * d.z) / den, 0.f, 1.f);
+  float v = clampf(a.y + u * d.y, -h, h);
+  if (dd > 0.f) u = clampf((d.x * -a.x + d.y * (v - a.y) + d.z * -a.z) / dd, 0.f, 1.f);
+  v = clampf(a.y + u * d.y, -h, h);
+  const V3 q = v3(a.x + u * d.x, a.y + u * d.y - v, a.z + u * d.z);
+  return dot(q, q) <= reach * reach;
+}
+
 // Curve reach test (the forward's batched pass, flagged curves). Every sample where
 // alpha reaches the cut is within r_max + tau of the curve (the SDF uses the distance
 // to one curve point, no less than the true distance), the curve within eps of its
@@ -278,6 +307,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_con
               const float* rec = S.recs + size_t(slot) * REC_FLOATS;
               const int rb = __float_as_int(rec[R_KIND]) & 15;
               const bool reach = rb == B_SPHERE        ? ellipsoid_reachable(rec, c)
+                                 : rb == B_CAPSULE     ? capsule_reachable(rec, c)
                                  : rb <= B_TETRAHEDRON ? polytope_reachable(rec, c)
                                                        : curve_reachable(rec, c, fabsf(S.cull_b[slot]), lane);
               if (!reach) atomicOr(kill + kk, 1u << bit);
@@ -973,10 +1003,17 @@ __global__ void prep_kernel(const PrepLaunch P) {
   // Per-axis-scaled spheres (ellipsoids): alpha reaches the cut only where the local
   // radius |p| <= 1 + tau_local, tau_local = m_cut delta r / (kappa f) with the radius
   // factor f >= s_min under inv_scale_radius (f = 1 without it).
+  // Capsules (h > 0) with one scale: the SDF is the exact distance to the axis segment
+  // minus 1 (Lg = 1), so tau_local = cm / s per unit radius; the capsule fills 1/(h+1)^2
+  // of its bounding sphere's cross-section. (A slab test for boxes culls 12 % of their
+  // candidates and costs more than it saves: the batched pass reads 32 strokes'
+  // records per lane, a bank conflict per record load.)
   const bool ell = base == B_SPHERE && s3 && cull && bound_ok;
+  const bool cap = base == B_CAPSULE && rec[R_BP] > 0.f && !s3 && cull && bound_ok;
   const bool plane = ((base == B_OCTAHEDRON || base == B_TETRAHEDRON) && !s3 && cull && bound_ok) ||
-                     (base >= B_QUAD_BEZIER && cull && bound_ok) || ell;  // curves: the piece test
+                     (base >= B_QUAD_BEZIER && cull && bound_ok) || ell || cap;  // curves: the piece test
   if (plane && (base == B_OCTAHEDRON || base == B_TETRAHEDRON)) rec[R_PLANE] = 1.7320508f * cm * Lg / sc.x;
+  if (cap) rec[R_PLANE] = cm * Lg / sc.x;
   if (ell) {
     const float mc = mode == STEP_HARD ? 0.f : (mode == STEP_LINEAR ? 0.5f : P.cull_m);
     rec[R_PLANE] = fmaxf(mc, 0.f) * delta / kappa / (P.inv_scale_radius ? smin : 1.f);

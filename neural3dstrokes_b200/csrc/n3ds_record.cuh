@@ -77,7 +77,7 @@ constexpr int R_SINV = 24;     // q6: 1/scale per axis
 constexpr int R_BP2 = 28;      // torus tube radius, line radius change
 constexpr int R_TSIN = 29, R_TCOS = 30;  // sin, cos of the torus cap angle
 constexpr int R_PLANE = 31;    // reach test per unit sample radius: tetrahedron / octahedron sqrt(3) tau_local,
-                               // per-axis-scaled sphere tau_local
+                               // per-axis-scaled sphere and capsule tau_local
 // quadratic Bezier
 constexpr int R_QA = 8, R_QKK = 11;    // q2: A, 1/|b|^2
 constexpr int R_Qa = 12, R_QKX = 15;   // q3: a = B - A, kk (a.b)

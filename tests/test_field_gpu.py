@@ -79,7 +79,7 @@ def test_config0_forward(cuda):
     assert e1 < FWD_TOL and e2 < FWD_TOL
 
 
-@pytest.mark.parametrize("kind", ["mixed", "every", "ellipsoid"])
+@pytest.mark.parametrize("kind", ["mixed", "every", "ellipsoid", "capsule", "cube", "roundcube"])
 @pytest.mark.parametrize("schedule", SCHEDULES)
 def test_culling_is_invisible(cuda, schedule, kind):
     sc, rays = small_workload(kind, n_strokes=64, n_rays=256, n_samples=64, seed=11)
