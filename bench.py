@@ -17,14 +17,22 @@ over 65,536 rays x 64 samples; one step = zero the table gradient, forward, tabl
 backward; value in (point, level) lookups per second; the reference's own kernels,
 built from its sources, are timed beside it when present.
 
+Third (--workload ops): every other operator once at a stated size through its
+public API (the drop-in _strokelib operators, the composition modes, a colour field,
+the texture, proposal resampling, stroke insertion, the field at a tenth of config 3
+and its Adam step), timed with CUDA events; it is the command the all-kernels ncu
+summary runs.
+
 Usage:
   python bench.py [--gpus N] [--steps K] [--warmup W] [--config C] [--impl reference]
   python bench.py --workload grid [--steps K] [--warmup W] [--impl reference]
+  python bench.py --workload ops [--steps K] [--warmup W]
 Multi-GPU (torchrun): every rank runs the same workload on its own GPU (replicas, no
 data-path collective); the value is the sum over ranks of evals divided by the
 slowest rank's time.
 """
 import argparse
+import glob
 import json
 import math
 import os
@@ -589,6 +597,136 @@ def run_grid(args, world, rank, local):
             "gpu_launches": 3 * args.steps, "gpu_launches_per_step": 3}), flush=True)
 
 
+def run_ops(args, rank, local):
+    """Each operator at a stated size, events around ``args.steps`` calls after
+    ``args.warmup``; one JSON line with per-op ms and algorithmic GB/s."""
+    from neural3dstrokes_b200 import scenes, stepfun, strokelib, strokes, textures
+    from neural3dstrokes_b200.insertion import StrokeInserter
+    from neural3dstrokes_b200.train import BatchedField, GraphedTrainer
+    dev = torch.device("cuda", local)
+    g = torch.Generator().manual_seed(0)
+    res = []
+
+    def time_of(fn):
+        for _ in range(max(1, args.warmup)):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / args.steps
+
+    jobs = []
+
+    def timed(name, fn, nbytes, ref_fn=None):
+        fn()  # every kernel launches once before the timed (and profiled) window
+        if ref_fn is not None:
+            ref_fn()
+        jobs.append((name, fn, nbytes, ref_fn))
+
+    ref = None
+    hits = sorted(glob.glob(os.path.join(ROOT, "oracle", "_ref", "_strokelib*.so")))
+    if hits:
+        import importlib.machinery
+        import importlib.util
+        loader = importlib.machinery.ExtensionFileLoader("_strokelib", hits[0])
+        ref = importlib.util.module_from_spec(importlib.util.spec_from_file_location("_strokelib", hits[0],
+                                                                                    loader=loader))
+        loader.exec_module(ref)
+
+    # drop-in operators: 256 cubes x 65,536 samples ([P, S] tensors of 67 / 201 MB)
+    P, S = 65536, 256
+    sc = scenes.make_strokes(["cube"] * S, g)
+    rays = scenes.make_rays(P // 64, 64, g)
+    sid = scenes.SDF_ID["cube"]
+    ps = sc.shape_params[:, :7].contiguous().to(dev)
+    col = sc.color_params.to(dev)
+    x = rays.x.reshape(-1, 3).contiguous().to(dev)
+    r = rays.radius.reshape(-1).contiguous().to(dev)
+    vd = rays.dirs.to(dev)
+    a = torch.empty(P, S, device=dev)
+    c = torch.empty(P, S, 3, device=dev)
+    none = torch.empty(0, device=dev)
+    R = (lambda f: f) if ref is not None else (lambda f: None)
+    timed("stroke_forward (cube, 65536 x 256)", lambda: strokelib.stroke_forward(
+        a, c, none, none, x, r, vd, ps, col, sid, 0, 0.02, True, True), P * S * 16,
+        R(lambda: ref.stroke_forward(a, c, none, none, x, r, vd, ps, col, sid, 0, 0.02, True, True)))
+    ga, gc = torch.randn(P, S, device=dev), torch.randn(P, S, 3, device=dev)
+    gps, gcol, gx = torch.zeros_like(ps), torch.zeros_like(col), torch.zeros_like(x)
+    timed("stroke_backward (cube, 65536 x 256)", lambda: strokelib.stroke_backward(
+        gps, gcol, gx, ga, gc, none, x, r, vd, a, ps, col, sid, 0, 0.02, True, True), P * S * 20,
+        R(lambda: ref.stroke_backward(gps, gcol, gx, ga, gc, none, x, r, vd, a, ps, col, sid, 0, 0.02, True, True)))
+    dp = torch.rand(S, device=dev) * 10
+    dens, ccol = torch.empty(P, device=dev), torch.empty(P, 3, device=dev)
+    timed("compose_forward over (65536 x 256)", lambda: strokelib.compose_forward(dens, ccol, a, c, dp), P * S * 16,
+          R(lambda: ref.compose_forward(dens, ccol, a, c, dp)))
+    gda, gdc, gdp = torch.zeros_like(a), torch.zeros_like(c), torch.zeros_like(dp)
+    gd, gcc = torch.randn(P, device=dev), torch.randn(P, 3, device=dev)
+    # the backward reads alphas and colours and accumulates into both gradient tensors
+    timed("compose_backward over (65536 x 256)", lambda: strokelib.compose_backward(
+        gda, gdc, gdp, gd, gcc, a, c, dp), P * S * 48,
+        R(lambda: ref.compose_backward(gda, gdc, gdp, gd, gcc, a, c, dp)))
+    a_req = a.detach().requires_grad_(True)
+
+    def softmax_fb():
+        d_, c_ = strokes.compose_strokes(a_req, c, dp, "softmax_density_weighted")
+        (d_.sum() + c_.sum()).backward()
+    timed("compose softmax_density_weighted fwd+bwd (65536 x 256)", softmax_fb, P * S * 32)
+    # colour field: SH3 on 128 spheres
+    sph = scenes.make_strokes(["sphere"] * 128, g)
+    sh = torch.randn(128, 27, generator=g).to(dev)
+    a2, c2 = torch.empty(P, 128, device=dev), torch.empty(P, 128, 3, device=dev)
+    vdn = torch.nn.functional.normalize(vd, dim=-1)
+    timed("stroke_forward sphere + SH3 colour (65536 x 128)", lambda: strokelib.stroke_forward(
+        a2, c2, none, none, x, r, vdn, sph.shape_params[:, :4].contiguous().to(dev), sh, scenes.SDF_ID["sphere"], 3,
+        0.02, True, True), P * 128 * 16)
+    # texture on the cube pairs
+    tex = textures.ImageTexture(torch.rand(256, 256, 3, generator=g) * 255, (256, 256)).to(dev)
+    tc = torch.rand(P, S, 2, device=dev)
+    c_req = c.detach().requires_grad_(True)
+
+    def tex_fb():
+        co, al = tex(tc, c_req, a)
+        co.sum().backward()
+    timed("ImageTexture fwd+bwd (65536 x 256)", tex_fb, P * S * (40 + 20))
+    # proposal resampling: 65,536 rays, 64 bins -> 32 samples, dilation
+    sd = torch.sort(torch.rand(65536, 65, device=dev), -1).values
+    sd[:, 0], sd[:, -1] = 0, 1
+    wts = torch.rand(65536, 64, device=dev)
+    timed("resample_intervals (65536 rays, 64 -> 32, dilation)", lambda: stepfun.resample_intervals(
+        sd, wts, 32, rand=True, dilation=0.01, resample_padding=0.01), 65536 * (65 + 64 + 33) * 4)
+    # stroke insertion: 2000 strokes, 30,000 error points
+    ins = StrokeInserter("sphere", max_num_strokes=2000, init_num_strokes=10, device=dev)
+    ec, _ = ins.sample_error_coords()
+    err = torch.rand(ec.shape[0], device=dev)
+    step = [100]
+
+    def ins_step():
+        ins.step_update(step[0], 200000, errors=err, error_coords=ec)
+        step[0] += 7
+    timed("insertion step_update (2000 strokes, 30000 error points)", ins_step, 0)
+    # the field at a tenth of config 3, forward + MSE + backward + Adam (eager)
+    w = scenes.config(3, scale=0.1)
+    field = BatchedField(w.scenes, w.rays, device=dev)
+    trainer = GraphedTrainer(field, torch.zeros_like(field.rgb), lr=1e-3)
+    timed("field training step (config 3 at 0.1 of its rays, eager)", trainer._step, 0)
+    torch.cuda.synchronize(dev)
+    torch.cuda.profiler.start()  # the window an ncu --profile-from-start off capture sees
+    for name, fn, nbytes, ref_fn in jobs:
+        ms = time_of(fn)
+        item = {"op": name, "ms": round(ms, 4), "bytes": int(nbytes),
+                "gbs": round(nbytes / ms / 1e6, 1) if nbytes else None}
+        if ref_fn is not None:  # the reference's operator on the same tensors
+            item["reference_ms"] = round(time_of(ref_fn), 4)
+        res.append(item)
+    torch.cuda.profiler.stop()
+    if rank == 0:
+        print(json.dumps({"workload": "ops", "steps": args.steps, "warmup": args.warmup, "ops": res}), flush=True)
+
+
 def hbm_peak():
     """Measured HBM copy bandwidth (GB/s) from MEASURED_PEAKS.json, else the fallback."""
     try:
@@ -608,8 +746,9 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--config", type=int, default=3)
-    ap.add_argument("--workload", default="field", choices=["field", "grid"],
-                    help="field: the stroke field (default); grid: the proposal hash-grid encoder")
+    ap.add_argument("--workload", default="field", choices=["field", "grid", "ops"],
+                    help="field: the stroke field (default); grid: the proposal hash-grid encoder; "
+                         "ops: every other operator once (profiling)")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--scale", type=float, default=1.0, help="ray-count scale (profiling small cases)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -625,6 +764,11 @@ def main():
     ap.add_argument("--curve-out", default="", help="write the loss curves as JSON to this file")
     args = ap.parse_args()
     world, rank, local = dist_setup(args.gpus)
+    if args.workload == "ops":
+        run_ops(args, rank, local)
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
     if args.workload == "grid":
         run_grid(args, world, rank, local)
         if world > 1:

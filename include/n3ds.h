@@ -93,8 +93,8 @@ int n3ds_compose_forward(float* density_out, float* color_out, const float* alph
                          const float* colors, const float* density_params, int64_t n_points,
                          int64_t n_strokes, int64_t color_dim, n3ds_stream_t stream);
 
-/* Workspace bytes of n3ds_compose_backward: P*S floats in exact mode (the
- * transmittance in front of every stroke), 0 in compat mode. */
+/* Workspace bytes of n3ds_compose_backward: P*ceil(S/32) floats in exact mode (the
+ * transmittance in front of every 32-stroke chunk of a row), 0 in compat mode. */
 size_t n3ds_compose_workspace_bytes(int64_t n_points, int64_t n_strokes, int grad_mode);
 
 /* Replaces compose_backward (compositing.cu:206-263; declared compositing.h:25-32).
@@ -280,6 +280,21 @@ int n3ds_texture_backward(float* grad_colors, float* grad_alphas, const float* g
                           const float* grad_alpha_out, const float* texcoords, int64_t n, const float* image,
                           int32_t channels, int32_t height, int32_t width, float tint_ratio,
                           int32_t modulate_alpha, n3ds_stream_t stream);
+/* The same with the texture packed once by n3ds_texture_pack into [height, width]
+ * float4 texels (r, g, b, 0; a grayscale texture replicated), one 16-byte load per
+ * bilinear corner instead of one per corner and channel; packed must be 16-byte
+ * aligned and hold height * width * 4 floats. channels is the original count. Results
+ * equal the planar functions'. */
+int n3ds_texture_pack(float* packed, const float* image, int32_t channels, int32_t height, int32_t width,
+                      n3ds_stream_t stream);
+int n3ds_texture_forward_packed(float* color_out, float* alpha_out, const float* texcoords, const float* colors,
+                                const float* alphas, int64_t n, const float* packed, int32_t channels,
+                                int32_t height, int32_t width, float tint_ratio, int32_t modulate_alpha,
+                                n3ds_stream_t stream);
+int n3ds_texture_backward_packed(float* grad_colors, float* grad_alphas, const float* grad_color_out,
+                                 const float* grad_alpha_out, const float* texcoords, int64_t n,
+                                 const float* packed, int32_t channels, int32_t height, int32_t width,
+                                 float tint_ratio, int32_t modulate_alpha, n3ds_stream_t stream);
 
 /* Proposal resampling of ray intervals (source/utils/stepfun.py; the step that makes
  * the stroke level's fence posts, models.py:147-185). One warp per ray; n_bins <= 2048.

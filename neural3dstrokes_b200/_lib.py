@@ -94,6 +94,11 @@ _SIGS = {
                                             c_i32, _P]),
     "n3ds_texture_backward": (ctypes.c_int, [_P, _P, _P, _P, _P, c_i64, _P, c_i32, c_i32, c_i32, ctypes.c_float,
                                              c_i32, _P]),
+    "n3ds_texture_pack": (ctypes.c_int, [_P, _P, c_i32, c_i32, c_i32, _P]),
+    "n3ds_texture_forward_packed": (ctypes.c_int, [_P, _P, _P, _P, _P, c_i64, _P, c_i32, c_i32, c_i32,
+                                                   ctypes.c_float, c_i32, _P]),
+    "n3ds_texture_backward_packed": (ctypes.c_int, [_P, _P, _P, _P, _P, c_i64, _P, c_i32, c_i32, c_i32,
+                                                    ctypes.c_float, c_i32, _P]),
     "n3ds_field_launch_count": (ctypes.c_int, [ctypes.POINTER(Batch), ctypes.POINTER(Options),
                                                ctypes.POINTER(c_i32), ctypes.POINTER(c_i32)]),
     "n3ds_field_resolve_options": (ctypes.c_int, [ctypes.POINTER(Options), ctypes.POINTER(Options)]),

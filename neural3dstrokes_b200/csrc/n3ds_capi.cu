@@ -837,7 +837,7 @@ int n3ds_compose_forward(float* density_out, float* color_out, const float* alph
 
 size_t n3ds_compose_workspace_bytes(int64_t n_points, int64_t n_strokes, int grad_mode) {
   if (grad_mode == N3DS_GRAD_COMPAT || n_points <= 0 || n_strokes <= 0) return 0;
-  return size_t(n_points) * size_t(n_strokes) * 4;
+  return size_t(n_points) * size_t((n_strokes + 31) / 32) * 4;  // one transmittance per row and 32 strokes
 }
 
 int n3ds_compose_backward(float* grad_alphas, float* grad_colors, float* grad_density_params,
@@ -853,7 +853,7 @@ int n3ds_compose_backward(float* grad_alphas, float* grad_colors, float* grad_de
     return fail(N3DS_ERR_INVALID, "null tensor pointer");
   const int compat = grad_mode == N3DS_GRAD_COMPAT;
   if (!compat && (!workspace || workspace_bytes < n3ds_compose_workspace_bytes(n_points, n_strokes, grad_mode)))
-    return fail(N3DS_ERR_WORKSPACE, "exact compose backward needs P*S*4 bytes of workspace");
+    return fail(N3DS_ERR_WORKSPACE, "exact compose backward needs P*ceil(S/32)*4 bytes of workspace");
   n3ds::UfCompose L{};
   L.alphas = alphas;
   L.colors = colors;

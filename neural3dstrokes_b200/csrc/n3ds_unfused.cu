@@ -9,11 +9,15 @@
 // - stroke backward: lane = stroke; each lane accumulates its stroke's reduced
 //   gradient slots in registers across all samples the warp visits (no per-pair
 //   atomics), grad_x is a warp sum per sample;
-// - compose forward / backward: lane = sample with the serial stroke loop of the
-//   reference (same multiplication order), fed by coalesced tile loads transposed in
-//   shared memory. The exact backward uses a top-down sweep for T_s and a bottom-up
-//   "under" sweep, so it needs no division by (1 - alpha).
+// - compose forward / exact backward: a warp per sample row, lane = stroke within a
+//   32-stroke chunk, transmittance by shuffle product-scans and the composites under
+//   each stroke by a shuffle scan of affine maps (no division by 1 - alpha); rows are
+//   streamed coalesced, nothing is staged in shared memory. The compat backward (the
+//   reference's own formulas, which divide by 1 - alpha) keeps lane = sample with the
+//   reference's serial loop over 32-row tiles transposed in shared memory.
 // All indices are 64-bit.
+#include <algorithm>
+
 #include "n3ds_eval.cuh"
 #include "n3ds_unfused.cuh"
 
@@ -149,8 +153,7 @@ __global__ void __launch_bounds__(UF_WARPS * 32) uf_stroke_bwd_kernel(const UfSt
 
 // ------------------------------------------------------------------ compose
 
-constexpr int UC_WARPS = 4;     // compose forward
-constexpr int UCB_WARPS = 2;    // compose backward (twice the tiles per warp)
+constexpr int UCB_WARPS = 2;    // compat compose backward (twice the tiles per warp)
 
 template <int C, int W>
 struct ComposeTiles {
@@ -185,43 +188,207 @@ __device__ __forceinline__ void load_tile(ComposeTiles<C, W>& t, int warp, int l
   }
 }
 
+// One warp per sample row [S] (compositing.cu:10-59 restated): lanes take 32
+// strokes at a time, top chunk first, lane 0 the topmost stroke of its chunk. The
+// transmittance above each stroke is the chunk's incoming T times an exclusive
+// shuffle product-scan of (1 - a) over the lanes above; every lane keeps partial
+// density / colour sums, reduced over the warp at the end of the row. Loads are
+// coalesced row segments, nothing is staged: the kernel streams alphas and colours
+// once (16 B per pair for C = 3).
+constexpr int UCR_WARPS = 8;  // row kernels: warps per block
+
+__device__ __forceinline__ float excl_prod_up(float v, int lane) {
+  // exclusive product over lanes below (lower index); lane 0 gets 1
+  for (int o = 1; o < 32; o <<= 1) {
+    const float y = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v *= y;
+  }
+  const float e = __shfl_up_sync(0xffffffffu, v, 1);
+  return lane == 0 ? 1.0f : e;
+}
+
 template <int C>
-__global__ void __launch_bounds__(UC_WARPS * 32) uf_compose_fwd_kernel(const UfCompose L) {
-  extern __shared__ __align__(16) unsigned char dsm[];
-  ComposeTiles<C, UC_WARPS>& t = *reinterpret_cast<ComposeTiles<C, UC_WARPS>*>(dsm);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int S = L.n_strokes;
-  for (long long p0 = ((long long)blockIdx.x * UC_WARPS + warp) * 32; p0 < L.n_points;
-       p0 += (long long)gridDim.x * UC_WARPS * 32) {
-    const int rows = (int)min(32LL, L.n_points - p0);
+__global__ void __launch_bounds__(UCR_WARPS * 32) uf_compose_fwd_rows(const UfCompose L) {
+  const int lane = threadIdx.x & 31;
+  const long long S = L.n_strokes;
+  const int nch = (int)((S + 31) / 32);
+  for (long long p = (long long)blockIdx.x * UCR_WARPS + (threadIdx.x >> 5); p < L.n_points;
+       p += (long long)gridDim.x * UCR_WARPS) {
+    const float* __restrict__ arow = L.alphas + p * S;
+    const float* __restrict__ crow = L.colors + p * S * C;
     float T = 1.0f, dens = 0.0f, col[C];
 #pragma unroll
     for (int ch = 0; ch < C; ch++) col[ch] = 0.0f;
-    for (int hi = S - 1; hi >= 0; hi -= 32) {
-      const int nb = min(32, hi + 1);
-      load_tile<C, UC_WARPS>(t, warp, lane, L, p0, rows, hi, nb, -1, nullptr, nullptr);
-      __syncwarp();
-      if (lane < rows) {
-        for (int j = 0; j < nb; j++) {
-          const float a = t.a[warp][lane][j];
-          if (a == 0.0f) continue;  // compositing.cu:37
-          const float w = a * T;
-          T *= (1.0f - a);
-          dens += L.density[hi - j] * w;
+    for (int k = nch - 1; k >= 0; k--) {
+      const long long s = (long long)k * 32 + 31 - lane;  // descending within the chunk
+      const bool in = s < S;
+      const float a = in ? __ldg(arow + s) : 0.0f;
+      const float om = 1.0f - a;
+      const float Ts = T * excl_prod_up(om, lane);
+      if (in && a != 0.0f) {  // compositing.cu:37
+        const float w = a * Ts;
+        dens += __ldg(L.density + s) * w;
 #pragma unroll
-          for (int ch = 0; ch < C; ch++) col[ch] += t.c[warp][lane][j * C + ch] * w;
-        }
+        for (int ch = 0; ch < C; ch++) col[ch] += __ldg(crow + s * C + ch) * w;
       }
-      __syncwarp();
+      // T below the chunk: the product of every lane's factor
+      float all = om;
+      for (int o = 16; o > 0; o >>= 1) all *= __shfl_xor_sync(0xffffffffu, all, o);
+      T *= all;
     }
-    if (lane < rows) {
-      const long long p = p0 + lane;
+    dens = warp_sum(dens);
+#pragma unroll
+    for (int ch = 0; ch < C; ch++) col[ch] = warp_sum(col[ch]);
+    if (lane == 0) {
       const float scale = 1.0f / (1.0f + 1e-6f - T);
       L.density_out[p] = dens;
 #pragma unroll
       for (int ch = 0; ch < C; ch++) L.color_out[p * C + ch] = clampf(col[ch] * scale, 0.0f, 1.0f);
     }
   }
+}
+
+// Exact adjoint, one warp per row. Pass 1 (top-down, as the forward) gives the
+// totals and stores each chunk's incoming transmittance (one float per 32 strokes).
+// Pass 2 (bottom-up) needs, per stroke s, T_s (the chunk's T times a suffix product
+// over the lanes above) and U, V, B: density, colour and transmittance composited
+// over the strokes below s, i.e. the affine recurrences x <- (1 - a) x + b (b = d a,
+// c a, 0) run from the bottom. They come from an inclusive shuffle scan of the lanes'
+// affine maps (m = 1 - a, b), shifted by one lane and applied to the carry from the
+// chunks below. Then dL/da_s = T_s [g_d (d_s - U) + g_C.(c_s - V) - g_T B] and
+// dL/dc_s = g_C a_s T_s, accumulated into the caller's buffers; the density-parameter
+// gradient sum_p g_d a_s T_s goes through a per-block shared array (one global atomic
+// per stroke and block).
+constexpr int UCR_ACC_MAX = 12288;  // strokes with a shared accumulator (48 KB)
+
+template <int C>
+__global__ void __launch_bounds__(UCR_WARPS * 32) uf_compose_bwd_rows(const UfCompose L) {
+  extern __shared__ float gdp_acc[];
+  const int lane = threadIdx.x & 31;
+  const long long S = L.n_strokes;
+  const int nch = (int)((S + 31) / 32);
+  const int nacc = L.g_density_params ? (int)(S < UCR_ACC_MAX ? S : UCR_ACC_MAX) : 0;
+  for (int i = threadIdx.x; i < nacc; i += blockDim.x) gdp_acc[i] = 0.0f;
+  __syncthreads();
+  for (long long p = (long long)blockIdx.x * UCR_WARPS + (threadIdx.x >> 5); p < L.n_points;
+       p += (long long)gridDim.x * UCR_WARPS) {
+    const float* __restrict__ arow = L.alphas + p * S;
+    const float* __restrict__ crow = L.colors + p * S * C;
+    float* tin = L.t_scratch + p * nch;
+    // pass 1: totals, chunk transmittances
+    float T = 1.0f, dens = 0.0f, col[C];
+#pragma unroll
+    for (int ch = 0; ch < C; ch++) col[ch] = 0.0f;
+    for (int k = nch - 1; k >= 0; k--) {
+      if (lane == 0) tin[k] = T;
+      const long long s = (long long)k * 32 + 31 - lane;
+      const bool in = s < S;
+      const float a = in ? __ldg(arow + s) : 0.0f;
+      const float om = 1.0f - a;
+      const float Ts = T * excl_prod_up(om, lane);
+      if (in && a != 0.0f) {
+        const float w = a * Ts;
+        dens += __ldg(L.density + s) * w;
+#pragma unroll
+        for (int ch = 0; ch < C; ch++) col[ch] += __ldg(crow + s * C + ch) * w;
+      }
+      float all = om;
+      for (int o = 16; o > 0; o >>= 1) all *= __shfl_xor_sync(0xffffffffu, all, o);
+      T *= all;
+    }
+    for (int o = 16; o > 0; o >>= 1) {  // butterfly: every lane gets the totals
+      dens += __shfl_xor_sync(0xffffffffu, dens, o);
+#pragma unroll
+      for (int ch = 0; ch < C; ch++) col[ch] += __shfl_xor_sync(0xffffffffu, col[ch], o);
+    }
+    __syncwarp();  // pass 1's chunk transmittances are visible to the whole warp
+    const float gd = L.g_density ? L.g_density[p] : 0.0f;
+    const float scale = 1.0f / (1.0f + 1e-6f - T);
+    float gC[C], gT = 0.0f;
+#pragma unroll
+    for (int ch = 0; ch < C; ch++) {
+      const float sc = col[ch] * scale;
+      const float gc = (L.g_color && sc >= 0.0f && sc <= 1.0f) ? L.g_color[p * C + ch] : 0.0f;
+      gC[ch] = gc * scale;
+      gT += gc * col[ch] * scale * scale;
+    }
+    // pass 2: bottom-up
+    float cU = 0.0f, cV[C], cB = 1.0f;
+#pragma unroll
+    for (int ch = 0; ch < C; ch++) cV[ch] = 0.0f;
+    for (int k = 0; k < nch; k++) {
+      const long long s = (long long)k * 32 + lane;  // ascending within the chunk
+      const bool in = s < S;
+      const float a = in ? __ldg(arow + s) : 0.0f;
+      const float d = in ? __ldg(L.density + s) : 0.0f;
+      float c[C];
+#pragma unroll
+      for (int ch = 0; ch < C; ch++) c[ch] = in ? __ldg(crow + s * C + ch) : 0.0f;
+      const float om = 1.0f - a;
+      // T_s: chunk T times the product over the lanes above (higher index)
+      float suf = om;
+      for (int o = 1; o < 32; o <<= 1) {
+        const float y = __shfl_down_sync(0xffffffffu, suf, o);
+        if (lane + o < 32) suf *= y;
+      }
+      float sx = __shfl_down_sync(0xffffffffu, suf, 1);
+      if (lane == 31) sx = 1.0f;
+      const float Ts = tin[k] * sx;
+      // inclusive scan of the affine maps x -> m x + b over the lanes below and this one
+      float m = om, bU = d * a, bV[C];
+#pragma unroll
+      for (int ch = 0; ch < C; ch++) bV[ch] = c[ch] * a;
+      for (int o = 1; o < 32; o <<= 1) {
+        const float ym = __shfl_up_sync(0xffffffffu, m, o);
+        const float yU = __shfl_up_sync(0xffffffffu, bU, o);
+        float yV[C];
+#pragma unroll
+        for (int ch = 0; ch < C; ch++) yV[ch] = __shfl_up_sync(0xffffffffu, bV[ch], o);
+        if (lane >= o) {
+          bU = fmaf(m, yU, bU);
+#pragma unroll
+          for (int ch = 0; ch < C; ch++) bV[ch] = fmaf(m, yV[ch], bV[ch]);
+          m *= ym;
+        }
+      }
+      // exclusive (the strokes below s) = the previous lane's inclusive map
+      float em = __shfl_up_sync(0xffffffffu, m, 1), eU = __shfl_up_sync(0xffffffffu, bU, 1), eV[C];
+#pragma unroll
+      for (int ch = 0; ch < C; ch++) eV[ch] = __shfl_up_sync(0xffffffffu, bV[ch], 1);
+      if (lane == 0) {
+        em = 1.0f;
+        eU = 0.0f;
+#pragma unroll
+        for (int ch = 0; ch < C; ch++) eV[ch] = 0.0f;
+      }
+      const float U = fmaf(em, cU, eU), Bs = em * cB;
+      float inner = gd * (d - U) - gT * Bs;
+#pragma unroll
+      for (int ch = 0; ch < C; ch++) inner += gC[ch] * (c[ch] - fmaf(em, cV[ch], eV[ch]));
+      if (in) {
+        const float w = a * Ts;
+        L.g_alphas[p * S + s] += Ts * inner;
+#pragma unroll
+        for (int ch = 0; ch < C; ch++) L.g_colors[(p * S + s) * C + ch] += gC[ch] * w;
+        if (L.g_density_params) {
+          const float g = gd * w;
+          if (g != 0.0f) {
+            if (s < nacc) atomicAdd(gdp_acc + s, g);
+            else atomicAdd(L.g_density_params + s, g);
+          }
+        }
+      }
+      // carry: the whole chunk's map (lane 31's inclusive)
+      const float am = __shfl_sync(0xffffffffu, m, 31), aU = __shfl_sync(0xffffffffu, bU, 31);
+      cU = fmaf(am, cU, aU);
+#pragma unroll
+      for (int ch = 0; ch < C; ch++) cV[ch] = fmaf(am, cV[ch], __shfl_sync(0xffffffffu, bV[ch], 31));
+      cB *= am;
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nacc; i += blockDim.x)
+    if (gdp_acc[i] != 0.0f) atomicAdd(L.g_density_params + i, gdp_acc[i]);
 }
 
 template <int C>
@@ -414,13 +581,25 @@ static cudaError_t launch_dyn(K kernel, int grid, int threads, size_t smem, cons
 }
 
 cudaError_t launch_uf_compose_fwd(const UfCompose& L, cudaStream_t st) {
-  const int grid = grid_for(L.n_points, UC_WARPS * 32);
+  const int grid = grid_for(L.n_points, UCR_WARPS);  // one row per warp
   if (L.color_dim == 1)
-    return launch_dyn(uf_compose_fwd_kernel<1>, grid, UC_WARPS * 32, sizeof(ComposeTiles<1, UC_WARPS>), L, st);
-  return launch_dyn(uf_compose_fwd_kernel<3>, grid, UC_WARPS * 32, sizeof(ComposeTiles<3, UC_WARPS>), L, st);
+    uf_compose_fwd_rows<1><<<grid, UCR_WARPS * 32, 0, st>>>(L);
+  else
+    uf_compose_fwd_rows<3><<<grid, UCR_WARPS * 32, 0, st>>>(L);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_uf_compose_bwd(const UfCompose& L, cudaStream_t st) {
+  if (!L.compat) {  // exact adjoint: one row per warp
+    const int grid = grid_for(L.n_points, UCR_WARPS);
+    const size_t smem = L.g_density_params ? size_t(std::min<long long>(L.n_strokes, UCR_ACC_MAX)) * 4 : 0;
+    if (L.color_dim == 1)
+      uf_compose_bwd_rows<1><<<grid, UCR_WARPS * 32, smem, st>>>(L);
+    else
+      uf_compose_bwd_rows<3><<<grid, UCR_WARPS * 32, smem, st>>>(L);
+    return cudaGetLastError();
+  }
+  // the reference's formulas (compat): 32-row tiles in shared memory
   const int grid = grid_for(L.n_points, UCB_WARPS * 32);
   if (L.color_dim == 1)
     return launch_dyn(uf_compose_bwd_kernel<1>, grid, UCB_WARPS * 32, sizeof(ComposeBwdTiles<1, UCB_WARPS>), L, st);

@@ -44,31 +44,35 @@ class _TextureFn(torch.autograd.Function):
         C, H, W = img.shape
         col_out = torch.empty_like(col)
         al_out = torch.empty_like(al)
+        # texels interleaved as float4 (r, g, b, 0): one load per bilinear corner
+        packed = torch.empty(H, W, 4, device=col.device)
         lib = _lib.load()
         with torch.cuda.device(col.device):
-            _lib.check(lib.n3ds_texture_forward(_lib.ptr(col_out), _lib.ptr(al_out), _lib.ptr(tc), _lib.ptr(col),
-                                                _lib.ptr(al), n, _lib.ptr(img), C, H, W, float(tint_ratio),
-                                                int(bool(modulate_alpha)), _lib.stream_ptr()))
-        ctx.save_for_backward(tc, img)
-        ctx.meta = (float(tint_ratio), bool(modulate_alpha), colors.shape, alphas.shape)
+            st = _lib.stream_ptr()
+            _lib.check(lib.n3ds_texture_pack(_lib.ptr(packed), _lib.ptr(img), C, H, W, st))
+            _lib.check(lib.n3ds_texture_forward_packed(_lib.ptr(col_out), _lib.ptr(al_out), _lib.ptr(tc),
+                                                       _lib.ptr(col), _lib.ptr(al), n, _lib.ptr(packed), C, H, W,
+                                                       float(tint_ratio), int(bool(modulate_alpha)), st))
+        ctx.save_for_backward(tc, packed)
+        ctx.meta = (float(tint_ratio), bool(modulate_alpha), colors.shape, alphas.shape, C)
         return col_out.reshape(colors.shape), al_out.reshape(alphas.shape)
 
     @staticmethod
     @once_differentiable
     def backward(ctx, g_col, g_al):
-        tc, img = ctx.saved_tensors
-        tint_ratio, modulate, cshape, ashape = ctx.meta
+        tc, packed = ctx.saved_tensors
+        tint_ratio, modulate, cshape, ashape, C = ctx.meta
         n = tc.shape[0]
-        C, H, W = img.shape
+        H, W = packed.shape[0], packed.shape[1]
         gc = None if g_col is None else g_col.contiguous().float().reshape(n, 3)
         ga = None if g_al is None else g_al.contiguous().float().reshape(n)
         gcol = torch.empty(n, 3, device=tc.device) if ctx.needs_input_grad[1] else None
         gal = torch.empty(n, device=tc.device) if ctx.needs_input_grad[2] else None
         lib = _lib.load()
         with torch.cuda.device(tc.device):
-            _lib.check(lib.n3ds_texture_backward(_lib.ptr(gcol), _lib.ptr(gal), _lib.ptr(gc), _lib.ptr(ga),
-                                                 _lib.ptr(tc), n, _lib.ptr(img), C, H, W, tint_ratio, int(modulate),
-                                                 _lib.stream_ptr()))
+            _lib.check(lib.n3ds_texture_backward_packed(_lib.ptr(gcol), _lib.ptr(gal), _lib.ptr(gc), _lib.ptr(ga),
+                                                        _lib.ptr(tc), n, _lib.ptr(packed), C, H, W, tint_ratio,
+                                                        int(modulate), _lib.stream_ptr()))
         return (None, None if gcol is None else gcol.reshape(cshape), None if gal is None else gal.reshape(ashape),
                 None, None, None)
 

@@ -29,7 +29,8 @@ def test_pure_host_calls():
     lib = _lib.load()
     assert lib.n3ds_version() >= 100
     assert lib.n3ds_stroke_workspace_bytes(1000) >= 1000 * 256
-    assert lib.n3ds_compose_workspace_bytes(10, 20, 0) == 10 * 20 * 4
+    assert lib.n3ds_compose_workspace_bytes(10, 20, 0) == 10 * 1 * 4  # one float per row and 32 strokes
+    assert lib.n3ds_compose_workspace_bytes(10, 70, 0) == 10 * 3 * 4
     assert lib.n3ds_compose_workspace_bytes(10, 20, 1) == 0
     o = _lib.default_options()
     assert abs(o.cull_alpha - 1e-9) < 1e-15 and o.grad_mode == 0

@@ -126,14 +126,21 @@ def compose_inputs(P=700, S=45, C=3, seed=0, amax=1.0):
     g = torch.Generator().manual_seed(seed)
     a = torch.rand(P, S, generator=g) ** 3 * amax
     a[torch.rand(P, S, generator=g) < 0.3] = 0.0
+    if S == 1:
+        # one stroke: the colour is c a / (a + 1e-6), whose float32 denominator
+        # 1 + 1e-6 - (1 - a) cancels for tiny a (1 + 1e-6 - 1 is 9.54e-7 in float32,
+        # in the reference too); keep a >= 0.05 there
+        a = a * (amax - 0.05) / amax + 0.05
     c = torch.rand(P, S, C, generator=g)
     d = torch.rand(S, generator=g) * 10
     return a, c, d
 
 
-@pytest.mark.parametrize("C", [1, 3])
-def test_compose_forward_matches_oracle(cuda, C):
-    a, c, d = compose_inputs(C=C)
+@pytest.mark.parametrize("C,S", [(1, 45), (3, 45), (3, 1), (3, 32), (3, 100), (1, 300)])
+def test_compose_forward_matches_oracle(cuda, C, S):
+    """One warp per row, 32 strokes per lane step: a lone stroke, an exact chunk,
+    partial and many chunks; 30 % of the alphas are exactly 0 (skipped)."""
+    a, c, d = compose_inputs(C=C, S=S)
     dens = torch.empty(a.shape[0], device=cuda)
     col = torch.empty(a.shape[0], C, device=cuda)
     sl.compose_forward(dens, col, a.to(cuda), c.to(cuda), d.to(cuda))
@@ -141,12 +148,15 @@ def test_compose_forward_matches_oracle(cuda, C):
     assert rel(dens, dr) < FWD_TOL and rel(col, cr) < FWD_TOL
 
 
-@pytest.mark.parametrize("mode", ["exact", "compat"])
-def test_compose_backward(cuda, mode):
+@pytest.mark.parametrize("mode,S", [("exact", 45), ("compat", 45), ("exact", 1), ("exact", 32), ("exact", 100),
+                                    ("exact", 300)])
+def test_compose_backward(cuda, mode, S):
     # compat: the reference formula divides by max(1 - alpha, 1e-6), which amplifies
     # float32 cancellation as alpha -> 1; against the float64 restatement keep alpha
     # <= 0.9 (agreement with the reference op itself is checked at all alphas below)
-    a, c, d = compose_inputs(seed=1, amax=0.9 if mode == "compat" else 1.0)
+    a, c, d = compose_inputs(seed=1, S=S, amax=0.9 if mode == "compat" else 1.0)
+    if mode == "exact" and S >= 32:
+        a[::7, S // 2] = 1.0  # opaque strokes: nothing below them shows
     g = torch.Generator().manual_seed(2)
     gd = torch.randn(a.shape[0], generator=g)
     gcol = torch.randn(a.shape[0], 3, generator=g)

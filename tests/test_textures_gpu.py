@@ -76,3 +76,36 @@ def test_texture_in_stroke_pipeline(cuda):
                                      alphas.double().reshape(-1).cpu(), tex.image_texture[0].double(), 1.0, True)
     assert rel(c2.reshape(-1, 3), ref_c) < 1e-5 and rel(a2.reshape(-1), ref_a) < 1e-5
     assert torch.isfinite(rgb).all() and torch.isfinite(dens).all()
+
+
+@pytest.mark.parametrize("C,modulate", [(3, True), (1, True), (3, False)])
+def test_packed_texture_equals_planar(cuda, C, modulate):
+    """n3ds_texture_forward/backward_packed (float4 texels, what ImageTexture runs) give
+    the planar entry points' results to a few ulps (the compiler contracts the two
+    four-term sums into FMAs differently), outside and non-finite coordinates
+    included."""
+    from neural3dstrokes_b200 import _lib
+    g = torch.Generator().manual_seed(C)
+    H, W, n = 37, 53, 5000
+    img = torch.rand(C, H, W, generator=g).to(cuda)
+    tc = (torch.rand(n, 2, generator=g) * 1.4 - 0.2).to(cuda)
+    tc[:5, 0] = float("nan")
+    tc[5:10, 1] = float("inf")
+    col = torch.rand(n, 3, generator=g).to(cuda)
+    al = torch.rand(n, generator=g).to(cuda)
+    gco, gal = torch.randn(n, 3, generator=g).to(cuda), torch.randn(n, generator=g).to(cuda)
+    packed = torch.empty(H, W, 4, device=cuda)
+    lib, st = _lib.load(), _lib.stream_ptr()
+    P = _lib.ptr
+    _lib.check(lib.n3ds_texture_pack(P(packed), P(img), C, H, W, st))
+    outs = []
+    for fwd, bwd, im in ((lib.n3ds_texture_forward, lib.n3ds_texture_backward, img),
+                         (lib.n3ds_texture_forward_packed, lib.n3ds_texture_backward_packed, packed)):
+        co, ao = torch.empty_like(col), torch.empty_like(al)
+        gc, ga = torch.empty_like(col), torch.empty_like(al)
+        _lib.check(fwd(P(co), P(ao), P(tc), P(col), P(al), n, P(im), C, H, W, 0.7, int(modulate), st))
+        _lib.check(bwd(P(gc), P(ga), P(gco), P(gal), P(tc), n, P(im), C, H, W, 0.7, int(modulate), st))
+        outs.append((co, ao, gc, ga))
+    torch.cuda.synchronize(cuda)
+    for a, b in zip(*outs):
+        assert rel(a, b) < 1e-6
