@@ -82,17 +82,44 @@ __global__ void __launch_bounds__(UF_WARPS * 32) uf_stroke_bwd_kernel(const UfSt
   float v[NV];
 #pragma unroll
   for (int j = 0; j < NV; j++) v[j] = 0.f;
-  for (long long p = (long long)blockIdx.x * UF_WARPS + warp; p < L.n_points; p += (long long)gridDim.x * UF_WARPS) {
-    const V3 x = v3(L.x[3 * p], L.x[3 * p + 1], L.x[3 * p + 2]);
-    const float rinv = 1.f / L.radius[p];
-    const long long pi = p * S + s0 + lane;
-    const float ga = active ? L.g_alpha[pi] : 0.f;
-    const float a = active ? L.alpha_in[pi] : 0.f;
-    const float gs = (active && L.g_sdf) ? L.g_sdf[pi] : 0.f;
+  // The next sample's inputs are fetched (read-only path) before this sample's
+  // recompute and adjoint, so their latency overlaps the work: without it each
+  // iteration's loads wait behind the previous iteration's grad_x atomics.
+  struct In {
+    float x0, x1, x2, r, ga, a, gs, gc0, gc1, gc2;
+  };
+  auto fetch = [&](long long q, In& in) {
+    in = In{0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (q >= L.n_points) return;
+    in.x0 = __ldg(L.x + 3 * q);
+    in.x1 = __ldg(L.x + 3 * q + 1);
+    in.x2 = __ldg(L.x + 3 * q + 2);
+    in.r = __ldg(L.radius + q);
+    if (!active) return;
+    const long long qi = q * S + s0 + lane;
+    in.ga = __ldg(L.g_alpha + qi);
+    in.a = __ldg(L.alpha_in + qi);
+    if (L.g_sdf) in.gs = __ldg(L.g_sdf + qi);
+    if (L.color_const) {
+      in.gc0 = __ldg(L.g_color + 3 * qi);
+      in.gc1 = __ldg(L.g_color + 3 * qi + 1);
+      in.gc2 = __ldg(L.g_color + 3 * qi + 2);
+    }
+  };
+  const long long pstep = (long long)gridDim.x * UF_WARPS;
+  long long p = (long long)blockIdx.x * UF_WARPS + warp;
+  In cur;
+  fetch(p, cur);
+  for (; p < L.n_points; p += pstep) {
+    In nxt;
+    fetch(p + pstep, nxt);
+    const V3 x = v3(cur.x0, cur.x1, cur.x2);
+    const float rinv = 1.f / cur.r;
+    const float ga = cur.ga, a = cur.a, gs = cur.gs;
     if (active && L.color_const) {
-      v[G_COLOR] += L.g_color[3 * pi];
-      v[G_COLOR + 1] += L.g_color[3 * pi + 1];
-      v[G_COLOR + 2] += L.g_color[3 * pi + 2];
+      v[G_COLOR] += cur.gc0;
+      v[G_COLOR + 1] += cur.gc1;
+      v[G_COLOR + 2] += cur.gc2;
     }
     float sdf, f = 1.f;
     V3 pl;
@@ -142,6 +169,7 @@ __global__ void __launch_bounds__(UF_WARPS * 32) uf_stroke_bwd_kernel(const UfSt
         atomicAdd(L.grad_x + 3 * p + 2, sz);
       }
     }
+    cur = nxt;
   }
   if (active) {
     float* dst = L.gslots + (long long)(s0 + lane) * GRAD_SLOTS;
