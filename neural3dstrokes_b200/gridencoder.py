@@ -46,7 +46,8 @@ def _need(cond, msg):
         raise RuntimeError(msg)
 
 
-def _geometry(D, C, L):
+def _geometry(D, C, L, B):
+    _need(0 <= B < 2 ** 32, "B must be in [0, 2^32) (a uint32, as in the reference)")
     _need(C in (1, 2, 4, 8), "GridEncoding: C must be 1, 2, 4, or 8.")
     _need(D in (2, 3, 4, 5), "GridEncoding: D must be 2, 3, 4, or 5.")
     _need(L >= 1, "GridEncoding: L must be >= 1")
@@ -58,6 +59,8 @@ def _check_offsets(offsets, L, rows):
     _need(offsets.numel() >= L + 1, "offsets must hold L + 1 entries")
     key = (offsets.data_ptr(), offsets._version, offsets.numel(), rows)
     if key not in _checked_offsets:
+        if len(_checked_offsets) > 4096:  # a bounded memo, not a registry
+            _checked_offsets.clear()
         o = offsets[:L + 1].cpu().numpy().astype(np.int64)
         _need(o[0] >= 0 and (np.diff(o) > 0).all() and o[-1] <= rows,
               "offsets must increase strictly from >= 0 and end within the embedding table")
@@ -74,7 +77,7 @@ def grid_encode_forward(inputs, embeddings, offsets, outputs, B, D, C, L, S, H, 
     for n, t in (("inputs", inputs), ("embeddings", embeddings), ("outputs", outputs)):
         _check(t, n)
     _need(inputs.dtype == torch.float32, "inputs must be a float32 tensor")
-    _geometry(D, C, L)
+    _geometry(D, C, L, B)
     _need(outputs.dtype == embeddings.dtype, "outputs must have the embeddings' dtype")
     _need(inputs.numel() >= B * D, "inputs must hold B * D values")
     _need(embeddings.dim() == 2 and embeddings.size(1) == C, "embeddings must be [rows, C]")
@@ -99,7 +102,7 @@ def grid_encode_backward(grad, inputs, embeddings, offsets, grad_embeddings, B, 
                  ("grad_embeddings", grad_embeddings)):
         _check(t, n)
     _need(inputs.dtype == torch.float32, "inputs must be a float32 tensor")
-    _geometry(D, C, L)
+    _geometry(D, C, L, B)
     _need(grad.dtype == embeddings.dtype == grad_embeddings.dtype, "grad, embeddings and grad_embeddings "
           "must share a dtype")
     _need(inputs.numel() >= B * D and grad.numel() >= L * B * C, "inputs / grad are too small")
@@ -125,7 +128,7 @@ def grad_total_variation(inputs, embeddings, grad, offsets, weight, B, D, C, L, 
     inputs have the embeddings' dtype (the reference reads them as scalar_t)."""
     for n, t in (("inputs", inputs), ("embeddings", embeddings), ("grad", grad)):
         _check(t, n)
-    _geometry(D, C, L)
+    _geometry(D, C, L, B)
     _need(inputs.dtype == embeddings.dtype == grad.dtype, "inputs, embeddings and grad must share a dtype")
     _need(inputs.numel() >= B * D, "inputs must hold B * D values")
     _need(grad.shape == embeddings.shape and embeddings.dim() == 2 and embeddings.size(1) == C,
