@@ -1,7 +1,7 @@
 """The reference stroke-field step on CPU cores (labelled port) and on the GPU (the
 unmodified reference op from oracle/_ref).
 
-TEST / BASELINE INFRASTRUCTURE ONLY: used by tests and by bench.py's CPU-baseline
+TEST / CPU-BASELINE INFRASTRUCTURE ONLY: used by tests and by bench.py's CPU-baseline
 and reference legs, never by the product package.
 
 Both run the chain the reference model runs for one training step of the stroke
