@@ -205,7 +205,7 @@ typedef struct n3ds_options {
   /* optional: 4 cudaEvent_t recorded on the stream around the segment kernels
    * (forward begin/end, backward begin/end), or NULL */
   void* const* timing_events;
-  int32_t warps_bwd;  /* warps per CTA, backward: 4, 8, 16, 20, 24 (0 = auto) */
+  int32_t warps_bwd;  /* warps per CTA, backward: 4, 8, 16, 20, 24, 32 (0 = auto) */
   /* 1: no backward follows this forward, so the segment kernels skip recording which
    * strokes the backward needs (a backward after such a forward culls by itself) */
   int32_t forward_only;

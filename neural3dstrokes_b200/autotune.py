@@ -6,7 +6,10 @@ on its own data for each candidate launch configuration and keeps the fastest:
 * work decomposition (``schedule``): 32-sample segments with every lane evaluating
   each surviving stroke, or 64-sample units with packed (sample, stroke) pairs;
 * warps per CTA (rays in flight per SM), forward and backward separately (the
-  segment kernels fit 32 / 24 warps, the run kernels 16);
+  segment kernels fit 32 warps; the backward's 32-warp build is held to 64 registers
+  and spills a little: on config 3 its backward alone measured 5.12 against 5.27 ms
+  and a whole tuned step within noise of 24 warps, on Bezier tubes (config 2) 26.2
+  against 25.1 ms, so the tuner decides per workload; the run kernels 16);
 * strokes per shared-memory stage: the largest that fits, or half of it (more passes,
   less shared memory per CTA).
 
@@ -44,10 +47,10 @@ def signature(field) -> str:
 def candidates(grad_mode: str = "exact", cull_alpha: float = 1e-9, forward_only: bool = False,
                count_pairs: bool = False) -> List[FieldOptions]:
     out = []
-    # (schedule, forward warps, backward warps): the segment kernels' register use
-    # allows up to 32 / 24 warps per CTA, the run kernels 16
-    shapes = [("segments", 32, 24), ("segments", 32, 20), ("segments", 24, 16), ("segments", 16, 16),
-              ("runs", 16, 16)]
+    # (schedule, forward warps, backward warps): up to 32 warps per CTA for the
+    # segment kernels, 16 for the run kernels
+    shapes = [("segments", 32, 32), ("segments", 32, 24), ("segments", 32, 20), ("segments", 24, 16),
+              ("segments", 16, 16), ("runs", 16, 16)]
     for schedule, wf, wb in shapes:
         for half in (False, True):
             # chunk 0 = the largest stage that fits; the halved stage (-1) is resolved later

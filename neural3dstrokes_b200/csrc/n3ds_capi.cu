@@ -137,7 +137,7 @@ Resolved resolve(const n3ds_options_t* o) {
   const int wf = o->warps > 0 ? o->warps : (runs ? 16 : 32);
   const int wb = o->warps_bwd > 0 ? o->warps_bwd : (runs ? 16 : 24);
   r.warps_fwd = runs ? pick(wf, {4, 8, 16}) : pick(wf, {4, 8, 16, 24, 32});
-  r.warps_bwd = runs ? pick(wb, {4, 8, 16}) : pick(wb, {4, 8, 16, 20, 24});
+  r.warps_bwd = runs ? pick(wb, {4, 8, 16}) : pick(wb, {4, 8, 16, 20, 24, 32});
   r.warps = r.warps_bwd;
   const size_t budget = size_t(di.smem_optin) - 256;  // room for static shared memory
   // default stages: the largest multiple of 32 strokes that fits the shared memory

@@ -1215,6 +1215,7 @@ cudaError_t launch_seg_bwd(const SegLaunch& L, int grid, int warps, size_t smem,
     case 16: return launch_bwd_w<16>(L, grid, smem, st);
     case 20: return launch_bwd_w<20>(L, grid, smem, st);
     case 24: return launch_bwd_w<24>(L, grid, smem, st);
+    case 32: return launch_bwd_w<32>(L, grid, smem, st);  // 64 registers, a small spill
     default: return cudaErrorInvalidValue;
   }
 }

@@ -222,3 +222,18 @@ def test_pair_counters_only_when_requested(cuda):
         out.append((f.rgb.clone(), f.grad_shape.clone()))
     assert torch.equal(out[0][0], out[1][0])
     assert rel(out[0][1], out[1][1]) < 1e-5
+
+
+@pytest.mark.parametrize("chunk", [0, 64])
+def test_backward_warp_counts_agree(cuda, chunk):
+    """The 32-warp backward build (64 registers) gives the 24-warp results."""
+    sc, rays = small_workload("every", n_strokes=90, n_rays=80, n_samples=64, seed=8)
+    g_rgb = torch.randn(rays.n_rays, 3, generator=torch.Generator().manual_seed(3)).to(cuda)
+    outs = []
+    for wb in (24, 32):
+        opts = FieldOptions(schedule="segments", warps_bwd=wb, chunk_bwd=chunk)
+        (rgb, acc, depth), (x, sp, col, den, dl) = run_field(sc, rays, cuda, opts=opts, requires_grad=True)
+        ((rgb * g_rgb).sum() + acc.sum()).backward()
+        outs.append((x.grad, sp.grad, col.grad, den.grad, dl.grad))
+    for a, b in zip(*outs):
+        assert rel(a, b) < 1e-5
