@@ -215,3 +215,30 @@ def rel(a, b):
     a = torch.as_tensor(a).double()
     b = torch.as_tensor(b).double()
     return float((a - b).abs().max() / max(float(b.abs().max()), 1e-30))
+
+
+SHIM = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "neural3dstrokes_b200", "shim")
+
+
+def _with_shim(fn):
+    import sys
+    sys.path.insert(0, SHIM)
+    saved = sys.modules.pop("_gridencoder", None)
+    try:
+        return fn()
+    finally:
+        sys.path.remove(SHIM)
+        sys.modules.pop("_gridencoder", None)
+        if saved is not None:
+            sys.modules["_gridencoder"] = saved
+
+
+def test_shim_exposes_the_backend_functions():
+    from neural3dstrokes_b200 import gridencoder as ge
+
+    def check():
+        import _gridencoder
+        assert _gridencoder.grid_encode_forward is ge.grid_encode_forward
+        assert _gridencoder.grid_encode_backward is ge.grid_encode_backward
+        assert _gridencoder.grad_total_variation is ge.grad_total_variation
+    _with_shim(check)
