@@ -211,34 +211,54 @@ def fp32_peak(device, repeats=8):
     return best
 
 
-def cpu_baseline(workload, budget_s=15.0):
-    """The labelled float32 CPU port of the reference step (oracle/cpu_port.py) on a
-    bounded ray sample of the same workload, all host threads."""
+# The CPU legs (this arm's cpu_baseline and the reference arm) time the same fixed
+# sample of each workload: these evenly spaced rays of every scene (first and last
+# included), with every stroke of the scene, and fixed N(0,1) upstream gradients.
+CPU_SAMPLE_RAYS = {0: 512, 1: 64, 2: 16, 3: 24, 4: 8}
+
+
+def cpu_sample(workload, cfg):
+    """The fixed CPU sample of a workload: per scene (scene, rays subset, upstream
+    gradients), and its nominal pairs."""
+    from oracle.accuracy import ray_subset, take_rays
+    k = CPU_SAMPLE_RAYS.get(cfg, 16)
+    g = torch.Generator().manual_seed(11)
+    items, pairs = [], 0
+    for sc, rays in zip(workload.scenes, workload.rays):
+        idx = ray_subset(rays.n_rays, k)
+        sub = take_rays(rays, idx)
+        n = idx.numel()
+        gr = (torch.randn(n, 3, generator=g), torch.randn(n, generator=g), torch.randn(n, generator=g))
+        items.append((sc, sub, gr))
+        pairs += sc.n_strokes * n * rays.n_samples
+    desc = (f"{k} evenly spaced rays of each scene ({pairs} nominal pairs per pass, every stroke): float32 "
+            f"torch restatement of the reference strokelib kernels + render.py, forward + backward")
+    return items, pairs, desc
+
+
+def cpu_pass(workload, items):
     from oracle import cpu_port
+    for sc, sub, gr in items:
+        cpu_port.port_step(sc, sub.x, sub.radius, sub.tdist, sub.dirs, *gr, delta=workload.sdf_delta,
+                           laplace=workload.use_laplace, inv=workload.inv_scale_radius)
+
+
+def cpu_baseline(workload, cfg, budget_s=15.0):
+    """The labelled float32 CPU port of the reference step (oracle/cpu_port.py) on the
+    fixed ray sample of the workload, all host threads, repeated for about budget_s."""
     threads = os.cpu_count() or 1
     torch.set_num_threads(threads)
-    g = torch.Generator().manual_seed(11)
-
-    def run(k):
-        t0 = time.perf_counter()
-        pairs = 0
-        for sc, rays in zip(workload.scenes, workload.rays):
-            n = min(k, rays.n_rays)
-            sl = slice(0, n)
-            gr = (torch.randn(n, 3, generator=g), torch.randn(n, generator=g), torch.randn(n, generator=g))
-            cpu_port.port_step(sc, rays.x[sl], rays.radius[sl], rays.tdist[sl], rays.dirs[sl], *gr,
-                               delta=workload.sdf_delta, laplace=workload.use_laplace, inv=workload.inv_scale_radius)
-            pairs += sc.n_strokes * n * rays.n_samples
-        return pairs, time.perf_counter() - t0
-
-    # size the sample from a small probe so the measured round takes about budget_s
-    k = 2
-    pairs, dt = run(k)
-    k = max(k, min(4096, int(k * budget_s / max(dt, 1e-3))))
-    pairs, dt = run(k)
-    return {"value": pairs / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"first {k} rays of each scene ({pairs} nominal pairs, {dt:.1f} s): float32 torch "
-                      f"restatement of the reference strokelib kernels + render.py, forward + backward"}
+    items, pairs, desc = cpu_sample(workload, cfg)
+    cpu_pass(workload, items)  # warm-up
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        cpu_pass(workload, items)
+        reps += 1
+        if time.perf_counter() - t0 >= budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": pairs * reps / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{desc}; {reps} passes in {dt:.1f} s"}
 
 
 def run_reference(args, world, rank):
@@ -248,39 +268,25 @@ def run_reference(args, world, rank):
     if rank != 0:
         return
     from neural3dstrokes_b200 import scenes
-    from oracle import cpu_port
     w = scenes.config(args.config)
     threads = os.cpu_count() or 1
     torch.set_num_threads(threads)
-    g = torch.Generator().manual_seed(5)
-    # one step = a bounded ray sample of every scene, sized by the first (warm-up) step
-    # to ~3 s of CPU work
-    n = 4 if args.config in (3, 4) else 16
+    # one step = one pass over the same fixed ray sample as this arm's cpu_baseline leg
+    items, pairs, desc = cpu_sample(w, args.config)
     rates = []
     for it in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        pairs = 0
-        for sc, rays in zip(w.scenes, w.rays):
-            m = min(n, rays.n_rays)
-            r0 = (it * m) % max(1, rays.n_rays - m)
-            sl = slice(r0, r0 + m)
-            gr = (torch.randn(m, 3, generator=g), torch.randn(m, generator=g), torch.randn(m, generator=g))
-            cpu_port.port_step(sc, rays.x[sl], rays.radius[sl], rays.tdist[sl], rays.dirs[sl], *gr,
-                               delta=w.sdf_delta, laplace=w.use_laplace, inv=w.inv_scale_radius)
-            pairs += sc.n_strokes * m * rays.n_samples
+        cpu_pass(w, items)
         dt = time.perf_counter() - t0
         if it >= args.warmup:
             rates.append(pairs / dt)
-        if it == 0:
-            n = max(1, min(max(r.n_rays for r in w.rays), int(n * 3.0 / max(dt, 1e-3))))
     value = statistics.mean(rates)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
             "config": {"workload": w.name, "nominal_pairs_per_full_step": w.nominal_pairs},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"{n} rays of each scene per step, float32 torch restatement of the "
-                                       f"reference strokelib kernels + render.py, forward + backward"},
+                             "sample": f"one step = one pass over {desc}"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if torch.cuda.is_available() and not args.no_plain_op:
         try:
@@ -324,6 +330,27 @@ def plain_op_gpu(w, args, max_seconds=60.0):
     return {"value": w.nominal_pairs / t, "unit": UNIT, "ms_per_step": t * 1e3, "steps": len(times),
             "note": "reference _strokelib built from its own sources for sm_100a, per scene, per primitive "
                     "group, ray-chunked (P_chunk*S < 2^29), torch autograd for render.py, grad_x requested"}
+
+
+# evenly spaced rays per scene that the float64 oracle checks in the accuracy leg
+ACCURACY_RAYS = {0: 128, 1: 64, 2: 16, 3: 16, 4: 6}
+
+
+def accuracy_leg(field, w, args):
+    """Every output and gradient of the benchmarked field against the float64 oracle
+    and the reference op (oracle/accuracy.py), untimed; errors are normwise relative,
+    worst scene."""
+    from oracle import accuracy, cpu_port
+    torch.set_num_threads(os.cpu_count() or 1)
+    ref = cpu_port.reference_extension()
+    t0 = time.perf_counter()
+    out = accuracy.subset_accuracy(field, w, ACCURACY_RAYS.get(args.config, 16), ref=ref)
+    if args.config == 3 and ref is not None and args.scale == 1.0:
+        out["vs_16_sequential_plain_op_calls"] = accuracy.plain_op_compare(field, w, ref)
+    if args.config == 2:
+        out["fd_slice"] = accuracy.fd_slice(w.scenes[0], w.rays[0], 32, 8, device=field.device)
+    out["seconds"] = round(time.perf_counter() - t0, 1)
+    return out
 
 
 def loss_curves(args):
@@ -755,6 +782,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain-op", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the untimed accuracy leg")
     ap.add_argument("--schedule", default="auto", choices=["auto", "runs", "segments"],
                     help="field kernel work decomposition (auto: the autotuner picks)")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (library defaults)")
@@ -893,8 +921,9 @@ def main():
     if not args.no_e2e:
         ins = [field.x, field.radius, field.tdist, field.dirs, field.g_rgb, field.g_acc, field.g_depth, field.shape,
                field.color, field.density, field.delta, field.sdf_ids]
+        # every result of the step comes back, the sample-position gradient included
         outs = [field.rgb, field.acc, field.depth, field.grad_shape, field.grad_color, field.grad_density,
-                field.grad_delta]
+                field.grad_delta] + ([field.grad_x] if field.grad_x is not None else [])
         h_in = [t.detach().cpu().pin_memory() for t in ins]
         h_out = [torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for t in outs]
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -923,9 +952,17 @@ def main():
                "d2h_bytes_per_step": sum(t.numel() * t.element_size() for t in h_out),
                "overlap": "uploads and downloads on a copy stream, double-buffered, overlapping compute"}
 
+    # accuracy at the workload's own shape (untimed; the float64 oracle and the
+    # reference op are the checkers): the whole workload with upstream gradients on a
+    # fixed ray subset, plus the 16 sequential plain-op calls (config 3) and the FP64
+    # finite-difference slice (config 2)
+    accuracy = None
+    if rank == 0 and not args.no_accuracy:
+        accuracy = accuracy_leg(field, w, args)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(w, args.cpu_seconds)
+        cpu = cpu_baseline(w, args.config, args.cpu_seconds)
 
     lf, lb = field.launch_count()
     launches_per_step = lf + lb + (3 if trainer is not None else 0)  # + 3 Adam launches when training
@@ -947,7 +984,7 @@ def main():
                                   "chunk_bwd": field.options.chunk_bwd,
                                   "picked_by": "autotuner" if tuned is not None else "flags",
                                   "tried_ms": tune_table}},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "accuracy": accuracy,
             "gpu_launches": launches_per_step * args.steps,
             "gpu_launches_per_step": launches_per_step,
         }

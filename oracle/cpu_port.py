@@ -86,10 +86,11 @@ def reference_extension():
 
 
 def plain_op_step(ref, scene, x, radius, tdist, dirs, g_rgb, g_acc, g_depth, delta=0.02, laplace=True, inv=True,
-                  bg=1.0, max_pairs=1 << 29):
+                  bg=1.0, max_pairs=1 << 29, return_grad_x=False):
     """One forward + backward through the reference CUDA op, ray-chunked, with the
     sample-position gradient requested as well. All tensors on the GPU. Returns
-    (rgb, acc, depth, grad_shape, grad_color, grad_density)."""
+    (rgb, acc, depth, grad_shape, grad_color, grad_density), plus grad_x [R*N, 3]
+    when ``return_grad_x``."""
     dev = x.device
     R, N, _ = x.shape
     S = scene.n_strokes
@@ -102,6 +103,7 @@ def plain_op_step(ref, scene, x, radius, tdist, dirs, g_rgb, g_acc, g_depth, del
     grad_color = torch.zeros_like(scene.color_params)
     grad_density = torch.zeros_like(scene.density)
     empty = torch.empty(0, device=dev)
+    grad_x = torch.empty(R * N, 3, device=dev) if return_grad_x else None
     for r0 in range(0, R, chunk):
         r1 = min(R, r0 + chunk)
         xc = x[r0:r1].reshape(-1, 3).contiguous()
@@ -142,6 +144,10 @@ def plain_op_step(ref, scene, x, radius, tdist, dirs, g_rgb, g_acc, g_depth, del
                                 vd, a, ps, cp, sid, 0, delta, laplace, inv)
             grad_shape[idx, :ps.shape[1]] += gs
             grad_color[idx] += gcol
+        if return_grad_x:
+            grad_x[r0 * N:r1 * N] = gx
+    if return_grad_x:
+        return rgb, acc, depth, grad_shape, grad_color, grad_density, grad_x
     return rgb, acc, depth, grad_shape, grad_color, grad_density
 
 
