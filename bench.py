@@ -943,14 +943,15 @@ def main():
         e0.record()
         pipe.copy.wait_event(e0)  # the first upload is inside the timed region
         e2e_run(n_e2e)
-        pipe.compute.wait_stream(pipe.copy)  # ... and so is the last download
+        pipe.compute.wait_stream(pipe.down)  # ... and so is the last download
         e1.record()
         torch.cuda.synchronize(dev)
         t_e2e = max_over_ranks(e0.elapsed_time(e1) * 1e-3 / n_e2e, world, dev)
         e2e = {"value": pairs * world / t_e2e, "unit": UNIT, "ms_per_step": t_e2e * 1e3,
                "h2d_bytes_per_step": sum(t.numel() * t.element_size() for t in h_in),
                "d2h_bytes_per_step": sum(t.numel() * t.element_size() for t in h_out),
-               "overlap": "uploads and downloads on a copy stream, double-buffered, overlapping compute"}
+               "overlap": "uploads and downloads on two copy streams (both link directions at once), "
+                          "double-buffered, overlapping compute"}
 
     # accuracy at the workload's own shape (untimed; the float64 oracle and the
     # reference op are the checkers): the whole workload with upstream gradients on a

@@ -144,7 +144,9 @@ int n3ds_compose_mode_backward(int mode, float* grad_alphas, float* grad_colors,
  * race on that scratch; calls on one stream are ordered. The first call on a device
  * (with that device current) looks the array's address up with cudaGetSymbolAddress;
  * a caller that records the call into a stream capture makes one call on that device
- * before capturing. Same arguments, outputs and errors as n3ds_stroke_forward. */
+ * before capturing. The address is kept for the process's life: do not call this entry
+ * point after a cudaDeviceReset of that device. Same arguments, outputs and errors as
+ * n3ds_stroke_forward. */
 int n3ds_stroke_forward_static(float* alpha_out, float* color_out, float* sdf_out, float* texcoord_out,
                                int64_t n_texcoord,
                                const float* x, const float* radius, const float* viewdir,
@@ -192,6 +194,16 @@ typedef struct n3ds_strokes {
   const float* sdf_delta;     /* [S] softness per stroke */
   int32_t use_laplace_transform;
   int32_t inv_scale_radius;
+  /* Optional stroke window per scene, device int32 [n_scenes*2] = (frozen, active)
+   * pairs, or NULL (every stroke active). Read on the device by the kernels, so the
+   * window can follow a device-side stroke count with no host round trip (the
+   * truncation of StrokeField.predict_density, models.py:665-673, 686-702). Scene
+   * strokes at local index >= active are absent: no alpha, no gradient. Strokes below
+   * frozen are composited as usual but receive no gradient and contribute none to
+   * grad_x (the reference evaluates them under torch.no_grad and concatenates them
+   * before the optimised ones, which keeps the stroke order). Needs the segment
+   * schedule and at most 40 scenes. */
+  const int32_t* stroke_window;
 } n3ds_strokes_t;
 
 typedef struct n3ds_options {
@@ -214,6 +226,15 @@ typedef struct n3ds_options {
    * _read_backward_pairs); 0 (default): those counters stay 0 and the kernels skip the
    * per-candidate bookkeeping */
   int32_t count_pairs;
+  /* limit of every bounded device-side wait (the stroke staging barrier), in
+   * microseconds; 0 = the default, one second. A wait that runs out sets status bit 2
+   * (N3DS_ERR_DEVICE through n3ds_field_read_status) and its CTA stops; the launch's
+   * outputs are then invalid */
+  int32_t wait_limit_us;
+  /* test of the bounded wait: 1 arms the staging barrier for the stage's bytes
+   * without issuing the copies, so every wait runs out and reports (no copy is left
+   * in flight). 0 in any real use */
+  int32_t test_stall_staging;
 } n3ds_options_t;
 
 /* Fill *opt with the defaults. */

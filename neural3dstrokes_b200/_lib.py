@@ -39,14 +39,15 @@ class Strokes(ctypes.Structure):
     _fields_ = [("sdf_ids", ctypes.c_void_p), ("shape_params", ctypes.c_void_p), ("param_stride", c_i32),
                 ("color_params", ctypes.c_void_p), ("density", ctypes.c_void_p),
                 ("sdf_delta", ctypes.c_void_p), ("use_laplace_transform", c_i32),
-                ("inv_scale_radius", c_i32)]
+                ("inv_scale_radius", c_i32), ("stroke_window", ctypes.c_void_p)]
 
 
 class Options(ctypes.Structure):
     _fields_ = [("cull_alpha", ctypes.c_float), ("chunk_fwd", c_i32), ("chunk_bwd", c_i32),
                 ("warps", c_i32), ("schedule", c_i32), ("grad_mode", c_i32),
                 ("timing_events", ctypes.POINTER(ctypes.c_void_p)), ("warps_bwd", c_i32),
-                ("forward_only", c_i32), ("count_pairs", c_i32)]
+                ("forward_only", c_i32), ("count_pairs", c_i32), ("wait_limit_us", c_i32),
+                ("test_stall_staging", c_i32)]
 
 
 _P = ctypes.c_void_p

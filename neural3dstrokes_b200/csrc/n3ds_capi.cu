@@ -103,6 +103,8 @@ struct Resolved {
   void* const* events;
   int forward_only;
   int count_pairs;
+  unsigned long long wait_limit_ns;
+  int test_stall;
 };
 
 void record_event(const Resolved& rv, int i, cudaStream_t st) {
@@ -156,6 +158,8 @@ Resolved resolve(const n3ds_options_t* o) {
   r.forward_only = o->forward_only != 0;
   r.count_pairs = o->count_pairs != 0;
   r.events = o->timing_events;
+  r.wait_limit_ns = o->wait_limit_us > 0 ? (unsigned long long)o->wait_limit_us * 1000ull : 1000000000ull;
+  r.test_stall = o->test_stall_staging != 0;
   return r;
 }
 
@@ -291,6 +295,8 @@ void n3ds_default_options(n3ds_options_t* opt) {
   opt->warps_bwd = 0;
   opt->forward_only = 0;
   opt->count_pairs = 0;
+  opt->wait_limit_us = 0;
+  opt->test_stall_staging = 0;
 }
 
 size_t n3ds_field_workspace_bytes(const n3ds_batch_t* batch, const n3ds_options_t* opt) {
@@ -313,12 +319,31 @@ static int field_common(const n3ds_batch_t* batch, const n3ds_rays_t* rays, cons
     return fail(N3DS_ERR_INVALID, "strokes: sdf_ids, shape_params, color_params, density, sdf_delta required");
   if (*S > 0 && (strokes->param_stride < 1 || strokes->param_stride > 64))
     return fail(N3DS_ERR_INVALID, "strokes: param_stride must be in [1, 64]");
+  if (strokes && strokes->stroke_window && batch->n_scenes > n3ds::MAX_SCENES_PER_LAUNCH)
+    return fail(N3DS_ERR_UNSUPPORTED, "strokes: a stroke window covers at most " +
+                                          std::to_string(n3ds::MAX_SCENES_PER_LAUNCH) + " scenes");
   *lay = ws_layout(*R, batch->n_samples, *S, mask_words(batch));
   if (!ws || ws_bytes < lay->total)
     return fail(N3DS_ERR_WORKSPACE, "workspace too small: need " + std::to_string(lay->total) + " bytes");
   if (reinterpret_cast<uintptr_t>(ws) % 256)
     return fail(N3DS_ERR_INVALID, "workspace must be 256-byte aligned");
   return N3DS_OK;
+}
+
+// Stroke window of a batch (at most MAX_SCENES_PER_LAUNCH scenes): the device pairs
+// and the scenes' stroke offsets.
+static void fill_window(const n3ds_batch_t* b, const n3ds_strokes_t* s, const int** window, int* n_scenes,
+                        int* begin) {
+  *window = s->stroke_window;
+  *n_scenes = 0;
+  if (!s->stroke_window) return;
+  *n_scenes = b->n_scenes;
+  int off = 0;
+  for (int i = 0; i < b->n_scenes; i++) {
+    begin[i] = off;
+    off += b->n_strokes[i];
+  }
+  begin[b->n_scenes] = off;
 }
 
 static n3ds::PrepLaunch make_prep(const n3ds_strokes_t* s, long long S, const Resolved& rv, char* ws,
@@ -379,6 +404,8 @@ static n3ds::SegLaunch make_seg(const n3ds_batch_t* b, const n3ds_rays_t* rays, 
   L.stats = reinterpret_cast<unsigned long long*>(ws + lay.stats);
   L.block_masks = reinterpret_cast<unsigned*>(ws + lay.masks);
   L.mask_tag = reinterpret_cast<const int*>(ws + lay.mask_tag);
+  L.wait_limit_ns = 1000000000ull;  // one second unless the options say otherwise
+  L.test_stall = 0;
   return L;
 }
 
@@ -406,15 +433,21 @@ int n3ds_field_forward(const n3ds_batch_t* batch, const n3ds_rays_t* rays, const
   if (rc) return rc;
   if (R > 0 && (!rgb || !acc || !depth)) return fail(N3DS_ERR_INVALID, "rgb, acc and depth outputs are required");
   const Resolved rv = resolve(opt);
+  if (strokes->stroke_window && rv.schedule != N3DS_SCHEDULE_SEGMENTS)
+    return fail(N3DS_ERR_UNSUPPORTED, "a stroke window needs the segment schedule");
   char* ws = static_cast<char*>(workspace);
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   // the status word covers one forward and the backward after it (the prep kernel
   // sets bits of it, so it is cleared before that kernel rather than by it)
   N3DS_CUDA_TRY(cudaMemsetAsync(ws + lay.status, 0, sizeof(int32_t), st));
-  n3ds::launch_prep(make_prep(strokes, S, rv, ws, lay, false), st);
+  n3ds::PrepLaunch prep = make_prep(strokes, S, rv, ws, lay, false);
+  fill_window(batch, strokes, &prep.window, &prep.n_win_scenes, prep.win_begin);
+  n3ds::launch_prep(prep, st);
   N3DS_CUDA_TRY(cudaGetLastError());
   record_event(rv, 0, st);
   n3ds::SegLaunch FL = make_seg(batch, rays, ws, lay, 0);
+  FL.wait_limit_ns = rv.wait_limit_ns;
+  FL.test_stall = rv.test_stall;
   FL.skip_alpha = rv.cull_alpha;
   if (!rv.count_pairs) FL.stats = nullptr;
   if (rv.forward_only || rv.schedule != N3DS_SCHEDULE_SEGMENTS) {
@@ -449,10 +482,14 @@ int n3ds_field_backward(const n3ds_batch_t* batch, const n3ds_rays_t* rays, cons
   if (S > 0 && (!grad_shape || !grad_color || !grad_density))
     return fail(N3DS_ERR_INVALID, "grad_shape, grad_color and grad_density outputs are required");
   const Resolved rv = resolve(opt);
+  if (strokes->stroke_window && rv.schedule != N3DS_SCHEDULE_SEGMENTS)
+    return fail(N3DS_ERR_UNSUPPORTED, "a stroke window needs the segment schedule");
   const int compat = rv.grad_mode == N3DS_GRAD_COMPAT;
   char* ws = static_cast<char*>(workspace);
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  n3ds::launch_prep(make_prep(strokes, S, rv, ws, lay, true), st);
+  n3ds::PrepLaunch prep = make_prep(strokes, S, rv, ws, lay, true);
+  fill_window(batch, strokes, &prep.window, &prep.n_win_scenes, prep.win_begin);
+  n3ds::launch_prep(prep, st);
   N3DS_CUDA_TRY(cudaGetLastError());
   if (R > 0) {
     n3ds::RayLaunch L = make_ray(batch, rays, ws, lay, R);
@@ -463,6 +500,8 @@ int n3ds_field_backward(const n3ds_batch_t* batch, const n3ds_rays_t* rays, cons
     N3DS_CUDA_TRY(cudaGetLastError());
   }
   n3ds::SegLaunch SL = make_seg(batch, rays, ws, lay, compat);
+  SL.wait_limit_ns = rv.wait_limit_ns;
+  SL.test_stall = rv.test_stall;
   SL.grad_x = grad_x;
   SL.stats = rv.count_pairs ? reinterpret_cast<unsigned long long*>(ws + lay.stats) + 17 : nullptr;  // pairs
   SL.skip_alpha = rv.cull_alpha;
@@ -486,6 +525,7 @@ int n3ds_field_backward(const n3ds_batch_t* batch, const n3ds_rays_t* rays, cons
     F.grad_delta = grad_sdf_delta;
     F.accumulate = 0;
     F.color_stride = 3;
+    fill_window(batch, strokes, &F.window, &F.n_win_scenes, F.win_begin);
     n3ds::launch_finalize(F, st);
     N3DS_CUDA_TRY(cudaGetLastError());
   }
@@ -594,10 +634,7 @@ int n3ds_field_read_status(void* workspace, int32_t* status, uint64_t* evaluated
 
 size_t n3ds_stroke_workspace_bytes(int64_t n_strokes) {
   if (n_strokes < 0) return 0;
-  // header, records, culling arrays (unused but written by the shared prep kernel),
-  // reduced gradient slots
-  return 256 + align256(size_t(n_strokes) * n3ds::REC_FLOATS * 4) + align256(size_t(n_strokes) * 16) +
-         align256(size_t(n_strokes + 4) * 4) + align256(size_t(n_strokes) * n3ds::GRAD_SLOTS * 4) + 256;
+  return n3ds::stroke_workspace_bytes(size_t(n_strokes));
 }
 
 namespace {

@@ -8,6 +8,7 @@ namespace n3ds {
 // extra kind-word bits set by the prep kernel
 constexpr int K_S3FAC = 1 << 10;  // multi-scale radius factor applies (S3 and inv_scale_radius)
 constexpr int K_S1K = 1 << 11;    // single-scale s is folded into the soft-step slope
+constexpr int K_FROZEN = 1 << 12; // composited, but no gradient of its own and none into grad_x
 
 __device__ __forceinline__ float soft_alpha(int mode, float m) {
   if (mode == STEP_LAPLACE) return laplace_alpha(m);

@@ -539,7 +539,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
               const float kk = h.y * f * c.rinv;
               const float m = -sdf * kk;
               const float a = mode == STEP_HARD ? (sdf <= 0.f ? 1.f : 0.f) : soft_alpha(mode, m);
-              if (__all_sync(0xffffffffu, !c.active || a < L.skip_alpha)) {
+              const bool below = __all_sync(0xffffffffu, !c.active || a < L.skip_alpha);
+              if (below || (kind & K_FROZEN)) {  // the kind word is warp-uniform
                 compose_skip(rec, a, s);
                 continue;
               }
@@ -558,7 +559,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
               const float kk = h.y * c.rinv;
               const float m = -sdf * kk;
               const float a = mode == STEP_HARD ? (sdf <= 0.f ? 1.f : 0.f) : soft_alpha(mode, m);
-              if (__all_sync(0xffffffffu, !c.active || a < L.skip_alpha)) {
+              const bool below = __all_sync(0xffffffffu, !c.active || a < L.skip_alpha);
+              if (below || (kind & K_FROZEN)) {  // the kind word is warp-uniform
                 compose_skip(rec, a, s);
                 continue;
               }
@@ -576,7 +578,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
               const float kk = h.y * c.rinv;
               const float m = -sdf * kk;
               const float a = mode == STEP_HARD ? (sdf <= 0.f ? 1.f : 0.f) : soft_alpha(mode, m);
-              if (__all_sync(0xffffffffu, !c.active || a < L.skip_alpha)) {
+              const bool below = __all_sync(0xffffffffu, !c.active || a < L.skip_alpha);
+              if (below || (kind & K_FROZEN)) {  // the kind word is warp-uniform
                 compose_skip(rec, a, s);
                 continue;
               }
@@ -801,11 +804,26 @@ __global__ void prep_kernel(const PrepLaunch P) {
 #pragma unroll
     for (int j = 0; j < GRAD_SLOTS; j++) g[j] = 0.f;
   }
+  float* rec = P.recs + s * REC_FLOATS;
+  const int wstate = window_state(P.window, P.n_win_scenes, P.win_begin, s);
+  if (wstate == 2) {
+    // Absent stroke (beyond its scene's active count): a culling sphere of radius
+    // -inf keeps it out of every candidate set, and should a sample with NaN
+    // coordinates reach it anyway, the record is a hard-step round cube whose SDF is
+    // +1 everywhere (p = 0, radius -2) with a zero slope: alpha and every gradient
+    // contribution are exactly 0. Its parameters are never read.
+    for (int j = 0; j < REC_FLOATS; j++) rec[j] = 0.f;
+    rec[R_KIND] = __int_as_float(B_ROUND_CUBE | (STEP_HARD << 8));
+    rec[R_BP] = -2.f;
+    P.cull_a[4 * s] = 0.f; P.cull_a[4 * s + 1] = 0.f; P.cull_a[4 * s + 2] = 0.f;
+    P.cull_a[4 * s + 3] = __int_as_float(0xff800000);
+    P.cull_b[s] = 0.f;
+    return;
+  }
   const int sid = P.sdf_ids ? P.sdf_ids[s] : P.uniform_sdf_id;
   const int base = (sid >> 4) & 15;
   const int flags = sid & 15;
   const float* prm = P.shape_params + s * (long long)P.param_stride;
-  float* rec = P.recs + s * REC_FLOATS;
   const int np = sdf_id_param_count(sid);
   const bool s1 = flags & F_S1;
   const bool s3 = !s1 && (flags & F_S3);
@@ -839,6 +857,7 @@ __global__ void prep_kernel(const PrepLaunch P) {
   const bool s3f = s3 && P.inv_scale_radius;
   if (s1k) kind |= K_S1K;
   if (s3f) kind |= K_S3FAC;
+  if (wstate == 1) kind |= K_FROZEN;
   for (int j = 0; j < REC_FLOATS; j++) rec[j] = 0.f;
   rec[R_KIND] = __int_as_float(kind);
   const float* col = P.color_params + s * (long long)P.color_stride;
@@ -1037,6 +1056,16 @@ __global__ void finalize_kernel(const FinalizeLaunch F) {
   const int flags = sid & 15;
   const bool acc = F.accumulate != 0;
   auto put = [&](float* dst, float v) { *dst = acc ? *dst + v : v; };
+  if (window_state(F.window, F.n_win_scenes, F.win_begin, s) != 0) {
+    // frozen or absent: no gradient
+    float* gc = F.grad_color + s * (long long)F.color_stride;
+    put(gc, 0.f); put(gc + 1, 0.f); put(gc + 2, 0.f);
+    if (F.grad_density) put(F.grad_density + s, 0.f);
+    if (F.grad_delta) put(F.grad_delta + s, 0.f);
+    float* out = F.grad_shape + s * (long long)F.param_stride;
+    for (int j = 0; j < F.param_stride; j++) put(out + j, 0.f);
+    return;
+  }
   float* gc = F.grad_color + s * (long long)F.color_stride;
   put(gc, g[G_COLOR]);
   put(gc + 1, g[G_COLOR + 1]);

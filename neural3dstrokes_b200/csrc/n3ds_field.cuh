@@ -59,6 +59,8 @@ struct SegLaunch {
   // forward's prep kernel).
   unsigned* block_masks;
   const int* mask_tag;
+  unsigned long long wait_limit_ns;  // bounded waits give up after this long
+  int test_stall;                    // arm the staging barrier without the copies (test of the wait limit)
   SceneDesc sc[MAX_SCENES_PER_LAUNCH];
 };
 
@@ -106,6 +108,11 @@ struct PrepLaunch {
   unsigned long long* stats;
   int* mask_tag;           // set to mask_tag_value when non-null
   int mask_tag_value;
+  // optional per-scene stroke windows (n3ds_strokes_t::stroke_window): device
+  // (frozen, active) pairs; win_begin[b] .. win_begin[b+1] are scene b's strokes
+  const int* window;
+  int n_win_scenes;
+  int win_begin[MAX_SCENES_PER_LAUNCH + 1];
 };
 
 struct FinalizeLaunch {
@@ -125,7 +132,22 @@ struct FinalizeLaunch {
   float* grad_delta;       // [S] or null
   int accumulate;          // 1: add into the outputs instead of overwriting
   int color_stride;        // floats per stroke row of grad_color (3 for the fused path)
+  // optional stroke windows, as in PrepLaunch: strokes outside [frozen, active) get
+  // zero gradients
+  const int* window;
+  int n_win_scenes;
+  int win_begin[MAX_SCENES_PER_LAUNCH + 1];
 };
+
+// Window state of stroke s: 0 active, 1 frozen (no gradient), 2 absent.
+__device__ __forceinline__ int window_state(const int* window, int n_win_scenes, const int* win_begin, long long s) {
+  if (!window) return 0;
+  int b = 0;
+  while (b + 1 < n_win_scenes && s >= win_begin[b + 1]) b++;
+  const long long i = s - win_begin[b];
+  if (i >= window[2 * b + 1]) return 2;
+  return i < window[2 * b] ? 1 : 0;
+}
 
 // status word bits
 constexpr int ST_BAD_KIND = 1;

@@ -114,4 +114,14 @@ constexpr int G_CTRL = 5;      // quad: 9 + r1, r2 (5..15); cubic / Catmull-Rom:
 
 __device__ __forceinline__ V3 ld3(const float* p) { return v3(p[0], p[1], p[2]); }
 
+// Scratch bytes of the drop-in stroke operators for n strokes: a 256-byte header
+// (status word), the prepared records, culling spheres (float4) and margins (n + 4
+// floats; written by the shared prep kernel), GRAD_SLOTS reduction slots per stroke,
+// and 256 bytes of tail padding, each block 256-byte aligned. The one formula behind
+// n3ds_stroke_workspace_bytes and the static scratch of n3ds_stroke_forward_static.
+__host__ __device__ constexpr size_t stroke_workspace_bytes(size_t n) {
+  return 256 + ((n * REC_FLOATS * 4 + 255) & ~size_t(255)) + ((n * 16 + 255) & ~size_t(255)) +
+         (((n + 4) * 4 + 255) & ~size_t(255)) + ((n * GRAD_SLOTS * 4 + 255) & ~size_t(255)) + 256;
+}
+
 }  // namespace n3ds

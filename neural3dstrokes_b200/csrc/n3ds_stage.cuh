@@ -42,12 +42,12 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-// Wait for the mbarrier phase with a one-second limit; false on timeout.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase) {
+// Wait for the mbarrier phase for at most limit_ns; false on timeout.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase, unsigned long long limit_ns) {
   if (mbar_try_wait(bar, phase)) return true;
   uint64_t t0 = globaltimer_ns();
   while (!mbar_try_wait(bar, phase)) {
-    if (globaltimer_ns() - t0 > 1000000000ull) return false;
+    if (globaltimer_ns() - t0 > limit_ns) return false;
   }
   return true;
 }
@@ -108,7 +108,12 @@ __device__ __forceinline__ Stage carve(unsigned char* smem, int cap, bool with_g
 }
 
 // Stage the scene's current chunk: records and culling spheres by bulk copy,
-// culling margins by plain loads. Returns false on an mbarrier timeout.
+// culling margins by plain loads. Returns false on an mbarrier timeout. A timeout is
+// terminal for the launch: the caller sets ST_WAIT_TIMEOUT in the status word and its
+// CTA returns, so the host treats every output of the launch as invalid; the copies
+// of a barrier that did not complete within the limit (one second by default) are
+// not waited for. (test_stall arms the barrier without issuing the copies: every
+// wait runs out and no copy is in flight when the CTA leaves.)
 __device__ __forceinline__ bool stage_chunk(const SegLaunch& L, const SceneDesc& sc, const Stage& S, uint64_t* bar,
                             uint32_t& phase, int* s_fail) {
   const int n = sc.chunk_n;
@@ -119,11 +124,13 @@ __device__ __forceinline__ bool stage_chunk(const SegLaunch& L, const SceneDesc&
       const uint32_t b_rec = uint32_t(n) * REC_FLOATS * 4;
       const uint32_t b_cull = uint32_t(n) * 16;
       mbar_expect_tx(bar, b_rec + b_cull);
-      bulk_g2s(S.recs, L.recs + g0 * REC_FLOATS, b_rec, bar);
-      bulk_g2s(S.cull_a, L.cull_a + g0 * 4, b_cull, bar);
+      if (!L.test_stall) {
+        bulk_g2s(S.recs, L.recs + g0 * REC_FLOATS, b_rec, bar);
+        bulk_g2s(S.cull_a, L.cull_a + g0 * 4, b_cull, bar);
+      }
     }
     for (int i = threadIdx.x; i < n; i += blockDim.x) S.cull_b[i] = L.cull_b[g0 + i];
-    if (!mbar_wait_bounded(bar, phase)) *s_fail = 1;
+    if (!mbar_wait_bounded(bar, phase, L.wait_limit_ns)) *s_fail = 1;
     phase ^= 1u;
   }
   __syncthreads();

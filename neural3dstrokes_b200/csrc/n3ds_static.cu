@@ -14,11 +14,14 @@
 // The first call on a device (with that device current) looks up the array's device
 // address with cudaGetSymbolAddress, which may load the module; that one-time setup
 // is not a stream operation, so a caller that records the call into a stream capture
-// makes one call on that device before capturing.
+// makes one call on that device before capturing. The address is kept for the life
+// of the process: after cudaDeviceReset (which rebuilds the device's context and
+// modules) this entry point must not be called again.
 #include <mutex>
 #include <string>
 
 #include "../../include/n3ds.h"
+#include "n3ds_record.cuh"
 
 namespace n3ds {
 int report_error(int code, const std::string& msg);  // sets n3ds_last_error (n3ds_capi.cu)
@@ -26,16 +29,12 @@ int report_error(int code, const std::string& msg);  // sets n3ds_last_error (n3
 
 namespace {
 
-constexpr size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
-
-// Same sum as n3ds_stroke_workspace_bytes(n): header, 64-float records, culling
-// spheres (float4), culling margins (n + 4 floats), 32 reduction slots per stroke,
-// tail padding.
-constexpr size_t stroke_scratch_bytes(size_t n) {
-  return 256 + align256(n * 64 * 4) + align256(n * 16) + align256((n + 4) * 4) + align256(n * 32 * 4) + 256;
-}
-
-constexpr size_t kScratchBytes = stroke_scratch_bytes(N3DS_STATIC_MAX_STROKES);
+// The layout n3ds_stroke_forward uses for N3DS_STATIC_MAX_STROKES strokes (one formula
+// for both, built from the record and slot sizes).
+constexpr size_t kScratchBytes = n3ds::stroke_workspace_bytes(N3DS_STATIC_MAX_STROKES);
+static_assert(kScratchBytes >= n3ds::stroke_workspace_bytes(N3DS_STATIC_MAX_STROKES),
+              "static scratch must hold the stroke workspace of N3DS_STATIC_MAX_STROKES strokes");
+static_assert(kScratchBytes % 256 == 0, "static scratch keeps the workspace's 256-byte blocks aligned");
 
 __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 

@@ -30,6 +30,8 @@ class FieldOptions:
     grad_mode: str = "exact"   # 'exact' or 'compat'
     forward_only: bool = False  # no backward follows: skip the bookkeeping the backward reads
     count_pairs: bool = False   # count evaluated pairs (statistics; a few % of the forward's work)
+    wait_limit_us: int = 0      # limit of the device's bounded waits (0: one second)
+    test_stall_staging: bool = False  # test of the wait limit only: every staging wait runs out
 
     def c(self, events=None):
         """ctypes options; ``events``: optional 4 torch.cuda.Event(enable_timing=True)
@@ -45,7 +47,8 @@ class FieldOptions:
         return _lib.Options(float(self.cull_alpha), int(self.chunk_fwd), int(self.chunk_bwd), int(self.warps),
                             {"auto": 0, "segments": 1, "runs": 2}[self.schedule],
                             _lib.N3DS_GRAD_COMPAT if self.grad_mode == "compat" else _lib.N3DS_GRAD_EXACT, ev,
-                            int(self.warps_bwd), int(bool(self.forward_only)), int(bool(self.count_pairs)))
+                            int(self.warps_bwd), int(bool(self.forward_only)), int(bool(self.count_pairs)),
+                            int(self.wait_limit_us), int(bool(self.test_stall_staging)))
 
 
 class _Native:
@@ -53,7 +56,7 @@ class _Native:
 
     def __init__(self, scene_rays, scene_strokes, n_samples, x, radius, tdist, dirs, bg, bg_value, opaque,
                  sdf_ids, shape_params, color_params, density, delta, laplace, inv_scale, options, origins=None,
-                 radii=None):
+                 radii=None, window=None):
         n = len(scene_rays)
         self.nr = (ctypes.c_int64 * n)(*[int(v) for v in scene_rays])
         self.ns = (ctypes.c_int32 * n)(*[int(v) for v in scene_strokes])
@@ -62,7 +65,7 @@ class _Native:
                               float(bg_value), int(bool(opaque)), _lib.ptr(origins), _lib.ptr(radii))
         self.strokes = _lib.Strokes(_lib.ptr(sdf_ids), _lib.ptr(shape_params), int(shape_params.shape[1]),
                                     _lib.ptr(color_params), _lib.ptr(density), _lib.ptr(delta), int(bool(laplace)),
-                                    int(bool(inv_scale)))
+                                    int(bool(inv_scale)), _lib.ptr(window))
         self.opt = options.c()
 
     def ws_bytes(self):
@@ -78,7 +81,8 @@ def _f32(t, name):
 class _FieldFn(torch.autograd.Function):
     @staticmethod
     def forward(ctx, x, radius, tdist, dirs, shape_params, color_params, density, delta, bg_t, sdf_ids,
-                scene_rays, scene_strokes, bg_value, opaque, laplace, inv_scale, options, origins=None, radii=None):
+                scene_rays, scene_strokes, bg_value, opaque, laplace, inv_scale, options, origins=None, radii=None,
+                window=None):
         R, N = tdist.shape[0], tdist.shape[1] - 1
         tdist, dirs = _f32(tdist, "tdist"), _f32(dirs, "dirs")
         if x is not None:
@@ -91,11 +95,16 @@ class _FieldFn(torch.autograd.Function):
         if sdf_ids.dtype != torch.int32 or not sdf_ids.is_cuda:
             raise RuntimeError("sdf_ids must be a CUDA int32 tensor")
         sdf_ids = sdf_ids.contiguous()
+        if window is not None:
+            if window.dtype != torch.int32 or not window.is_cuda or window.numel() != 2 * len(scene_rays):
+                raise RuntimeError("stroke_window must be a CUDA int32 tensor of (frozen, active) per scene")
+            window = window.contiguous()
         bg_c = _f32(bg_t, "bg") if bg_t is not None else None
         # without any input that needs a gradient no backward can follow
         fwd_opts = options if any(ctx.needs_input_grad) else dataclasses.replace(options, forward_only=True)
         nat = _Native(scene_rays, scene_strokes, N, x, radius, tdist, dirs, bg_c, bg_value, opaque, sdf_ids,
-                      shape_params, color_params, density, delta, laplace, inv_scale, fwd_opts, origins, radii)
+                      shape_params, color_params, density, delta, laplace, inv_scale, fwd_opts, origins, radii,
+                      window)
         lib = _lib.load()
         dev = tdist.device
         with torch.cuda.device(dev):
@@ -111,7 +120,7 @@ class _FieldFn(torch.autograd.Function):
                                         _lib.ptr(ws), ws_bytes, _lib.stream_ptr())
         _lib.check(rc)
         ctx.save_for_backward(x, radius, tdist, dirs, shape_params, color_params, density, delta, sdf_ids, origins,
-                              radii)
+                              radii, window)
         ctx.bg = bg_c
         ctx.ws, ctx.ws_bytes = ws, ws_bytes
         ctx.meta = (scene_rays, scene_strokes, bg_value, opaque, laplace, inv_scale, options)
@@ -119,12 +128,13 @@ class _FieldFn(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, g_rgb, g_acc, g_depth):
-        x, radius, tdist, dirs, shape_params, color_params, density, delta, sdf_ids, origins, radii = \
+        x, radius, tdist, dirs, shape_params, color_params, density, delta, sdf_ids, origins, radii, window = \
             ctx.saved_tensors
         scene_rays, scene_strokes, bg_value, opaque, laplace, inv_scale, options = ctx.meta
         N = tdist.shape[1] - 1
         nat = _Native(scene_rays, scene_strokes, N, x, radius, tdist, dirs, ctx.bg, bg_value, opaque, sdf_ids,
-                      shape_params, color_params, density, delta, laplace, inv_scale, options, origins, radii)
+                      shape_params, color_params, density, delta, laplace, inv_scale, options, origins, radii,
+                      window)
         gx = torch.empty_like(x) if (x is not None and ctx.needs_input_grad[0]) else None
         gshape = torch.empty_like(shape_params)
         gcol = torch.empty_like(color_params)
@@ -139,14 +149,15 @@ class _FieldFn(torch.autograd.Function):
                                          _lib.ptr(gdel), _lib.ptr(ctx.ws), ctx.ws_bytes, _lib.stream_ptr())
         _lib.check(rc)
         return (gx, None, None, None, gshape, gcol, gden, gdel, None, None, None, None, None, None, None, None,
-                None, None, None)
+                None, None, None, None)
 
 
 def render_strokes(x: torch.Tensor, radius: torch.Tensor, tdist: torch.Tensor, dirs: torch.Tensor,
                    shape_params: torch.Tensor, sdf_ids: torch.Tensor, color_params: torch.Tensor,
                    density: torch.Tensor, sdf_delta, use_laplace_transform: bool = True,
                    inv_scale_radius: bool = True, bg=1.0, opaque_background: bool = False,
-                   options: Optional[FieldOptions] = None, scene_sizes: Optional[Sequence] = None):
+                   options: Optional[FieldOptions] = None, scene_sizes: Optional[Sequence] = None,
+                   stroke_window: Optional[torch.Tensor] = None):
     """Render rays through a stroke field.
 
     x [R,N,3] sample positions, radius [R,N], tdist [R,N+1], dirs [R,3];
@@ -154,7 +165,11 @@ def render_strokes(x: torch.Tensor, radius: torch.Tensor, tdist: torch.Tensor, d
     color_params [S,3], density [S] (already multiplied by density_scale), sdf_delta a
     float, a 0-d tensor or a per-stroke [S] tensor. ``scene_sizes``: list of
     (n_rays, n_strokes) for a batch of scenes concatenated along rays and strokes
-    (default: one scene). bg: float or [R,3] tensor.
+    (default: one scene). bg: float or [R,3] tensor. ``stroke_window``: optional CUDA
+    int32 [n_scenes, 2] of (frozen, active) per scene, read on the device: strokes at
+    or beyond ``active`` are absent, strokes below ``frozen`` are composited but get
+    no gradient and pass none to ``x`` (the truncation of
+    StrokeField.predict_density, models.py:665-702, without a host read of the count).
     Returns rgb [R,3], acc [R], depth [R].
     """
     S = int(sdf_ids.numel())
@@ -182,7 +197,7 @@ def render_strokes(x: torch.Tensor, radius: torch.Tensor, tdist: torch.Tensor, d
     opts = options or FieldOptions()
     return _FieldFn.apply(x, radius, tdist, dirs, shape_params, color_params, density, delta, bg_t, sdf_ids,
                           scene_rays, scene_strokes, bg_value, opaque_background, use_laplace_transform,
-                          inv_scale_radius, opts)
+                          inv_scale_radius, opts, None, None, stroke_window)
 
 
 def render_rays(origins: torch.Tensor, directions: torch.Tensor, radii: torch.Tensor, tdist: torch.Tensor,

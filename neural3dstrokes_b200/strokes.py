@@ -75,6 +75,18 @@ def make_sdf_id(base_name, t, r, s1, s3):
     return (_BASE[base_name] << 4) | (1 if t else 0) | (2 if r else 0) | (4 if s1 else 0) | (8 if s3 else 0)
 
 
+def sdf_id_of(shape_type: str) -> int:
+    """The sdf_id get_stroke binds for a shape type."""
+    base, _, _, t, r, s1, s3 = _SHAPES[shape_type]
+    return make_sdf_id(base, t, r, s1, s3)
+
+
+def num_shape_params(shape_type: str) -> int:
+    """The shape-parameter count (dim_shape) get_stroke returns for a shape type."""
+    base, base_ranges, _, t, r, s1, s3 = _SHAPES[shape_type]
+    return len(base_ranges) + (1 if s1 else 3 if s3 else 0) + (3 if r else 0) + (3 if t else 0)
+
+
 class _StrokeFn(torch.autograd.Function):
     """alpha / colour of a batch of strokes of one sdf_id at the samples
     (reference _stroke_fn, strokes.py:109-224)."""

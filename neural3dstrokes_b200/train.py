@@ -215,11 +215,13 @@ class HostPipeline:
 
     ``inputs`` / ``outputs``: the device tensors the captured step reads / writes
     (for a BatchedField: rays, upstream gradients, parameters / rgb, acc, depth,
-    parameter gradients). A copy stream uploads step i+1's host inputs into one of two
-    device staging sets while step i computes; the compute stream copies the staged
-    inputs into the step's own buffers (device to device), replays the step and copies
-    the results into an output staging set, which the copy stream downloads to the
-    host. Events order every hand-over. Usage::
+    parameter and position gradients). An upload stream copies step i+1's host inputs
+    into one of two device staging sets while step i computes; the compute stream
+    copies the staged inputs into the step's own buffers (device to device), replays
+    the step and copies the results into an output staging set, which a download
+    stream copies to the host. Uploads and downloads run on separate streams, so the
+    two directions of the host link (separate copy engines) overlap each other as well
+    as the compute. Events order every hand-over. Usage::
 
         pipe.upload(0, host_in)
         for i in range(n):
@@ -235,7 +237,8 @@ class HostPipeline:
         self.outputs = list(outputs)
         self.device = torch.device(device)
         self.compute = torch.cuda.current_stream(self.device)
-        self.copy = torch.cuda.Stream(self.device)
+        self.copy = torch.cuda.Stream(self.device)   # host -> device
+        self.down = torch.cuda.Stream(self.device)   # device -> host
         self.stage_in = [[torch.empty_like(t) for t in self.inputs] for _ in range(2)]
         self.stage_out = [[torch.empty_like(t) for t in self.outputs] for _ in range(2)]
         self.loaded = [torch.cuda.Event() for _ in range(2)]   # upload into input stage k done
@@ -271,13 +274,14 @@ class HostPipeline:
         for s, d in zip(self.stage_out[k], self.outputs):
             s.copy_(d, non_blocking=True)
         self.stored[k].record(c)
-        self.copy.wait_event(self.stored[k])
-        with torch.cuda.stream(self.copy):
+        self.down.wait_event(self.stored[k])
+        with torch.cuda.stream(self.down):
             for h, s in zip(host_outputs, self.stage_out[k]):
                 h.copy_(s, non_blocking=True)
-        self.fetched[k].record(self.copy)
+        self.fetched[k].record(self.down)
         self.fetched_used[k] = True
 
     def synchronize(self):
         self.copy.synchronize()
+        self.down.synchronize()
         self.compute.synchronize()

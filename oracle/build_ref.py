@@ -19,7 +19,11 @@ the same way, as backend.py:33-39 of that package does, into ``oracle/_ref/grid/
 as ``_gridencoder*.so``; its flags ask for C++14, which torch's headers no longer
 accept, so it is compiled as C++17 like the strokelib.
 
-Usage: python oracle/build_ref.py [--ref /root/reference] [--jobs 3] [--only strokes|grid]
+The checkout is found through ``reference_root()``: the ``N3DS_REFERENCE``
+environment variable, else the default location below (this recipe's only machine
+path).
+
+Usage: python oracle/build_ref.py [--ref PATH] [--jobs 3] [--only strokes|grid]
 """
 import argparse
 import glob
@@ -29,6 +33,14 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
 SOURCES = ["strokes_forward.cu", "strokes_backward.cu", "compositing.cu", "bindings.cpp"]
+
+
+DEFAULT_REFERENCE = "/root/reference"
+
+
+def reference_root():
+    """The read-only reference checkout: $N3DS_REFERENCE, else DEFAULT_REFERENCE."""
+    return os.environ.get("N3DS_REFERENCE") or DEFAULT_REFERENCE
 
 
 GRID_OUT = os.path.join(OUT, "grid")
@@ -49,7 +61,8 @@ def grid_built_path():
     return hits[0] if hits else None
 
 
-def build_grid(ref_root="/root/reference", jobs=3, verbose=True):
+def build_grid(ref_root=None, jobs=3, verbose=True):
+    ref_root = ref_root or reference_root()
     src_dir = os.path.join(ref_root, "source", "gridencoder", "src")
     if not os.path.isdir(src_dir):
         raise FileNotFoundError(f"reference gridencoder sources not found at {src_dir}")
@@ -67,7 +80,8 @@ def build_grid(ref_root="/root/reference", jobs=3, verbose=True):
     return grid_built_path()
 
 
-def build(ref_root="/root/reference", jobs=3, verbose=True):
+def build(ref_root=None, jobs=3, verbose=True):
+    ref_root = ref_root or reference_root()
     src_dir = os.path.join(ref_root, "source", "strokelib", "src")
     if not os.path.isdir(src_dir):
         raise FileNotFoundError(f"reference strokelib sources not found at {src_dir}")
@@ -88,7 +102,7 @@ def build(ref_root="/root/reference", jobs=3, verbose=True):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=None, help="reference checkout (default: reference_root())")
     ap.add_argument("--jobs", type=int, default=3)
     ap.add_argument("--only", choices=["strokes", "grid"], default=None)
     a = ap.parse_args()

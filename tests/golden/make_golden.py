@@ -10,6 +10,14 @@ Three sources, each a seeded, small input set:
             source/utils/render.py and runs compute_alpha_weights (plain and opaque
             background) and volumetric_rendering in float64 on seeded inputs.
             -> render_golden.npz
+--cast      (CPU, needs the reference checkout): imports the reference
+            source/utils/render.py and runs cast_rays (render.py:5-26) in float32 on
+            rays of the benchmark geometry. -> cast_golden.npz
+--strokespy (CPU, needs the reference checkout): imports the reference
+            source/strokelib/strokes.py with a recording ``_strokelib`` (the oracle's
+            float32 port) and drives get_stroke / stroke_fn / compose_strokes and the
+            backward per shape type as models.py does; records every backend call's
+            arguments and results. -> strokes_py_calls.json, strokes_py_calls.npz
 --compose   (CPU, needs the reference checkout): imports the reference strokes.py with a
             stub ``_strokelib`` and runs its torch compositing modes (max,
             max_density_weighted, softmax, softmax_density_weighted,
@@ -36,9 +44,9 @@ Three sources, each a seeded, small input set:
             linear and smoothstep, both corner alignments, D 2 and 3, C 1 to 8, in
             float32, float64 and float16. -> grid_golden.npz
 
-Usage: python tests/golden/make_golden.py [--layouts] [--render] [--compose] [--stepfun] [--strokelib]
+Usage: python tests/golden/make_golden.py [--layouts] [--render] [--cast] [--strokespy] [--compose] [--stepfun] [--strokelib]
        [--gridlayout] [--grid]
-       [--ref /root/reference] [--out tests/golden]
+       [--ref PATH] [--out tests/golden]
 """
 import argparse
 import copy
@@ -133,6 +141,142 @@ def make_render(ref_root, out):
                         depth=rend["depth"].numpy(), acc=rend["acc"].numpy(), rgb_opaque=rend1["rgb"].numpy(),
                         depth_opaque=rend1["depth"].numpy(), acc_opaque=rend1["acc"].numpy())
     print("render golden written")
+
+
+def make_cast(ref_root, out):
+    """The reference cast_rays (render.py:5-26) in float32 on rays of the benchmark
+    geometry (origins on the radius-4 sphere, jittered directions, stratified fence
+    posts in [2, 6]) with per-ray base radii [R, 1] as batch['radii']."""
+    sys.path.insert(0, ref_root)
+    from source.utils import render as ref_render  # noqa: E402
+    from neural3dstrokes_b200 import scenes
+    g = torch.Generator().manual_seed(4321)
+    R, N = 256, 48
+    rays = scenes.make_rays(R, N, g)
+    radii = (torch.rand(R, 1, generator=g) * 0.004 + 0.001).float()
+    tdist, origins, dirs = rays.tdist.float(), rays.origins.float(), rays.dirs.float()
+    coords, radius, t = ref_render.cast_rays(tdist, origins, dirs, radii)
+    np.savez_compressed(os.path.join(out, "cast_golden.npz"), tdist=tdist.numpy(), origins=origins.numpy(),
+                        directions=dirs.numpy(), radii=radii.numpy(), coords=coords.numpy(),
+                        radius=radius.numpy(), t=t.numpy())
+    print("cast golden written")
+
+
+# output arguments (written by the call) of each _strokelib function, by position
+STROKELIB_OUTPUTS = {"stroke_forward": (0, 1, 2, 3), "stroke_backward": (0, 1, 2), "compose_forward": (0, 1),
+                     "compose_backward": (0, 1, 2)}
+
+
+class _RecordingBackend(types.ModuleType):
+    """A ``_strokelib`` module whose four functions compute with the oracle's float32
+    port on the host and record every call the reference strokes.py makes: each
+    argument's shape, dtype and value (outputs before and after the call)."""
+
+    def __init__(self):
+        super().__init__("_strokelib")
+        self.calls, self.arrays = [], {}
+        from oracle import strokefield as sf
+        self.sf = sf
+
+    def _record(self, name, args, fn):
+        k = len(self.calls)
+        outs = STROKELIB_OUTPUTS[name]
+        meta = []
+        for i, a in enumerate(args):
+            if torch.is_tensor(a):
+                key = f"c{k}/a{i}"
+                meta.append({"tensor": key, "shape": list(a.shape), "dtype": str(a.dtype).replace("torch.", ""),
+                             "contiguous": bool(a.is_contiguous()), "output": i in outs,
+                             "zero_before": bool(a.numel() == 0 or not bool(a.any()))})
+                if i not in outs:
+                    self.arrays[key] = a.detach().numpy().copy()
+            else:
+                meta.append({"value": a, "type": type(a).__name__})
+        fn()
+        for i in outs:
+            self.arrays[f"c{k}/a{i}"] = args[i].detach().numpy().copy()
+        self.calls.append({"fn": name, "args": meta})
+
+    def stroke_forward(self, *args):
+        def run():
+            a, c, sdf, tex, x, r, vd, ps, cp, sid, cid, delta, lap, inv = args
+            aa, cc = self.sf.stroke_forward(x, r, ps, cp, sid, delta, lap, inv, color_id=cid, viewdir=vd)
+            a.copy_(aa)
+            c.copy_(cc)
+        self._record("stroke_forward", args, run)
+
+    def stroke_backward(self, *args):
+        def run():
+            gs, gcol, gx, ga, gc, gsdf, x, r, vd, a, ps, cp, sid, cid, delta, lap, inv = args
+            s_, c_, x_ = self.sf.stroke_backward_compat(ga, gc, x, r, a, ps, cp, sid, delta, lap, inv)
+            gs += s_
+            gcol += c_
+            if gx.numel():
+                gx += x_
+        self._record("stroke_backward", args, run)
+
+    def compose_forward(self, *args):
+        def run():
+            d, c, alphas, colors, dp = args
+            dd, cc = self.sf.compose_forward(alphas, colors, dp)
+            d.copy_(dd)
+            c.copy_(cc)
+        self._record("compose_forward", args, run)
+
+    def compose_backward(self, *args):
+        def run():
+            ga, gc, gdp, gd, gcol, alphas, colors, dp = args
+            a_, c_, p_ = self.sf.compose_backward_compat(gd, gcol, alphas, colors, dp)
+            ga += a_
+            gc += c_
+            gdp += p_
+        self._record("compose_backward", args, run)
+
+
+def make_strokes_py(ref_root, out):
+    """The reference's own strokes.py (source/strokelib/strokes.py) driven as the
+    model drives it (models.py:681-684, 709): per shape type, get_stroke(type,
+    'constant_rgb', 'recon'), stroke_fn(coords, radius, viewdirs, shape, colour,
+    sdf_delta, laplace, inv_scale_radius, True, False), compose_strokes(..., 'over'),
+    and a backward. Its backend is a recording module, so the log holds exactly the
+    calls strokes.py makes into _strokelib. -> strokes_py_calls.json / .npz"""
+    from neural3dstrokes_b200 import scenes
+    rec = _RecordingBackend()
+    saved = sys.modules.get("_strokelib")
+    sys.modules["_strokelib"] = rec
+    try:
+        path = os.path.join(ref_root, "source", "strokelib", "strokes.py")
+        spec = importlib.util.spec_from_file_location("ref_strokes_recorded", path)
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        assert mod._backend is rec
+        g = torch.Generator().manual_seed(99)
+        groups = []
+        for kind in scenes.EVERY_KIND:
+            stroke_fn, d_shape, _, _, _, _, _ = mod.get_stroke(kind, "constant_rgb", "recon")
+            R, N, S = 4, 8, 5
+            sc = scenes.make_strokes([kind] * S, g)
+            rays = scenes.make_rays(R, N, g)
+            x = rays.x.clone().requires_grad_(True)
+            shape = sc.shape_params[:, :d_shape].clone().requires_grad_(True)
+            color = sc.color_params.clone().requires_grad_(True)
+            dens = (torch.rand(S, generator=g) * 0.8 + 0.2).requires_grad_(True)
+            first = len(rec.calls)
+            alphas, colors, _, _ = stroke_fn(x, rays.radius, rays.dirs, shape, color, 0.05, True, True, True, False)
+            density, col = mod.compose_strokes(alphas, colors, dens * 20.0, "over")
+            w1, w2 = torch.randn(density.shape, generator=g), torch.randn(col.shape, generator=g)
+            ((density * w1).sum() + (col * w2).sum()).backward()
+            groups.append({"kind": kind, "calls": list(range(first, len(rec.calls)))})
+    finally:
+        if saved is None:
+            sys.modules.pop("_strokelib", None)
+        else:
+            sys.modules["_strokelib"] = saved
+    with open(os.path.join(out, "strokes_py_calls.json"), "w") as f:
+        json.dump({"source": "source/strokelib/strokes.py (reference), recorded backend", "groups": groups,
+                   "calls": rec.calls}, f)
+    np.savez_compressed(os.path.join(out, "strokes_py_calls.npz"), **rec.arrays)
+    print("strokes.py call log written:", len(rec.calls), "calls")
 
 
 def make_stepfun(ref_root, out):
@@ -408,19 +552,28 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--layouts", action="store_true")
     ap.add_argument("--render", action="store_true")
+    ap.add_argument("--cast", action="store_true")
+    ap.add_argument("--strokespy", action="store_true")
     ap.add_argument("--strokelib", action="store_true")
     ap.add_argument("--compose", action="store_true")
     ap.add_argument("--stepfun", action="store_true")
     ap.add_argument("--gridlayout", action="store_true")
     ap.add_argument("--grid", action="store_true")
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=None, help="reference checkout (default: oracle.build_ref.reference_root())")
     ap.add_argument("--out", default=HERE)
     a = ap.parse_args()
+    if a.ref is None:
+        from oracle.build_ref import reference_root
+        a.ref = reference_root()
     os.makedirs(a.out, exist_ok=True)
     if a.layouts:
         make_layouts(a.ref, a.out)
     if a.render:
         make_render(a.ref, a.out)
+    if a.cast:
+        make_cast(a.ref, a.out)
+    if a.strokespy:
+        make_strokes_py(a.ref, a.out)
     if a.strokelib:
         make_strokelib(a.out)
     if a.compose:

@@ -123,3 +123,44 @@ def test_batched_field_cast_mode(cuda, schedule):
     for name in ("grad_shape", "grad_color", "grad_density", "grad_delta"):
         assert rel(getattr(a, name), getattr(b, name)) < 1e-6, name
     assert a.status()[0] == 0
+
+
+def test_in_kernel_cast_matches_reference_cast_rays_golden(cuda):
+    """The samples the kernels cast from the rays are the reference cast_rays' own
+    (tests/golden/cast_golden.npz, float32 outputs of render.py:5-26): render_rays on
+    the golden rays equals render_strokes on the golden coords and radii, forward bit
+    for bit and gradients to 1e-6, and both are within 1e-5 / 1e-4 of the float64
+    oracle evaluated at the golden samples."""
+    import os
+
+    import numpy as np
+
+    from helpers import GRAD_TOL, FWD_TOL, oracle_grads
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "cast_golden.npz"))
+    t = lambda k: torch.from_numpy(z[k])
+    R = t("tdist").shape[0]
+    g = torch.Generator().manual_seed(6)
+    sc = scenes.make_strokes([scenes.MIXED_PRIMS[int(i)] for i in torch.randint(0, 6, (48,), generator=g)], g)
+    delta = 2.0  # sample radii are ~0.01: a soft width comparable to the strokes
+    up = [torch.randn(R, 3, generator=g), torch.randn(R, generator=g)]
+    outs, grads = [], []
+    for mode in ("cast", "explicit"):
+        sp, col, den, dl = params(sc, cuda, delta)
+        ids = sc.sdf_ids.to(cuda)
+        if mode == "cast":
+            out = render_rays(t("origins").to(cuda), t("directions").to(cuda), t("radii").to(cuda),
+                              t("tdist").to(cuda), sp, ids, col, den, dl)
+        else:
+            out = render_strokes(t("coords").to(cuda), t("radius").to(cuda), t("tdist").to(cuda),
+                                 t("directions").to(cuda), sp, ids, col, den, dl)
+        ((out[0] * up[0].to(cuda)).sum() + (out[1] * up[1].to(cuda)).sum()).backward()
+        outs.append([o.detach() for o in out])
+        grads.append([p.grad for p in (sp, col, den, dl)])
+    for a, b in zip(*outs):
+        assert torch.equal(a, b)
+    for a, b in zip(*grads):
+        assert rel(a, b) < 1e-6
+    rays = scenes.RaySet(t("origins"), t("directions"), t("tdist"), t("coords"), t("radius"))
+    ref = oracle_grads(sc, rays, up[0], up[1], torch.zeros(R), delta=delta)
+    assert rel(outs[0][0], ref["rgb"]) < FWD_TOL and rel(outs[0][1], ref["acc"]) < FWD_TOL
+    assert rel(grads[0][0], ref["shape"]) < GRAD_TOL and rel(grads[0][1], ref["color"]) < GRAD_TOL

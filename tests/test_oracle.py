@@ -249,3 +249,12 @@ def test_texcoord_matches_reference_strokelib(kind):
     d = (tex - ref).abs()
     d = torch.minimum(d, (1.0 - d).abs())  # the seam of v
     assert float(d.max()) < 1e-5, float(d.max())
+
+
+def test_cast_rays_restatement_matches_reference_cast_rays():
+    """oracle.render.cast_rays against the reference cast_rays' float32 outputs
+    (tests/golden/cast_golden.npz, render.py:5-26): bit for bit."""
+    z = np.load(os.path.join(GOLDEN, "cast_golden.npz"))
+    t = lambda k: torch.from_numpy(z[k])
+    coords, radius, tm = orr.cast_rays(t("tdist"), t("origins"), t("directions"), t("radii"))
+    assert torch.equal(coords, t("coords")) and torch.equal(radius, t("radius")) and torch.equal(tm, t("t"))

@@ -1,0 +1,227 @@
+"""The predict_density drop-in (neural3dstrokes_b200/strokefield.py) against the
+reference chain it replaces: StrokeField.predict_density (models.py:660-711) with
+the reference CUDA op (oracle/_ref) for stroke_fn / compose_strokes, then the render
+math (render.py:29-88, its float64-pinned restatement), and against the float64
+oracle.
+
+Cases: stroke_step below and above max_opt_strokes (fixed strokes composited first
+without gradient), training (sdf_delta annealed by stroke_step / max_num_strokes) and
+eval (sdf_delta_eval), the bbox warp, an empty field (stroke_step 0), and no host
+synchronisation in forward + backward.
+
+Tolerances (helpers.rel, normwise): forward 1e-5, gradients 1e-4. Against the
+reference op the gradients are the compat mode's (the reference's formulas).
+"""
+import pytest
+import torch
+
+from helpers import FWD_TOL, GRAD_TOL, rel
+from neural3dstrokes_b200 import scenes
+from neural3dstrokes_b200 import strokes as st
+from neural3dstrokes_b200.field import FieldOptions
+from neural3dstrokes_b200.strokefield import StrokeField, warp_coords
+from oracle import cpu_port
+from oracle import render as orr
+
+pytestmark = pytest.mark.gpu
+
+MAX, MAX_OPT = 64, 40
+
+
+def make_field(shape_type, step, training, dev, limit=None):
+    f = StrokeField(shape_type, max_num_strokes=MAX, max_opt_strokes=MAX_OPT, density_scale=20.0, sdf_delta=0.08,
+                    sdf_delta_eval=0.02, use_laplace_transform=True, inv_scale_radius=True, bbox_size=4.0,
+                    stroke_step_limit=limit).to(dev)
+    g = torch.Generator().manual_seed(3)
+    sc = scenes.make_strokes([shape_type] * MAX, g)
+    d = st.num_shape_params(shape_type)
+    with torch.no_grad():
+        f.shape_params.copy_(sc.shape_params[:, :d])
+        f.color_params.copy_(sc.color_params)
+        f.density_params.copy_(torch.rand(MAX, generator=g) * 0.8 + 0.2)
+        f.stroke_step.fill_(step)
+    f.train(training)
+    return f
+
+
+def rays_for(dev, n_rays=48, n_samples=40):
+    g = torch.Generator().manual_seed(8)
+    r = scenes.make_rays(n_rays, n_samples, g)
+    # the warp halves world coordinates (bbox 4): place the strokes' world box at [-2, 2]
+    return r.x.to(dev) * 2.0, r.radius.to(dev), r.tdist.to(dev), r.dirs.to(dev)
+
+
+def upstream(R, dev):
+    g = torch.Generator().manual_seed(9)
+    return (torch.randn(R, 3, generator=g).to(dev), torch.randn(R, generator=g).to(dev),
+            torch.randn(R, generator=g).to(dev))
+
+
+def window_of(f):
+    step = int(f.stroke_step)
+    fixed = max(0, step - f.max_opt_strokes)
+    if f.stroke_step_limit is not None:
+        step, fixed = min(step, f.stroke_step_limit), min(fixed, f.stroke_step_limit)
+    return fixed, step
+
+
+def delta_of(f, step):
+    if not f.training:
+        return f.sdf_delta_eval
+    frac = min(max(step / f.max_num_strokes, 0), 1)
+    return f.sdf_delta * (1 - frac) + f.sdf_delta_eval * frac
+
+
+def reference_chain(ref, f, coords, radius, tdist, dirs, g_rgb, g_acc, g_depth):
+    """predict_density + render as the reference runs them, on the reference op:
+    returns rgb, acc, depth and the gradients of shape / colour / density params and
+    of coords (the optimised window's rows; other rows zero)."""
+    dev = coords.device
+    fixed, step = window_of(f)
+    sid = st.sdf_id_of(f.shape_type)
+    delta = delta_of(f, step)
+    R, N, _ = coords.shape
+    xw = warp_coords(None, coords, f.bbox_size)
+    x = xw.reshape(-1, 3).contiguous()
+    r = radius.reshape(-1).contiguous()
+    P = x.shape[0]
+    e = torch.empty(0, device=dev)
+    sp, cp, dp = f.shape_params.detach(), f.color_params.detach(), f.density_params.detach()
+
+    def fwd(lo, hi):
+        a = torch.empty(P, hi - lo, device=dev)
+        c = torch.empty(P, hi - lo, 3, device=dev)
+        if hi > lo:
+            ref.stroke_forward(a, c, e, e, x, r, dirs.contiguous(), sp[lo:hi].contiguous(), cp[lo:hi].contiguous(),
+                               sid, 0, delta, True, True)
+        return a, c
+    a_fix, c_fix = fwd(0, fixed)
+    a_opt, c_opt = fwd(fixed, step)
+    alphas = torch.cat([a_fix, a_opt], 1).contiguous()
+    colors = torch.cat([c_fix, c_opt], 1).contiguous()
+    density = torch.cat([dp[:fixed] * f.density_scale, dp[fixed:step] * f.density_scale]).contiguous()
+    dens = torch.empty(P, device=dev)
+    col = torch.empty(P, 3, device=dev)
+    ref.compose_forward(dens, col, alphas, colors, density)
+    dens_t = dens.reshape(R, N).requires_grad_(True)
+    col_t = col.reshape(R, N, 3).requires_grad_(True)
+    w = orr.compute_alpha_weights(dens_t, tdist, dirs)[0]
+    rgb, depth, acc = orr.volumetric_rendering(col_t, w, tdist, 1.0)
+    L = (rgb * g_rgb).sum() + (acc * g_acc).sum() + (depth * g_depth).sum()
+    g_dens, g_col = torch.autograd.grad(L, [dens_t, col_t])
+    ga, gc, gd = torch.zeros_like(alphas), torch.zeros_like(colors), torch.zeros_like(density)
+    ref.compose_backward(ga, gc, gd, g_dens.reshape(-1).contiguous(), g_col.reshape(-1, 3).contiguous(), alphas,
+                         colors, density)
+    gs, gcol, gdp = torch.zeros_like(sp), torch.zeros_like(cp), torch.zeros_like(dp)
+    gx = torch.zeros(P, 3, device=dev)
+    if step > fixed:
+        gs_o, gc_o = torch.zeros_like(sp[fixed:step]), torch.zeros_like(cp[fixed:step])
+        ref.stroke_backward(gs_o, gc_o, gx, ga[:, fixed:].contiguous(), gc[:, fixed:].contiguous(), e, x, r,
+                            dirs.contiguous(), a_opt, sp[fixed:step].contiguous(), cp[fixed:step].contiguous(), sid, 0,
+                            delta, True, True)
+        gs[fixed:step], gcol[fixed:step] = gs_o, gc_o
+        gdp[fixed:step] = gd[fixed:] * f.density_scale
+    gx = gx.reshape(R, N, 3) / (f.bbox_size / 2)
+    return dict(rgb=rgb.detach(), acc=acc.detach(), depth=depth.detach(), shape=gs, color=gcol, density=gdp, x=gx)
+
+
+def oracle_chain(f, coords, radius, tdist, dirs, g_rgb, g_acc, g_depth):
+    """The same chain in float64 (oracle.render.render_strokes) with exact gradients."""
+    fixed, step = window_of(f)
+    delta = delta_of(f, step)
+    d = lambda t: t.detach().double().cpu()
+    c = d(coords).requires_grad_(True)
+    sp = d(f.shape_params).requires_grad_(True)
+    cp = d(f.color_params).requires_grad_(True)
+    dp = d(f.density_params).requires_grad_(True)
+    sp_w = torch.cat([sp[:fixed].detach(), sp[fixed:step]])
+    cp_w = torch.cat([cp[:fixed].detach(), cp[fixed:step]])
+    dp_w = torch.cat([dp[:fixed].detach(), dp[fixed:step]]) * f.density_scale
+    ids = torch.full((step,), st.sdf_id_of(f.shape_type), dtype=torch.int32)
+    xw = c / (f.bbox_size / 2)
+    rgb, acc, depth = orr.render_strokes(xw, d(radius), d(tdist), d(dirs), sp_w, ids, cp_w, dp_w, delta, True, True)
+    L = (rgb * d(g_rgb)).sum() + (acc * d(g_acc)).sum() + (depth * d(g_depth)).sum()
+    gs = torch.autograd.grad(L, [sp, cp, dp, c], allow_unused=True)
+    z = lambda g, t: torch.zeros_like(t) if g is None else g
+    return dict(rgb=rgb.detach(), acc=acc.detach(), depth=depth.detach(), shape=z(gs[0], sp), color=z(gs[1], cp),
+                density=z(gs[2], dp), x=z(gs[3], c))
+
+
+def run_ours(f, coords, radius, tdist, dirs, g_rgb, g_acc, g_depth, mode):
+    for p in f.parameters():
+        p.grad = None
+    c = coords.clone().requires_grad_(True)
+    rgb, acc, depth = f.render(c, radius, tdist, dirs, options=FieldOptions(grad_mode=mode))
+    L = (rgb * g_rgb).sum() + (acc * g_acc).sum() + (depth * g_depth).sum()
+    L.backward()
+    torch.cuda.synchronize()
+    z = lambda p: torch.zeros_like(p) if p.grad is None else p.grad
+    return dict(rgb=rgb.detach(), acc=acc.detach(), depth=depth.detach(), shape=z(f.shape_params),
+                color=z(f.color_params), density=z(f.density_params), x=c.grad)
+
+
+def depth_mask(acc, g_depth, floor=0.05):
+    return g_depth * (acc >= floor).to(g_depth.dtype)
+
+
+def compare(ours, ref, acc_ref):
+    m = acc_ref.cpu() >= 1e-2
+    e = {"rgb": rel(ours["rgb"], ref["rgb"]), "acc": rel(ours["acc"], ref["acc"]),
+         "depth": rel(ours["depth"].cpu()[m], ref["depth"].cpu()[m]) if bool(m.any()) else 0.0}
+    for k in ("shape", "color", "density", "x"):
+        e["grad_" + k] = rel(ours[k], ref[k])
+    return e
+
+
+CASES = [("ellipsoid", 52, True, None), ("ellipsoid", 30, True, None), ("cube", 52, False, None),
+         ("capsule", 64, True, None), ("ellipsoid", 60, True, 50)]
+
+
+@pytest.mark.parametrize("shape_type,step,training,limit", CASES)
+def test_matches_reference_chain_and_oracle(cuda, shape_type, step, training, limit):
+    f = make_field(shape_type, step, training, cuda, limit)
+    coords, radius, tdist, dirs = rays_for(cuda)
+    g_rgb, g_acc, g_depth = upstream(coords.shape[0], cuda)
+    o64 = oracle_chain(f, coords, radius, tdist, dirs, g_rgb, g_acc, torch.zeros_like(g_depth))
+    g_depth = depth_mask(o64["acc"].to(cuda).float(), g_depth)
+    o64 = oracle_chain(f, coords, radius, tdist, dirs, g_rgb, g_acc, g_depth)
+    exact = run_ours(f, coords, radius, tdist, dirs, g_rgb, g_acc, g_depth, "exact")
+    e = compare(exact, o64, o64["acc"].to(cuda))
+    assert all(v < (GRAD_TOL if k.startswith("grad") else FWD_TOL) for k, v in e.items()), e
+    fixed, active = window_of(f)
+    # rows outside the optimised window get exactly zero gradient
+    for k in ("shape", "color", "density"):
+        assert float(exact[k][:fixed].abs().max() if fixed else 0.0) == 0.0
+        assert float(exact[k][active:].abs().max() if active < MAX else 0.0) == 0.0
+    ref = cpu_port.reference_extension()
+    if ref is None:
+        pytest.skip("reference extension not built (oracle/_ref)")
+    rr = reference_chain(ref, f, coords, radius, tdist, dirs, g_rgb, g_acc, g_depth)
+    compat = run_ours(f, coords, radius, tdist, dirs, g_rgb, g_acc, g_depth, "compat")
+    e = compare(compat, rr, rr["acc"])
+    assert all(v < (GRAD_TOL if k.startswith("grad") else FWD_TOL) for k, v in e.items()), e
+
+
+def test_empty_field_renders_background(cuda):
+    f = make_field("ellipsoid", 0, True, cuda)
+    coords, radius, tdist, dirs = rays_for(cuda)
+    rgb, acc, depth = f.render(coords, radius, tdist, dirs)
+    assert float(rgb.detach().sub(1.0).abs().max()) == 0.0 and float(acc.detach().abs().max()) == 0.0
+    assert torch.equal(depth, tdist[:, 0])
+
+
+def test_no_host_synchronisation(cuda):
+    f = make_field("ellipsoid", 52, True, cuda)
+    coords, radius, tdist, dirs = rays_for(cuda)
+    g_rgb = torch.randn(coords.shape[0], 3, device=cuda)
+    f.render(coords, radius, tdist, dirs)  # first call: library load and caches
+    torch.cuda.synchronize()
+    torch.cuda.set_sync_debug_mode("error")
+    try:
+        rgb, acc, depth = f.render(coords, radius, tdist, dirs)
+        (rgb * g_rgb).sum().backward()
+        f.stroke_step.add_(3)  # the window follows the device count
+        rgb2, _, _ = f.render(coords, radius, tdist, dirs)
+    finally:
+        torch.cuda.set_sync_debug_mode(0)
+    assert not torch.equal(rgb, rgb2)
