@@ -344,6 +344,7 @@ def accuracy_leg(field, w, args):
     torch.set_num_threads(os.cpu_count() or 1)
     ref = cpu_port.reference_extension()
     t0 = time.perf_counter()
+    w = accuracy.workload_from_field(field, w)  # the parameters as the timed (training) steps left them
     out = accuracy.subset_accuracy(field, w, ACCURACY_RAYS.get(args.config, 16), ref=ref)
     if args.config == 3 and ref is not None and args.scale == 1.0:
         out["vs_16_sequential_plain_op_calls"] = accuracy.plain_op_compare(field, w, ref)
@@ -362,7 +363,8 @@ def loss_curves(args):
     from neural3dstrokes_b200.train import BatchedField, GraphedTrainer
     from oracle import cpu_port
     dev = torch.device("cuda", 0)
-    w = scenes.config(4, scale=args.scale)
+    exclude = tuple(k for k in args.exclude_kinds.split(",") if k)
+    w = scenes.config(4, scale=args.scale, exclude=exclude)
     ref = cpu_port.reference_extension()
     grad_mode = "compat"
     tf = BatchedField(w.target_scenes, w.rays, w.sdf_delta, w.use_laplace, w.inv_scale_radius, device=dev,
@@ -371,7 +373,8 @@ def loss_curves(args):
     target = tf.rgb.clone()
     del tf
     field = BatchedField(w.scenes, w.rays, w.sdf_delta, w.use_laplace, w.inv_scale_radius,
-                         options=FieldOptions(grad_mode=grad_mode), device=dev, need_grad_x=False)
+                         options=FieldOptions(grad_mode=grad_mode, cull_alpha=args.cull_alpha), device=dev,
+                         need_grad_x=False)
     trainer = GraphedTrainer(field, target, lr=1e-3)
     ours = []
     t0 = time.time()
@@ -379,8 +382,9 @@ def loss_curves(args):
         trainer.step()
         ours.append(float(trainer.loss))
     t_ours = time.time() - t0
-    line = {"mode": "loss_curve", "config": w.name, "scale": args.scale, "steps": args.loss_curve,
-            "grad_mode": grad_mode, "ours": ours, "ours_s": t_ours}
+    line = {"mode": "loss_curve", "config": w.name, "excluded_kinds": list(exclude), "scale": args.scale,
+            "steps": args.loss_curve,
+            "grad_mode": grad_mode, "cull_alpha": args.cull_alpha, "ours": ours, "ours_s": t_ours}
     if ref is None:
         line["plain_op"] = "unavailable: oracle/_ref holds no reference extension"
     else:
@@ -400,6 +404,16 @@ def loss_curves(args):
         line["plain_op"] = theirs
         line["plain_op_s"] = time.time() - t0
         line["max_rel_diff"] = max(abs(a - b) / max(abs(b), 1e-30) for a, b in zip(ours, theirs))
+        if args.ref_twice:
+            # the reference op trained again from the same start: its own run-to-run
+            # spread (its gradients are sums of float atomics in varying order, and
+            # Adam with eps 1e-15 turns a gradient's sign into a full lr step)
+            again, _ = cpu_port.plain_op_train(ref, [s.to(dev) for s in w.scenes], [r.to(dev) for r in w.rays],
+                                               targets, args.loss_curve, lr=1e-3, delta=w.sdf_delta,
+                                               laplace=w.use_laplace, inv=w.inv_scale_radius, ranges=ranges)
+            line["plain_op_again"] = again
+            line["plain_op_vs_itself_max_rel_diff"] = max(abs(a - b) / max(abs(b), 1e-30)
+                                                          for a, b in zip(again, theirs))
     print(json.dumps(line), flush=True)
     if args.curve_out:
         with open(args.curve_out, "w") as f:
@@ -790,6 +804,12 @@ def main():
                     help="config 4 only: train K steps with the graphed step and with the plain reference op "
                          "from the same start, print both loss curves (not a throughput run)")
     ap.add_argument("--curve-out", default="", help="write the loss curves as JSON to this file")
+    ap.add_argument("--exclude-kinds", default="",
+                    help="loss-curve runs: comma-separated stroke kinds left out of config 4's draw")
+    ap.add_argument("--ref-twice", action="store_true",
+                    help="loss-curve runs: train the reference op a second time (its run-to-run spread)")
+    ap.add_argument("--cull-alpha", type=float, default=1e-9,
+                    help="loss-curve runs: the field's culling threshold (0: every pair evaluated)")
     args = ap.parse_args()
     world, rank, local = dist_setup(args.gpus)
     if args.workload == "ops":

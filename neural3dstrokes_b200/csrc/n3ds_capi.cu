@@ -747,11 +747,21 @@ int n3ds_stroke_forward(float* alpha_out, float* color_out, float* sdf_out, floa
     return fail(N3DS_ERR_INVALID, "null tensor pointer");
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   StrokeWs w = stroke_ws(workspace, n_strokes);
-  n3ds::launch_prep(uniform_prep(w, shape_params, n_shape_params, color_params, n_color_params, n_strokes, sdf_id,
-                                 sdf_delta, use_laplace_transform, inv_scale_radius, false),
-                    st);
+  // With alpha the only per-pair output, pairs whose alpha is exactly 0 in float32 are
+  // not evaluated: the culling bound keeps the soft-step argument beyond m = 104 for the
+  // laplace step (alpha = exp(-m) / 2 < 2^-150 rounds to 0, the reference's own float32
+  // value, even with denormals), beyond the linear step's zero (m >= 0.5) and outside
+  // the hard step's surface. (A looser cut would not be exact for a caller: compose's
+  // colour normalisation 1 / (1 + 1e-6 - T) magnifies alphas near 1e-9 at empty samples.)
+  const bool cull = sdf_out == nullptr && n_texcoord == 0;
+  n3ds::PrepLaunch prep = uniform_prep(w, shape_params, n_shape_params, color_params, n_color_params, n_strokes,
+                                       sdf_id, sdf_delta, use_laplace_transform, inv_scale_radius, false);
+  if (cull) prep.cull_m = 104.f;
+  n3ds::launch_prep(prep, st);
   N3DS_CUDA_TRY(cudaGetLastError());
   n3ds::UfStroke L{};
+  L.cull_a = cull ? w.cull_a : nullptr;
+  L.cull_b = cull ? w.cull_b : nullptr;
   L.x = x;
   L.radius = radius;
   L.recs = w.recs;

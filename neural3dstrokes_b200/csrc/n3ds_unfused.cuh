@@ -24,6 +24,10 @@ struct UfStroke {
   float* gslots;           // [S*32] reduced slots
   int compat;
   int color_const;         // 1: constant rgb colour (written / reduced here); else a colour field kernel runs
+  // forward culling (only alpha requested): [S] culling spheres (centre, radius) and
+  // margins per unit sample radius from the prep kernel, or null (every pair evaluated)
+  const float* cull_a;
+  const float* cull_b;
 };
 
 // Colour fields (n3ds_colors.cu): gradient rgb (color_id 1), SH2 (2), SH3 (3).

@@ -197,9 +197,10 @@ class Workload:
         return sum(s.n_strokes * r.n_rays * r.n_samples for s, r in zip(self.scenes, self.rays))
 
 
-def config(idx, seed=0, scale=1.0):
+def config(idx, seed=0, scale=1.0, exclude=()):
     """Workload of benchmark configuration ``idx`` (0..4). ``scale`` < 1 shrinks the
-    ray counts (tests); stroke counts and distributions are kept."""
+    ray counts (tests); stroke counts and distributions are kept. ``exclude``: stroke
+    kinds left out of config 4's draw (a diagnostic variant of that workload)."""
     g = torch.Generator().manual_seed(seed + 1000 * idx)
     gr = torch.Generator().manual_seed(seed + 1000 * idx + 1)  # rays: own stream, so scale keeps the strokes
     R = lambda n: max(32, int(n * scale))
@@ -229,12 +230,13 @@ def config(idx, seed=0, scale=1.0):
         return Workload("cfg3: 16 uneven scenes (S~logU[50,2000], R~logU[4096,65536]) x 64 samples, "
                         "batched fwd+bwd", scenes, rays)
     if idx == 4:
+        pool = [k for k in ALL_KINDS if k not in exclude]
         scenes, rays, targets = [], [], []
         for _ in range(4):
-            kinds = [ALL_KINDS[int(i)] for i in torch.randint(0, 8, (2000,), generator=g)]
+            kinds = [pool[int(i)] for i in torch.randint(0, len(pool), (2000,), generator=g)]
             scenes.append(make_strokes(kinds, g))
             rays.append(make_rays(R(131072), 96, gr))
-            kt = [ALL_KINDS[int(i)] for i in torch.randint(0, 8, (2000,), generator=g)]
+            kt = [pool[int(i)] for i in torch.randint(0, len(pool), (2000,), generator=g)]
             targets.append(make_strokes(kt, g))
         w = Workload("cfg4: 4 scenes x 2000 mixed strokes, 131072 rays x 96 samples, graphed training step",
                      scenes, rays)

@@ -167,6 +167,23 @@ def _split(res, r0, r1, s0, s1, idx):
     return out
 
 
+def workload_from_field(field, w):
+    """A copy of workload ``w`` whose scenes carry the field's current parameters
+    (after training steps have moved them away from the generated ones)."""
+    import copy
+    from neural3dstrokes_b200.scenes import Scene
+    out = copy.copy(w)
+    out.scenes = []
+    s0 = 0
+    shape, color, dens = field.shape.detach().cpu(), field.color.detach().cpu(), field.density.detach().cpu()
+    for sc in w.scenes:
+        n = sc.n_strokes
+        out.scenes.append(Scene(sc.kinds, sc.sdf_ids, shape[s0:s0 + n].clone(), color[s0:s0 + n].clone(),
+                                dens[s0:s0 + n].clone()))
+        s0 += n
+    return out
+
+
 def subset_accuracy(field, w, rays_per_scene, seed=0, ref=None):
     """Accuracy statement of ``field`` (a BatchedField over workload ``w``) on a fixed
     subset of ``rays_per_scene`` evenly spaced rays per scene. ``ref``: the reference

@@ -785,6 +785,23 @@ def stroke_forward_mixed(x, radius, shape_params, sdf_ids, color_params, sdf_del
 
 # ------------------------------------------------------------------- compose
 
+def _over_step(T, dens, col, a, d, c):
+    """One stroke of 'over' compositing. The reference skips a zero alpha
+    (compositing.cu:37); that changes the sums only where the stroke's colour or
+    density is not finite, so only there is the term dropped (elsewhere the skip is
+    the identity, and float64 autograd keeps the derivative at alpha = 0)."""
+    w = a * T
+    T = T * (1.0 - a)
+    if torch.is_tensor(d):
+        fin = torch.isfinite(c).all(dim=-1) & torch.isfinite(d)
+    else:
+        fin = torch.isfinite(c).all(dim=-1) & bool(torch.isfinite(torch.tensor(d)))
+    keep = (a != 0) | fin
+    dens = dens + torch.where(keep, d * w, torch.zeros_like(w))
+    col = col + torch.where(keep[:, None], c * w[:, None], torch.zeros_like(c))
+    return T, dens, col
+
+
 def compose_forward(alphas, colors, density_params):
     """'over' compositing, last stroke on top (compositing.cu:10-59)."""
     P, S = alphas.shape
@@ -792,11 +809,7 @@ def compose_forward(alphas, colors, density_params):
     dens = torch.zeros(P, dtype=alphas.dtype)
     col = torch.zeros(P, colors.shape[-1], dtype=alphas.dtype)
     for s in range(S - 1, -1, -1):
-        a = alphas[:, s]
-        w = a * T
-        T = T * (1.0 - a)
-        dens = dens + density_params[s] * w
-        col = col + colors[:, s] * w[:, None]
+        T, dens, col = _over_step(T, dens, col, alphas[:, s], density_params[s], colors[:, s])
     col = cu_clamp(col * (1.0 / (1.0 + 1e-6 - T))[:, None], 0.0, 1.0)
     return dens, col
 
@@ -808,11 +821,7 @@ def compose_state(alphas, colors, density_params):
     dens = torch.zeros(P, dtype=alphas.dtype)
     col = torch.zeros(P, colors.shape[-1], dtype=alphas.dtype)
     for s in range(S - 1, -1, -1):
-        a = alphas[:, s]
-        w = a * T
-        T = T * (1.0 - a)
-        dens = dens + density_params[s] * w
-        col = col + colors[:, s] * w[:, None]
+        T, dens, col = _over_step(T, dens, col, alphas[:, s], density_params[s], colors[:, s])
     return dens, col, T
 
 

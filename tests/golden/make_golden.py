@@ -257,6 +257,23 @@ def make_strokes_py(ref_root, out):
             R, N, S = 4, 8, 5
             sc = scenes.make_strokes([kind] * S, g)
             rays = scenes.make_rays(R, N, g)
+            # centre every stroke on a sample of the rays, so that each call carries
+            # alphas well above any culling threshold
+            pts = rays.x.reshape(-1, 3)
+            pick = torch.randint(0, pts.shape[0], (S,), generator=g)
+            # (off the sample itself: the per-axis radius factor is 0/0 at a stroke's centre)
+            pts = pts.clone()
+            pts[pick] += torch.randn(S, 3, generator=g) * 0.03
+            n = sc.shape_params.shape[1]
+            for i in range(S):
+                k = scenes.N_PARAMS[kind]
+                row = sc.shape_params[i]
+                if kind in ("quadratic_bezier", "cubic_bezier", "catmull_rom"):
+                    m = (k - 2) // 3
+                    ctrl = row[:3 * m].reshape(m, 3)
+                    row[:3 * m] = (ctrl - ctrl.mean(0) + pts[pick[i]]).reshape(-1)
+                else:
+                    row[k - 3:k] = pts[pick[i]]
             x = rays.x.clone().requires_grad_(True)
             shape = sc.shape_params[:, :d_shape].clone().requires_grad_(True)
             color = sc.color_params.clone().requires_grad_(True)

@@ -136,16 +136,61 @@ def compose_inputs(P=700, S=45, C=3, seed=0, amax=1.0):
     return a, c, d
 
 
-@pytest.mark.parametrize("C,S", [(1, 45), (3, 45), (3, 1), (3, 32), (3, 100), (1, 300)])
+@pytest.mark.parametrize("C,S", [(1, 45), (3, 45), (3, 1), (3, 32), (3, 100), (1, 300), (3, 256), (1, 128),
+                                 (3, 1028)])
 def test_compose_forward_matches_oracle(cuda, C, S):
-    """One warp per row, 32 strokes per lane step: a lone stroke, an exact chunk,
-    partial and many chunks; 30 % of the alphas are exactly 0 (skipped)."""
+    """A lone stroke, exact and partial 32-stroke chunks (rows whose stroke count is
+    not a multiple of 4 take the lane-per-stroke kernel), and the float4 kernel with
+    one to four groups per lane and several rounds per row; 30 % of the alphas are
+    exactly 0 (skipped)."""
     a, c, d = compose_inputs(C=C, S=S)
     dens = torch.empty(a.shape[0], device=cuda)
     col = torch.empty(a.shape[0], C, device=cuda)
     sl.compose_forward(dens, col, a.to(cuda), c.to(cuda), d.to(cuda))
     dr, cr = sf.compose_forward(a.double(), c.double(), d.double())
     assert rel(dens, dr) < FWD_TOL and rel(col, cr) < FWD_TOL
+
+
+def test_compose_forward_misaligned_rows_and_skipped_nan_colour(cuda):
+    """Tensors that start off a 16-byte boundary take the scalar kernel; a NaN colour
+    under alpha 0 is skipped (compositing.cu:37) by both kernels."""
+    a, c, d = compose_inputs(P=300, S=64, C=3, seed=4)
+    c[a == 0] = float("nan")
+    dr, cr = sf.compose_forward(a.double(), c.double(), d.double())
+    assert torch.isfinite(cr).all()
+    for off in (0, 1):
+        buf_a = torch.empty(a.numel() + off, device=cuda)
+        buf_c = torch.empty(c.numel() + off, device=cuda)
+        aa = buf_a[off:].view(a.shape)
+        cc = buf_c[off:].view(c.shape)
+        aa.copy_(a)
+        cc.copy_(c)
+        dens = torch.empty(a.shape[0], device=cuda)
+        col = torch.empty(a.shape[0], 3, device=cuda)
+        sl.compose_forward(dens, col, aa, cc, d.to(cuda))
+        assert rel(dens, dr) < FWD_TOL and rel(col, cr) < FWD_TOL
+
+
+@pytest.mark.parametrize("kind,S,lap,inv", [("ellipsoid", 96, True, True), ("cube", 40, True, False),
+                                            ("capsule", 64, False, True), ("tetrahedron", 33, True, True),
+                                            ("cubic_bezier", 64, True, True), ("sphere", 32, True, True)])
+def test_alpha_only_forward_culls_within_bound(cuda, kind, S, lap, inv):
+    """stroke_forward without sdf / texcoord outputs (the reference model's call,
+    no_sdf=True): pairs whose float32 alpha is exactly 0 (laplace beyond m = 104, the
+    linear step's zero, outside the hard step) are culled and store 0, the same value
+    the full evaluation gives; everything else as the float64 oracle. Point counts off
+    a multiple of 32 and stroke blocks of fewer than 32 included."""
+    sid, ps, col, x, r, vd, _ = group(kind, n_strokes=S, n_points=2000, seed=12)
+    x, r = x[:1979].contiguous(), r[:1979].contiguous()
+    a, c, _ = run_forward(sl, sid, ps, col, x, r, vd, 0.02, lap, inv, cuda, want_sdf=False)
+    a64, c64 = sf.stroke_forward(x.double(), r.double(), ps.double(), col.double(), sid, 0.02, lap, inv)
+    assert rel(a, a64) < FWD_TOL and rel(c, c64) < FWD_TOL
+    zero = a.cpu() == 0
+    assert bool(zero.any())
+    assert float(a64[zero].abs().max()) <= 1e-30                # only where alpha underflows
+    # the same call with the sdf output requested evaluates every pair: identical alphas
+    a_full, _, _ = run_forward(sl, sid, ps, col, x, r, vd, 0.02, lap, inv, cuda, want_sdf=True)
+    assert torch.equal(a, a_full)
 
 
 @pytest.mark.parametrize("mode,S", [("exact", 45), ("compat", 45), ("exact", 1), ("exact", 32), ("exact", 100),
