@@ -204,6 +204,12 @@ typedef struct n3ds_strokes {
    * before the optimised ones, which keeps the stroke order). Needs the segment
    * schedule and at most 40 scenes. */
   const int32_t* stroke_window;
+  /* Optional hint: bit b set when strokes of base b (sdf_id >> 4) may occur, 0 = any.
+   * When the hint names only the common primitives (sphere / ellipsoid, cube / box,
+   * round cube / box, capsule, octahedron, tetrahedron), the forward runs a build
+   * that carries only their code. A stroke outside the hint is an unsupported kind
+   * (status bit 1, NaN outputs). */
+  uint32_t base_mask;
 } n3ds_strokes_t;
 
 typedef struct n3ds_options {

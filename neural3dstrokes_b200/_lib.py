@@ -39,7 +39,7 @@ class Strokes(ctypes.Structure):
     _fields_ = [("sdf_ids", ctypes.c_void_p), ("shape_params", ctypes.c_void_p), ("param_stride", c_i32),
                 ("color_params", ctypes.c_void_p), ("density", ctypes.c_void_p),
                 ("sdf_delta", ctypes.c_void_p), ("use_laplace_transform", c_i32),
-                ("inv_scale_radius", c_i32), ("stroke_window", ctypes.c_void_p)]
+                ("inv_scale_radius", c_i32), ("stroke_window", ctypes.c_void_p), ("base_mask", ctypes.c_uint32)]
 
 
 class Options(ctypes.Structure):

@@ -442,12 +442,14 @@ int n3ds_field_forward(const n3ds_batch_t* batch, const n3ds_rays_t* rays, const
   N3DS_CUDA_TRY(cudaMemsetAsync(ws + lay.status, 0, sizeof(int32_t), st));
   n3ds::PrepLaunch prep = make_prep(strokes, S, rv, ws, lay, false);
   fill_window(batch, strokes, &prep.window, &prep.n_win_scenes, prep.win_begin);
+  prep.base_mask = strokes->base_mask;
   n3ds::launch_prep(prep, st);
   N3DS_CUDA_TRY(cudaGetLastError());
   record_event(rv, 0, st);
   n3ds::SegLaunch FL = make_seg(batch, rays, ws, lay, 0);
   FL.wait_limit_ns = rv.wait_limit_ns;
   FL.test_stall = rv.test_stall;
+  FL.common_only = strokes->base_mask != 0 && (strokes->base_mask & ~n3ds::COMMON_BASES) == 0;
   FL.skip_alpha = rv.cull_alpha;
   if (!rv.count_pairs) FL.stats = nullptr;
   if (rv.forward_only || rv.schedule != N3DS_SCHEDULE_SEGMENTS) {
@@ -489,6 +491,7 @@ int n3ds_field_backward(const n3ds_batch_t* batch, const n3ds_rays_t* rays, cons
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   n3ds::PrepLaunch prep = make_prep(strokes, S, rv, ws, lay, true);
   fill_window(batch, strokes, &prep.window, &prep.n_win_scenes, prep.win_begin);
+  prep.base_mask = strokes->base_mask;
   n3ds::launch_prep(prep, st);
   N3DS_CUDA_TRY(cudaGetLastError());
   if (R > 0) {

@@ -51,6 +51,35 @@ __device__ __forceinline__ float pair_alpha(const float* rec, V3 x, float rinv, 
   return soft_alpha(mode, -sdf * k);
 }
 
+template <int BASE>
+__device__ __forceinline__ float common_sdf(V3 p, int kind, const float* rec, float* f) {
+  const float sdf = prim_sdf(BASE, p, rec);
+  if (kind & K_S3FAC) *f = s3_factor(BASE, p, xyz(rec4(rec)[R_S / 4]), rec);
+  return sdf;
+}
+
+// pair_alpha for a launch whose strokes are all common primitives: the dispatch (and
+// so the kernel's code) covers those six bases only; any other base gives NaN (the
+// prep kernel flags such a stroke as an unsupported kind before this runs).
+__device__ __forceinline__ float pair_alpha_common(const float* rec, V3 x, float rinv) {
+  const float4 h = rec4(rec)[0];
+  const int kind = __float_as_int(h.x);
+  const int mode = (kind >> 8) & 3;
+  const V3 p = prim_local(rec, x);
+  float sdf, f = 1.f;
+  switch (kind & 15) {
+    case B_SPHERE: sdf = common_sdf<B_SPHERE>(p, kind, rec, &f); break;
+    case B_CUBE: sdf = common_sdf<B_CUBE>(p, kind, rec, &f); break;
+    case B_ROUND_CUBE: sdf = common_sdf<B_ROUND_CUBE>(p, kind, rec, &f); break;
+    case B_CAPSULE: sdf = common_sdf<B_CAPSULE>(p, kind, rec, &f); break;
+    case B_OCTAHEDRON: sdf = common_sdf<B_OCTAHEDRON>(p, kind, rec, &f); break;
+    case B_TETRAHEDRON: sdf = common_sdf<B_TETRAHEDRON>(p, kind, rec, &f); break;
+    default: sdf = __int_as_float(0x7fc00000); break;
+  }
+  if (mode == STEP_HARD) return sdf <= 0.f ? 1.f : 0.f;
+  return soft_alpha(mode, -sdf * (h.y * f * rinv));
+}
+
 // dL/dm of the soft step given G = (1 - alpha) dL/dalpha (division-safe form).
 __device__ __forceinline__ float soft_dm_from_G(int mode, float m, float alpha, float G) {
   if (mode == STEP_LAPLACE) return m <= 0.f ? G * alpha / (1.f - alpha) : G;

@@ -221,7 +221,9 @@ __device__ __forceinline__ unsigned cull_block_sphere(const Stage& S, const SegC
 
 // RECORD: write the stroke-block masks (L.block_masks non-null) for the backward.
 // STATS: count evaluated pairs per base type into L.stats (non-null).
-template <int WARPS, bool RECORD, bool STATS>
+// COMMON: every stroke of the launch is a common primitive (the caller's hint, checked
+// by the prep kernel): the kernel carries only those six bases' evaluation code.
+template <int WARPS, bool RECORD, bool STATS, bool COMMON>
 __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_constant__ SegLaunch L) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t bar;
@@ -309,6 +311,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_con
               const bool reach = rb == B_SPHERE        ? ellipsoid_reachable(rec, c)
                                  : rb == B_CAPSULE     ? capsule_reachable(rec, c)
                                  : rb <= B_TETRAHEDRON ? polytope_reachable(rec, c)
+                                 : COMMON              ? true
                                                        : curve_reachable(rec, c, fabsf(S.cull_b[slot]), lane);
               if (!reach) atomicOr(kill + kk, 1u << bit);
             }
@@ -328,7 +331,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_con
             const int b = __ffs(mask) - 1;
             mask &= mask - 1;
             const float* rec = S.recs + size_t(hi - b) * REC_FLOATS;
-            const float a = pair_alpha(rec, c.x, c.rinv);
+            const float a = COMMON ? pair_alpha_common(rec, c.x, c.rinv) : pair_alpha(rec, c.x, c.rinv);
             if (RECORD && a >= L.skip_alpha) kept |= 1u << b;
             if (STATS && lane == (__float_as_int(rec[R_KIND]) & 15)) kcount += nact;
             const float w = a * T;
@@ -828,7 +831,7 @@ __global__ void prep_kernel(const PrepLaunch P) {
   const bool s1 = flags & F_S1;
   const bool s3 = !s1 && (flags & F_S3);
   if (!base_supported(base) || np > P.param_stride || sid < 0 || sid > 255 ||
-      ((base > B_TETRAHEDRON) && flags != 0)) {
+      ((base > B_TETRAHEDRON) && flags != 0) || (P.base_mask && !((P.base_mask >> base) & 1u))) {
     // Unsupported stroke: flag it, never read its parameters, and make every
     // sample that meets it NaN (the culling sphere is infinite) so that the error
     // cannot pass silently.
@@ -1209,14 +1212,18 @@ void launch_prep(const PrepLaunch& p, cudaStream_t st) {
   prep_kernel<<<(unsigned)((n + threads - 1) / threads), threads, 0, st>>>(p);
 }
 
-template <int W>
-static cudaError_t launch_fwd_w(const SegLaunch& L, int grid, size_t smem, cudaStream_t st) {
-  auto* k = L.block_masks ? (L.stats ? seg_fwd_kernel<W, true, true> : seg_fwd_kernel<W, true, false>)
-                          : (L.stats ? seg_fwd_kernel<W, false, true> : seg_fwd_kernel<W, false, false>);
+template <int W, bool COMMON>
+static cudaError_t launch_fwd_wc(const SegLaunch& L, int grid, size_t smem, cudaStream_t st) {
+  auto* k = L.block_masks ? (L.stats ? seg_fwd_kernel<W, true, true, COMMON> : seg_fwd_kernel<W, true, false, COMMON>)
+                          : (L.stats ? seg_fwd_kernel<W, false, true, COMMON> : seg_fwd_kernel<W, false, false, COMMON>);
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   k<<<grid, W * 32, smem, st>>>(L);
   return cudaGetLastError();
+}
+template <int W>
+static cudaError_t launch_fwd_w(const SegLaunch& L, int grid, size_t smem, cudaStream_t st) {
+  return L.common_only ? launch_fwd_wc<W, true>(L, grid, smem, st) : launch_fwd_wc<W, false>(L, grid, smem, st);
 }
 template <int W>
 static cudaError_t launch_bwd_w(const SegLaunch& L, int grid, size_t smem, cudaStream_t st) {

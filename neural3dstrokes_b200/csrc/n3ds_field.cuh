@@ -59,6 +59,7 @@ struct SegLaunch {
   // forward's prep kernel).
   unsigned* block_masks;
   const int* mask_tag;
+  int common_only;                   // forward: every stroke is a common primitive (pair_alpha_common)
   unsigned long long wait_limit_ns;  // bounded waits give up after this long
   int test_stall;                    // arm the staging barrier without the copies (test of the wait limit)
   SceneDesc sc[MAX_SCENES_PER_LAUNCH];
@@ -113,6 +114,9 @@ struct PrepLaunch {
   const int* window;
   int n_win_scenes;
   int win_begin[MAX_SCENES_PER_LAUNCH + 1];
+  // the caller's hint of the bases present (bit b = base b; 0 = any): a stroke of
+  // another base is treated as an unsupported kind
+  unsigned base_mask;
 };
 
 struct FinalizeLaunch {

@@ -20,6 +20,10 @@ enum Base : int {
   B_CATMULL_ROM = 11
 };
 constexpr int F_T = 1, F_R = 2, F_S1 = 4, F_S3 = 8;
+// The common primitives: sphere / ellipsoid, cube / box, round cube / box, capsule,
+// octahedron, tetrahedron (every stroke of the reference's primitive configurations).
+constexpr unsigned COMMON_BASES = (1u << B_SPHERE) | (1u << B_CUBE) | (1u << B_ROUND_CUBE) | (1u << B_CAPSULE) |
+                                  (1u << B_OCTAHEDRON) | (1u << B_TETRAHEDRON);
 enum StepMode : int { STEP_HARD = 0, STEP_LAPLACE = 1, STEP_LINEAR = 2 };
 
 __host__ __device__ __forceinline__ int kind_base(int k) { return k & 15; }

@@ -19,7 +19,7 @@ import torch
 
 from . import _lib
 from .field import FieldOptions
-from .scenes import PARAM_STRIDE, RaySet, Scene, param_ranges
+from .scenes import PARAM_STRIDE, SDF_ID, RaySet, Scene, param_ranges
 
 
 class BatchedField:
@@ -84,9 +84,14 @@ class BatchedField:
         self.c_batch = _lib.Batch(n, self._nr, self._ns, self.n_samples)
         self.c_rays = _lib.Rays(_lib.ptr(self.x), _lib.ptr(self.radius), _lib.ptr(self.tdist), _lib.ptr(self.dirs),
                                 None, self.bg_value, int(self.opaque), _lib.ptr(self.origins), _lib.ptr(self.radii))
+        # the bases present (from the host's kind list): a field of common primitives
+        # only runs the forward build that carries just their code
+        base_mask = 0
+        for k in set(self.kinds):
+            base_mask |= 1 << (SDF_ID[k] >> 4)
         self.c_strokes = _lib.Strokes(_lib.ptr(self.sdf_ids), _lib.ptr(self.shape), PARAM_STRIDE,
                                       _lib.ptr(self.color), _lib.ptr(self.density), _lib.ptr(self.delta),
-                                      int(self.laplace), int(self.inv_scale))
+                                      int(self.laplace), int(self.inv_scale), None, base_mask)
         self.c_opt = self.options.c()
         lib = _lib.load()
         self.ws_bytes = lib.n3ds_field_workspace_bytes(ctypes.byref(self.c_batch), ctypes.byref(self.c_opt))

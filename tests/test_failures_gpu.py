@@ -87,3 +87,19 @@ def test_bounded_wait_runs_out_and_reports(cuda, schedule):
     assert st == 0
     rgb_r, acc_r, _ = oracle_forward(sc, rays)
     assert rel(ok.rgb, rgb_r) < FWD_TOL and rel(ok.acc, acc_r) < FWD_TOL
+
+
+def test_base_hint_that_leaves_out_a_present_base_is_reported(cuda):
+    """The base hint is checked on the device: a stroke whose base the hint leaves out
+    sets ST_BAD_KIND and evaluates to NaN (here a cubic Bezier under a hint of the
+    common primitives, which also selects their specialised forward)."""
+    sc, rays = small_workload("mixed", n_strokes=24, n_rays=64, n_samples=48, seed=4)
+    assert "cubic_bezier" in sc.kinds
+    f = field_of(sc, rays, cuda)
+    common = sum(1 << b for b in (0, 1, 2, 4, 7, 8))
+    f.c_strokes.base_mask = common
+    f.forward()
+    torch.cuda.synchronize()
+    st, _ = f.status()
+    assert st & ST_BAD_KIND
+    assert bool(torch.isnan(f.rgb).any())

@@ -237,3 +237,22 @@ def test_backward_warp_counts_agree(cuda, chunk):
         outs.append((x.grad, sp.grad, col.grad, den.grad, dl.grad))
     for a, b in zip(*outs):
         assert rel(a, b) < 1e-5
+
+
+@pytest.mark.parametrize("kind", ["mixed_primitives", "ellipsoid", "capsule"])
+def test_common_primitive_build_matches_general_build(cuda, kind):
+    """A field whose strokes are all common primitives (its kind list gives the base
+    hint) runs the forward build that carries only their code; it matches the general
+    build (render_strokes passes no hint) on the same inputs."""
+    from neural3dstrokes_b200.train import BatchedField
+    g = torch.Generator().manual_seed(41)
+    kinds = ([scenes.MIXED_PRIMS[i % 6] for i in range(60)] if kind == "mixed_primitives" else [kind] * 60)
+    sc = scenes.make_strokes(kinds, g)
+    rays = scenes.make_rays(80, 64, g)
+    f = BatchedField([sc], [rays], device=cuda)
+    assert f.c_strokes.base_mask != 0
+    f.forward()
+    torch.cuda.synchronize()
+    (rgb, acc, depth), _ = run_field(sc, rays, cuda)
+    assert rel(f.rgb, rgb) < 1e-6 and rel(f.acc, acc) < 1e-6
+    assert f.status()[0] == 0
