@@ -466,6 +466,74 @@ int n3ds_grid_total_variation(const void* inputs, const void* embeddings, void* 
                               float weight, uint32_t B, uint32_t D, uint32_t C, uint32_t L, float S, uint32_t H,
                               uint32_t gridtype, int32_t align_corners, int32_t dtype, n3ds_stream_t stream);
 
+/* Fused density network of the proposal and error fields: MLP.predict_density plus
+ * the density activation with disable_rgb (source/models.py:362-372, 430-431; PropMLP
+ * :501-504, ErrorMLP.sample_error :513-523). Per point: warp the coordinates
+ * (`warp`), map them to [0, 1] by the encoder's bound, encode them on the hash grid
+ * (n_levels x level_dim features, as n3ds_grid_encode_forward), then
+ * raw = w2 . relu(w1 f + b1) + b2 and density = softplus(raw + density_bias)
+ * (torch's softplus: the identity above 20). The first layer runs on the tensor
+ * cores (tcgen05, tf32 with a three-term split: float32 accuracy). The reference
+ * runs it as torch layers; this network has no counterpart in its native code.
+ * Constraints: level_dim in {1, 2, 4}, n_levels * level_dim <= 16, 64 hidden units,
+ * float32 everywhere, linear interpolation. */
+#define N3DS_WARP_SCALE 0    /* coords * warp_scale (the reference's warp_fn None: / (bbox_size / 2)) */
+#define N3DS_WARP_CONTRACT 1 /* coord.contract(coords) / 2 (warp_fn 'contract') */
+#define N3DS_WARP_NONE 2     /* coords as given (no_warp=True) */
+#define N3DS_DENSITY_HIDDEN 64
+typedef struct n3ds_density_net {
+  const float* table;          /* [offsets[L], level_dim] GridEncoder.embeddings */
+  const int32_t* offsets;      /* [n_levels + 1] GridEncoder.offsets */
+  uint32_t n_levels;           /* L */
+  uint32_t level_dim;          /* C */
+  float log2_per_level_scale;  /* S = log2(per_level_scale) */
+  uint32_t base_resolution;    /* H */
+  uint32_t gridtype;           /* N3DS_GRID_HASH or N3DS_GRID_TILED */
+  int32_t align_corners;
+  const float* w1;             /* [64, L * C] density_layer[0].weight */
+  const float* b1;             /* [64] density_layer[0].bias */
+  const float* w2;             /* [64] density_layer[2].weight ([1, 64]) */
+  const float* b2;             /* [1] density_layer[2].bias */
+  float density_bias;          /* MLP.density_bias */
+  int32_t warp;                /* N3DS_WARP_* */
+  float warp_scale;            /* float32(1 / (bbox_size / 2)) for N3DS_WARP_SCALE */
+  float grid_bound;            /* GridEncoder.forward's bound (1.0 in predict_density) */
+  int32_t raw_output;          /* nonzero: `density` receives raw (predict_density's
+                                  raw_density, no bias or softplus) and the backward
+                                  takes its gradient */
+  int32_t* status;             /* device int32 or NULL; bit 2 (value 2) is ORed in when
+                                  a bounded wait for the tensor cores ran out (the
+                                  call's outputs are then invalid) */
+  int32_t wait_limit_us;       /* limit of each such wait; 0: one second */
+  int32_t test_stall;          /* test hook: withhold the tensor-core work so that the
+                                  first wait runs out (0 in normal use) */
+} n3ds_density_net_t;
+/* Floats per point of the feature record written by the forward for the backward:
+ * L * C rounded up to a multiple of 4. */
+int n3ds_density_net_feature_stride(uint32_t n_levels, uint32_t level_dim);
+/* density [n] (and, when not NULL, features [n, stride] for the backward and the
+ * warped coordinates [n, 3], the module's `coord` output); coords [n, 3]. */
+int n3ds_density_net_forward(const n3ds_density_net_t* net, const float* coords, int64_t n_points, float* density,
+                             float* features, float* coords_warped, n3ds_stream_t stream);
+/* The adjoint of the forward with respect to the table and the four layer tensors,
+ * accumulated into grad_table [offsets[L], C], grad_w1 [64, L * C], grad_b1 [64],
+ * grad_w2 [64] and grad_b2 [1] (zero them first); features are the forward's
+ * record, grad_density [n]. No gradient with respect to the coordinates. */
+int n3ds_density_net_backward(const n3ds_density_net_t* net, const float* coords, const float* features,
+                              const float* grad_density, int64_t n_points, float* grad_table, float* grad_w1,
+                              float* grad_b1, float* grad_w2, float* grad_b2, n3ds_stream_t stream);
+/* Hash-decay statistics of a float32 table (source/models.py:472-488):
+ * out[l, c] = mean over level l's rows of table[row, c]^2, for every channel when
+ * all_channels is nonzero (torch_scatter's segment_coo), else for channel 0 with
+ * the other channels 0 (the scatter_reduce_ fallback the reference takes without
+ * torch_scatter). out [L, C] is overwritten. The backward adds
+ * grad_out[l, c] * 2 * table[row, c] / rows(l) to grad_table. */
+int n3ds_grid_level_mean_sq(const float* table, const int32_t* offsets, uint32_t n_levels, uint32_t level_dim,
+                            int32_t all_channels, float* out, n3ds_stream_t stream);
+int n3ds_grid_level_mean_sq_backward(const float* table, const int32_t* offsets, uint32_t n_levels,
+                                     uint32_t level_dim, int32_t all_channels, const float* grad_out,
+                                     float* grad_table, n3ds_stream_t stream);
+
 /* FP32 FMA throughput probe (no counterpart in the reference; a measurement aid for
  * the roofline of these FP32-bound kernels): one launch of `blocks` x 256 threads,
  * each doing iters x 16 fused multiply-adds, i.e. blocks*256*iters*32 flops.

@@ -50,7 +50,17 @@ class Options(ctypes.Structure):
                 ("test_stall_staging", c_i32)]
 
 
+class DensityNet(ctypes.Structure):
+    _fields_ = [("table", ctypes.c_void_p), ("offsets", ctypes.c_void_p), ("n_levels", c_u32),
+                ("level_dim", c_u32), ("log2_per_level_scale", ctypes.c_float), ("base_resolution", c_u32),
+                ("gridtype", c_u32), ("align_corners", c_i32), ("w1", ctypes.c_void_p), ("b1", ctypes.c_void_p),
+                ("w2", ctypes.c_void_p), ("b2", ctypes.c_void_p), ("density_bias", ctypes.c_float),
+                ("warp", c_i32), ("warp_scale", ctypes.c_float), ("grid_bound", ctypes.c_float),
+                ("raw_output", c_i32), ("status", ctypes.c_void_p), ("wait_limit_us", c_i32), ("test_stall", c_i32)]
+
+
 _P = ctypes.c_void_p
+_DN = ctypes.POINTER(DensityNet)
 _SIGS = {
     "n3ds_last_error": (ctypes.c_char_p, []),
     "n3ds_version": (ctypes.c_int, []),
@@ -112,6 +122,11 @@ _SIGS = {
                                                  c_u32, _P, _P, c_u32, c_i32, c_u32, c_i32, _P]),
     "n3ds_grid_total_variation": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_float, c_u32, c_u32, c_u32, c_u32,
                                                  ctypes.c_float, c_u32, c_u32, c_i32, c_i32, _P]),
+    "n3ds_density_net_feature_stride": (ctypes.c_int, [c_u32, c_u32]),
+    "n3ds_density_net_forward": (ctypes.c_int, [_DN, _P, c_i64, _P, _P, _P, _P]),
+    "n3ds_density_net_backward": (ctypes.c_int, [_DN, _P, _P, _P, c_i64, _P, _P, _P, _P, _P, _P]),
+    "n3ds_grid_level_mean_sq": (ctypes.c_int, [_P, _P, c_u32, c_u32, c_i32, _P, _P]),
+    "n3ds_grid_level_mean_sq_backward": (ctypes.c_int, [_P, _P, c_u32, c_u32, c_i32, _P, _P, _P]),
     "n3ds_stroke_forward_static": (ctypes.c_int, [_P, _P, _P, _P, c_i64, _P, _P, _P, _P, _P, c_i64, c_i64, c_i64,
                                                   c_i64, c_i64, c_u32, c_u32, ctypes.c_float, ctypes.c_int,
                                                   ctypes.c_int, _P]),

@@ -1,0 +1,881 @@
+// Fused density network of the proposal and error fields (source/models.py:285-523:
+// MLP.predict_density on the hash-grid encoder, density_layer = Linear(L*C, 64),
+// ReLU, Linear(64, 1), then softplus(raw + density_bias); PropMLP and ErrorMLP with
+// disable_rgb). The reference evaluates it as its grid kernels plus torch layers,
+// which write and read the [points, 64] hidden activations several times; here one
+// kernel per direction keeps them on chip.
+//
+// Schedule: persistent CTAs of 128 threads, one point per thread, tiles of 128
+// points (the MMA's M).
+// Forward, per tile: each thread warps its point, encodes it on the grid into
+// registers and writes its feature row into the tile's A operand (hi and lo tf32
+// halves); one thread issues the first layer as tcgen05.mma kind::tf32 (M 128, N 64,
+// K = L*C padded to 8 or 16, three products per K step for the split) into tensor
+// memory; every thread reads its accumulator row back with tcgen05.ld and finishes
+// bias, ReLU, the 64-wide second layer and softplus on the CUDA cores.
+// Backward, per tile: the forward's feature record is reloaded and the first layer
+// recomputed on the tensor cores; each thread forms d raw = g e^z / (e^z + 1) (torch's
+// softplus backward) and the ReLU mask of its 64 hidden units. Because the mask is
+// exactly 0 or 1, the adjoint dh = d raw w2 mask factors into two bf16 products with
+// float32 accuracy (kind::f16, K-major operands): dfeat = d raw (.) (mask . W1') with
+// W1' = w2 (.) W1 in three bf16 terms (M 128 points, N 16, K 64), and
+// dW1 = w2 (.) (mask^T . (d raw feat)) with d raw feat in three bf16 terms and d raw
+// itself as one more column, which gives db1 (M 64 hidden, N 16, K 128 points),
+// accumulated in tensor memory over all of the CTA's tiles. dW2 and db2 are warp
+// reductions. dfeat goes straight into the grid's table scatter, runs of points in
+// one cell summed in the warp before the atomic.
+//
+// Each wait for the tensor cores is bounded (one second unless set); when one runs
+// out the kernel ORs bit 2 into the status word, waits once more (bounded) for
+// anything still in flight, frees its tensor memory and returns.
+#include <cstdint>
+#include <string>
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "../../include/n3ds.h"
+#include "n3ds_grid.cuh"
+#include "n3ds_tc.cuh"
+
+namespace n3ds {
+int report_error(int code, const std::string& msg);  // sets n3ds_last_error (n3ds_capi.cu)
+}
+
+namespace {
+
+using namespace n3ds::grid;
+using namespace n3ds::tc;
+
+constexpr int kTile = 128;                 // points per tile: MMA M and threads per CTA
+constexpr int kHidden = N3DS_DENSITY_HIDDEN;
+constexpr int kMaxFeat = 16;               // feature columns in shared memory (L * C <= 15, then d raw)
+constexpr int kStatusWait = 2;             // the field's ST_WAIT_TIMEOUT bit
+
+// Shared-memory layout (bytes), every tensor-core operand K-major without swizzle
+// (n3ds_tc.cuh; tf32 takes 4 values, bf16 8 values per 16-byte core-matrix row).
+// Forward and backward, tf32 hi and lo halves:
+//   feature rows: element (p, f) at (f / 4) * 2048 + p * 16 + (f % 4) * 4 (A of the
+//     first layer: M = points, K = features);
+//   W1: element (j, f) at (f / 4) * 1024 + j * 16 + (f % 4) * 4 (B: N = hidden, K = f).
+// Backward only, bf16:
+//   W1' = w2 (.) W1 in three terms: element (f, j) at (j / 8) * 256 + f * 16 + (j % 8) * 2
+//     (B of dfeat: N = f, K = hidden);
+//   ReLU mask rows: element (p, j) at (j / 8) * 2048 + p * 16 + (j % 8) * 2 (A of dfeat:
+//     M = points, K = hidden);
+//   ReLU mask transposed: element (j, p) at (j / 8) * 2304 + (j % 8) * 16 + (p / 8) * 144
+//     + (p % 8) * 2 (A of dW1: M = hidden, K = points);
+//   dr (.) feat in three terms, dr itself in column L*C: element (f, p) at (f / 8) * 2304
+//     + (f % 8) * 16 + (p / 8) * 144 + (p % 8) * 2 (B of dW1: N = f, K = points).
+// The transposed tiles are written a column per thread; their 144-byte K chunks (128 +
+// 16 of padding) put a warp's 32 columns on distinct banks.
+constexpr uint32_t kFeatBytes = kTile * kMaxFeat * 4;   // 8 KB
+constexpr uint32_t kW1Bytes = kHidden * kMaxFeat * 4;   // 4 KB
+constexpr uint32_t kW1pBytes = kMaxFeat * kHidden * 2;  // 2 KB per term
+constexpr uint32_t kMaskBytes = kTile * kHidden * 2;    // 16 KB
+constexpr uint32_t kPadChunk = 144, kPadGroup = 16 * kPadChunk;
+constexpr uint32_t kMaskTBytes = (kHidden / 8) * kPadGroup;   // 18 KB
+constexpr uint32_t kBpBytes = (kMaxFeat / 8) * kPadGroup;     // 4.5 KB per term
+constexpr uint32_t OFF_FEAT_HI = 0;
+constexpr uint32_t OFF_FEAT_LO = OFF_FEAT_HI + kFeatBytes;
+constexpr uint32_t OFF_W1_HI = OFF_FEAT_LO + kFeatBytes;
+constexpr uint32_t OFF_W1_LO = OFF_W1_HI + kW1Bytes;
+constexpr uint32_t OFF_W1P = OFF_W1_LO + kW1Bytes;            // backward only from here
+constexpr uint32_t OFF_MASK = OFF_W1P + 3 * kW1pBytes;
+constexpr uint32_t OFF_MASKT = OFF_MASK + kMaskBytes;
+constexpr uint32_t OFF_BP = OFF_MASKT + kMaskTBytes;
+constexpr uint32_t OFF_MISC_BWD = OFF_BP + 3 * kBpBytes;
+struct Misc {
+  float b1[kHidden];
+  float w2[kHidden];
+  Level lv[kMaxFeat];
+  uint64_t bar;
+  uint32_t tmem;
+  float b2;
+};
+constexpr uint32_t kSmemFwd = OFF_W1P + sizeof(Misc);
+constexpr uint32_t kSmemBwd = OFF_MISC_BWD + sizeof(Misc);
+static_assert(OFF_MISC_BWD % 16 == 0 && OFF_BP % 16 == 0 && OFF_MASKT % 16 == 0, "16-byte operand alignment");
+
+// Tensor-memory columns: first-layer accumulator [128 x 64], mask . W1' [128 x 16],
+// mask^T . (dr feat) [64 x 16] (rows in lanes 0-15 of each 32-lane quarter, the
+// M = 64 layout).
+constexpr uint32_t COL_D1 = 0, COL_DF = 64, COL_DW = 96;
+constexpr uint32_t kColsFwd = 64, kColsBwd = 128;
+
+constexpr uint32_t IDESC_L1 = idesc_tf32(kTile, kHidden, false, false);  // feat x W1, tf32
+constexpr uint32_t IDESC_DF = idesc_bf16(kTile, 16);                     // mask x W1', bf16
+constexpr uint32_t IDESC_DW = idesc_bf16(kHidden, 16);                   // mask^T x (dr feat), bf16
+
+struct NetLaunch {
+  const float* coords;
+  const float* table;
+  const int32_t* offsets;
+  const float *w1, *b1, *w2, *b2;
+  const float* features_in;  // backward: the forward's record
+  const float* grad_density;
+  float* density;
+  float* features_out;       // forward: the record, or null
+  float* coords_warped;
+  float *g_table, *g_w1, *g_b1, *g_w2, *g_b2;
+  int32_t* status;
+  long long n;
+  uint32_t L, F, stride;     // levels, features (L * C), record floats per point
+  float S;
+  uint32_t H;
+  float density_bias, warp_scale, grid_bound, inv_two_bound;
+  int warp;
+  bool raw_output;
+  bool hash, align, vec_table, vec_pair;
+  unsigned long long wait_ns;
+  int test_stall;
+};
+
+// ------------------------------------------------------------ per-point steps
+
+// The coordinate map of models.py:19-33 (and coord.contract, source/utils/coord.py:
+// 5-11), then GridEncoder.forward's (x + bound) / (2 bound), rounded as torch's CUDA
+// ops round them (a division by a Python scalar is a multiplication by its float32
+// reciprocal; sqrt and division correctly rounded).
+__device__ __forceinline__ void warp_point(const NetLaunch& P, float x0, float x1, float x2, float (&w)[3],
+                                           float (&u)[3]) {
+  w[0] = x0; w[1] = x1; w[2] = x2;
+  if (P.warp == N3DS_WARP_SCALE) {
+#pragma unroll
+    for (int d = 0; d < 3; d++) w[d] = w[d] * P.warp_scale;
+  } else if (P.warp == N3DS_WARP_CONTRACT) {
+    const float eps = 1.1920928955078125e-7f;  // torch.finfo(float32).eps
+    // torch.sum(x ** 2, dim=-1) as torch's CUDA reduction forms it for three values:
+    // squares rounded, then (x0^2 + x2^2) + x1^2, no fused multiply-add
+    const float m = fmaxf(__fadd_rn(__fadd_rn(__fmul_rn(x0, x0), __fmul_rn(x2, x2)), __fmul_rn(x1, x1)), eps);
+    if (!(m <= 1.f)) {
+      // correctly rounded square root and division, as torch's ops (the library is
+      // built with approximate sqrt and division)
+      const float k = __fdiv_rn(__fsub_rn(__fmul_rn(2.f, __fsqrt_rn(m)), 1.f), m);
+#pragma unroll
+      for (int d = 0; d < 3; d++) w[d] = k * w[d];
+    }
+#pragma unroll
+    for (int d = 0; d < 3; d++) w[d] = w[d] * 0.5f;
+  }
+#pragma unroll
+  for (int d = 0; d < 3; d++) u[d] = (w[d] + P.grid_bound) * P.inv_two_bound;
+}
+
+// L * C features of point u (grid_fwd_kernel's arithmetic, n3ds_grid.cu), zero when
+// u leaves [0, 1]^3 as in the reference.
+template <int C>
+__device__ __forceinline__ void encode_point(const NetLaunch& P, const Level* lvs, const float (&u)[3],
+                                             float (&f)[kMaxFeat]) {
+#pragma unroll
+  for (int i = 0; i < kMaxFeat; i++) f[i] = 0.f;
+  if (!point_in_range(u, 3)) return;
+#pragma unroll
+  for (int l = 0; l < kMaxFeat / C; l++) {
+    if (l < (int)P.L) {
+      const Level lv = lvs[l];
+      const float* tab = P.table + (size_t)lv.base * C;
+      uint32_t cell[3];
+      float frac[3], deriv[3];
+      locate<3>(u, lv, P.align, false, cell, frac, deriv);
+      const bool pair_level = P.vec_pair && !(lv.base & 1u) && lv.hsize >= kPairMinRows;
+      float res[C];
+#pragma unroll
+      for (int c = 0; c < C; c++) res[c] = 0.f;
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        uint32_t c0[3], c1[3];
+        const float w0 = corner_of<3>(2 * j, cell, frac, c0);
+        const float w1 = corner_of<3>(2 * j + 1, cell, frac, c1);
+        float v0[C], v1[C];
+        const uint32_t r0 = cell_row<3>(c0, lv, P.hash, P.align), r1 = cell_row<3>(c1, lv, P.hash, P.align);
+        load_rows2<float, C>(tab, r0, r1, P.vec_table, pair_level && (r0 | 1u) < lv.hsize, v0, v1);
+#pragma unroll
+        for (int c = 0; c < C; c++) res[c] += w0 * v0[c];
+#pragma unroll
+        for (int c = 0; c < C; c++) res[c] += w1 * v1[c];
+      }
+#pragma unroll
+      for (int c = 0; c < C; c++) f[l * C + c] = res[c];
+    }
+  }
+}
+
+// The first n_chunks 4-value chunks of a 16-value row into the tile's hi and lo
+// buffers.
+__device__ __forceinline__ void store_split_row(uint8_t* hi_base, uint8_t* lo_base, uint32_t row_off,
+                                                uint32_t chunk_stride, const float (&v)[16], int n_chunks) {
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    if (c >= n_chunks) break;
+    float h[4], l[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) split_tf32(v[4 * c + k], h[k], l[k]);
+    *reinterpret_cast<float4*>(hi_base + c * chunk_stride + row_off) = make_float4(h[0], h[1], h[2], h[3]);
+    *reinterpret_cast<float4*>(lo_base + c * chunk_stride + row_off) = make_float4(l[0], l[1], l[2], l[3]);
+  }
+}
+
+// torch.relu: NaN stays NaN.
+__device__ __forceinline__ float relu_t(float x) { return (x > 0.f || x != x) ? x : 0.f; }
+
+// torch's softplus (beta 1, threshold 20) and its backward, g * e^z / (e^z + 1)
+// evaluated in that order.
+__device__ __forceinline__ float softplus_t(float z) { return z > 20.f ? z : log1pf(expf(z)); }
+__device__ __forceinline__ float softplus_backward_t(float g, float z) {
+  if (z > 20.f) return g;
+  const float e = expf(z);
+  return __fdiv_rn(__fmul_rn(g, e), __fadd_rn(e, 1.f));
+}
+
+// Sum of v[0..15] over the warp's lanes by transposition: lane l returns the sum of
+// slot l >> 1 (each slot ends in two lanes).
+__device__ __forceinline__ float warp_slot_sum16(float (&v)[16], int lane) {
+#pragma unroll
+  for (int s = 0; s < 4; s++) {
+    const int o = 16 >> s, n = 8 >> s;
+    const bool up = (lane & o) != 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      if (i < n) {
+        const float send = up ? v[i] : v[i + n];
+        const float keep = up ? v[i + n] : v[i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+      }
+    }
+  }
+  return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
+}
+
+// bf16 bits of x (round to nearest even) and x = h + m + l in three bf16 terms (each
+// remainder exact in float32): 24 significant bits, a float32 value to about 2^-24.
+__device__ __forceinline__ uint16_t bf16_bits(float x) { return __bfloat16_as_ushort(__float2bfloat16_rn(x)); }
+__device__ __forceinline__ void split3_bf16(float x, uint16_t& h, uint16_t& m, uint16_t& l) {
+  const __nv_bfloat16 bh = __float2bfloat16_rn(x);
+  const float r1 = x - __bfloat162float(bh);
+  const __nv_bfloat16 bm = __float2bfloat16_rn(r1);
+  const float r2 = r1 - __bfloat162float(bm);
+  h = __bfloat16_as_ushort(bh);
+  m = __bfloat16_as_ushort(bm);
+  l = bf16_bits(r2);
+}
+
+// CTA set-up shared by both kernels: W1 split into its tile buffers (and, for the
+// backward, W1' = w2 (.) W1 in three bf16 terms), biases, the second layer, level
+// geometry, the mbarrier and the tensor memory.
+__device__ __forceinline__ void setup_cta(const NetLaunch& P, uint8_t* smem, Misc* M, uint32_t cols, bool backward) {
+  const int tid = threadIdx.x;
+  for (int i = tid; i < kHidden * kMaxFeat; i += kTile) {
+    const int j = i / kMaxFeat, f = i % kMaxFeat;
+    const float w = f < (int)P.F ? P.w1[j * P.F + f] : 0.f;
+    float h, l;
+    split_tf32(w, h, l);
+    const uint32_t off = (f / 4) * 1024 + j * 16 + (f % 4) * 4;
+    *reinterpret_cast<float*>(smem + OFF_W1_HI + off) = h;
+    *reinterpret_cast<float*>(smem + OFF_W1_LO + off) = l;
+    if (backward) {
+      uint16_t t[3];
+      split3_bf16(w * P.w2[j], t[0], t[1], t[2]);
+      const uint32_t o2 = (j / 8) * 256 + f * 16 + (j % 8) * 2;
+#pragma unroll
+      for (int k = 0; k < 3; k++) *reinterpret_cast<uint16_t*>(smem + OFF_W1P + k * kW1pBytes + o2) = t[k];
+    }
+  }
+  if (tid < kHidden) {
+    M->b1[tid] = P.b1[tid];
+    M->w2[tid] = P.w2[tid];
+  }
+  if (tid < (int)P.L) M->lv[tid] = level_of(P.offsets, tid, P.S, P.H);
+  if (tid == 0) {
+    M->b2 = P.b2[0];
+    mbar_init(&M->bar, 1);
+  }
+  if (tid < 32) tmem_alloc(&M->tmem, cols);
+  fence_proxy_async();
+  tc_fence_before_sync();
+  __syncthreads();
+  tc_fence_after_sync();
+}
+
+// Wait for the tensor cores' arrival on the barrier (bounded); CTA-uniform result.
+// The phase advances only on success, so that a later wait still watches the phase
+// that work in flight will complete.
+__device__ __forceinline__ bool wait_mma(const NetLaunch& P, Misc* M, uint32_t& phase) {
+  const bool ok = __syncthreads_and(mbar_wait_bounded(&M->bar, phase, P.wait_ns)) != 0;
+  if (ok) {
+    phase ^= 1u;
+    tc_fence_after_sync();
+  }
+  return ok;
+}
+
+// Leave: after a timeout, one more bounded wait for work still in flight; then the
+// tensor memory is freed by the warp that allocated it.
+__device__ __forceinline__ void teardown(const NetLaunch& P, Misc* M, uint32_t phase, bool timed_out, uint32_t cols) {
+  if (timed_out) {
+    if (threadIdx.x == 0) {
+      if (P.status) atomicOr(P.status, kStatusWait);
+      if (!P.test_stall) mbar_wait_bounded(&M->bar, phase, P.wait_ns);
+    }
+  }
+  tc_fence_before_sync();
+  __syncthreads();
+  tc_fence_after_sync();
+  if (threadIdx.x < 32) tmem_dealloc(M->tmem, cols);
+}
+
+// ------------------------------------------------------------ forward
+
+template <int C>
+__global__ void __launch_bounds__(kTile, 4) density_fwd_kernel(NetLaunch P) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  Misc* M = reinterpret_cast<Misc*>(smem + OFF_W1P);
+  setup_cta(P, smem, M, kColsFwd, false);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const uint32_t tmem = M->tmem;
+  const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+  const int ks_count = (int)((P.F + 7) / 8);
+  const long long n_tiles = (P.n + kTile - 1) / kTile;
+  uint32_t phase = 0;
+  bool timed_out = false;
+  for (long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const long long b = tile * kTile + tid;
+    const bool valid = b < P.n;
+    float f[kMaxFeat];
+    {
+      float x[3] = {0.f, 0.f, 0.f}, w[3], u[3];
+      if (valid) {
+        x[0] = P.coords[3 * b];
+        x[1] = P.coords[3 * b + 1];
+        x[2] = P.coords[3 * b + 2];
+      }
+      warp_point(P, x[0], x[1], x[2], w, u);
+      if (valid) {
+        encode_point<C>(P, M->lv, u, f);
+        if (P.coords_warped) {
+          P.coords_warped[3 * b] = w[0];
+          P.coords_warped[3 * b + 1] = w[1];
+          P.coords_warped[3 * b + 2] = w[2];
+        }
+        if (P.features_out) {
+          float4* rec = reinterpret_cast<float4*>(P.features_out + b * P.stride);
+#pragma unroll
+          for (int c = 0; c < kMaxFeat / 4; c++) {
+            if (c < (int)(P.stride / 4)) rec[c] = make_float4(f[4 * c], f[4 * c + 1], f[4 * c + 2], f[4 * c + 3]);
+          }
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < kMaxFeat; i++) f[i] = 0.f;
+      }
+    }
+    store_split_row(smem + OFF_FEAT_HI, smem + OFF_FEAT_LO, tid * 16, 2048, f, 2 * ks_count);
+    fence_proxy_async();
+    tc_fence_before_sync();
+    __syncthreads();
+    tc_fence_after_sync();
+    if (tid == 0 && !P.test_stall) {
+      const uint32_t fh = smem_u32(smem + OFF_FEAT_HI), fl = smem_u32(smem + OFF_FEAT_LO);
+      const uint32_t wh = smem_u32(smem + OFF_W1_HI), wl = smem_u32(smem + OFF_W1_LO);
+      for (int ks = 0; ks < ks_count; ks++) {
+        const uint64_t a_hi = smem_desc(fh + ks * 4096, 2048, 128), a_lo = smem_desc(fl + ks * 4096, 2048, 128);
+        const uint64_t b_hi = smem_desc(wh + ks * 2048, 1024, 128), b_lo = smem_desc(wl + ks * 2048, 1024, 128);
+        mma_tf32(tmem + COL_D1, a_lo, b_hi, IDESC_L1, ks > 0);
+        mma_tf32(tmem + COL_D1, a_hi, b_lo, IDESC_L1, true);
+        mma_tf32(tmem + COL_D1, a_hi, b_hi, IDESC_L1, true);
+      }
+      mma_commit(&M->bar);
+    }
+    if (!wait_mma(P, M, phase)) {
+      timed_out = true;
+      break;
+    }
+    float raw = M->b2;
+#pragma unroll
+    for (int c = 0; c < kHidden / 16; c++) {
+      float v[16];
+      tmem_ld16(lane_addr + COL_D1 + c * 16, v);
+#pragma unroll
+      for (int k = 0; k < 16; k++) raw = fmaf(relu_t(v[k] + M->b1[c * 16 + k]), M->w2[c * 16 + k], raw);
+    }
+    if (valid) P.density[b] = P.raw_output ? raw : softplus_t(raw + P.density_bias);
+  }
+  teardown(P, M, phase, timed_out, kColsFwd);
+}
+
+// ------------------------------------------------------------ backward
+
+// grad_table[corner rows of point u at level lv] += w * g, with runs of lanes in one
+// cell summed first (grid_bwd_kernel's scheme, n3ds_grid.cu). Every lane calls it.
+template <int C>
+__device__ __forceinline__ void scatter_level(const NetLaunch& P, const Level& lv, const float (&u)[3], bool valid,
+                                              const float (&g)[C], int lane) {
+  constexpr unsigned kFull = 0xffffffffu;
+  float* tab = P.g_table + (size_t)lv.base * C;
+  uint32_t cell[3];
+  float frac[3], deriv[3];
+  locate<3>(u, lv, P.align, false, cell, frac, deriv);
+  const int prev_valid = __shfl_up_sync(kFull, (int)valid, 1);
+  bool head = !valid || lane == 0 || !prev_valid;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const uint32_t prev = __shfl_up_sync(kFull, cell[d], 1);
+    head = head || prev != cell[d];
+  }
+  const unsigned heads = __ballot_sync(kFull, head);
+  if (heads == kFull) {
+    if (!valid) return;
+#pragma unroll
+    for (int corner = 0; corner < 8; corner++) {
+      uint32_t cc[3];
+      const float w = corner_of<3>(corner, cell, frac, cc);
+      float v[C];
+#pragma unroll
+      for (int c = 0; c < C; c++) v[c] = w * g[c];
+      scatter_row<float, C>(tab + (size_t)cell_row<3>(cc, lv, P.hash, P.align) * C, P.vec_table, v);
+    }
+    return;
+  }
+  const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
+  const int head_lane = 31 - __clz(heads & (kFull >> (31 - lane)));
+  const unsigned longest = __reduce_max_sync(kFull, tail ? (unsigned)(lane - head_lane + 1) : 0u);
+#pragma unroll
+  for (int corner = 0; corner < 8; corner++) {
+    uint32_t cc[3];
+    const float w = valid ? corner_of<3>(corner, cell, frac, cc) : 0.f;
+    float v[C];
+#pragma unroll
+    for (int c = 0; c < C; c++) v[c] = w * g[c];
+    for (unsigned off = 1; off < longest; off <<= 1) {
+#pragma unroll
+      for (int c = 0; c < C; c++) {
+        const float t = __shfl_up_sync(kFull, v[c], off);
+        if (lane - (int)off >= head_lane) v[c] += t;
+      }
+    }
+    if (tail && valid) scatter_row<float, C>(tab + (size_t)cell_row<3>(cc, lv, P.hash, P.align) * C, P.vec_table, v);
+  }
+}
+
+// Backward. With mask[p, j] = [pre > 0] (exactly 0 or 1 in bf16) the ReLU adjoint
+// dh = dr w2 mask factors as
+//   dfeat[p, f] = dr[p] sum_j mask[p, j] W1'[j, f],      W1' = w2 (.) W1,
+//   dW1[j, f]   = w2[j] sum_p mask[p, j] (dr feat)[p, f],  db1 the same with feat = 1,
+// two bf16 products whose operand terms are exact (the mask) or float32 split in three
+// bf16 terms, accumulated in float32: float32 accuracy from kind::f16 MMAs with
+// K-major operands only.
+template <int C>
+__global__ void __launch_bounds__(kTile, 2) density_bwd_kernel(NetLaunch P) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  Misc* M = reinterpret_cast<Misc*>(smem + OFF_MISC_BWD);
+  setup_cta(P, smem, M, kColsBwd, true);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t tmem = M->tmem;
+  const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+  const int ks_count = (int)((P.F + 7) / 8);
+  const long long n_tiles = (P.n + kTile - 1) / kTile;
+  uint32_t phase = 0;
+  bool timed_out = false, any = false;
+  float acc_w2[kHidden / 16] = {0.f, 0.f, 0.f, 0.f};
+  float acc_b2 = 0.f;
+  const uint32_t fh = smem_u32(smem + OFF_FEAT_HI), fl = smem_u32(smem + OFF_FEAT_LO);
+  const uint32_t wh = smem_u32(smem + OFF_W1_HI), wl = smem_u32(smem + OFF_W1_LO);
+  const uint32_t w1p = smem_u32(smem + OFF_W1P), mask = smem_u32(smem + OFF_MASK);
+  const uint32_t maskt = smem_u32(smem + OFF_MASKT), bp = smem_u32(smem + OFF_BP);
+  // this thread's column offset in the transposed tiles
+  const uint32_t col_off = (uint32_t)(tid / 8) * kPadChunk + (uint32_t)(tid % 8) * 2;
+  for (long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const long long b = tile * kTile + tid;
+    const bool valid = b < P.n;
+    float u[3] = {0.f, 0.f, 0.f};
+    float g = 0.f;
+    float f[kMaxFeat];
+#pragma unroll
+    for (int i = 0; i < kMaxFeat; i++) f[i] = 0.f;
+    if (valid) {
+      float w[3];
+      warp_point(P, P.coords[3 * b], P.coords[3 * b + 1], P.coords[3 * b + 2], w, u);
+      const float4* rec = reinterpret_cast<const float4*>(P.features_in + b * P.stride);
+#pragma unroll
+      for (int c = 0; c < kMaxFeat / 4; c++) {
+        if (c < (int)(P.stride / 4)) {
+          const float4 r = rec[c];
+          f[4 * c] = r.x; f[4 * c + 1] = r.y; f[4 * c + 2] = r.z; f[4 * c + 3] = r.w;
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < kMaxFeat; i++) {
+        if (i >= (int)P.F) f[i] = 0.f;
+      }
+      g = P.grad_density[b];
+    }
+    store_split_row(smem + OFF_FEAT_HI, smem + OFF_FEAT_LO, tid * 16, 2048, f, 2 * ks_count);
+    fence_proxy_async();
+    tc_fence_before_sync();
+    __syncthreads();
+    tc_fence_after_sync();
+    if (tid == 0 && !P.test_stall) {
+      for (int ks = 0; ks < ks_count; ks++) {
+        const uint64_t a_hi = smem_desc(fh + ks * 4096, 2048, 128), a_lo = smem_desc(fl + ks * 4096, 2048, 128);
+        const uint64_t b_hi = smem_desc(wh + ks * 2048, 1024, 128), b_lo = smem_desc(wl + ks * 2048, 1024, 128);
+        mma_tf32(tmem + COL_D1, a_lo, b_hi, IDESC_L1, ks > 0);
+        mma_tf32(tmem + COL_D1, a_hi, b_lo, IDESC_L1, true);
+        mma_tf32(tmem + COL_D1, a_hi, b_hi, IDESC_L1, true);
+      }
+      mma_commit(&M->bar);
+    }
+    if (!wait_mma(P, M, phase)) {
+      timed_out = true;
+      break;
+    }
+    // raw, then d raw through softplus
+    float raw = M->b2;
+#pragma unroll
+    for (int c = 0; c < kHidden / 16; c++) {
+      float v[16];
+      tmem_ld16(lane_addr + COL_D1 + c * 16, v);
+#pragma unroll
+      for (int k = 0; k < 16; k++) raw = fmaf(relu_t(v[k] + M->b1[c * 16 + k]), M->w2[c * 16 + k], raw);
+    }
+    const float dr = P.raw_output ? g : softplus_backward_t(g, raw + P.density_bias);
+    {
+      float s = dr;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      acc_b2 += s;
+    }
+    // the ReLU mask (rows and transposed) and dW2 (warp sums of dr relu(pre))
+#pragma unroll
+    for (int c = 0; c < kHidden / 16; c++) {
+      float v[16];
+      tmem_ld16(lane_addr + COL_D1 + c * 16, v);
+      uint32_t words[8];
+#pragma unroll
+      for (int k = 0; k < 16; k++) {
+        const float pre = v[k] + M->b1[c * 16 + k];
+        // torch.relu's backward passes the gradient unless the output is <= 0 (NaN passes)
+        const uint32_t one = pre <= 0.f ? 0u : 0x3F80u;
+        if (k % 2 == 0) words[k / 2] = one;
+        else words[k / 2] |= one << 16;
+        const int j = c * 16 + k;
+        *reinterpret_cast<uint16_t*>(smem + OFF_MASKT + (j / 8) * kPadGroup + (j % 8) * 16 + col_off) =
+            (uint16_t)one;
+        v[k] = dr * relu_t(pre);
+      }
+      *reinterpret_cast<uint4*>(smem + OFF_MASK + (2 * c) * 2048 + tid * 16) =
+          make_uint4(words[0], words[1], words[2], words[3]);
+      *reinterpret_cast<uint4*>(smem + OFF_MASK + (2 * c + 1) * 2048 + tid * 16) =
+          make_uint4(words[4], words[5], words[6], words[7]);
+      acc_w2[c] += warp_slot_sum16(v, lane);
+    }
+    // dr (.) feat and dr, three bf16 terms, transposed
+#pragma unroll
+    for (int i = 0; i < kMaxFeat; i++) {
+      const float x = i < (int)P.F ? dr * f[i] : (i == (int)P.F ? dr : 0.f);
+      uint16_t t[3];
+      split3_bf16(x, t[0], t[1], t[2]);
+      const uint32_t o = (i / 8) * kPadGroup + (i % 8) * 16 + col_off;
+#pragma unroll
+      for (int k = 0; k < 3; k++) *reinterpret_cast<uint16_t*>(smem + OFF_BP + k * kBpBytes + o) = t[k];
+    }
+    fence_proxy_async();
+    tc_fence_before_sync();
+    __syncthreads();
+    tc_fence_after_sync();
+    if (tid == 0 && !P.test_stall) {
+      // mask . W1' (M 128 points, N 16, K 64 hidden)
+      for (int ks = 0; ks < kHidden / 16; ks++) {
+        const uint64_t a = smem_desc(mask + ks * 4096, 2048, 128);
+#pragma unroll
+        for (int t = 0; t < 3; t++)
+          mma_bf16(tmem + COL_DF, a, smem_desc(w1p + t * kW1pBytes + ks * 512, 256, 128), IDESC_DF, ks > 0 || t > 0);
+      }
+      // mask^T . (dr feat) (M 64 hidden, N 16, K 128 points), accumulated over tiles
+      for (int ks = 0; ks < kTile / 16; ks++) {
+        const uint64_t a = smem_desc(maskt + ks * 2 * kPadChunk, kPadChunk, kPadGroup);
+#pragma unroll
+        for (int t = 0; t < 3; t++)
+          mma_bf16(tmem + COL_DW, a, smem_desc(bp + t * kBpBytes + ks * 2 * kPadChunk, kPadChunk, kPadGroup),
+                   IDESC_DW, any || ks > 0 || t > 0);
+      }
+      mma_commit(&M->bar);
+    }
+    any = true;
+    if (!wait_mma(P, M, phase)) {
+      timed_out = true;
+      break;
+    }
+    float df[16];
+    tmem_ld16(lane_addr + COL_DF, df);
+    const bool in_grid = valid && point_in_range(u, 3);
+#pragma unroll
+    for (int l = 0; l < kMaxFeat / C; l++) {
+      if (l < (int)P.L) {
+        float gl[C];
+#pragma unroll
+        for (int c = 0; c < C; c++) gl[c] = in_grid ? dr * df[l * C + c] : 0.f;
+        scatter_level<C>(P, M->lv[l], u, in_grid, gl, lane);
+      }
+    }
+  }
+  if (any && !timed_out) {
+    float v[16];
+    tmem_ld16(lane_addr + COL_DW, v);
+    if (lane < 16) {  // M = 64 rows: lanes 0-15 of each quarter
+      const int j = warp * 16 + lane;
+      const float w2j = M->w2[j];
+#pragma unroll
+      for (int i = 0; i < kMaxFeat; i++) {
+        if (i < (int)P.F) atomicAdd(P.g_w1 + j * P.F + i, w2j * v[i]);
+        else if (i == (int)P.F) atomicAdd(P.g_b1 + j, w2j * v[i]);
+      }
+    }
+    if ((lane & 1) == 0) {
+#pragma unroll
+      for (int c = 0; c < kHidden / 16; c++) atomicAdd(P.g_w2 + c * 16 + (lane >> 1), acc_w2[c]);
+    }
+    if (lane == 0) atomicAdd(P.g_b2, acc_b2);
+  }
+  teardown(P, M, phase, timed_out, kColsBwd);
+}
+
+// ------------------------------------------------------------ hash-decay statistics
+
+constexpr int kRedThreads = 256;
+
+// Per (level, channel) sums of squares: blocks of one level stride over its rows.
+__global__ void __launch_bounds__(kRedThreads) level_sumsq_kernel(const float* __restrict__ table,
+                                                                  const int32_t* __restrict__ offsets, uint32_t C,
+                                                                  uint32_t n_ch, float* __restrict__ out) {
+  const uint32_t l = blockIdx.y;
+  const uint32_t r0 = (uint32_t)offsets[l], r1 = (uint32_t)offsets[l + 1];
+  const float inv_rows = 1.f / (float)(r1 - r0);
+  __shared__ float red[kRedThreads / 32][8];
+  float acc[8];
+#pragma unroll
+  for (int c = 0; c < 8; c++) acc[c] = 0.f;
+  for (uint32_t r = r0 + blockIdx.x * kRedThreads + threadIdx.x; r < r1; r += gridDim.x * kRedThreads) {
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      if (c < (int)n_ch) {
+        const float t = table[(size_t)r * C + c];
+        acc[c] = fmaf(t, t, acc[c]);
+      }
+    }
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int c = 0; c < 8; c++) {
+    float s = acc[c];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) red[w][c] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < n_ch) {
+    float s = 0.f;
+    for (int i = 0; i < kRedThreads / 32; i++) s += red[i][threadIdx.x];
+    atomicAdd(out + l * C + threadIdx.x, s * inv_rows);
+  }
+}
+
+__global__ void __launch_bounds__(kRedThreads) level_sumsq_bwd_kernel(const float* __restrict__ table,
+                                                                      const int32_t* __restrict__ offsets,
+                                                                      uint32_t C, uint32_t n_ch,
+                                                                      const float* __restrict__ grad_out,
+                                                                      float* __restrict__ grad_table) {
+  const uint32_t l = blockIdx.y;
+  const uint32_t r0 = (uint32_t)offsets[l], r1 = (uint32_t)offsets[l + 1];
+  const float inv_rows = 1.f / (float)(r1 - r0);
+  for (uint32_t r = r0 + blockIdx.x * kRedThreads + threadIdx.x; r < r1; r += gridDim.x * kRedThreads) {
+    for (uint32_t c = 0; c < n_ch; c++) {
+      const size_t i = (size_t)r * C + c;
+      grad_table[i] += grad_out[l * C + c] * 2.f * table[i] * inv_rows;
+    }
+  }
+}
+
+// ------------------------------------------------------------ host side
+
+int launch_error(const char* what) {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return n3ds::report_error(N3DS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  return N3DS_OK;
+}
+
+bool aligned(const void* p, size_t bytes) { return ((uintptr_t)p % bytes) == 0; }
+
+int check_net(const n3ds_density_net_t* net, int64_t n) {
+  if (!net) return n3ds::report_error(N3DS_ERR_INVALID, "density net: null descriptor");
+  if (n < 0) return n3ds::report_error(N3DS_ERR_INVALID, "density net: negative point count");
+  const uint32_t C = net->level_dim, L = net->n_levels;
+  if (C != 1 && C != 2 && C != 4)
+    return n3ds::report_error(N3DS_ERR_UNSUPPORTED, "density net: level_dim must be 1, 2 or 4");
+  // the product tiles have 16 columns: L * C features and the column of d raw
+  if (L < 1 || L * C > (uint32_t)kMaxFeat - 1)
+    return n3ds::report_error(N3DS_ERR_UNSUPPORTED, "density net: n_levels * level_dim must be in [1, 15]");
+  if (net->base_resolution < 1) return n3ds::report_error(N3DS_ERR_INVALID, "density net: base resolution must be >= 1");
+  if (net->warp != N3DS_WARP_SCALE && net->warp != N3DS_WARP_CONTRACT && net->warp != N3DS_WARP_NONE)
+    return n3ds::report_error(N3DS_ERR_INVALID, "density net: unknown warp");
+  if (!(net->grid_bound > 0.f)) return n3ds::report_error(N3DS_ERR_INVALID, "density net: grid_bound must be > 0");
+  if (n > 0 && (!net->table || !net->offsets || !net->w1 || !net->b1 || !net->w2 || !net->b2))
+    return n3ds::report_error(N3DS_ERR_INVALID, "density net: table, offsets and the four layer tensors are required");
+  return N3DS_OK;
+}
+
+NetLaunch make_launch(const n3ds_density_net_t* net, const float* coords, int64_t n) {
+  NetLaunch P{};
+  P.coords = coords;
+  P.table = net->table;
+  P.offsets = net->offsets;
+  P.w1 = net->w1;
+  P.b1 = net->b1;
+  P.w2 = net->w2;
+  P.b2 = net->b2;
+  P.status = net->status;
+  P.n = n;
+  P.L = net->n_levels;
+  P.F = net->n_levels * net->level_dim;
+  P.stride = (P.F + 3) / 4 * 4;
+  P.S = net->log2_per_level_scale;
+  P.H = net->base_resolution;
+  P.density_bias = net->density_bias;
+  P.warp = net->warp;
+  P.raw_output = net->raw_output != 0;
+  P.warp_scale = net->warp_scale;
+  P.grid_bound = net->grid_bound;
+  P.inv_two_bound = 1.f / (2.f * net->grid_bound);
+  P.hash = net->gridtype == N3DS_GRID_HASH;
+  P.align = net->align_corners != 0;
+  const uint32_t C = net->level_dim;
+  const size_t vw = C * 4 < 16 ? C * 4 : 16;
+  P.vec_table = vw > 4 && aligned(net->table, vw);
+  // a pair of rows is one load of 2 C floats (8, 16 or 32 bytes), aligned to its size
+  P.vec_pair = aligned(net->table, 2 * C * 4);
+  P.wait_ns = (unsigned long long)(net->wait_limit_us > 0 ? net->wait_limit_us : 1000000) * 1000ull;
+  P.test_stall = net->test_stall;
+  return P;
+}
+
+// CTAs the kernel can keep resident on the device (cached per kernel and device):
+// the occupancy limit, and at most 512 / cols per SM so that every resident CTA's
+// tensor-memory allocation succeeds at once.
+template <typename K>
+int resident(K kernel, uint32_t smem, uint32_t cols, int* cache) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 16) dev = 0;
+  if (cache[dev] == 0) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int blocks = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, kTile, smem);
+    if (blocks > (int)(512 / cols)) blocks = (int)(512 / cols);
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cache[dev] = (blocks > 0 ? blocks : 1) * (sms > 0 ? sms : 1);
+  }
+  return cache[dev];
+}
+
+template <int C>
+int fwd_c(const NetLaunch& P, cudaStream_t st) {
+  static int cache[16] = {0};
+  const int slots = resident(density_fwd_kernel<C>, kSmemFwd, kColsFwd, cache);
+  const long long tiles = (P.n + kTile - 1) / kTile;
+  const int grid = (int)(tiles < slots ? tiles : slots);
+  density_fwd_kernel<C><<<grid, kTile, kSmemFwd, st>>>(P);
+  return launch_error("density net forward");
+}
+
+template <int C>
+int bwd_c(const NetLaunch& P, cudaStream_t st) {
+  static int cache[16] = {0};
+  const int slots = resident(density_bwd_kernel<C>, kSmemBwd, kColsBwd, cache);
+  const long long tiles = (P.n + kTile - 1) / kTile;
+  const int grid = (int)(tiles < slots ? tiles : slots);
+  density_bwd_kernel<C><<<grid, kTile, kSmemBwd, st>>>(P);
+  return launch_error("density net backward");
+}
+
+int check_levels(const float* table, const int32_t* offsets, uint32_t L, uint32_t C, const void* out) {
+  if (L < 1 || L > 65535) return n3ds::report_error(N3DS_ERR_INVALID, "level statistics: levels must be in [1, 65535]");
+  if (C < 1 || C > 8) return n3ds::report_error(N3DS_ERR_INVALID, "level statistics: level_dim must be in [1, 8]");
+  if (!table || !offsets || !out) return n3ds::report_error(N3DS_ERR_INVALID, "level statistics: null pointer");
+  return N3DS_OK;
+}
+
+}  // namespace
+
+extern "C" int n3ds_density_net_feature_stride(uint32_t n_levels, uint32_t level_dim) {
+  return (int)((n_levels * level_dim + 3) / 4 * 4);
+}
+
+extern "C" int n3ds_density_net_forward(const n3ds_density_net_t* net, const float* coords, int64_t n_points,
+                                        float* density, float* features, float* coords_warped,
+                                        n3ds_stream_t stream) {
+  if (int rc = check_net(net, n_points)) return rc;
+  if (n_points == 0) return N3DS_OK;
+  if (!coords || !density) return n3ds::report_error(N3DS_ERR_INVALID, "density net: coords and density are required");
+  if (features && !aligned(features, 16))
+    return n3ds::report_error(N3DS_ERR_INVALID, "density net: the feature record must be 16-byte aligned");
+  NetLaunch P = make_launch(net, coords, n_points);
+  P.density = density;
+  P.features_out = features;
+  P.coords_warped = coords_warped;
+  const cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  switch (net->level_dim) {
+    case 1: return fwd_c<1>(P, st);
+    case 2: return fwd_c<2>(P, st);
+    default: return fwd_c<4>(P, st);
+  }
+}
+
+extern "C" int n3ds_density_net_backward(const n3ds_density_net_t* net, const float* coords, const float* features,
+                                         const float* grad_density, int64_t n_points, float* grad_table,
+                                         float* grad_w1, float* grad_b1, float* grad_w2, float* grad_b2,
+                                         n3ds_stream_t stream) {
+  if (int rc = check_net(net, n_points)) return rc;
+  if (n_points == 0) return N3DS_OK;
+  if (!coords || !features || !grad_density || !grad_table || !grad_w1 || !grad_b1 || !grad_w2 || !grad_b2)
+    return n3ds::report_error(N3DS_ERR_INVALID, "density net backward: every input and gradient pointer is required");
+  if (!aligned(features, 16))
+    return n3ds::report_error(N3DS_ERR_INVALID, "density net: the feature record must be 16-byte aligned");
+  NetLaunch P = make_launch(net, coords, n_points);
+  P.features_in = features;
+  P.grad_density = grad_density;
+  P.g_table = grad_table;
+  P.g_w1 = grad_w1;
+  P.g_b1 = grad_b1;
+  P.g_w2 = grad_w2;
+  P.g_b2 = grad_b2;
+  const size_t vw = net->level_dim * 4 < 16 ? net->level_dim * 4 : 16;
+  P.vec_table = vw > 4 && aligned(grad_table, vw);
+  const cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  switch (net->level_dim) {
+    case 1: return bwd_c<1>(P, st);
+    case 2: return bwd_c<2>(P, st);
+    default: return bwd_c<4>(P, st);
+  }
+}
+
+extern "C" int n3ds_grid_level_mean_sq(const float* table, const int32_t* offsets, uint32_t n_levels,
+                                       uint32_t level_dim, int32_t all_channels, float* out, n3ds_stream_t stream) {
+  if (int rc = check_levels(table, offsets, n_levels, level_dim, out)) return rc;
+  const cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  if (cudaMemsetAsync(out, 0, sizeof(float) * n_levels * level_dim, st) != cudaSuccess)
+    return launch_error("level statistics: clear");
+  const dim3 grid(64, n_levels);
+  level_sumsq_kernel<<<grid, kRedThreads, 0, st>>>(table, offsets, level_dim, all_channels ? level_dim : 1u, out);
+  return launch_error("level statistics");
+}
+
+extern "C" int n3ds_grid_level_mean_sq_backward(const float* table, const int32_t* offsets, uint32_t n_levels,
+                                                uint32_t level_dim, int32_t all_channels, const float* grad_out,
+                                                float* grad_table, n3ds_stream_t stream) {
+  if (int rc = check_levels(table, offsets, n_levels, level_dim, grad_table)) return rc;
+  if (!grad_out) return n3ds::report_error(N3DS_ERR_INVALID, "level statistics backward: null gradient");
+  const dim3 grid(256, n_levels);
+  level_sumsq_bwd_kernel<<<grid, kRedThreads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+      table, offsets, level_dim, all_channels ? level_dim : 1u, grad_out, grad_table);
+  return launch_error("level statistics backward");
+}

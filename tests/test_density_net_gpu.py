@@ -1,0 +1,334 @@
+"""The fused density network of the proposal and error fields (n3ds_density_net_*,
+neural3dstrokes_b200/mlp.py) on the GPU, against
+
+- the float64 oracle (oracle/density_net.py): density within 1e-5 and every
+  gradient (table, both weights, both biases) within 1e-4, max-norm relative, the
+  tolerances of the stroke path; the warped coordinates bit-equal to the oracle's
+  restatement of torch's CUDA ops;
+- the reference's own chain on the same GPU: its grid kernels built from their
+  sources (oracle/_ref/grid) and torch float32 nn.Linear / ReLU / nn.Linear /
+  F.softplus composed as source/models.py:362-372 and :430-431 compose them, torch
+  autograd for the gradients; same bars.
+
+Cases: the stroke model's three networks (PropMLP at the default desired
+resolutions 512 and 2048: 6 and 8 levels x 1 channel; ErrorMLP at 256: 5 x 2) and a
+4-channel grid (3 x 4), under each coordinate map (bbox scale, contract, none),
+with points inside and outside the grid, along rays (runs of one cell), and a
+count that is not a multiple of the 128-point tile.
+"""
+import glob
+import importlib.machinery
+import importlib.util
+import os
+
+import numpy as np
+import pytest
+import torch
+import torch.nn.functional as F
+
+from helpers import FWD_TOL, GRAD_TOL, rel
+from neural3dstrokes_b200 import mlp
+from oracle import density_net as odn
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+CASES = {
+    "prop512_bbox": (mlp.PropMLP, dict(grid_disired_resolution=512, warp_fn=None, bbox_size=3.0)),
+    "prop2048_contract": (mlp.PropMLP, dict(grid_disired_resolution=2048, warp_fn="contract")),
+    "error256_bbox": (mlp.ErrorMLP, dict(grid_disired_resolution=256, disable_rgb=True, warp_fn=None,
+                                         bbox_size=2.0)),
+    "c4_contract": (mlp.MLP, dict(disable_rgb=True, grid_level_dim=4, grid_disired_resolution=64,
+                                  grid_log2_hashmap_size=12, warp_fn="contract")),
+}
+
+
+def make_net(name, cuda, seed=0):
+    cls, kw = CASES[name]
+    torch.manual_seed(seed)
+    net = cls(**kw).to(cuda)
+    g = torch.Generator(device=cuda).manual_seed(seed + 1)
+    with torch.no_grad():
+        net.encoder.embeddings.uniform_(-1, 1, generator=g)
+        net.density_layer[0].bias.uniform_(-0.5, 0.5, generator=g)
+        net.density_layer[2].bias.uniform_(-0.5, 0.5, generator=g)
+    return net
+
+
+def ray_points(cuda, n_rays, n_samples, extent, seed=2):
+    """Points along rays (consecutive samples share cells at coarse levels), some of
+    them outside the grid's domain."""
+    g = torch.Generator(device=cuda).manual_seed(seed)
+    o = (torch.rand(n_rays, 1, 3, device=cuda, generator=g) * 2 - 1) * extent
+    d = F.normalize(torch.randn(n_rays, 1, 3, device=cuda, generator=g), dim=-1)
+    t = torch.linspace(0, extent, n_samples, device=cuda)[None, :, None]
+    return (o + d * t).reshape(-1, 3).contiguous()
+
+
+def warp_args(net):
+    mode = {None: odn.WARP_SCALE, "contract": odn.WARP_CONTRACT}[net.warp_fn]
+    return dict(density_bias=net.density_bias, warp=mode, bbox_size=net.bbox_size)
+
+
+def oracle_of(net, x, g, raw_output=False):
+    enc, lay = net.encoder, net.density_layer
+    S, H = float(np.log2(enc.per_level_scale)), enc.base_resolution
+    args = (enc.embeddings, enc.offsets, S, H, lay[0].weight, lay[0].bias, lay[2].weight, lay[2].bias)
+    dens, warped, _ = odn.forward(x, *args, raw_output=raw_output, **warp_args(net))
+    grads = odn.backward(g, x, *args, raw_output=raw_output, **warp_args(net))
+    return dens, warped, grads
+
+
+def params_of(net):
+    return [net.encoder.embeddings, net.density_layer[0].weight, net.density_layer[0].bias,
+            net.density_layer[2].weight, net.density_layer[2].bias]
+
+
+def run_fused(net, x, g, raw_output=False):
+    for p in params_of(net):
+        p.grad = None
+    dens, warped = mlp.density_net(x, net.encoder, net.density_layer, net.density_bias, net.warp_fn, net.bbox_size,
+                                   raw_output=raw_output)
+    torch.autograd.backward(dens, g)
+    torch.cuda.synchronize()
+    return dens.detach(), warped, [p.grad.detach().clone() for p in params_of(net)]
+
+
+def check_warped(name, warped, ref):
+    """Warped coordinates bit-equal to the reference's (torch's CUDA ops, or their
+    restatement in the oracle)."""
+    wd = (warped - ref).abs()
+    print(name, "warped coords: differing", int((wd > 0).sum()), "max |diff|", float(wd.max()))
+    assert torch.equal(warped, ref)
+
+
+def check_against(dens, grads, dens_ref, grads_ref, what):
+    errs = {"density": rel(dens, dens_ref)}
+    for name, a, b in zip(("table", "w1", "b1", "w2", "b2"), grads, grads_ref):
+        errs[name] = rel(a, b)
+    print(what, {k: f"{v:.2e}" for k, v in errs.items()})
+    assert errs["density"] < FWD_TOL, (what, errs)
+    for k, v in errs.items():
+        if k != "density":
+            assert v < GRAD_TOL, (what, k, errs)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_fused_network_matches_float64_oracle(cuda, name):
+    net = make_net(name, cuda)
+    extent = 1.7 if name.endswith("bbox") else 2.5
+    x = ray_points(cuda, 47, 64, extent)[:2999]
+    g = torch.randn(x.shape[0], device=cuda, generator=torch.Generator(device=cuda).manual_seed(5))
+    dens, warped, grads = run_fused(net, x, g)
+    dens_o, warped_o, grads_o = oracle_of(net, x, g)
+    check_warped(name, warped, warped_o.reshape(warped.shape).to(warped.device))
+    check_against(dens, grads, dens_o, grads_o, name)
+
+
+@pytest.mark.parametrize("name", ["prop512_bbox", "error256_bbox"])
+def test_raw_output_matches_oracle(cuda, name):
+    """predict_density's raw density (no bias, no softplus) and its gradients."""
+    net = make_net(name, cuda, seed=3)
+    x = ray_points(cuda, 20, 50, 1.4, seed=4)
+    g = torch.randn(x.shape[0], device=cuda, generator=torch.Generator(device=cuda).manual_seed(6))
+    dens, _, grads = run_fused(net, x, g, raw_output=True)
+    dens_o, _, grads_o = oracle_of(net, x, g, raw_output=True)
+    check_against(dens, grads, dens_o, grads_o, name + " raw")
+    raw, xd, _ = net.predict_density(x)
+    assert torch.equal(raw, dens) and xd.shape == (x.shape[0], 1)
+
+
+def reference_grid():
+    hits = glob.glob(os.path.join(ROOT, "oracle", "_ref", "grid", "_gridencoder*.so"))
+    if not hits:
+        return None
+    loader = importlib.machinery.ExtensionFileLoader("_gridencoder", hits[0])
+    spec = importlib.util.spec_from_file_location("_gridencoder", hits[0], loader=loader)
+    mod = importlib.util.module_from_spec(spec)
+    loader.exec_module(mod)
+    return mod
+
+
+class _RefGrid(torch.autograd.Function):
+    """The reference's grid kernels with the table as the differentiable input
+    (grid.py:24-88 without input gradients)."""
+
+    @staticmethod
+    def forward(ctx, inputs, embeddings, offsets, S, H, mod):
+        B, L, C = inputs.shape[0], offsets.shape[0] - 1, embeddings.shape[1]
+        out = torch.empty(L, B, C, device=inputs.device)
+        mod.grid_encode_forward(inputs, embeddings, offsets, out, B, 3, C, L, S, H, None, 0, False, 0)
+        ctx.save_for_backward(inputs, embeddings, offsets)
+        ctx.dims = (S, H, mod)
+        return out.permute(1, 0, 2).reshape(B, L * C)
+
+    @staticmethod
+    def backward(ctx, grad):
+        inputs, embeddings, offsets = ctx.saved_tensors
+        S, H, mod = ctx.dims
+        B, L, C = inputs.shape[0], offsets.shape[0] - 1, embeddings.shape[1]
+        g = grad.reshape(B, L, C).permute(1, 0, 2).contiguous()
+        gemb = torch.zeros_like(embeddings)
+        mod.grid_encode_backward(g, inputs, embeddings, offsets, gemb, B, 3, C, L, S, H, None, None, 0, False, 0)
+        return None, gemb, None, None, None, None
+
+
+def reference_chain(net, x, mod):
+    """models.py:19-33 (_warp_coords), grid.py:158-160, models.py:362-372, 430-431 as
+    torch float32 ops on the GPU with the reference's grid kernels."""
+    if net.warp_fn is None:
+        w = x / (net.bbox_size / 2)
+    else:
+        eps = torch.finfo(x.dtype).eps
+        m = torch.sum(x ** 2, dim=-1, keepdim=True).clamp_min(eps)
+        w = torch.where(m <= 1, x, ((2 * torch.sqrt(m) - 1) / m) * x) / 2.0
+    u = ((w + 1.0) / (2 * 1.0)).contiguous()
+    enc = net.encoder
+    feats = _RefGrid.apply(u, enc.embeddings, enc.offsets, float(np.log2(enc.per_level_scale)),
+                           enc.base_resolution, mod)
+    raw = net.density_layer(feats)[..., 0]
+    return F.softplus(raw + net.density_bias), w
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_fused_network_matches_reference_chain(cuda, name):
+    mod = reference_grid()
+    if mod is None:
+        pytest.skip("reference grid encoder not built (oracle/build_ref.py --only grid)")
+    net = make_net(name, cuda, seed=7)
+    extent = 1.7 if name.endswith("bbox") else 2.5
+    x = ray_points(cuda, 300, 64, extent, seed=8)
+    g = torch.randn(x.shape[0], device=cuda, generator=torch.Generator(device=cuda).manual_seed(9))
+    dens, warped, grads = run_fused(net, x, g)
+    for p in params_of(net):
+        p.grad = None
+    dens_r, w_r = reference_chain(net, x, mod)
+    torch.autograd.backward(dens_r, g)
+    grads_r = [p.grad.detach().clone() for p in params_of(net)]
+    check_warped(name, warped, w_r)
+    check_against(dens, grads, dens_r.detach(), grads_r, name + " vs reference chain")
+
+
+def test_module_forward_training_dict_and_hash_decay(cuda):
+    """PropMLP.forward in training: the reference's dict, hash_levelwise_mean as its
+    scatter_reduce_ fallback computes it (restated here on the same tensors), and the
+    gradient of density + hash decay through both kernels."""
+    net = make_net("prop2048_contract", cuda, seed=11)
+    net.train()
+    R, N = 33, 64
+    x = ray_points(cuda, R, N, 2.0, seed=12).reshape(R, N, 3)
+    out = net(x, torch.ones(R, N, device=cuda))
+    assert set(out) == {"coord", "density", "rgb", "normals", "hash_levelwise_mean"}
+    assert out["density"].shape == (R, N) and out["rgb"].shape == (R, N, 3) and out["normals"] is None
+    assert out["coord"].shape == (R, N, 3) and not bool(out["rgb"].any())
+    emb = net.encoder.embeddings
+    # the reference's formula in float64 (in float32 its atomics over 2^21 rows per
+    # level drift by ~1e-3; printed for the record)
+    hlm_ref = torch.zeros(net.encoder.num_levels, emb.shape[-1], device=cuda, dtype=torch.float64).scatter_reduce_(
+        0, net.encoder.idx.unsqueeze(1), torch.square(emb.double()), reduce="mean", include_self=False)
+    hlm_f32 = torch.zeros(net.encoder.num_levels, emb.shape[-1], device=cuda).scatter_reduce_(
+        0, net.encoder.idx.unsqueeze(1), torch.square(emb), reduce="mean", include_self=False)
+    print("hash_levelwise_mean: ours", rel(out["hash_levelwise_mean"], hlm_ref), "torch float32",
+          rel(hlm_f32, hlm_ref))
+    assert rel(out["hash_levelwise_mean"], hlm_ref) < FWD_TOL
+    assert rel(out["hash_levelwise_mean"], odn.level_mean_sq(emb, net.encoder.offsets)) < FWD_TOL
+    loss = out["density"].sum() + 0.1 * out["hash_levelwise_mean"].mean()
+    loss.backward()
+    g_emb = emb.grad.detach().clone()
+    dens_o, _, grads_o = oracle_of(net, x.reshape(-1, 3), torch.ones(R * N, device=cuda))
+    L = net.encoder.num_levels
+    ref_decay = torch.zeros_like(emb, dtype=torch.float64).cpu()
+    offs = [int(o) for o in net.encoder.offsets]
+    e64 = emb.detach().double().cpu()
+    for lv in range(L):
+        n = offs[lv + 1] - offs[lv]
+        ref_decay[offs[lv]:offs[lv + 1]] = 0.1 / L * 2 * e64[offs[lv]:offs[lv + 1]] / n
+    assert rel(out["density"].reshape(-1), dens_o) < FWD_TOL
+    assert rel(g_emb, grads_o[0] + ref_decay) < GRAD_TOL
+
+
+def test_error_field_sample_error(cuda):
+    net = make_net("error256_bbox", cuda, seed=13)
+    x = (torch.rand(30000, 3, device=cuda, generator=torch.Generator(device=cuda).manual_seed(14)) * 2 - 1)
+    with torch.no_grad():
+        e = net.sample_error(x)
+    dens_o, _, _ = oracle_of(net, x, torch.zeros(x.shape[0], device=cuda))
+    assert e.shape == (30000,) and rel(e, dens_o) < FWD_TOL
+
+
+@pytest.mark.parametrize("n", [0, 1, 127, 129])
+def test_point_counts_around_the_tile(cuda, n):
+    net = make_net("prop512_bbox", cuda, seed=15)
+    x = ray_points(cuda, 3, 64, 1.2, seed=16)[:n]
+    g = torch.randn(n, device=cuda, generator=torch.Generator(device=cuda).manual_seed(17))
+    dens, _, grads = run_fused(net, x, g)
+    assert dens.shape == (n,)
+    if n:
+        dens_o, _, grads_o = oracle_of(net, x, g)
+        check_against(dens, grads, dens_o, grads_o, f"n={n}")
+    else:
+        assert all(float(t.abs().max()) == 0.0 for t in grads)
+
+
+def test_cuda_graph_replay_matches_eager(cuda):
+    """Forward + backward captured in one CUDA graph, replayed: the eager results."""
+    net = make_net("prop2048_contract", cuda, seed=18)
+    x = ray_points(cuda, 64, 64, 2.0, seed=19)
+    g = torch.randn(x.shape[0], device=cuda, generator=torch.Generator(device=cuda).manual_seed(20))
+    dens_e, _, grads_e = run_fused(net, x, g)
+    params = params_of(net)
+    s = torch.cuda.Stream(cuda)
+    s.wait_stream(torch.cuda.current_stream(cuda))
+    with torch.cuda.stream(s):
+        for _ in range(2):
+            for p in params:
+                p.grad = None
+            d, _ = mlp.density_net(x, net.encoder, net.density_layer, net.density_bias, net.warp_fn, net.bbox_size)
+            torch.autograd.backward(d, g)
+    torch.cuda.current_stream(cuda).wait_stream(s)
+    graph = torch.cuda.CUDAGraph()
+    for p in params:
+        p.grad = None
+    with torch.cuda.graph(graph):
+        d, _ = mlp.density_net(x, net.encoder, net.density_layer, net.density_bias, net.warp_fn, net.bbox_size)
+        torch.autograd.backward(d, g)
+    for _ in range(3):
+        for p in params:
+            p.grad.zero_()
+        graph.replay()
+    torch.cuda.synchronize(cuda)
+    assert torch.equal(d, dens_e)
+    for a, b in zip([p.grad for p in params], grads_e):
+        assert rel(a, b) < 1e-6  # float atomics: the order of the table and weight sums varies
+
+
+def test_bounded_wait_runs_out_and_reports(cuda):
+    """With the tensor-core work withheld (test hook, nothing left in flight) and a
+    50 us limit, the wait runs out: status bit 2, the kernel returns, tensor memory
+    is freed, and a normal call right after is correct."""
+    net = make_net("prop512_bbox", cuda, seed=21)
+    x = ray_points(cuda, 8, 64, 1.2, seed=22)
+    status = torch.zeros(1, dtype=torch.int32, device=cuda)
+    with torch.no_grad():
+        mlp.density_net(x, net.encoder, net.density_layer, net.density_bias, net.warp_fn, net.bbox_size,
+                        status=status, wait_limit_us=50, test_stall=True)
+    torch.cuda.synchronize(cuda)
+    assert int(status.item()) & 2
+    status.zero_()
+    g = torch.randn(x.shape[0], device=cuda, generator=torch.Generator(device=cuda).manual_seed(23))
+    for p in params_of(net):
+        p.grad = None
+    d, _ = mlp.density_net(x, net.encoder, net.density_layer, net.density_bias, net.warp_fn, net.bbox_size,
+                           status=status)
+    torch.autograd.backward(d, g)
+    torch.cuda.synchronize(cuda)
+    assert int(status.item()) == 0
+    dens_o, _, grads_o = oracle_of(net, x, g)
+    check_against(d.detach(), [p.grad for p in params_of(net)], dens_o, grads_o, "after a timeout")
+
+
+def test_coordinate_gradient_request_raises(cuda):
+    net = make_net("prop512_bbox", cuda)
+    x = ray_points(cuda, 2, 8, 1.0).requires_grad_(True)
+    with pytest.raises(RuntimeError, match="no coordinate gradient"):
+        net(x, None)
