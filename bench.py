@@ -11,13 +11,19 @@ Default workload: 16 uneven scenes (strokes log-uniform in [50, 2000], rays
 log-uniform in [4096, 65536], 64 samples each, six primitive types mixed) in one
 batched launch per pass + CUDA graph. Other workloads: --config 0..4.
 
-Second workload (--workload grid): the proposal network's multi-resolution hash-grid
-encoder (10 levels x 4 channels, 2^21 rows per fine level, 240 MB of float32 table)
-over 65,536 rays x 64 samples; one step = zero the table gradient, forward, table
-backward; value in (point, level) lookups per second; the reference's own kernels,
-built from its sources, are timed beside it when present.
+Second workload (--workload grid): the multi-resolution hash-grid encoder alone at
+the MLP class defaults (10 levels x 4 channels, 2^21 rows per fine level, 240 MB of
+float32 table) over 65,536 rays x 64 samples; one step = zero the table gradient,
+forward, table backward; value in (point, level) lookups per second; the reference's
+own kernels, built from its sources, are timed beside it when present.
 
-Third (--workload ops): every other operator once at a stated size through its
+Third (--workload prop): the proposal and error fields' density networks of one
+training step (PropMLP at 512 and 2048, ErrorMLP at 256; 2^14 rays x 64 samples
+each): warp, grid encoding, Linear-ReLU-Linear, softplus, hash decay statistics and
+their backward, fused (tensor cores for the layers); value in points per second; the
+reference's formulation (its grid kernels + torch layers + autograd) timed beside it.
+
+Fourth (--workload ops): every other operator once at a stated size through its
 public API (the drop-in _strokelib operators, the composition modes, a colour field,
 the texture, proposal resampling, stroke insertion, the field at a tenth of config 3
 and its Adam step), timed with CUDA events; it is the command the all-kernels ncu
@@ -25,7 +31,7 @@ summary runs.
 
 Usage:
   python bench.py [--gpus N] [--steps K] [--warmup W] [--config C] [--impl reference]
-  python bench.py --workload grid [--steps K] [--warmup W] [--impl reference]
+  python bench.py --workload grid|prop [--steps K] [--warmup W] [--impl reference]
   python bench.py --workload ops [--steps K] [--warmup W]
 Multi-GPU (torchrun): every rank runs the same workload on its own GPU (replicas, no
 data-path collective); the value is the sum over ranks of evals divided by the
@@ -420,15 +426,17 @@ def loss_curves(args):
             json.dump(line, f)
 
 
-GRID_METRIC = ("grid-encoder fwd+bwd (point, level) lookups/s on 1 B200: proposal hash grid "
-               "(10 levels x 4 ch, 2^21 rows/level)")
+GRID_METRIC = ("grid-encoder fwd+bwd (point, level) lookups/s on 1 B200: hash grid of the MLP class "
+               "defaults (10 levels x 4 ch, 2^21 rows/level)")
 GRID_UNIT = "lookups/s"
 
 
 def grid_workload(dev, scale=1.0, seed=0):
-    """The proposal network's grid (models.py:305-333: 10 levels, 4 channels, base 16,
-    finest 8192, 2^21 rows) and 65,536 x scale rays of 64 samples inside the unit
-    cube, points ordered along each ray as the proposal sampler emits them."""
+    """The largest grid the reference defines, the MLP class defaults (models.py:305-333:
+    10 levels, 4 channels, base 16, finest 8192, 2^21 rows; NerfMLP's; PropMLP and
+    ErrorMLP narrow it, see --workload prop) and 65,536 x scale rays of 64 samples
+    inside the unit cube, points ordered along each ray as the proposal sampler emits
+    them."""
     from neural3dstrokes_b200 import gridencoder as ge
     enc = ge.GridEncoder(input_dim=3, num_levels=10, level_dim=4, base_resolution=16, desired_resolution=8192,
                          log2_hashmap_size=21).to(dev)
@@ -530,7 +538,7 @@ def run_grid(args, world, rank, local):
                               "unit": GRID_UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                               "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
                               "dtype": "f32", "data": "synthetic", "clocks": clk,
-                              "config": {"workload": "proposal grid", "points": B, "levels": L},
+                              "config": {"workload": "MLP-default hash grid", "points": B, "levels": L},
                               "note": "the reference's grid_encode_forward / grid_encode_backward kernels built "
                                       "from its sources for sm_100a, eager on the default stream"}), flush=True)
         return
@@ -629,13 +637,346 @@ def run_grid(args, world, rank, local):
             "metric": GRID_METRIC, "value": lookups * world / t_step, "unit": GRID_UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded rays in the unit cube)",
-            "config": {"workload": "proposal grid, 65,536 rays x 64 samples" if args.scale == 1.0 else
-                       f"proposal grid, {B // 64} rays x 64 samples", "points": B, "levels": L, "channels": C,
+            "config": {"workload": "MLP-default hash grid, 65,536 rays x 64 samples" if args.scale == 1.0 else
+                       f"MLP-default hash grid, {B // 64} rays x 64 samples", "points": B, "levels": L, "channels": C,
                        "table_mb": table_bytes / 1e6, "l2": "inputs larger than L2 (outputs %.0f MB, table %.0f MB)"
                        % (L * B * C * 4 / 1e6, table_bytes / 1e6),
                        "graph": "zero + forward + backward captured in one CUDA graph"},
             "roofline": roofline, "plain_op": plain, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
             "gpu_launches": 3 * args.steps, "gpu_launches_per_step": 3}), flush=True)
+
+
+PROP_METRIC = ("proposal-side density networks fwd+bwd points/s on 1 B200: PropMLP (512) + PropMLP (2048) + "
+               "ErrorMLP (256) of one training step, 2^14 rays x 64 samples each")
+PROP_UNIT = "points/s"
+
+
+def prop_workload(dev, scale=1.0, seed=0):
+    """The networks one training step runs before the stroke level, at the reference's
+    defaults: Model.num_prop_samples = 64 on two proposal levels whose grids reach
+    desired resolutions 512 and 2048 (models.py:56-58, 73, 86-96; 6 and 8 levels x 1
+    channel), and the error field (256: 5 levels x 2 channels) on the first level's
+    samples (models.py:247-249), over Config.batch_size = 2^14 rays (configs.py:30),
+    scaled by `scale`. The blender config's coordinate map (configs/blender.gin:44-45:
+    warp_fn None, bbox_size 3). Synthetic rays from a sphere of radius 4 towards the
+    origin, samples in t [2, 6] in ray order; reference initialisation; upstream
+    density gradients N(0, 1)."""
+    import torch.nn.functional as F
+    from neural3dstrokes_b200 import mlp
+    torch.manual_seed(seed)
+    nets = [mlp.PropMLP(grid_disired_resolution=512, warp_fn=None, bbox_size=3.0),
+            mlp.PropMLP(grid_disired_resolution=2048, warp_fn=None, bbox_size=3.0),
+            mlp.ErrorMLP(grid_disired_resolution=256, disable_rgb=True, warp_fn=None, bbox_size=3.0)]
+    nets = [n.to(dev).train() for n in nets]
+    R, N = max(1, int(16384 * scale)), 64
+    g = torch.Generator(device=dev).manual_seed(seed)
+    xs = []
+    for _ in range(2):
+        o = F.normalize(torch.randn(R, 3, device=dev, generator=g), dim=-1) * 4.0
+        d = F.normalize(-o + 0.5 * torch.randn(R, 3, device=dev, generator=g), dim=-1)
+        t = torch.sort(torch.rand(R, N, device=dev, generator=g) * 4 + 2, dim=-1).values
+        xs.append((o[:, None] + d[:, None] * t[..., None]).reshape(R * N, 3).contiguous())
+    coords = [xs[0], xs[1], xs[0]]
+    grads = [torch.randn(R * N, device=dev, generator=g) for _ in nets]
+    return nets, coords, grads
+
+
+class _RefGridFn(torch.autograd.Function):
+    """The reference's grid kernels with the table as the differentiable input, as
+    source/gridencoder/grid.py:24-88 calls them (no input gradient)."""
+
+    @staticmethod
+    def forward(ctx, inputs, embeddings, offsets, S, H, mod):
+        B, L, C = inputs.shape[0], offsets.shape[0] - 1, embeddings.shape[1]
+        out = torch.empty(L, B, C, device=inputs.device)
+        mod.grid_encode_forward(inputs, embeddings, offsets, out, B, 3, C, L, S, H, None, 0, False, 0)
+        ctx.save_for_backward(inputs, embeddings, offsets)
+        ctx.dims = (S, H, mod)
+        return out.permute(1, 0, 2).reshape(B, L * C)
+
+    @staticmethod
+    def backward(ctx, grad):
+        inputs, embeddings, offsets = ctx.saved_tensors
+        S, H, mod = ctx.dims
+        B, L, C = inputs.shape[0], offsets.shape[0] - 1, embeddings.shape[1]
+        gg = grad.reshape(B, L, C).permute(1, 0, 2).contiguous()
+        gemb = torch.zeros_like(embeddings)
+        mod.grid_encode_backward(gg, inputs, embeddings, offsets, gemb, B, 3, C, L, S, H, None, None, 0, False, 0)
+        return None, gemb, None, None, None, None
+
+
+def prop_reference_step_fn(nets, coords, grads, mod):
+    """One step of the reference's formulation on the GPU: _warp_coords, GridEncoder
+    (its own kernels), density_layer as torch layers, softplus, the hash decay
+    statistics by scatter_reduce_ (models.py:19-33, 362-372, 430-431, 472-488), then
+    autograd with the upstream density gradients and the hash-decay loss of the two
+    proposal networks (loss.py:371-378, hash_decay_mult 0.1)."""
+    import numpy as np
+    import torch.nn.functional as F
+
+    def step():
+        outs, ups = [], []
+        for i, (net, x, g) in enumerate(zip(nets, coords, grads)):
+            for p in net.parameters():
+                p.grad = None
+            w = x / (net.bbox_size / 2)
+            u = ((w + 1.0) / (2 * 1.0)).contiguous()
+            enc = net.encoder
+            feats = _RefGridFn.apply(u, enc.embeddings, enc.offsets, float(np.log2(enc.per_level_scale)),
+                                     enc.base_resolution, mod)
+            raw = net.density_layer(feats)[..., 0]
+            dens = F.softplus(raw + net.density_bias)
+            hlm = torch.zeros(enc.num_levels, enc.embeddings.shape[-1], device=x.device).scatter_reduce_(
+                0, enc.idx.unsqueeze(1), torch.square(enc.embeddings), reduce="mean", include_self=False)
+            outs.append(dens)
+            ups.append(g)
+            if i < 2:
+                outs.append(0.1 * hlm.mean())
+                ups.append(None)
+        torch.autograd.backward([o for o in outs], [u if u is not None else torch.ones_like(o)
+                                                    for o, u in zip(outs, ups)])
+    return step
+
+
+def prop_fused_step_fn(nets, coords, grads):
+    """One step through the fused kernels (the C ABI, buffers allocated once): per
+    network the forward (density, feature record, warped coordinates) and the hash
+    decay statistics, then the backward into zeroed gradients and, for the two
+    proposal networks, the hash-decay gradient (0.1 / (L C) per entry)."""
+    import ctypes
+    from neural3dstrokes_b200 import _lib, mlp
+    lib = _lib.load()
+    state = []
+    for net, x, g in zip(nets, coords, grads):
+        enc, lay = net.encoder, net.density_layer
+        L, C = enc.num_levels, enc.level_dim
+        n = x.shape[0]
+        stride = lib.n3ds_density_net_feature_stride(L, C)
+        st = dict(net=net, x=x, g=g, n=n, L=L, C=C,
+                  desc=mlp._net_struct(enc, lay[0].weight, lay[0].bias, lay[2].weight, lay[2].bias,
+                                       net.density_bias, mlp.WARP_SCALE, net.bbox_size, False),
+                  density=torch.empty(n, device=x.device), feats=torch.empty(n, stride, device=x.device),
+                  warped=torch.empty(n, 3, device=x.device), hlm=torch.empty(L, C, device=x.device),
+                  hlm_grad=torch.full((L, C), 0.1 / (L * C), device=x.device),
+                  grads=[torch.zeros_like(t) for t in (enc.embeddings, lay[0].weight, lay[0].bias, lay[2].weight,
+                                                        lay[2].bias)])
+        state.append(st)
+
+    def step():
+        sp = _lib.stream_ptr()
+        for i, st in enumerate(state):
+            enc = st["net"].encoder
+            for t in st["grads"]:
+                t.zero_()
+            _lib.check(lib.n3ds_density_net_forward(ctypes.byref(st["desc"]), _lib.ptr(st["x"]), st["n"],
+                                                    _lib.ptr(st["density"]), _lib.ptr(st["feats"]),
+                                                    _lib.ptr(st["warped"]), sp))
+            _lib.check(lib.n3ds_grid_level_mean_sq(_lib.ptr(enc.embeddings), _lib.ptr(enc.offsets), st["L"],
+                                                   st["C"], 0, _lib.ptr(st["hlm"]), sp))
+            _lib.check(lib.n3ds_density_net_backward(ctypes.byref(st["desc"]), _lib.ptr(st["x"]),
+                                                     _lib.ptr(st["feats"]), _lib.ptr(st["g"]), st["n"],
+                                                     *[_lib.ptr(t) for t in st["grads"]], sp))
+            if i < 2:
+                _lib.check(lib.n3ds_grid_level_mean_sq_backward(_lib.ptr(enc.embeddings), _lib.ptr(enc.offsets),
+                                                                st["L"], st["C"], 0, _lib.ptr(st["hlm_grad"]),
+                                                                _lib.ptr(st["grads"][0]), sp))
+    return step, state
+
+
+def prop_cpu_baseline(nets, coords, grads, budget_s=15.0):
+    """The float64 oracle's forward + backward of the three networks on host threads,
+    on the first `n` points of each network's samples, in points/s."""
+    import numpy as np
+    from oracle import density_net as odn
+    n = 2048
+    done, t0 = 0, time.perf_counter()
+    while True:
+        for net, x, g in zip(nets, coords, grads):
+            enc, lay = net.encoder, net.density_layer
+            args = (enc.embeddings, enc.offsets, float(np.log2(enc.per_level_scale)), enc.base_resolution,
+                    lay[0].weight, lay[0].bias, lay[2].weight, lay[2].bias)
+            kw = dict(density_bias=net.density_bias, warp=odn.WARP_SCALE, bbox_size=net.bbox_size)
+            odn.forward(x[:n], *args, **kw)
+            odn.backward(g[:n], x[:n], *args, **kw)
+            done += n
+        if time.perf_counter() - t0 > budget_s / 3:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": done / dt, "unit": PROP_UNIT, "cores": torch.get_num_threads(), "kind": "port",
+            "sample": f"the first {n} points of each network, repeated {done // (3 * n)}x (oracle float64, "
+                      "torch on the host threads)"}
+
+
+def run_prop(args, world, rank, local):
+    from neural3dstrokes_b200.train import capture
+    dev = torch.device("cuda", local)
+    nets, coords, grads = prop_workload(dev, args.scale)
+    points = sum(x.shape[0] for x in coords)
+    R = coords[0].shape[0] // 64
+    cfg = {"workload": f"proposal-side networks of one training step, {R} rays x 64 samples per network",
+           "networks": "PropMLP(512): 6 x 1, PropMLP(2048): 8 x 1, ErrorMLP(256): 5 x 2; Linear(L*C, 64), ReLU, "
+                       "Linear(64, 1), softplus; hash decay statistics", "points": points,
+           "l2": "tables 2 x 43 MB + 21 MB; feature records and gradients stream from HBM"}
+    ref = grid_reference_module()
+    if args.impl == "reference":
+        if ref is None:
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "reference grid encoder not built "
+                                  "(python oracle/build_ref.py --only grid)"}), flush=True)
+            return
+        step = prop_reference_step_fn(nets, coords, grads, ref)
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize(dev)
+        clocks = ClockSampler(local)
+        clocks.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        lo = time.monotonic()
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        clk = clocks.stop(lo, time.monotonic())
+        t = max_over_ranks(e0.elapsed_time(e1) * 1e-3 / args.steps, world, dev)
+        if rank == 0:
+            v = points * world / t
+            print(json.dumps({"impl": "reference", "metric": PROP_METRIC, "value": v, "unit": PROP_UNIT,
+                              "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+                              "higher_is_better": True, "scaling": "weak", "dtype": "f32", "data": "synthetic",
+                              "clocks": clk, "config": cfg,
+                              "cpu_baseline": None,
+                              "e2e": {"value": v, "unit": PROP_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                              "note": "the reference's formulation on the GPU: its grid kernels built from their "
+                                      "sources, torch layers and autograd, eager"}), flush=True)
+        return
+
+    step, state = prop_fused_step_fn(nets, coords, grads)
+    step()  # resolves occupancy and sets the kernels' shared-memory limits before capture
+    graph = capture(step, dev, warmup=1)
+    for _ in range(args.warmup):
+        graph.replay()
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    lo = time.monotonic()
+    e0.record()
+    for _ in range(args.steps):
+        graph.replay()
+    e1.record()
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop(lo, time.monotonic())
+    t_step = max_over_ranks(e0.elapsed_time(e1) * 1e-3 / args.steps, world, dev)
+
+    # per-kernel durations by events on the launching stream (the largest network)
+    import ctypes
+    from neural3dstrokes_b200 import _lib
+    lib = _lib.load()
+    st = state[1]
+    enc = st["net"].encoder
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    tf, tb = [], []
+    sp = _lib.stream_ptr()
+    for _ in range(5):
+        for t in st["grads"]:
+            t.zero_()
+        ev[0].record()
+        _lib.check(lib.n3ds_density_net_forward(ctypes.byref(st["desc"]), _lib.ptr(st["x"]), st["n"],
+                                                _lib.ptr(st["density"]), _lib.ptr(st["feats"]),
+                                                _lib.ptr(st["warped"]), sp))
+        ev[1].record()
+        _lib.check(lib.n3ds_density_net_backward(ctypes.byref(st["desc"]), _lib.ptr(st["x"]), _lib.ptr(st["feats"]),
+                                                 _lib.ptr(st["g"]), st["n"], *[_lib.ptr(t) for t in st["grads"]], sp))
+        ev[2].record()
+        torch.cuda.synchronize(dev)
+        tf.append(ev[0].elapsed_time(ev[1]) * 1e-3)
+        tb.append(ev[1].elapsed_time(ev[2]) * 1e-3)
+    t_fwd, t_bwd = statistics.mean(tf), statistics.mean(tb)
+    cfg["ctas"] = {"forward": lib.n3ds_density_net_resident_ctas(0), "backward": lib.n3ds_density_net_resident_ctas(1)}
+    n, stride = st["n"], st["feats"].shape[1]
+    table_bytes = enc.embeddings.numel() * 4
+    # algorithmic bytes: coordinates, density, feature record and warped coordinates
+    # once and the table once (forward); coordinates, record, upstream gradient once
+    # and a read + write of the table gradient (backward)
+    fwd_bytes = n * (12 + 4 + 4 * stride + 12) + table_bytes
+    bwd_bytes = n * (12 + 4 * stride + 4) + 2 * table_bytes
+    peak, src = hbm_peak()
+    roofline = {"bound": "hbm", "kernel": "density_bwd_kernel (PropMLP 2048: tensor-core adjoint + table scatter)",
+                "achieved": bwd_bytes / t_bwd / 1e9, "peak": peak, "unit": "GB/s",
+                "frac": bwd_bytes / t_bwd / 1e9 / peak, "traffic": None, "peak_source": src,
+                "bytes_per_launch": bwd_bytes, "launch_ms": t_bwd * 1e3,
+                "forward_kernel": {"name": "density_fwd_kernel", "achieved": fwd_bytes / t_fwd / 1e9,
+                                   "launch_ms": t_fwd * 1e3, "frac": fwd_bytes / t_fwd / 1e9 / peak}}
+
+    plain = None
+    if ref is not None and not args.no_plain_op:
+        rstep = prop_reference_step_fn(nets, coords, grads, ref)
+        for _ in range(2):
+            rstep()
+        torch.cuda.synchronize(dev)
+        e0.record()
+        for _ in range(args.steps):
+            rstep()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        tr = e0.elapsed_time(e1) * 1e-3 / args.steps
+        plain = {"value": points / tr, "unit": PROP_UNIT, "ms_per_step": tr * 1e3, "speedup": tr / t_step,
+                 "what": "the reference's formulation on this GPU: its grid kernels built from their sources, "
+                         "torch layers, autograd"}
+
+    # end to end through the public API: coordinates and upstream gradients uploaded
+    # from pinned host memory, module forward + autograd backward, densities read back
+    e2e = None
+    if not args.no_e2e:
+        hx = [x.cpu().pin_memory() for x in coords]
+        hg = [g.cpu().pin_memory() for g in grads]
+        hd = [torch.empty(x.shape[0], pin_memory=True) for x in coords]
+        dx = [torch.empty_like(x) for x in coords]
+        dg = [torch.empty_like(g) for g in grads]
+
+        def api_step():
+            outs, ups = [], []
+            for i, net in enumerate(nets):
+                dx[i].copy_(hx[i], non_blocking=True)
+                dg[i].copy_(hg[i], non_blocking=True)
+                for p in net.parameters():
+                    p.grad = None
+                out = net(dx[i], None)
+                outs.append(out["density"])
+                ups.append(dg[i])
+                if i < 2:
+                    outs.append(0.1 * out["hash_levelwise_mean"].mean())
+                    ups.append(torch.ones((), device=dev))
+                hd[i].copy_(out["density"].detach(), non_blocking=True)
+            torch.autograd.backward(outs, ups)
+        for _ in range(2):
+            api_step()
+        k = max(3, min(args.steps, 10))
+        torch.cuda.synchronize(dev)
+        e0.record()
+        for _ in range(k):
+            api_step()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        te = max_over_ranks(e0.elapsed_time(e1) * 1e-3 / k, world, dev)
+        e2e = {"value": points * world / te, "unit": PROP_UNIT, "ms_per_step": te * 1e3,
+               "h2d_bytes_per_step": sum(x.numel() * 4 for x in hx) + sum(g.numel() * 4 for g in hg),
+               "d2h_bytes_per_step": sum(d.numel() * 4 for d in hd)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = prop_cpu_baseline(nets, coords, grads, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps({
+            "metric": PROP_METRIC, "value": points * world / t_step, "unit": PROP_UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (first layer tf32 x3 split, adjoint bf16 x3 split)",
+            "data": "synthetic (seeded rays, reference initialisation)", "config": cfg,
+            "graph": "three networks' forward, hash decay statistics and backward in one CUDA graph",
+            "roofline": roofline, "plain_op": plain, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+            "gpu_launches": 11 * args.steps, "gpu_launches_per_step": 11}), flush=True)
 
 
 def run_ops(args, rank, local):
@@ -787,9 +1128,9 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--config", type=int, default=3)
-    ap.add_argument("--workload", default="field", choices=["field", "grid", "ops"],
-                    help="field: the stroke field (default); grid: the proposal hash-grid encoder; "
-                         "ops: every other operator once (profiling)")
+    ap.add_argument("--workload", default="field", choices=["field", "grid", "prop", "ops"],
+                    help="field: the stroke field (default); grid: a hash-grid encoder alone; prop: the "
+                         "proposal and error fields' density networks; ops: every other operator once (profiling)")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--scale", type=float, default=1.0, help="ray-count scale (profiling small cases)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -817,8 +1158,8 @@ def main():
         if world > 1:
             torch.distributed.destroy_process_group()
         return
-    if args.workload == "grid":
-        run_grid(args, world, rank, local)
+    if args.workload in ("grid", "prop"):
+        (run_grid if args.workload == "grid" else run_prop)(args, world, rank, local)
         if world > 1:
             torch.distributed.destroy_process_group()
         return

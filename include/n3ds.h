@@ -508,6 +508,9 @@ typedef struct n3ds_density_net {
   int32_t test_stall;          /* test hook: withhold the tensor-core work so that the
                                   first wait runs out (0 in normal use) */
 } n3ds_density_net_t;
+/* Persistent CTAs the last forward (backward = 0) or backward launch of this process
+ * used (resident CTAs per SM x SMs), 0 before the first; a diagnostic. */
+int n3ds_density_net_resident_ctas(int32_t backward);
 /* Floats per point of the feature record written by the forward for the backward:
  * L * C rounded up to a multiple of 4. */
 int n3ds_density_net_feature_stride(uint32_t n_levels, uint32_t level_dim);

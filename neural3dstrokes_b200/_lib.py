@@ -123,6 +123,7 @@ _SIGS = {
     "n3ds_grid_total_variation": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_float, c_u32, c_u32, c_u32, c_u32,
                                                  ctypes.c_float, c_u32, c_u32, c_i32, c_i32, _P]),
     "n3ds_density_net_feature_stride": (ctypes.c_int, [c_u32, c_u32]),
+    "n3ds_density_net_resident_ctas": (ctypes.c_int, [c_i32]),
     "n3ds_density_net_forward": (ctypes.c_int, [_DN, _P, c_i64, _P, _P, _P, _P]),
     "n3ds_density_net_backward": (ctypes.c_int, [_DN, _P, _P, _P, c_i64, _P, _P, _P, _P, _P, _P]),
     "n3ds_grid_level_mean_sq": (ctypes.c_int, [_P, _P, c_u32, c_u32, c_i32, _P, _P]),

@@ -757,9 +757,11 @@ NetLaunch make_launch(const n3ds_density_net_t* net, const float* coords, int64_
   return P;
 }
 
-// CTAs the kernel can keep resident on the device (cached per kernel and device):
-// the occupancy limit, and at most 512 / cols per SM so that every resident CTA's
-// tensor-memory allocation succeeds at once.
+// CTAs the kernel can keep resident on the device (cached per kernel and device): the
+// limits of its registers, shared memory (carveout set to the maximum) and threads,
+// and at most 512 / cols per SM so that every resident CTA's tensor-memory
+// allocation succeeds at once. (The runtime's occupancy calculator answers one CTA
+// per SM for these tensor-memory kernels, below what the hardware runs.)
 template <typename K>
 int resident(K kernel, uint32_t smem, uint32_t cols, int* cache) {
   int dev = 0;
@@ -767,20 +769,34 @@ int resident(K kernel, uint32_t smem, uint32_t cols, int* cache) {
   if (dev < 0 || dev >= 16) dev = 0;
   if (cache[dev] == 0) {
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int blocks = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, kTile, smem);
-    if (blocks > (int)(512 / cols)) blocks = (int)(512 / cols);
-    int sms = 0;
+    cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaFuncAttributes fa{};
+    int regs_sm = 0, smem_sm = 0, reserved = 0, threads_sm = 0, sms = 0;
+    cudaFuncGetAttributes(&fa, kernel);
+    cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    cudaDeviceGetAttribute(&threads_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int regs_warp = ((fa.numRegs > 0 ? fa.numRegs : 255) * 32 + 255) / 256 * 256;  // 256-register units
+    const int by_regs = regs_sm / (regs_warp * (kTile / 32));
+    const int by_smem = smem_sm / ((int)smem + (int)fa.sharedSizeBytes + reserved);
+    const int by_threads = threads_sm / kTile;
+    int blocks = by_regs < by_smem ? by_regs : by_smem;
+    if (by_threads < blocks) blocks = by_threads;
+    if (blocks > (int)(512 / cols)) blocks = (int)(512 / cols);
     cache[dev] = (blocks > 0 ? blocks : 1) * (sms > 0 ? sms : 1);
   }
   return cache[dev];
 }
 
+int g_resident[2];  // CTAs of the last forward and backward launch
+
 template <int C>
 int fwd_c(const NetLaunch& P, cudaStream_t st) {
   static int cache[16] = {0};
   const int slots = resident(density_fwd_kernel<C>, kSmemFwd, kColsFwd, cache);
+  g_resident[0] = slots;
   const long long tiles = (P.n + kTile - 1) / kTile;
   const int grid = (int)(tiles < slots ? tiles : slots);
   density_fwd_kernel<C><<<grid, kTile, kSmemFwd, st>>>(P);
@@ -791,6 +807,7 @@ template <int C>
 int bwd_c(const NetLaunch& P, cudaStream_t st) {
   static int cache[16] = {0};
   const int slots = resident(density_bwd_kernel<C>, kSmemBwd, kColsBwd, cache);
+  g_resident[1] = slots;
   const long long tiles = (P.n + kTile - 1) / kTile;
   const int grid = (int)(tiles < slots ? tiles : slots);
   density_bwd_kernel<C><<<grid, kTile, kSmemBwd, st>>>(P);
@@ -805,6 +822,10 @@ int check_levels(const float* table, const int32_t* offsets, uint32_t L, uint32_
 }
 
 }  // namespace
+
+extern "C" int n3ds_density_net_resident_ctas(int32_t backward) {
+  return g_resident[backward ? 1 : 0];
+}
 
 extern "C" int n3ds_density_net_feature_stride(uint32_t n_levels, uint32_t level_dim) {
   return (int)((n_levels * level_dim + 3) / 4 * 4);

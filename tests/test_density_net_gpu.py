@@ -327,6 +327,20 @@ def test_bounded_wait_runs_out_and_reports(cuda):
     check_against(d.detach(), [p.grad for p in params_of(net)], dens_o, grads_o, "after a timeout")
 
 
+def test_persistent_grid_fills_the_device(cuda):
+    """The persistent kernels launch several CTAs per SM (the occupancy limits, capped by
+    tensor memory: 8 forward, 4 backward), not one."""
+    from neural3dstrokes_b200 import _lib
+    net = make_net("prop512_bbox", cuda, seed=24)
+    x = ray_points(cuda, 512, 64, 1.2, seed=25)
+    run_fused(net, x, torch.ones(x.shape[0], device=cuda))
+    sms = torch.cuda.get_device_properties(cuda).multi_processor_count
+    lib = _lib.load()
+    fwd, bwd = lib.n3ds_density_net_resident_ctas(0), lib.n3ds_density_net_resident_ctas(1)
+    print("resident CTAs: forward", fwd, "backward", bwd, "SMs", sms)
+    assert fwd >= 4 * sms and bwd >= 2 * sms
+
+
 def test_coordinate_gradient_request_raises(cuda):
     net = make_net("prop512_bbox", cuda)
     x = ray_points(cuda, 2, 8, 1.0).requires_grad_(True)
