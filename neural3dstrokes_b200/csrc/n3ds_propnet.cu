@@ -76,15 +76,6 @@ constexpr uint32_t kMaskBytes = kTile * kHidden * 2;    // 16 KB
 constexpr uint32_t kPadChunk = 144, kPadGroup = 16 * kPadChunk;
 constexpr uint32_t kMaskTBytes = (kHidden / 8) * kPadGroup;   // 18 KB
 constexpr uint32_t kBpBytes = (kMaxFeat / 8) * kPadGroup;     // 4.5 KB per term
-constexpr uint32_t OFF_FEAT_HI = 0;
-constexpr uint32_t OFF_FEAT_LO = OFF_FEAT_HI + kFeatBytes;
-constexpr uint32_t OFF_W1_HI = OFF_FEAT_LO + kFeatBytes;
-constexpr uint32_t OFF_W1_LO = OFF_W1_HI + kW1Bytes;
-constexpr uint32_t OFF_W1P = OFF_W1_LO + kW1Bytes;            // backward only from here
-constexpr uint32_t OFF_MASK = OFF_W1P + 3 * kW1pBytes;
-constexpr uint32_t OFF_MASKT = OFF_MASK + kMaskBytes;
-constexpr uint32_t OFF_BP = OFF_MASKT + kMaskTBytes;
-constexpr uint32_t OFF_MISC_BWD = OFF_BP + 3 * kBpBytes;
 struct Misc {
   float b1[kHidden];
   float w2[kHidden];
@@ -93,9 +84,28 @@ struct Misc {
   uint32_t tmem;
   float b2;
 };
-constexpr uint32_t kSmemFwd = OFF_W1P + sizeof(Misc);
-constexpr uint32_t kSmemBwd = OFF_MISC_BWD + sizeof(Misc);
-static_assert(OFF_MISC_BWD % 16 == 0 && OFF_BP % 16 == 0 && OFF_MASKT % 16 == 0, "16-byte operand alignment");
+// Offsets for kc 4-value feature chunks (2 when L * C <= 8, else 4): the feature and
+// W1 tiles hold only the chunks the first layer reads.
+struct Smem {
+  uint32_t feat_hi, feat_lo, w1_hi, w1_lo, w1p, mask, maskt, bp, misc_fwd, misc_bwd, fwd_bytes, bwd_bytes;
+};
+__host__ __device__ constexpr Smem smem_layout(int kc) {
+  Smem m{};
+  m.feat_hi = 0;
+  m.feat_lo = kc * 2048;
+  m.w1_hi = 2 * kc * 2048;
+  m.w1_lo = m.w1_hi + kc * 1024;
+  m.w1p = m.w1_lo + kc * 1024;  // the forward's Misc, then the backward's tiles
+  m.misc_fwd = m.w1p;
+  m.mask = m.w1p + 3 * kW1pBytes;
+  m.maskt = m.mask + kMaskBytes;
+  m.bp = m.maskt + kMaskTBytes;
+  m.misc_bwd = m.bp + 3 * kBpBytes;
+  m.fwd_bytes = m.misc_fwd + (uint32_t)sizeof(Misc);
+  m.bwd_bytes = m.misc_bwd + (uint32_t)sizeof(Misc);
+  return m;
+}
+static_assert(smem_layout(4).misc_bwd % 16 == 0 && smem_layout(2).misc_bwd % 16 == 0, "16-byte operand alignment");
 
 // Tensor-memory columns: first-layer accumulator [128 x 64], mask . W1' [128 x 16],
 // mask^T . (dr feat) [64 x 16] (rows in lanes 0-15 of each 32-lane quarter, the
@@ -164,14 +174,14 @@ __device__ __forceinline__ void warp_point(const NetLaunch& P, float x0, float x
 
 // L * C features of point u (grid_fwd_kernel's arithmetic, n3ds_grid.cu), zero when
 // u leaves [0, 1]^3 as in the reference.
-template <int C>
+template <int C, int LMAX>
 __device__ __forceinline__ void encode_point(const NetLaunch& P, const Level* lvs, const float (&u)[3],
                                              float (&f)[kMaxFeat]) {
 #pragma unroll
   for (int i = 0; i < kMaxFeat; i++) f[i] = 0.f;
   if (!point_in_range(u, 3)) return;
 #pragma unroll
-  for (int l = 0; l < kMaxFeat / C; l++) {
+  for (int l = 0; l < LMAX; l++) {
     if (l < (int)P.L) {
       const Level lv = lvs[l];
       const float* tab = P.table + (size_t)lv.base * C;
@@ -263,22 +273,26 @@ __device__ __forceinline__ void split3_bf16(float x, uint16_t& h, uint16_t& m, u
 // CTA set-up shared by both kernels: W1 split into its tile buffers (and, for the
 // backward, W1' = w2 (.) W1 in three bf16 terms), biases, the second layer, level
 // geometry, the mbarrier and the tensor memory.
-__device__ __forceinline__ void setup_cta(const NetLaunch& P, uint8_t* smem, Misc* M, uint32_t cols, bool backward) {
+__device__ __forceinline__ void setup_cta(const NetLaunch& P, uint8_t* smem, const Smem& L, Misc* M, uint32_t cols,
+                                          bool backward) {
   const int tid = threadIdx.x;
+  const int kc = (int)(L.feat_lo / 2048);
   for (int i = tid; i < kHidden * kMaxFeat; i += kTile) {
     const int j = i / kMaxFeat, f = i % kMaxFeat;
     const float w = f < (int)P.F ? P.w1[j * P.F + f] : 0.f;
-    float h, l;
-    split_tf32(w, h, l);
-    const uint32_t off = (f / 4) * 1024 + j * 16 + (f % 4) * 4;
-    *reinterpret_cast<float*>(smem + OFF_W1_HI + off) = h;
-    *reinterpret_cast<float*>(smem + OFF_W1_LO + off) = l;
+    if (f < 4 * kc) {
+      float h, l;
+      split_tf32(w, h, l);
+      const uint32_t off = (f / 4) * 1024 + j * 16 + (f % 4) * 4;
+      *reinterpret_cast<float*>(smem + L.w1_hi + off) = h;
+      *reinterpret_cast<float*>(smem + L.w1_lo + off) = l;
+    }
     if (backward) {
       uint16_t t[3];
       split3_bf16(w * P.w2[j], t[0], t[1], t[2]);
       const uint32_t o2 = (j / 8) * 256 + f * 16 + (j % 8) * 2;
 #pragma unroll
-      for (int k = 0; k < 3; k++) *reinterpret_cast<uint16_t*>(smem + OFF_W1P + k * kW1pBytes + o2) = t[k];
+      for (int k = 0; k < 3; k++) *reinterpret_cast<uint16_t*>(smem + L.w1p + k * kW1pBytes + o2) = t[k];
     }
   }
   if (tid < kHidden) {
@@ -326,11 +340,12 @@ __device__ __forceinline__ void teardown(const NetLaunch& P, Misc* M, uint32_t p
 
 // ------------------------------------------------------------ forward
 
-template <int C>
+template <int C, int LMAX>
 __global__ void __launch_bounds__(kTile, 4) density_fwd_kernel(NetLaunch P) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  Misc* M = reinterpret_cast<Misc*>(smem + OFF_W1P);
-  setup_cta(P, smem, M, kColsFwd, false);
+  const Smem SL = smem_layout(P.F > 8 ? 4 : 2);
+  Misc* M = reinterpret_cast<Misc*>(smem + SL.misc_fwd);
+  setup_cta(P, smem, SL, M, kColsFwd, false);
   const int tid = threadIdx.x, warp = tid >> 5;
   const uint32_t tmem = M->tmem;
   const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
@@ -351,7 +366,7 @@ __global__ void __launch_bounds__(kTile, 4) density_fwd_kernel(NetLaunch P) {
       }
       warp_point(P, x[0], x[1], x[2], w, u);
       if (valid) {
-        encode_point<C>(P, M->lv, u, f);
+        encode_point<C, LMAX>(P, M->lv, u, f);
         if (P.coords_warped) {
           P.coords_warped[3 * b] = w[0];
           P.coords_warped[3 * b + 1] = w[1];
@@ -369,14 +384,14 @@ __global__ void __launch_bounds__(kTile, 4) density_fwd_kernel(NetLaunch P) {
         for (int i = 0; i < kMaxFeat; i++) f[i] = 0.f;
       }
     }
-    store_split_row(smem + OFF_FEAT_HI, smem + OFF_FEAT_LO, tid * 16, 2048, f, 2 * ks_count);
+    store_split_row(smem + SL.feat_hi, smem + SL.feat_lo, tid * 16, 2048, f, 2 * ks_count);
     fence_proxy_async();
     tc_fence_before_sync();
     __syncthreads();
     tc_fence_after_sync();
     if (tid == 0 && !P.test_stall) {
-      const uint32_t fh = smem_u32(smem + OFF_FEAT_HI), fl = smem_u32(smem + OFF_FEAT_LO);
-      const uint32_t wh = smem_u32(smem + OFF_W1_HI), wl = smem_u32(smem + OFF_W1_LO);
+      const uint32_t fh = smem_u32(smem + SL.feat_hi), fl = smem_u32(smem + SL.feat_lo);
+      const uint32_t wh = smem_u32(smem + SL.w1_hi), wl = smem_u32(smem + SL.w1_lo);
       for (int ks = 0; ks < ks_count; ks++) {
         const uint64_t a_hi = smem_desc(fh + ks * 4096, 2048, 128), a_lo = smem_desc(fl + ks * 4096, 2048, 128);
         const uint64_t b_hi = smem_desc(wh + ks * 2048, 1024, 128), b_lo = smem_desc(wl + ks * 2048, 1024, 128);
@@ -464,11 +479,12 @@ __device__ __forceinline__ void scatter_level(const NetLaunch& P, const Level& l
 // two bf16 products whose operand terms are exact (the mask) or float32 split in three
 // bf16 terms, accumulated in float32: float32 accuracy from kind::f16 MMAs with
 // K-major operands only.
-template <int C>
-__global__ void __launch_bounds__(kTile, 2) density_bwd_kernel(NetLaunch P) {
+template <int C, int LMAX>
+__global__ void __launch_bounds__(kTile, 3) density_bwd_kernel(NetLaunch P) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  Misc* M = reinterpret_cast<Misc*>(smem + OFF_MISC_BWD);
-  setup_cta(P, smem, M, kColsBwd, true);
+  const Smem SL = smem_layout(P.F > 8 ? 4 : 2);
+  Misc* M = reinterpret_cast<Misc*>(smem + SL.misc_bwd);
+  setup_cta(P, smem, SL, M, kColsBwd, true);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t tmem = M->tmem;
   const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
@@ -478,10 +494,10 @@ __global__ void __launch_bounds__(kTile, 2) density_bwd_kernel(NetLaunch P) {
   bool timed_out = false, any = false;
   float acc_w2[kHidden / 16] = {0.f, 0.f, 0.f, 0.f};
   float acc_b2 = 0.f;
-  const uint32_t fh = smem_u32(smem + OFF_FEAT_HI), fl = smem_u32(smem + OFF_FEAT_LO);
-  const uint32_t wh = smem_u32(smem + OFF_W1_HI), wl = smem_u32(smem + OFF_W1_LO);
-  const uint32_t w1p = smem_u32(smem + OFF_W1P), mask = smem_u32(smem + OFF_MASK);
-  const uint32_t maskt = smem_u32(smem + OFF_MASKT), bp = smem_u32(smem + OFF_BP);
+  const uint32_t fh = smem_u32(smem + SL.feat_hi), fl = smem_u32(smem + SL.feat_lo);
+  const uint32_t wh = smem_u32(smem + SL.w1_hi), wl = smem_u32(smem + SL.w1_lo);
+  const uint32_t w1p = smem_u32(smem + SL.w1p), mask = smem_u32(smem + SL.mask);
+  const uint32_t maskt = smem_u32(smem + SL.maskt), bp = smem_u32(smem + SL.bp);
   // this thread's column offset in the transposed tiles
   const uint32_t col_off = (uint32_t)(tid / 8) * kPadChunk + (uint32_t)(tid % 8) * 2;
   for (long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
@@ -509,7 +525,7 @@ __global__ void __launch_bounds__(kTile, 2) density_bwd_kernel(NetLaunch P) {
       }
       g = P.grad_density[b];
     }
-    store_split_row(smem + OFF_FEAT_HI, smem + OFF_FEAT_LO, tid * 16, 2048, f, 2 * ks_count);
+    store_split_row(smem + SL.feat_hi, smem + SL.feat_lo, tid * 16, 2048, f, 2 * ks_count);
     fence_proxy_async();
     tc_fence_before_sync();
     __syncthreads();
@@ -558,13 +574,13 @@ __global__ void __launch_bounds__(kTile, 2) density_bwd_kernel(NetLaunch P) {
         if (k % 2 == 0) words[k / 2] = one;
         else words[k / 2] |= one << 16;
         const int j = c * 16 + k;
-        *reinterpret_cast<uint16_t*>(smem + OFF_MASKT + (j / 8) * kPadGroup + (j % 8) * 16 + col_off) =
+        *reinterpret_cast<uint16_t*>(smem + SL.maskt + (j / 8) * kPadGroup + (j % 8) * 16 + col_off) =
             (uint16_t)one;
         v[k] = dr * relu_t(pre);
       }
-      *reinterpret_cast<uint4*>(smem + OFF_MASK + (2 * c) * 2048 + tid * 16) =
+      *reinterpret_cast<uint4*>(smem + SL.mask + (2 * c) * 2048 + tid * 16) =
           make_uint4(words[0], words[1], words[2], words[3]);
-      *reinterpret_cast<uint4*>(smem + OFF_MASK + (2 * c + 1) * 2048 + tid * 16) =
+      *reinterpret_cast<uint4*>(smem + SL.mask + (2 * c + 1) * 2048 + tid * 16) =
           make_uint4(words[4], words[5], words[6], words[7]);
       acc_w2[c] += warp_slot_sum16(v, lane);
     }
@@ -576,7 +592,7 @@ __global__ void __launch_bounds__(kTile, 2) density_bwd_kernel(NetLaunch P) {
       split3_bf16(x, t[0], t[1], t[2]);
       const uint32_t o = (i / 8) * kPadGroup + (i % 8) * 16 + col_off;
 #pragma unroll
-      for (int k = 0; k < 3; k++) *reinterpret_cast<uint16_t*>(smem + OFF_BP + k * kBpBytes + o) = t[k];
+      for (int k = 0; k < 3; k++) *reinterpret_cast<uint16_t*>(smem + SL.bp + k * kBpBytes + o) = t[k];
     }
     fence_proxy_async();
     tc_fence_before_sync();
@@ -609,7 +625,7 @@ __global__ void __launch_bounds__(kTile, 2) density_bwd_kernel(NetLaunch P) {
     tmem_ld16(lane_addr + COL_DF, df);
     const bool in_grid = valid && point_in_range(u, 3);
 #pragma unroll
-    for (int l = 0; l < kMaxFeat / C; l++) {
+    for (int l = 0; l < LMAX; l++) {
       if (l < (int)P.L) {
         float gl[C];
 #pragma unroll
@@ -763,12 +779,13 @@ NetLaunch make_launch(const n3ds_density_net_t* net, const float* coords, int64_
 // allocation succeeds at once. (The runtime's occupancy calculator answers one CTA
 // per SM for these tensor-memory kernels, below what the hardware runs.)
 template <typename K>
-int resident(K kernel, uint32_t smem, uint32_t cols, int* cache) {
+int resident(K kernel, uint32_t smem_max, uint32_t smem, uint32_t cols, int* cache) {
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 16) dev = 0;
   if (cache[dev] == 0) {
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // the larger layout's size, so that either layout launches whichever came first
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max);
     cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     cudaFuncAttributes fa{};
     int regs_sm = 0, smem_sm = 0, reserved = 0, threads_sm = 0, sms = 0;
@@ -792,26 +809,42 @@ int resident(K kernel, uint32_t smem, uint32_t cols, int* cache) {
 
 int g_resident[2];  // CTAs of the last forward and backward launch
 
-template <int C>
+template <int C, int LMAX>
 int fwd_c(const NetLaunch& P, cudaStream_t st) {
-  static int cache[16] = {0};
-  const int slots = resident(density_fwd_kernel<C>, kSmemFwd, kColsFwd, cache);
+  static int cache[2][16] = {{0}};
+  const int kc = P.F > 8 ? 4 : 2;
+  const uint32_t smem = smem_layout(kc).fwd_bytes;
+  const int slots = resident(density_fwd_kernel<C, LMAX>, smem_layout(4).fwd_bytes, smem, kColsFwd, cache[kc / 4]);
   g_resident[0] = slots;
   const long long tiles = (P.n + kTile - 1) / kTile;
   const int grid = (int)(tiles < slots ? tiles : slots);
-  density_fwd_kernel<C><<<grid, kTile, kSmemFwd, st>>>(P);
+  density_fwd_kernel<C, LMAX><<<grid, kTile, smem, st>>>(P);
   return launch_error("density net forward");
 }
 
-template <int C>
+template <int C, int LMAX>
 int bwd_c(const NetLaunch& P, cudaStream_t st) {
-  static int cache[16] = {0};
-  const int slots = resident(density_bwd_kernel<C>, kSmemBwd, kColsBwd, cache);
+  static int cache[2][16] = {{0}};
+  const int kc = P.F > 8 ? 4 : 2;
+  const uint32_t smem = smem_layout(kc).bwd_bytes;
+  const int slots = resident(density_bwd_kernel<C, LMAX>, smem_layout(4).bwd_bytes, smem, kColsBwd, cache[kc / 4]);
   g_resident[1] = slots;
   const long long tiles = (P.n + kTile - 1) / kTile;
   const int grid = (int)(tiles < slots ? tiles : slots);
-  density_bwd_kernel<C><<<grid, kTile, kSmemBwd, st>>>(P);
+  density_bwd_kernel<C, LMAX><<<grid, kTile, smem, st>>>(P);
   return launch_error("density net backward");
+}
+
+// Instantiations by level_dim and a bound on the level count (the level loops are
+// unrolled to the bound: 8 levels cover the proposal and error networks).
+template <bool BWD>
+int dispatch_net(const NetLaunch& P, uint32_t C, cudaStream_t st) {
+  if (C == 1) {
+    if (P.L <= 8) return BWD ? bwd_c<1, 8>(P, st) : fwd_c<1, 8>(P, st);
+    return BWD ? bwd_c<1, 15>(P, st) : fwd_c<1, 15>(P, st);
+  }
+  if (C == 2) return BWD ? bwd_c<2, 7>(P, st) : fwd_c<2, 7>(P, st);
+  return BWD ? bwd_c<4, 3>(P, st) : fwd_c<4, 3>(P, st);
 }
 
 int check_levels(const float* table, const int32_t* offsets, uint32_t L, uint32_t C, const void* out) {
@@ -844,11 +877,7 @@ extern "C" int n3ds_density_net_forward(const n3ds_density_net_t* net, const flo
   P.features_out = features;
   P.coords_warped = coords_warped;
   const cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  switch (net->level_dim) {
-    case 1: return fwd_c<1>(P, st);
-    case 2: return fwd_c<2>(P, st);
-    default: return fwd_c<4>(P, st);
-  }
+  return dispatch_net<false>(P, net->level_dim, st);
 }
 
 extern "C" int n3ds_density_net_backward(const n3ds_density_net_t* net, const float* coords, const float* features,
@@ -872,11 +901,7 @@ extern "C" int n3ds_density_net_backward(const n3ds_density_net_t* net, const fl
   const size_t vw = net->level_dim * 4 < 16 ? net->level_dim * 4 : 16;
   P.vec_table = vw > 4 && aligned(grad_table, vw);
   const cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  switch (net->level_dim) {
-    case 1: return bwd_c<1>(P, st);
-    case 2: return bwd_c<2>(P, st);
-    default: return bwd_c<4>(P, st);
-  }
+  return dispatch_net<true>(P, net->level_dim, st);
 }
 
 extern "C" int n3ds_grid_level_mean_sq(const float* table, const int32_t* offsets, uint32_t n_levels,
