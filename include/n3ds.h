@@ -529,7 +529,7 @@ int n3ds_density_net_backward(const n3ds_density_net_t* net, const float* coords
  * out[l, c] = mean over level l's rows of table[row, c]^2, for every channel when
  * all_channels is nonzero (torch_scatter's segment_coo), else for channel 0 with
  * the other channels 0 (the scatter_reduce_ fallback the reference takes without
- * torch_scatter). out [L, C] is overwritten. The backward adds
+ * torch_scatter). level_dim 1, 2 or 4. out [L, C] is overwritten. The backward adds
  * grad_out[l, c] * 2 * table[row, c] / rows(l) to grad_table. */
 int n3ds_grid_level_mean_sq(const float* table, const int32_t* offsets, uint32_t n_levels, uint32_t level_dim,
                             int32_t all_channels, float* out, n3ds_stream_t stream);

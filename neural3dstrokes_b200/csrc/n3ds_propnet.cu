@@ -658,57 +658,127 @@ __global__ void __launch_bounds__(kTile, 3) density_bwd_kernel(NetLaunch P) {
 // ------------------------------------------------------------ hash-decay statistics
 
 constexpr int kRedThreads = 256;
+constexpr int kRedUnroll = 4;  // float4 loads in flight per thread
 
-// Per (level, channel) sums of squares: blocks of one level stride over its rows.
+// Level l's rows are one contiguous run of rows(l) * C floats, read as float4 when the
+// table is 16-byte aligned and the run starts and ends on a 4-float boundary (always
+// for GridEncoder's levels, rounded to multiples of 8 rows): element e of the run
+// holds channel e % C, and with C in 1, 2, 4 that is its float4 position % C.
+__device__ __forceinline__ void level_run(const int32_t* offsets, uint32_t l, uint32_t C, uint32_t& r0,
+                                          uint32_t& rows) {
+  r0 = (uint32_t)offsets[l];
+  rows = (uint32_t)offsets[l + 1] - r0;
+}
+
+// Per (level, channel) means of squares; blocks of one level stride over its run.
 __global__ void __launch_bounds__(kRedThreads) level_sumsq_kernel(const float* __restrict__ table,
                                                                   const int32_t* __restrict__ offsets, uint32_t C,
-                                                                  uint32_t n_ch, float* __restrict__ out) {
+                                                                  uint32_t n_ch, bool vec, float* __restrict__ out) {
   const uint32_t l = blockIdx.y;
-  const uint32_t r0 = (uint32_t)offsets[l], r1 = (uint32_t)offsets[l + 1];
-  const float inv_rows = 1.f / (float)(r1 - r0);
-  __shared__ float red[kRedThreads / 32][8];
-  float acc[8];
+  uint32_t r0, rows;
+  level_run(offsets, l, C, r0, rows);
+  const float inv_rows = 1.f / (float)rows;
+  const float* run = table + (size_t)r0 * C;
+  const size_t n = (size_t)rows * C;
+  float acc[4] = {0.f, 0.f, 0.f, 0.f};  // by position in a float4: channel = position % C
+  const size_t stride = (size_t)gridDim.x * kRedThreads;
+  if (vec && ((size_t)r0 * C) % 4 == 0 && n % 4 == 0) {
+    const float4* v = reinterpret_cast<const float4*>(run);
+    const size_t n4 = n / 4;
+    for (size_t i = (size_t)blockIdx.x * kRedThreads + threadIdx.x; i < n4; i += kRedUnroll * stride) {
+      float4 q[kRedUnroll];
 #pragma unroll
-  for (int c = 0; c < 8; c++) acc[c] = 0.f;
-  for (uint32_t r = r0 + blockIdx.x * kRedThreads + threadIdx.x; r < r1; r += gridDim.x * kRedThreads) {
+      for (int k = 0; k < kRedUnroll; k++) q[k] = i + k * stride < n4 ? __ldg(v + i + k * stride) : make_float4(0, 0, 0, 0);
 #pragma unroll
-    for (int c = 0; c < 8; c++) {
-      if (c < (int)n_ch) {
-        const float t = table[(size_t)r * C + c];
-        acc[c] = fmaf(t, t, acc[c]);
+      for (int k = 0; k < kRedUnroll; k++) {
+        acc[0] = fmaf(q[k].x, q[k].x, acc[0]);
+        acc[1] = fmaf(q[k].y, q[k].y, acc[1]);
+        acc[2] = fmaf(q[k].z, q[k].z, acc[2]);
+        acc[3] = fmaf(q[k].w, q[k].w, acc[3]);
       }
     }
+  } else {
+    for (size_t i = (size_t)blockIdx.x * kRedThreads + threadIdx.x; i < n; i += stride) {
+      const float t = run[i];
+      acc[i % 4] = fmaf(t, t, acc[i % 4]);
+    }
   }
+  // fold positions into channels (position p holds channel p % C)
+  float ch[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+  for (int q = 0; q < 4; q++) ch[q % C] += acc[q];
+  __shared__ float red[kRedThreads / 32][4];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
-  for (int c = 0; c < 8; c++) {
-    float s = acc[c];
+  for (int c = 0; c < 4; c++) {
+    float t = ch[c];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) red[w][c] = s;
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (lane == 0) red[w][c] = t;
   }
   __syncthreads();
   if (threadIdx.x < n_ch) {
-    float s = 0.f;
-    for (int i = 0; i < kRedThreads / 32; i++) s += red[i][threadIdx.x];
-    atomicAdd(out + l * C + threadIdx.x, s * inv_rows);
+    float t = 0.f;
+    for (int i = 0; i < kRedThreads / 32; i++) t += red[i][threadIdx.x];
+    atomicAdd(out + l * C + threadIdx.x, t * inv_rows);
   }
 }
 
+// grad_table[row, c] += grad_out[l, c] * 2 * table[row, c] / rows(l) for the reduced
+// channels c < n_ch.
 __global__ void __launch_bounds__(kRedThreads) level_sumsq_bwd_kernel(const float* __restrict__ table,
                                                                       const int32_t* __restrict__ offsets,
-                                                                      uint32_t C, uint32_t n_ch,
+                                                                      uint32_t C, uint32_t n_ch, bool vec,
                                                                       const float* __restrict__ grad_out,
                                                                       float* __restrict__ grad_table) {
   const uint32_t l = blockIdx.y;
-  const uint32_t r0 = (uint32_t)offsets[l], r1 = (uint32_t)offsets[l + 1];
-  const float inv_rows = 1.f / (float)(r1 - r0);
-  for (uint32_t r = r0 + blockIdx.x * kRedThreads + threadIdx.x; r < r1; r += gridDim.x * kRedThreads) {
-    for (uint32_t c = 0; c < n_ch; c++) {
-      const size_t i = (size_t)r * C + c;
-      grad_table[i] += grad_out[l * C + c] * 2.f * table[i] * inv_rows;
+  uint32_t r0, rows;
+  level_run(offsets, l, C, r0, rows);
+  const float s = 2.f / (float)rows;
+  float k4[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) k4[q] = (uint32_t)(q % C) < n_ch ? grad_out[l * C + q % C] * s : 0.f;
+  const size_t n = (size_t)rows * C;
+  const size_t stride = (size_t)gridDim.x * kRedThreads;
+  const float* run = table + (size_t)r0 * C;
+  float* grun = grad_table + (size_t)r0 * C;
+  if (vec && ((size_t)r0 * C) % 4 == 0 && n % 4 == 0) {
+    const float4* v = reinterpret_cast<const float4*>(run);
+    float4* gv = reinterpret_cast<float4*>(grun);
+    const size_t n4 = n / 4;
+    for (size_t i = (size_t)blockIdx.x * kRedThreads + threadIdx.x; i < n4; i += kRedUnroll * stride) {
+      float4 q[kRedUnroll], g[kRedUnroll];
+#pragma unroll
+      for (int k = 0; k < kRedUnroll; k++) {
+        if (i + k * stride < n4) {
+          q[k] = __ldg(v + i + k * stride);
+          g[k] = gv[i + k * stride];
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kRedUnroll; k++) {
+        if (i + k * stride < n4) {
+          g[k].x = fmaf(k4[0], q[k].x, g[k].x);
+          g[k].y = fmaf(k4[1], q[k].y, g[k].y);
+          g[k].z = fmaf(k4[2], q[k].z, g[k].z);
+          g[k].w = fmaf(k4[3], q[k].w, g[k].w);
+          gv[i + k * stride] = g[k];
+        }
+      }
     }
+  } else {
+    for (size_t i = (size_t)blockIdx.x * kRedThreads + threadIdx.x; i < n; i += stride)
+      grun[i] = fmaf(k4[i % 4], run[i], grun[i]);
   }
+}
+
+// Blocks per level: enough for about eight resident CTAs per SM over all levels.
+dim3 level_grid(uint32_t L) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  uint32_t per = (uint32_t)(sms * 8) / L;
+  return dim3(per < 16 ? 16 : per, L);
 }
 
 // ------------------------------------------------------------ host side
@@ -849,7 +919,8 @@ int dispatch_net(const NetLaunch& P, uint32_t C, cudaStream_t st) {
 
 int check_levels(const float* table, const int32_t* offsets, uint32_t L, uint32_t C, const void* out) {
   if (L < 1 || L > 65535) return n3ds::report_error(N3DS_ERR_INVALID, "level statistics: levels must be in [1, 65535]");
-  if (C < 1 || C > 8) return n3ds::report_error(N3DS_ERR_INVALID, "level statistics: level_dim must be in [1, 8]");
+  if (C != 1 && C != 2 && C != 4)
+    return n3ds::report_error(N3DS_ERR_UNSUPPORTED, "level statistics: level_dim must be 1, 2 or 4");
   if (!table || !offsets || !out) return n3ds::report_error(N3DS_ERR_INVALID, "level statistics: null pointer");
   return N3DS_OK;
 }
@@ -910,8 +981,9 @@ extern "C" int n3ds_grid_level_mean_sq(const float* table, const int32_t* offset
   const cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   if (cudaMemsetAsync(out, 0, sizeof(float) * n_levels * level_dim, st) != cudaSuccess)
     return launch_error("level statistics: clear");
-  const dim3 grid(64, n_levels);
-  level_sumsq_kernel<<<grid, kRedThreads, 0, st>>>(table, offsets, level_dim, all_channels ? level_dim : 1u, out);
+  const bool vec = level_dim <= 4 && 4 % level_dim == 0 && aligned(table, 16);
+  level_sumsq_kernel<<<level_grid(n_levels), kRedThreads, 0, st>>>(table, offsets, level_dim,
+                                                                  all_channels ? level_dim : 1u, vec, out);
   return launch_error("level statistics");
 }
 
@@ -920,8 +992,8 @@ extern "C" int n3ds_grid_level_mean_sq_backward(const float* table, const int32_
                                                 float* grad_table, n3ds_stream_t stream) {
   if (int rc = check_levels(table, offsets, n_levels, level_dim, grad_table)) return rc;
   if (!grad_out) return n3ds::report_error(N3DS_ERR_INVALID, "level statistics backward: null gradient");
-  const dim3 grid(256, n_levels);
-  level_sumsq_bwd_kernel<<<grid, kRedThreads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
-      table, offsets, level_dim, all_channels ? level_dim : 1u, grad_out, grad_table);
+  const bool vec = level_dim <= 4 && 4 % level_dim == 0 && aligned(table, 16) && aligned(grad_table, 16);
+  level_sumsq_bwd_kernel<<<level_grid(n_levels), kRedThreads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+      table, offsets, level_dim, all_channels ? level_dim : 1u, vec, grad_out, grad_table);
   return launch_error("level statistics backward");
 }

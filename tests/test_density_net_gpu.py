@@ -346,3 +346,36 @@ def test_coordinate_gradient_request_raises(cuda):
     x = ray_points(cuda, 2, 8, 1.0).requires_grad_(True)
     with pytest.raises(RuntimeError, match="no coordinate gradient"):
         net(x, None)
+
+
+@pytest.mark.parametrize("C,all_channels", [(1, False), (2, False), (2, True), (4, True)])
+def test_level_statistics_against_float64(cuda, C, all_channels):
+    """n3ds_grid_level_mean_sq and its backward on the float4 path (GridEncoder's
+    levels) and the scalar path (a table view whose levels start off 16 bytes)."""
+    from neural3dstrokes_b200.gridencoder import GridEncoder
+    enc = GridEncoder(input_dim=3, num_levels=5, level_dim=C, base_resolution=16, desired_resolution=256,
+                      log2_hashmap_size=14).to(cuda)
+    g = torch.Generator(device=cuda).manual_seed(C)
+    with torch.no_grad():
+        enc.embeddings.uniform_(-1, 1, generator=g)
+    for shifted in (False, True):
+        if shifted:  # the same values one float further into a buffer: scalar path
+            buf = torch.empty(enc.embeddings.numel() + 1, device=cuda)
+            buf[1:] = enc.embeddings.detach().reshape(-1)
+            emb = buf[1:].view(-1, C).requires_grad_(True)
+        else:
+            emb = enc.embeddings
+        out = mlp.level_mean_sq(emb, enc.offsets, all_channels)
+        ref = odn.level_mean_sq(emb, enc.offsets, all_channels)
+        assert rel(out, ref) < FWD_TOL
+        up = torch.randn(out.shape, device=cuda, generator=g)
+        (gt,) = torch.autograd.grad(out, emb, up)
+        offs = [int(o) for o in enc.offsets]
+        gref = torch.zeros(emb.shape, dtype=torch.float64)
+        e64 = emb.detach().double().cpu()
+        n_ch = C if all_channels else 1
+        for lv in range(len(offs) - 1):
+            rows = offs[lv + 1] - offs[lv]
+            gref[offs[lv]:offs[lv + 1], :n_ch] = (up[lv, :n_ch].double().cpu() * 2 / rows
+                                                  * e64[offs[lv]:offs[lv + 1], :n_ch])
+        assert rel(gt, gref) < FWD_TOL
