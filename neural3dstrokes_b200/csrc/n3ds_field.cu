@@ -532,10 +532,12 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
             const int kind = __float_as_int(h.x);
             const int base = kind & 15;
             const int mode = (kind >> 8) & 3;
+            // gradient slots start at -0.0: -0 + x == x exactly, so each slot's first
+            // `+=` compiles to a plain move (0 + x does not fold: it turns -0 into +0)
             if (base <= B_TETRAHEDRON) {
               float v[16];
   #pragma unroll
-              for (int j = 0; j < 16; j++) v[j] = 0.f;
+              for (int j = 0; j < 16; j++) v[j] = -0.f;
               const V3 p = prim_local(rec, c.x);
               const float sdf = prim_sdf(base, p, rec);
               const float f = (kind & K_S3FAC) ? s3_factor(base, p, xyz(rec4(rec)[R_S / 4]), rec) : 1.f;
@@ -556,7 +558,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
             } else if (base == B_QUAD_BEZIER) {
               float v[16];
   #pragma unroll
-              for (int j = 0; j < 16; j++) v[j] = 0.f;
+              for (int j = 0; j < 16; j++) v[j] = -0.f;
               QuadFwd qf;
               const float sdf = quad_eval(rec, c.x, qf);
               const float kk = h.y * c.rinv;
@@ -575,7 +577,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
             } else {
               float v[32];
   #pragma unroll
-              for (int j = 0; j < 32; j++) v[j] = 0.f;
+              for (int j = 0; j < 32; j++) v[j] = -0.f;
               CubicFwd cf;
               const float sdf = cubic_eval(rec, c.x, cf, base == B_CATMULL_ROM);
               const float kk = h.y * c.rinv;
