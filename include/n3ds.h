@@ -241,6 +241,10 @@ typedef struct n3ds_options {
    * without issuing the copies, so every wait runs out and reports (no copy is left
    * in flight). 0 in any real use */
   int32_t test_stall_staging;
+  /* rays a warp claims per work item in the segment schedule: 1, 2 or 4 (0 = 1), i.e.
+   * 64, 128 or 256 samples per claim at 64 samples per ray; larger claims take fewer
+   * atomics on the scene's work counter, smaller ones balance the tail better */
+  int32_t rays_per_item;
 } n3ds_options_t;
 
 /* Fill *opt with the defaults. */

@@ -47,7 +47,7 @@ class Options(ctypes.Structure):
                 ("warps", c_i32), ("schedule", c_i32), ("grad_mode", c_i32),
                 ("timing_events", ctypes.POINTER(ctypes.c_void_p)), ("warps_bwd", c_i32),
                 ("forward_only", c_i32), ("count_pairs", c_i32), ("wait_limit_us", c_i32),
-                ("test_stall_staging", c_i32)]
+                ("test_stall_staging", c_i32), ("rays_per_item", c_i32)]
 
 
 class DensityNet(ctypes.Structure):

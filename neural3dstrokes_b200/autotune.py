@@ -11,7 +11,10 @@ on its own data for each candidate launch configuration and keeps the fastest:
   and a whole tuned step within noise of 24 warps, on Bezier tubes (config 2) 26.2
   against 25.1 ms, so the tuner decides per workload; the run kernels 16);
 * strokes per shared-memory stage: the largest that fits, or half of it (more passes,
-  less shared memory per CTA).
+  less shared memory per CTA);
+* samples per warp claim (segment schedule): a warp takes 1, 2 or 4 rays (64, 128 or
+  256 samples) per atomic on its scene's work counter; tried on the best of the
+  configurations above.
 
 Results are cached per workload signature (scene count, per-scene stroke counts, ray
 counts rounded to powers of two, samples per ray, primitive mix, step mode) in memory
@@ -102,7 +105,8 @@ def resolved(opt: FieldOptions) -> FieldOptions:
     out = _lib.Options()
     _lib.check(_lib.load().n3ds_field_resolve_options(ctypes.byref(opt.c()), ctypes.byref(out)))
     return dataclasses.replace(opt, chunk_fwd=int(out.chunk_fwd), chunk_bwd=int(out.chunk_bwd),
-                               schedule={1: "segments", 2: "runs"}[int(out.schedule)])
+                               schedule={1: "segments", 2: "runs"}[int(out.schedule)],
+                               rays_per_item=int(out.rays_per_item))
 
 
 def tune(field, reps: int = 3, cands: Optional[List[FieldOptions]] = None, use_cache: bool = True,
@@ -132,6 +136,16 @@ def tune(field, reps: int = 3, cands: Optional[List[FieldOptions]] = None, use_c
             print(f"autotune {opt.schedule:8s} warps={opt.warps:2d}/{opt.warps_bwd:2d} "
                   f"chunk={opt.chunk_fwd}/{opt.chunk_bwd}: "
                   f"{ms:.3f} ms", flush=True)
+    ms, best = min(results, key=lambda t: t[0])
+    if cands is None and best.schedule == "segments":
+        for rpi in (2, 4):
+            opt = dataclasses.replace(best, rays_per_item=rpi)
+            field.options = opt
+            field._bind()
+            t = _time_step(field, reps)
+            results.append((t, opt))
+            if verbose:
+                print(f"autotune segments rays_per_item={rpi}: {t:.3f} ms", flush=True)
     last_results[:] = results
     ms, best = min(results, key=lambda t: t[0])
     field.options = best

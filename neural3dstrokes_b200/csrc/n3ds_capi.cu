@@ -105,6 +105,7 @@ struct Resolved {
   int count_pairs;
   unsigned long long wait_limit_ns;
   int test_stall;
+  int rays_per_item;
 };
 
 void record_event(const Resolved& rv, int i, cudaStream_t st) {
@@ -160,6 +161,7 @@ Resolved resolve(const n3ds_options_t* o) {
   r.events = o->timing_events;
   r.wait_limit_ns = o->wait_limit_us > 0 ? (unsigned long long)o->wait_limit_us * 1000ull : 1000000000ull;
   r.test_stall = o->test_stall_staging != 0;
+  r.rays_per_item = o->rays_per_item >= 4 ? 4 : (o->rays_per_item >= 2 ? 2 : 1);
   return r;
 }
 
@@ -297,6 +299,7 @@ void n3ds_default_options(n3ds_options_t* opt) {
   opt->count_pairs = 0;
   opt->wait_limit_us = 0;
   opt->test_stall_staging = 0;
+  opt->rays_per_item = 0;
 }
 
 size_t n3ds_field_workspace_bytes(const n3ds_batch_t* batch, const n3ds_options_t* opt) {
@@ -406,6 +409,7 @@ static n3ds::SegLaunch make_seg(const n3ds_batch_t* b, const n3ds_rays_t* rays, 
   L.mask_tag = reinterpret_cast<const int*>(ws + lay.mask_tag);
   L.wait_limit_ns = 1000000000ull;  // one second unless the options say otherwise
   L.test_stall = 0;
+  L.rays_per_item = 1;
   return L;
 }
 
@@ -449,6 +453,7 @@ int n3ds_field_forward(const n3ds_batch_t* batch, const n3ds_rays_t* rays, const
   n3ds::SegLaunch FL = make_seg(batch, rays, ws, lay, 0);
   FL.wait_limit_ns = rv.wait_limit_ns;
   FL.test_stall = rv.test_stall;
+  FL.rays_per_item = rv.rays_per_item;
   FL.common_only = strokes->base_mask != 0 && (strokes->base_mask & ~n3ds::COMMON_BASES) == 0;
   FL.skip_alpha = rv.cull_alpha;
   if (!rv.count_pairs) FL.stats = nullptr;
@@ -505,6 +510,7 @@ int n3ds_field_backward(const n3ds_batch_t* batch, const n3ds_rays_t* rays, cons
   n3ds::SegLaunch SL = make_seg(batch, rays, ws, lay, compat);
   SL.wait_limit_ns = rv.wait_limit_ns;
   SL.test_stall = rv.test_stall;
+  SL.rays_per_item = rv.rays_per_item;
   SL.grad_x = grad_x;
   SL.stats = rv.count_pairs ? reinterpret_cast<unsigned long long*>(ws + lay.stats) + 17 : nullptr;  // pairs
   SL.skip_alpha = rv.cull_alpha;
@@ -580,6 +586,7 @@ int n3ds_field_resolve_options(const n3ds_options_t* opt, n3ds_options_t* out) {
   out->warps_bwd = rv.warps_bwd;
   out->schedule = rv.schedule;
   out->grad_mode = rv.grad_mode;
+  out->rays_per_item = rv.rays_per_item;
   return N3DS_OK;
 }
 

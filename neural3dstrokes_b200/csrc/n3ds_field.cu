@@ -248,112 +248,114 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_con
     const SceneDesc& sc = L.sc[sci];
     int* counter = L.tile_counter + sci;
     int item = 0;
-    if (lane == 0) item = atomicAdd(counter, 1);
+    if (lane == 0) item = atomicAdd(counter, L.rays_per_item);
     item = __shfl_sync(0xffffffffu, item, 0);
     while (item < sc.n_rays) {
-      const int ray_local = item;
-      for (int g = 0; g < L.segs_per_ray; g++) {
-        SegCtx c = seg_setup(L, sc, ray_local * L.segs_per_ray + g, lane);
-        float T, sig, cr, cg, cb;
-        if (sc.first_pass) {
-          T = 1.f; sig = cr = cg = cb = 0.f;
-        } else {
-          const float* st = L.state + 5 * c.si;
-          T = st[0]; sig = st[1]; cr = st[2]; cg = st[3]; cb = st[4];
-        }
-        const unsigned nact = __popc(__ballot_sync(0xffffffffu, c.active));
-        unsigned* bm = RECORD ? L.block_masks + sc.mask_begin +
-                                    (long long)(ray_local * L.segs_per_ray + g) * sc.mask_words
-                              : nullptr;
-        // Culling in three steps. 1: the sphere test of every block of the chunk (at most
-        // 32 blocks); lane k keeps block k's survivors and its polytope-flagged subset.
-        const int nblk = (sc.chunk_n + 31) >> 5;
-        unsigned my_mask = 0u, my_poly = 0u;
-        for (int k = 0; k < nblk; k++) {
-          unsigned pm;
-          const unsigned m = cull_block_sphere(S, c, sc.chunk_n - 1 - 32 * k, lane, &pm);
-          if (lane == k) {
-            my_mask = m;
-            my_poly = pm;
+      const int item_end = min(item + L.rays_per_item, sc.n_rays);
+      for (int ray_local = item; ray_local < item_end; ray_local++) {
+        for (int g = 0; g < L.segs_per_ray; g++) {
+          SegCtx c = seg_setup(L, sc, ray_local * L.segs_per_ray + g, lane);
+          float T, sig, cr, cg, cb;
+          if (sc.first_pass) {
+            T = 1.f; sig = cr = cg = cb = 0.f;
+          } else {
+            const float* st = L.state + 5 * c.si;
+            T = st[0]; sig = st[1]; cr = st[2]; cg = st[3]; cb = st[4];
           }
-        }
-        // 2: the flagged candidates of all blocks, 32 per pass, one per lane: the owner
-        // block is the last with prefix count <= the candidate's index (5-step binary
-        // search over the lanes), the stroke its n-th flagged bit; rejections are
-        // collected in this warp's kill words.
-        if (__any_sync(0xffffffffu, my_poly != 0u)) {
-          const int cnt = __popc(my_poly);
-          int incl = cnt;
-#pragma unroll
-          for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-          }
-          const int off = incl - cnt;
-          const int total = __shfl_sync(0xffffffffu, incl, 31);
-          for (int g0 = 0; g0 < total; g0 += 32) {
-            const int g = g0 + lane;
-            int kk = 0;
-#pragma unroll
-            for (int step = 16; step > 0; step >>= 1) {
-              const int o = __shfl_sync(0xffffffffu, off, (kk + step) & 31);
-              if (o <= g) kk += step;
-            }
-            const unsigned pm = __shfl_sync(0xffffffffu, my_poly, kk);
-            const int okk = __shfl_sync(0xffffffffu, off, kk);
-            if (g < total) {
-              unsigned x = pm;
-              for (int n = g - okk; n > 0; n--) x &= x - 1u;
-              const int bit = __ffs(x) - 1;
-              const int slot = sc.chunk_n - 1 - 32 * kk - bit;
-              const float* rec = S.recs + size_t(slot) * REC_FLOATS;
-              const int rb = __float_as_int(rec[R_KIND]) & 15;
-              const bool reach = rb == B_SPHERE        ? ellipsoid_reachable(rec, c)
-                                 : rb == B_CAPSULE     ? capsule_reachable(rec, c)
-                                 : rb <= B_TETRAHEDRON ? polytope_reachable(rec, c)
-                                 : COMMON              ? true
-                                                       : curve_reachable(rec, c, fabsf(S.cull_b[slot]), lane);
-              if (!reach) atomicOr(kill + kk, 1u << bit);
+          const unsigned nact = __popc(__ballot_sync(0xffffffffu, c.active));
+          unsigned* bm = RECORD ? L.block_masks + sc.mask_begin +
+                                      (long long)(ray_local * L.segs_per_ray + g) * sc.mask_words
+                                : nullptr;
+          // Culling in three steps. 1: the sphere test of every block of the chunk (at most
+          // 32 blocks); lane k keeps block k's survivors and its polytope-flagged subset.
+          const int nblk = (sc.chunk_n + 31) >> 5;
+          unsigned my_mask = 0u, my_poly = 0u;
+          for (int k = 0; k < nblk; k++) {
+            unsigned pm;
+            const unsigned m = cull_block_sphere(S, c, sc.chunk_n - 1 - 32 * k, lane, &pm);
+            if (lane == k) {
+              my_mask = m;
+              my_poly = pm;
             }
           }
-          __syncwarp();
-          my_mask &= ~kill[lane];
-          kill[lane] = 0u;
-          __syncwarp();
-        }
-        // 3: evaluate the survivors block by block in compositing order
-        for (int k = 0; k < nblk; k++) {
-          const int hi = sc.chunk_n - 1 - 32 * k;
-          unsigned mask = __shfl_sync(0xffffffffu, my_mask, k);
-          const bool any = mask != 0;
-          unsigned kept = 0;  // this lane's strokes of the block whose adjoint the backward needs
-          while (mask) {
-            const int b = __ffs(mask) - 1;
-            mask &= mask - 1;
-            const float* rec = S.recs + size_t(hi - b) * REC_FLOATS;
-            const float a = COMMON ? pair_alpha_common(rec, c.x, c.rinv) : pair_alpha(rec, c.x, c.rinv);
-            if (RECORD && a >= L.skip_alpha) kept |= 1u << b;
-            if (STATS && lane == (__float_as_int(rec[R_KIND]) & 15)) kcount += nact;
-            const float w = a * T;
-            const float4 col = rec4(rec)[R_COLOR / 4];
-            T *= (1.0f - a);
-            sig += rec[R_DENSITY] * w;
-            cr += col.x * w;
-            cg += col.y * w;
-            cb += col.z * w;
+          // 2: the flagged candidates of all blocks, 32 per pass, one per lane: the owner
+          // block is the last with prefix count <= the candidate's index (5-step binary
+          // search over the lanes), the stroke its n-th flagged bit; rejections are
+          // collected in this warp's kill words.
+          if (__any_sync(0xffffffffu, my_poly != 0u)) {
+            const int cnt = __popc(my_poly);
+            int incl = cnt;
+  #pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+              const int y = __shfl_up_sync(0xffffffffu, incl, o);
+              if (lane >= o) incl += y;
+            }
+            const int off = incl - cnt;
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            for (int g0 = 0; g0 < total; g0 += 32) {
+              const int g = g0 + lane;
+              int kk = 0;
+  #pragma unroll
+              for (int step = 16; step > 0; step >>= 1) {
+                const int o = __shfl_sync(0xffffffffu, off, (kk + step) & 31);
+                if (o <= g) kk += step;
+              }
+              const unsigned pm = __shfl_sync(0xffffffffu, my_poly, kk);
+              const int okk = __shfl_sync(0xffffffffu, off, kk);
+              if (g < total) {
+                unsigned x = pm;
+                for (int n = g - okk; n > 0; n--) x &= x - 1u;
+                const int bit = __ffs(x) - 1;
+                const int slot = sc.chunk_n - 1 - 32 * kk - bit;
+                const float* rec = S.recs + size_t(slot) * REC_FLOATS;
+                const int rb = __float_as_int(rec[R_KIND]) & 15;
+                const bool reach = rb == B_SPHERE        ? ellipsoid_reachable(rec, c)
+                                   : rb == B_CAPSULE     ? capsule_reachable(rec, c)
+                                   : rb <= B_TETRAHEDRON ? polytope_reachable(rec, c)
+                                   : COMMON              ? true
+                                                         : curve_reachable(rec, c, fabsf(S.cull_b[slot]), lane);
+                if (!reach) atomicOr(kill + kk, 1u << bit);
+              }
+            }
+            __syncwarp();
+            my_mask &= ~kill[lane];
+            kill[lane] = 0u;
+            __syncwarp();
           }
-          // the words start at zero (cleared before the launch): store the non-empty ones
-          if (RECORD && any) {
-            kept = __reduce_or_sync(0xffffffffu, c.active ? kept : 0u);
-            if (lane == 0 && kept) bm[(sc.n_strokes - 1 - (sc.chunk_lo + hi)) >> 5] = kept;
+          // 3: evaluate the survivors block by block in compositing order
+          for (int k = 0; k < nblk; k++) {
+            const int hi = sc.chunk_n - 1 - 32 * k;
+            unsigned mask = __shfl_sync(0xffffffffu, my_mask, k);
+            const bool any = mask != 0;
+            unsigned kept = 0;  // this lane's strokes of the block whose adjoint the backward needs
+            while (mask) {
+              const int b = __ffs(mask) - 1;
+              mask &= mask - 1;
+              const float* rec = S.recs + size_t(hi - b) * REC_FLOATS;
+              const float a = COMMON ? pair_alpha_common(rec, c.x, c.rinv) : pair_alpha(rec, c.x, c.rinv);
+              if (RECORD && a >= L.skip_alpha) kept |= 1u << b;
+              if (STATS && lane == (__float_as_int(rec[R_KIND]) & 15)) kcount += nact;
+              const float w = a * T;
+              const float4 col = rec4(rec)[R_COLOR / 4];
+              T *= (1.0f - a);
+              sig += rec[R_DENSITY] * w;
+              cr += col.x * w;
+              cg += col.y * w;
+              cb += col.z * w;
+            }
+            // the words start at zero (cleared before the launch): store the non-empty ones
+            if (RECORD && any) {
+              kept = __reduce_or_sync(0xffffffffu, c.active ? kept : 0u);
+              if (lane == 0 && kept) bm[(sc.n_strokes - 1 - (sc.chunk_lo + hi)) >> 5] = kept;
+            }
           }
-        }
-        if (c.active) {
-          float* st = L.state + 5 * c.si;
-          st[0] = T; st[1] = sig; st[2] = cr; st[3] = cg; st[4] = cb;
+          if (c.active) {
+            float* st = L.state + 5 * c.si;
+            st[0] = T; st[1] = sig; st[2] = cr; st[3] = cg; st[4] = cb;
+          }
         }
       }
-      if (lane == 0) item = atomicAdd(counter, 1);
+      if (lane == 0) item = atomicAdd(counter, L.rays_per_item);
       item = __shfl_sync(0xffffffffu, item, 0);
     }
     __syncthreads();  // every warp is done with the staged chunk
@@ -478,143 +480,145 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
     const SceneDesc& sc = L.sc[sci];
     int* counter = L.tile_counter + sci;
     int item = 0;
-    if (lane == 0) item = atomicAdd(counter, 1);
+    if (lane == 0) item = atomicAdd(counter, L.rays_per_item);
     item = __shfl_sync(0xffffffffu, item, 0);
     while (item < sc.n_rays) {
-      const int ray_local = item;
-      for (int g = 0; g < L.segs_per_ray; g++) {
-        SegCtx c = seg_setup(L, sc, ray_local * L.segs_per_ray + g, lane);
-        CompAdj s;
-        {
-          const float* st = L.state + 5 * c.si;
-          s.Tf = st[0]; s.sig = st[1]; s.Cr = st[2]; s.Cg = st[3]; s.Cb = st[4];
-          const float* sd = L.seeds + 5 * c.si;
-          s.gs = sd[0]; s.gcr = sd[1]; s.gcg = sd[2]; s.gcb = sd[3]; s.gT = sd[4];
-          if (!c.active) {
-            s.gs = s.gcr = s.gcg = s.gcb = s.gT = 0.f;
-          }
-        }
-        V3 gx;
-        if (sc.first_pass) {
-          s.T = 1.f; s.Ps = s.Pr = s.Pg = s.Pb = 0.f;
-          gx = v3(0.f, 0.f, 0.f);
-        } else {
-          const float* b = L.bstate + 8 * c.si;
-          s.T = b[0]; s.Ps = b[1]; s.Pr = b[2]; s.Pg = b[3]; s.Pb = b[4];
-          gx = GX ? v3(b[5], b[6], b[7]) : v3(0.f, 0.f, 0.f);
-        }
-        const unsigned* bm =
-            masks ? masks + sc.mask_begin + (long long)(ray_local * L.segs_per_ray + g) * sc.mask_words : nullptr;
-        const unsigned nact = __popc(__ballot_sync(0xffffffffu, c.active));
-        unsigned held = 0;  // mask words (w & ~31) + lane of the current group of 32
-        for (int hi = sc.chunk_n - 1; hi >= 0; hi -= 32) {
-          unsigned mask;
-          if (bm) {
-            const int w = (sc.n_strokes - 1 - (sc.chunk_lo + hi)) >> 5;
-            if (hi == sc.chunk_n - 1 || (w & 31) == 0) {
-              const int wl = (w & ~31) + lane;
-              held = wl < sc.mask_words ? bm[wl] : 0u;
+      const int item_end = min(item + L.rays_per_item, sc.n_rays);
+      for (int ray_local = item; ray_local < item_end; ray_local++) {
+        for (int g = 0; g < L.segs_per_ray; g++) {
+          SegCtx c = seg_setup(L, sc, ray_local * L.segs_per_ray + g, lane);
+          CompAdj s;
+          {
+            const float* st = L.state + 5 * c.si;
+            s.Tf = st[0]; s.sig = st[1]; s.Cr = st[2]; s.Cg = st[3]; s.Cb = st[4];
+            const float* sd = L.seeds + 5 * c.si;
+            s.gs = sd[0]; s.gcr = sd[1]; s.gcg = sd[2]; s.gcb = sd[3]; s.gT = sd[4];
+            if (!c.active) {
+              s.gs = s.gcr = s.gcg = s.gcb = s.gT = 0.f;
             }
-            mask = __shfl_sync(0xffffffffu, held, w & 31);
-            if (hi < 31) mask &= (2u << hi) - 1u;  // only strokes hi .. 0 exist in the last block
-          } else {
-            unsigned unused;
-            mask = cull_block_sphere(S, c, hi, lane, &unused);  // conservative: no polytope test here
           }
-          while (mask) {
-            const int b = __ffs(mask) - 1;
-            mask &= mask - 1;
-            const int sl = hi - b;
-            const float* rec = S.recs + size_t(sl) * REC_FLOATS;
-            float* row = S.gacc + size_t(sl) * GRAD_SLOTS;
-            bcount += nact;
-            const float4 h = rec4(rec)[0];
-            const int kind = __float_as_int(h.x);
-            const int base = kind & 15;
-            const int mode = (kind >> 8) & 3;
-            // gradient slots start at -0.0: -0 + x == x exactly, so each slot's first
-            // `+=` compiles to a plain move (0 + x does not fold: it turns -0 into +0)
-            if (base <= B_TETRAHEDRON) {
-              float v[16];
-  #pragma unroll
-              for (int j = 0; j < 16; j++) v[j] = -0.f;
-              const V3 p = prim_local(rec, c.x);
-              const float sdf = prim_sdf(base, p, rec);
-              const float f = (kind & K_S3FAC) ? s3_factor(base, p, xyz(rec4(rec)[R_S / 4]), rec) : 1.f;
-              const float kk = h.y * f * c.rinv;
-              const float m = -sdf * kk;
-              const float a = mode == STEP_HARD ? (sdf <= 0.f ? 1.f : 0.f) : soft_alpha(mode, m);
-              const bool below = __all_sync(0xffffffffu, !c.active || a < L.skip_alpha);
-              if (below || (kind & K_FROZEN)) {  // the kind word is warp-uniform
-                compose_skip(rec, a, s);
-                continue;
+          V3 gx;
+          if (sc.first_pass) {
+            s.T = 1.f; s.Ps = s.Pr = s.Pg = s.Pb = 0.f;
+            gx = v3(0.f, 0.f, 0.f);
+          } else {
+            const float* b = L.bstate + 8 * c.si;
+            s.T = b[0]; s.Ps = b[1]; s.Pr = b[2]; s.Pg = b[3]; s.Pb = b[4];
+            gx = GX ? v3(b[5], b[6], b[7]) : v3(0.f, 0.f, 0.f);
+          }
+          const unsigned* bm =
+              masks ? masks + sc.mask_begin + (long long)(ray_local * L.segs_per_ray + g) * sc.mask_words : nullptr;
+          const unsigned nact = __popc(__ballot_sync(0xffffffffu, c.active));
+          unsigned held = 0;  // mask words (w & ~31) + lane of the current group of 32
+          for (int hi = sc.chunk_n - 1; hi >= 0; hi -= 32) {
+            unsigned mask;
+            if (bm) {
+              const int w = (sc.n_strokes - 1 - (sc.chunk_lo + hi)) >> 5;
+              if (hi == sc.chunk_n - 1 || (w & 31) == 0) {
+                const int wl = (w & ~31) + lane;
+                held = wl < sc.mask_words ? bm[wl] : 0u;
               }
-              const float dm = compose_step(rec, a, m, mode, s, v, compat);
-              const float K = m * dm;
-              v[G_K] += K;
-              const V3 gp = prim_backprop(rec, kind, p, -kk * dm, K, v, compat);
-              if (GX) gx += gp;
-              reduce_into<16>(v, row, lane);
-            } else if (base == B_QUAD_BEZIER) {
-              float v[16];
-  #pragma unroll
-              for (int j = 0; j < 16; j++) v[j] = -0.f;
-              QuadFwd qf;
-              const float sdf = quad_eval(rec, c.x, qf);
-              const float kk = h.y * c.rinv;
-              const float m = -sdf * kk;
-              const float a = mode == STEP_HARD ? (sdf <= 0.f ? 1.f : 0.f) : soft_alpha(mode, m);
-              const bool below = __all_sync(0xffffffffu, !c.active || a < L.skip_alpha);
-              if (below || (kind & K_FROZEN)) {  // the kind word is warp-uniform
-                compose_skip(rec, a, s);
-                continue;
-              }
-              const float dm = compose_step(rec, a, m, mode, s, v, compat);
-              v[G_K] += m * dm;
-              const V3 gq = quad_adjoint(rec, qf, -kk * dm, v + G_CTRL);
-              if (GX) gx += gq;
-              reduce_into<16>(v, row, lane);
+              mask = __shfl_sync(0xffffffffu, held, w & 31);
+              if (hi < 31) mask &= (2u << hi) - 1u;  // only strokes hi .. 0 exist in the last block
             } else {
-              float v[32];
-  #pragma unroll
-              for (int j = 0; j < 32; j++) v[j] = -0.f;
-              CubicFwd cf;
-              const float sdf = cubic_eval(rec, c.x, cf, base == B_CATMULL_ROM);
-              const float kk = h.y * c.rinv;
-              const float m = -sdf * kk;
-              const float a = mode == STEP_HARD ? (sdf <= 0.f ? 1.f : 0.f) : soft_alpha(mode, m);
-              const bool below = __all_sync(0xffffffffu, !c.active || a < L.skip_alpha);
-              if (below || (kind & K_FROZEN)) {  // the kind word is warp-uniform
-                compose_skip(rec, a, s);
-                continue;
+              unsigned unused;
+              mask = cull_block_sphere(S, c, hi, lane, &unused);  // conservative: no polytope test here
+            }
+            while (mask) {
+              const int b = __ffs(mask) - 1;
+              mask &= mask - 1;
+              const int sl = hi - b;
+              const float* rec = S.recs + size_t(sl) * REC_FLOATS;
+              float* row = S.gacc + size_t(sl) * GRAD_SLOTS;
+              bcount += nact;
+              const float4 h = rec4(rec)[0];
+              const int kind = __float_as_int(h.x);
+              const int base = kind & 15;
+              const int mode = (kind >> 8) & 3;
+              // gradient slots start at -0.0: -0 + x == x exactly, so each slot's first
+              // `+=` compiles to a plain move (0 + x does not fold: it turns -0 into +0)
+              if (base <= B_TETRAHEDRON) {
+                float v[16];
+    #pragma unroll
+                for (int j = 0; j < 16; j++) v[j] = -0.f;
+                const V3 p = prim_local(rec, c.x);
+                const float sdf = prim_sdf(base, p, rec);
+                const float f = (kind & K_S3FAC) ? s3_factor(base, p, xyz(rec4(rec)[R_S / 4]), rec) : 1.f;
+                const float kk = h.y * f * c.rinv;
+                const float m = -sdf * kk;
+                const float a = mode == STEP_HARD ? (sdf <= 0.f ? 1.f : 0.f) : soft_alpha(mode, m);
+                const bool below = __all_sync(0xffffffffu, !c.active || a < L.skip_alpha);
+                if (below || (kind & K_FROZEN)) {  // the kind word is warp-uniform
+                  compose_skip(rec, a, s);
+                  continue;
+                }
+                const float dm = compose_step(rec, a, m, mode, s, v, compat);
+                const float K = m * dm;
+                v[G_K] += K;
+                const V3 gp = prim_backprop(rec, kind, p, -kk * dm, K, v, compat);
+                if (GX) gx += gp;
+                reduce_into<16>(v, row, lane);
+              } else if (base == B_QUAD_BEZIER) {
+                float v[16];
+    #pragma unroll
+                for (int j = 0; j < 16; j++) v[j] = -0.f;
+                QuadFwd qf;
+                const float sdf = quad_eval(rec, c.x, qf);
+                const float kk = h.y * c.rinv;
+                const float m = -sdf * kk;
+                const float a = mode == STEP_HARD ? (sdf <= 0.f ? 1.f : 0.f) : soft_alpha(mode, m);
+                const bool below = __all_sync(0xffffffffu, !c.active || a < L.skip_alpha);
+                if (below || (kind & K_FROZEN)) {  // the kind word is warp-uniform
+                  compose_skip(rec, a, s);
+                  continue;
+                }
+                const float dm = compose_step(rec, a, m, mode, s, v, compat);
+                v[G_K] += m * dm;
+                const V3 gq = quad_adjoint(rec, qf, -kk * dm, v + G_CTRL);
+                if (GX) gx += gq;
+                reduce_into<16>(v, row, lane);
+              } else {
+                float v[32];
+    #pragma unroll
+                for (int j = 0; j < 32; j++) v[j] = -0.f;
+                CubicFwd cf;
+                const float sdf = cubic_eval(rec, c.x, cf, base == B_CATMULL_ROM);
+                const float kk = h.y * c.rinv;
+                const float m = -sdf * kk;
+                const float a = mode == STEP_HARD ? (sdf <= 0.f ? 1.f : 0.f) : soft_alpha(mode, m);
+                const bool below = __all_sync(0xffffffffu, !c.active || a < L.skip_alpha);
+                if (below || (kind & K_FROZEN)) {  // the kind word is warp-uniform
+                  compose_skip(rec, a, s);
+                  continue;
+                }
+                const float dm = compose_step(rec, a, m, mode, s, v, compat);
+                const float dsdf = -kk * dm;
+                v[G_K] += m * dm;
+                V3 g = cubic_adjoint(rec, c.x, cf, dsdf, v + G_CTRL, compat, base == B_CATMULL_ROM);
+                if (compat) g = g * dsdf;  // the reference multiplies by dL/dSDF again
+                if (GX) gx += g;
+                reduce_into<32>(v, row, lane);
               }
-              const float dm = compose_step(rec, a, m, mode, s, v, compat);
-              const float dsdf = -kk * dm;
-              v[G_K] += m * dm;
-              V3 g = cubic_adjoint(rec, c.x, cf, dsdf, v + G_CTRL, compat, base == B_CATMULL_ROM);
-              if (compat) g = g * dsdf;  // the reference multiplies by dL/dSDF again
-              if (GX) gx += g;
-              reduce_into<32>(v, row, lane);
             }
           }
-        }
-        if (c.active) {
-          if (sc.last_pass) {
-            if (GX) {
-              L.grad_x[3 * c.si] = gx.x;
-              L.grad_x[3 * c.si + 1] = gx.y;
-              L.grad_x[3 * c.si + 2] = gx.z;
-            }
-          } else {
-            float* b = L.bstate + 8 * c.si;
-            b[0] = s.T; b[1] = s.Ps; b[2] = s.Pr; b[3] = s.Pg; b[4] = s.Pb;
-            if (GX) {
-              b[5] = gx.x; b[6] = gx.y; b[7] = gx.z;
+          if (c.active) {
+            if (sc.last_pass) {
+              if (GX) {
+                L.grad_x[3 * c.si] = gx.x;
+                L.grad_x[3 * c.si + 1] = gx.y;
+                L.grad_x[3 * c.si + 2] = gx.z;
+              }
+            } else {
+              float* b = L.bstate + 8 * c.si;
+              b[0] = s.T; b[1] = s.Ps; b[2] = s.Pr; b[3] = s.Pg; b[4] = s.Pb;
+              if (GX) {
+                b[5] = gx.x; b[6] = gx.y; b[7] = gx.z;
+              }
             }
           }
         }
       }
-      if (lane == 0) item = atomicAdd(counter, 1);
+      if (lane == 0) item = atomicAdd(counter, L.rays_per_item);
       item = __shfl_sync(0xffffffffu, item, 0);
     }
     __syncthreads();  // every warp is done with the staged chunk

@@ -33,6 +33,7 @@ struct SegLaunch {
   const float* radii;      // [R] (cast mode)
   int n_samples;           // samples per ray
   int segs_per_ray;        // ceil(n_samples / 32)
+  int rays_per_item;       // rays a warp claims per atomic on the scene's work counter (>= 1)
   const float* recs;       // [S*64] prepared stroke records
   const float* cull_a;     // [S*4]  culling sphere (cx, cy, cz, R)
   const float* cull_b;     // [S(+pad)] culling margin per unit radius

@@ -32,6 +32,7 @@ class FieldOptions:
     count_pairs: bool = False   # count evaluated pairs (statistics; a few % of the forward's work)
     wait_limit_us: int = 0      # limit of the device's bounded waits (0: one second)
     test_stall_staging: bool = False  # test of the wait limit only: every staging wait runs out
+    rays_per_item: int = 0      # rays a warp claims at once, segment schedule: 1, 2, 4 (0: 1)
 
     def c(self, events=None):
         """ctypes options; ``events``: optional 4 torch.cuda.Event(enable_timing=True)
@@ -48,7 +49,7 @@ class FieldOptions:
                             {"auto": 0, "segments": 1, "runs": 2}[self.schedule],
                             _lib.N3DS_GRAD_COMPAT if self.grad_mode == "compat" else _lib.N3DS_GRAD_EXACT, ev,
                             int(self.warps_bwd), int(bool(self.forward_only)), int(bool(self.count_pairs)),
-                            int(self.wait_limit_us), int(bool(self.test_stall_staging)))
+                            int(self.wait_limit_us), int(bool(self.test_stall_staging)), int(self.rays_per_item))
 
 
 class _Native:

@@ -23,6 +23,36 @@ def test_resolved_options_fill_in_auto_values():
     assert (r.chunk_fwd, r.chunk_bwd) == (64, 96)
 
 
+def test_rays_per_item_resolves_to_one_two_or_four():
+    got = [autotune.resolved(FieldOptions(rays_per_item=r)).rays_per_item for r in (0, 1, 2, 3, 4, 9)]
+    assert got == [1, 1, 2, 2, 4, 4]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rpi", [2, 4])
+def test_rays_per_item_keeps_results(cuda, rpi):
+    """Larger work claims change which warp renders which ray, nothing else: forward
+    outputs bit-equal, gradients equal up to the order of float atomics."""
+    from neural3dstrokes_b200.train import BatchedField
+    w = scenes.config(3, scale=0.02)
+    out = []
+    for r in (1, rpi):
+        f = BatchedField(w.scenes[:5], w.rays[:5], options=FieldOptions(rays_per_item=r), device=cuda)
+        g = torch.Generator().manual_seed(1)
+        f.g_rgb.copy_(torch.randn(f.rgb.shape, generator=g))
+        f.g_acc.copy_(torch.randn(f.acc.shape, generator=g))
+        f.forward()
+        f.backward()
+        torch.cuda.synchronize()
+        out.append((f.rgb.clone(), f.acc.clone(), f.grad_shape.clone(), f.grad_x.clone() if f.grad_x is not None
+                    else None))
+    (r1, a1, s1, x1), (r2, a2, s2, x2) = out
+    assert torch.equal(r1, r2) and torch.equal(a1, a2)
+    assert rel(s2, s1) < 1e-5
+    if x1 is not None:
+        assert torch.equal(x1, x2)
+
+
 def test_candidate_set_covers_schedules_warps_and_stages():
     c = autotune.candidates()
     assert {o.schedule for o in c} == {"segments", "runs"}
