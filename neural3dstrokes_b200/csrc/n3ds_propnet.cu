@@ -69,8 +69,6 @@ constexpr int kStatusWait = 2;             // the field's ST_WAIT_TIMEOUT bit
 //     + (f % 8) * 16 + (p / 8) * 144 + (p % 8) * 2 (B of dW1: N = f, K = points).
 // The transposed tiles are written a column per thread; their 144-byte K chunks (128 +
 // 16 of padding) put a warp's 32 columns on distinct banks.
-constexpr uint32_t kFeatBytes = kTile * kMaxFeat * 4;   // 8 KB
-constexpr uint32_t kW1Bytes = kHidden * kMaxFeat * 4;   // 4 KB
 constexpr uint32_t kW1pBytes = kMaxFeat * kHidden * 2;  // 2 KB per term
 constexpr uint32_t kMaskBytes = kTile * kHidden * 2;    // 16 KB
 constexpr uint32_t kPadChunk = 144, kPadGroup = 16 * kPadChunk;
@@ -174,7 +172,7 @@ __device__ __forceinline__ void warp_point(const NetLaunch& P, float x0, float x
 
 // L * C features of point u (grid_fwd_kernel's arithmetic, n3ds_grid.cu), zero when
 // u leaves [0, 1]^3 as in the reference.
-template <int C, int LMAX>
+template <int C, int LMAX, bool EXACT>
 __device__ __forceinline__ void encode_point(const NetLaunch& P, const Level* lvs, const float (&u)[3],
                                              float (&f)[kMaxFeat]) {
 #pragma unroll
@@ -182,7 +180,7 @@ __device__ __forceinline__ void encode_point(const NetLaunch& P, const Level* lv
   if (!point_in_range(u, 3)) return;
 #pragma unroll
   for (int l = 0; l < LMAX; l++) {
-    if (l < (int)P.L) {
+    if (EXACT || l < (int)P.L) {  // EXACT: LMAX is the level count, no guard
       const Level lv = lvs[l];
       const float* tab = P.table + (size_t)lv.base * C;
       uint32_t cell[3];
@@ -340,7 +338,7 @@ __device__ __forceinline__ void teardown(const NetLaunch& P, Misc* M, uint32_t p
 
 // ------------------------------------------------------------ forward
 
-template <int C, int LMAX>
+template <int C, int LMAX, bool EXACT>
 __global__ void __launch_bounds__(kTile, 4) density_fwd_kernel(NetLaunch P) {
   extern __shared__ __align__(1024) uint8_t smem[];
   const Smem SL = smem_layout(P.F > 8 ? 4 : 2);
@@ -366,7 +364,7 @@ __global__ void __launch_bounds__(kTile, 4) density_fwd_kernel(NetLaunch P) {
       }
       warp_point(P, x[0], x[1], x[2], w, u);
       if (valid) {
-        encode_point<C, LMAX>(P, M->lv, u, f);
+        encode_point<C, LMAX, EXACT>(P, M->lv, u, f);
         if (P.coords_warped) {
           P.coords_warped[3 * b] = w[0];
           P.coords_warped[3 * b + 1] = w[1];
@@ -479,7 +477,7 @@ __device__ __forceinline__ void scatter_level(const NetLaunch& P, const Level& l
 // two bf16 products whose operand terms are exact (the mask) or float32 split in three
 // bf16 terms, accumulated in float32: float32 accuracy from kind::f16 MMAs with
 // K-major operands only.
-template <int C, int LMAX>
+template <int C, int LMAX, bool EXACT>
 __global__ void __launch_bounds__(kTile, 3) density_bwd_kernel(NetLaunch P) {
   extern __shared__ __align__(1024) uint8_t smem[];
   const Smem SL = smem_layout(P.F > 8 ? 4 : 2);
@@ -626,7 +624,7 @@ __global__ void __launch_bounds__(kTile, 3) density_bwd_kernel(NetLaunch P) {
     const bool in_grid = valid && point_in_range(u, 3);
 #pragma unroll
     for (int l = 0; l < LMAX; l++) {
-      if (l < (int)P.L) {
+      if (EXACT || l < (int)P.L) {
         float gl[C];
 #pragma unroll
         for (int c = 0; c < C; c++) gl[c] = in_grid ? dr * df[l * C + c] : 0.f;
@@ -879,42 +877,53 @@ int resident(K kernel, uint32_t smem_max, uint32_t smem, uint32_t cols, int* cac
 
 int g_resident[2];  // CTAs of the last forward and backward launch
 
-template <int C, int LMAX>
+template <int C, int LMAX, bool EXACT>
 int fwd_c(const NetLaunch& P, cudaStream_t st) {
   static int cache[2][16] = {{0}};
   const int kc = P.F > 8 ? 4 : 2;
   const uint32_t smem = smem_layout(kc).fwd_bytes;
-  const int slots = resident(density_fwd_kernel<C, LMAX>, smem_layout(4).fwd_bytes, smem, kColsFwd, cache[kc / 4]);
+  const int slots = resident(density_fwd_kernel<C, LMAX, EXACT>, smem_layout(4).fwd_bytes, smem, kColsFwd, cache[kc / 4]);
   g_resident[0] = slots;
   const long long tiles = (P.n + kTile - 1) / kTile;
   const int grid = (int)(tiles < slots ? tiles : slots);
-  density_fwd_kernel<C, LMAX><<<grid, kTile, smem, st>>>(P);
+  density_fwd_kernel<C, LMAX, EXACT><<<grid, kTile, smem, st>>>(P);
   return launch_error("density net forward");
 }
 
-template <int C, int LMAX>
+template <int C, int LMAX, bool EXACT>
 int bwd_c(const NetLaunch& P, cudaStream_t st) {
   static int cache[2][16] = {{0}};
   const int kc = P.F > 8 ? 4 : 2;
   const uint32_t smem = smem_layout(kc).bwd_bytes;
-  const int slots = resident(density_bwd_kernel<C, LMAX>, smem_layout(4).bwd_bytes, smem, kColsBwd, cache[kc / 4]);
+  const int slots = resident(density_bwd_kernel<C, LMAX, EXACT>, smem_layout(4).bwd_bytes, smem, kColsBwd, cache[kc / 4]);
   g_resident[1] = slots;
   const long long tiles = (P.n + kTile - 1) / kTile;
   const int grid = (int)(tiles < slots ? tiles : slots);
-  density_bwd_kernel<C, LMAX><<<grid, kTile, smem, st>>>(P);
+  density_bwd_kernel<C, LMAX, EXACT><<<grid, kTile, smem, st>>>(P);
   return launch_error("density net backward");
 }
 
-// Instantiations by level_dim and a bound on the level count (the level loops are
-// unrolled to the bound: 8 levels cover the proposal and error networks).
+// Instantiations by level_dim and the level count: exact counts for the stroke model's
+// networks (PropMLP 6 and 8 levels x 1 channel, ErrorMLP 5 x 2; unguarded level loops,
+// so every level's gathers can be in flight together), else a bound (8 or 15 levels
+// for C = 1, 7 for C = 2, 3 for C = 4) with a guard per level.
+template <bool BWD, int C, int LMAX, bool EXACT>
+int launch_net(const NetLaunch& P, cudaStream_t st) {
+  return BWD ? bwd_c<C, LMAX, EXACT>(P, st) : fwd_c<C, LMAX, EXACT>(P, st);
+}
 template <bool BWD>
 int dispatch_net(const NetLaunch& P, uint32_t C, cudaStream_t st) {
   if (C == 1) {
-    if (P.L <= 8) return BWD ? bwd_c<1, 8>(P, st) : fwd_c<1, 8>(P, st);
-    return BWD ? bwd_c<1, 15>(P, st) : fwd_c<1, 15>(P, st);
+    if (P.L == 6) return launch_net<BWD, 1, 6, true>(P, st);
+    if (P.L == 8) return launch_net<BWD, 1, 8, true>(P, st);
+    if (P.L < 8) return launch_net<BWD, 1, 8, false>(P, st);
+    return launch_net<BWD, 1, 15, false>(P, st);
   }
-  if (C == 2) return BWD ? bwd_c<2, 7>(P, st) : fwd_c<2, 7>(P, st);
-  return BWD ? bwd_c<4, 3>(P, st) : fwd_c<4, 3>(P, st);
+  if (C == 2) {
+    if (P.L == 5) return launch_net<BWD, 2, 5, true>(P, st);
+    return launch_net<BWD, 2, 7, false>(P, st);
+  }
+  return launch_net<BWD, 4, 3, false>(P, st);
 }
 
 int check_levels(const float* table, const int32_t* offsets, uint32_t L, uint32_t C, const void* out) {

@@ -328,8 +328,9 @@ def test_bounded_wait_runs_out_and_reports(cuda):
 
 
 def test_persistent_grid_fills_the_device(cuda):
-    """The persistent kernels launch several CTAs per SM (the occupancy limits, capped by
-    tensor memory: 8 forward, 4 backward), not one."""
+    """The persistent kernels launch several CTAs per SM (their register, shared-memory
+    and tensor-memory limits: 4 forward with the unguarded level loops, 3 backward),
+    not the one CTA per SM the runtime's occupancy calculator answers."""
     from neural3dstrokes_b200 import _lib
     net = make_net("prop512_bbox", cuda, seed=24)
     x = ray_points(cuda, 512, 64, 1.2, seed=25)
@@ -338,7 +339,7 @@ def test_persistent_grid_fills_the_device(cuda):
     lib = _lib.load()
     fwd, bwd = lib.n3ds_density_net_resident_ctas(0), lib.n3ds_density_net_resident_ctas(1)
     print("resident CTAs: forward", fwd, "backward", bwd, "SMs", sms)
-    assert fwd >= 6 * sms and bwd >= 3 * sms
+    assert fwd >= 4 * sms and bwd >= 3 * sms
 
 
 def test_coordinate_gradient_request_raises(cuda):
