@@ -211,10 +211,11 @@ __device__ __forceinline__ void encode_point(const NetLaunch& P, const Level* lv
 
 // The first n_chunks 4-value chunks of a 16-value row into the tile's hi and lo
 // buffers.
+template <int N>
 __device__ __forceinline__ void store_split_row(uint8_t* hi_base, uint8_t* lo_base, uint32_t row_off,
-                                                uint32_t chunk_stride, const float (&v)[16], int n_chunks) {
+                                                uint32_t chunk_stride, const float (&v)[N], int n_chunks) {
 #pragma unroll
-  for (int c = 0; c < 4; c++) {
+  for (int c = 0; c < N / 4; c++) {
     if (c >= n_chunks) break;
     float h[4], l[4];
 #pragma unroll
@@ -477,11 +478,46 @@ __device__ __forceinline__ void scatter_level(const NetLaunch& P, const Level& l
 // two bf16 products whose operand terms are exact (the mask) or float32 split in three
 // bf16 terms, accumulated in float32: float32 accuracy from kind::f16 MMAs with
 // K-major operands only.
+// The inputs of a tile (coordinates, feature record, upstream gradient) of this
+// thread's point; FP floats of features (8 when L * C <= 8, else 16).
+template <int FP>
+struct BwdIn {
+  float x[3];
+  float f[FP];
+  float g;
+  bool valid;
+};
+template <int FP>
+__device__ __forceinline__ void load_bwd_in(const NetLaunch& P, long long b, BwdIn<FP>& in) {
+  in.valid = b < P.n;
+  in.g = 0.f;
+#pragma unroll
+  for (int i = 0; i < 3; i++) in.x[i] = 0.f;
+#pragma unroll
+  for (int i = 0; i < FP; i++) in.f[i] = 0.f;
+  if (!in.valid) return;
+#pragma unroll
+  for (int i = 0; i < 3; i++) in.x[i] = P.coords[3 * b + i];
+  const float4* rec = reinterpret_cast<const float4*>(P.features_in + b * P.stride);
+#pragma unroll
+  for (int c = 0; c < FP / 4; c++) {
+    if (c < (int)(P.stride / 4)) {
+      const float4 r = rec[c];
+      in.f[4 * c] = r.x; in.f[4 * c + 1] = r.y; in.f[4 * c + 2] = r.z; in.f[4 * c + 3] = r.w;
+    }
+  }
+  in.g = P.grad_density[b];
+}
+
 template <int C, int LMAX, bool EXACT>
 __global__ void __launch_bounds__(kTile, 3) density_bwd_kernel(NetLaunch P) {
+  constexpr int FP = C * LMAX <= 8 ? 8 : 16;
   extern __shared__ __align__(1024) uint8_t smem[];
   const Smem SL = smem_layout(P.F > 8 ? 4 : 2);
   Misc* M = reinterpret_cast<Misc*>(smem + SL.misc_bwd);
+  // the d raw (.) feat tile's columns beyond L * C (d raw itself) stay zero: cleared
+  // once here, the tiles write columns 0 .. L * C only
+  for (uint32_t i = threadIdx.x; i < 3 * kBpBytes / 4; i += kTile) reinterpret_cast<float*>(smem + SL.bp)[i] = 0.f;
   setup_cta(P, smem, SL, M, kColsBwd, true);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t tmem = M->tmem;
@@ -498,32 +534,20 @@ __global__ void __launch_bounds__(kTile, 3) density_bwd_kernel(NetLaunch P) {
   const uint32_t maskt = smem_u32(smem + SL.maskt), bp = smem_u32(smem + SL.bp);
   // this thread's column offset in the transposed tiles
   const uint32_t col_off = (uint32_t)(tid / 8) * kPadChunk + (uint32_t)(tid % 8) * 2;
+  BwdIn<FP> in;
+  load_bwd_in<FP>(P, (long long)blockIdx.x * kTile + tid, in);
   for (long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
-    const long long b = tile * kTile + tid;
-    const bool valid = b < P.n;
+    const bool valid = in.valid;
+    const float g = in.g;
     float u[3] = {0.f, 0.f, 0.f};
-    float g = 0.f;
-    float f[kMaxFeat];
+    float f[FP];
 #pragma unroll
-    for (int i = 0; i < kMaxFeat; i++) f[i] = 0.f;
+    for (int i = 0; i < FP; i++) f[i] = i < (int)P.F ? in.f[i] : 0.f;
     if (valid) {
       float w[3];
-      warp_point(P, P.coords[3 * b], P.coords[3 * b + 1], P.coords[3 * b + 2], w, u);
-      const float4* rec = reinterpret_cast<const float4*>(P.features_in + b * P.stride);
-#pragma unroll
-      for (int c = 0; c < kMaxFeat / 4; c++) {
-        if (c < (int)(P.stride / 4)) {
-          const float4 r = rec[c];
-          f[4 * c] = r.x; f[4 * c + 1] = r.y; f[4 * c + 2] = r.z; f[4 * c + 3] = r.w;
-        }
-      }
-#pragma unroll
-      for (int i = 0; i < kMaxFeat; i++) {
-        if (i >= (int)P.F) f[i] = 0.f;
-      }
-      g = P.grad_density[b];
+      warp_point(P, in.x[0], in.x[1], in.x[2], w, u);
     }
-    store_split_row(smem + SL.feat_hi, smem + SL.feat_lo, tid * 16, 2048, f, 2 * ks_count);
+    store_split_row<FP>(smem + SL.feat_hi, smem + SL.feat_lo, tid * 16, 2048, f, 2 * ks_count);
     fence_proxy_async();
     tc_fence_before_sync();
     __syncthreads();
@@ -582,16 +606,19 @@ __global__ void __launch_bounds__(kTile, 3) density_bwd_kernel(NetLaunch P) {
           make_uint4(words[4], words[5], words[6], words[7]);
       acc_w2[c] += warp_slot_sum16(v, lane);
     }
-    // dr (.) feat and dr, three bf16 terms, transposed
-#pragma unroll
-    for (int i = 0; i < kMaxFeat; i++) {
-      const float x = i < (int)P.F ? dr * f[i] : (i == (int)P.F ? dr : 0.f);
+    // dr (.) feat and dr (column L * C), three bf16 terms, transposed
+    auto put_bp = [&](int i, float x) {
       uint16_t t[3];
       split3_bf16(x, t[0], t[1], t[2]);
       const uint32_t o = (i / 8) * kPadGroup + (i % 8) * 16 + col_off;
 #pragma unroll
       for (int k = 0; k < 3; k++) *reinterpret_cast<uint16_t*>(smem + SL.bp + k * kBpBytes + o) = t[k];
+    };
+#pragma unroll
+    for (int i = 0; i < FP; i++) {
+      if (i < (int)P.F) put_bp(i, dr * f[i]);
     }
+    put_bp((int)P.F, dr);
     fence_proxy_async();
     tc_fence_before_sync();
     __syncthreads();
@@ -615,6 +642,8 @@ __global__ void __launch_bounds__(kTile, 3) density_bwd_kernel(NetLaunch P) {
       mma_commit(&M->bar);
     }
     any = true;
+    // the next tile's inputs, fetched while the tensor cores work and the scatter runs
+    load_bwd_in<FP>(P, (tile + gridDim.x) * kTile + tid, in);
     if (!wait_mma(P, M, phase)) {
       timed_out = true;
       break;
