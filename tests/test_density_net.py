@@ -116,3 +116,48 @@ def test_level_mean_sq_oracle_is_the_scatter_reduce_fallback():
     assert bool((ours[:, 1:] == 0).all())
     all_ch = odn.level_mean_sq(emb, net.encoder.offsets, all_channels=True)
     assert float((all_ch[:, 0] - ours[:, 0]).abs().max()) == 0.0 and bool((all_ch[:, 1] > 0).all())
+
+
+def _net(**kw):
+    from neural3dstrokes_b200 import _lib
+    n = _lib.DensityNet()
+    fake = 0x10000  # never dereferenced: every case below fails its host checks first
+    n.table = n.offsets = n.w1 = n.b1 = n.w2 = n.b2 = fake
+    n.n_levels, n.level_dim = 8, 1
+    n.log2_per_level_scale, n.base_resolution = 1.0, 16
+    n.grid_bound = 1.0
+    n.warp_scale = 1.0
+    for k, v in kw.items():
+        setattr(n, k, v)
+    return n
+
+
+@pytest.mark.parametrize("kw,code", [(dict(level_dim=8), 2), (dict(n_levels=16), 2), (dict(level_dim=4, n_levels=4), 2),
+                                     (dict(n_levels=0), 2), (dict(warp=7), 1), (dict(grid_bound=0.0), 1),
+                                     (dict(base_resolution=0), 1), (dict(table=None), 1)])
+def test_density_net_host_checks(kw, code):
+    """Descriptors outside the supported network fail with N3DS_ERR_UNSUPPORTED (2) or
+    N3DS_ERR_INVALID (1) and a message, before anything reaches the device."""
+    import ctypes
+    from neural3dstrokes_b200 import _lib
+    lib = _lib.load()
+    rc = lib.n3ds_density_net_forward(ctypes.byref(_net(**kw)), ctypes.c_void_p(0x10000), 10,
+                                      ctypes.c_void_p(0x10000), None, None, None)
+    assert rc == code and lib.n3ds_last_error().decode()
+
+
+def test_density_net_host_checks_of_buffers():
+    import ctypes
+    from neural3dstrokes_b200 import _lib
+    lib = _lib.load()
+    p = ctypes.c_void_p(0x10000)
+    net = ctypes.byref(_net())
+    assert lib.n3ds_density_net_forward(net, p, -1, p, None, None, None) == 1         # negative count
+    assert lib.n3ds_density_net_forward(net, None, 10, p, None, None, None) == 1      # no coordinates
+    assert lib.n3ds_density_net_forward(net, p, 10, p, ctypes.c_void_p(0x10004), None, None) == 1  # record misaligned
+    assert lib.n3ds_density_net_backward(net, p, None, p, 10, p, p, p, p, p, None) == 1  # no record
+    assert lib.n3ds_density_net_backward(net, p, p, p, 10, None, p, p, p, p, None) == 1  # no table gradient
+    assert lib.n3ds_density_net_forward(net, p, 0, p, None, None, None) == 0          # nothing to do
+    assert lib.n3ds_grid_level_mean_sq(p, p, 8, 8, 0, p, None) == 2                   # level_dim 8
+    assert lib.n3ds_grid_level_mean_sq(p, p, 8, 1, 0, None, None) == 1                # no output
+    assert lib.n3ds_density_net_feature_stride(6, 1) == 8 and lib.n3ds_density_net_feature_stride(5, 2) == 12
