@@ -979,6 +979,72 @@ def run_prop(args, world, rank, local):
             "gpu_launches": 11 * args.steps, "gpu_launches_per_step": 11}), flush=True)
 
 
+def _ref_softmax_density_weighted(alphas, colors, density_params):
+    """compose_strokes(..., 'softmax_density_weighted') as the reference writes it in
+    torch (source/strokelib/strokes.py:408-415): the comparison leg of the ops workload."""
+    inv_temp = 1.0 / 0.05
+    adw = alphas * torch.broadcast_to(density_params, alphas.shape)
+    sm = torch.softmax(adw * inv_temp, dim=-1)
+    density = torch.einsum('...s,...s->...', sm, adw)
+    color = torch.einsum('...s,...sc->...c', sm, colors)
+    return density, color
+
+
+def _ref_image_texture(image, texcoords, colors, alphas, tint_ratio=1.0):
+    """ImageTexture.forward as the reference writes it (source/textures.py: grid_sample
+    with align_corners=True of the [1, C, H, W] image, tint by the colour)."""
+    import torch.nn.functional as F
+    pre = colors.shape[:-1]
+    uvs = texcoords.reshape(1, 1, -1, 2) * 2 - 1
+    tint = F.grid_sample(image, uvs, align_corners=True)[0, :, 0, :].permute(1, 0)
+    c = colors.reshape(-1, 3) * tint_ratio + (1.0 - tint_ratio)
+    return (c * tint).reshape(*pre, 3), alphas
+
+
+def _ref_resample(sdist, weights, num_samples, dilation, padding, domain=(0.0, 1.0)):
+    """One proposal level of the reference's sampling loop as torch ops
+    (source/models.py:160-185 with source/utils/stepfun.py: max_dilate_weights
+    renormalised, the end posts dropped, logits log(w + padding), sample_intervals with
+    single jitter and the mask-based sorted_interp)."""
+    eps = torch.finfo(torch.float32).eps
+
+    def sorted_interp(x, xp, fp):
+        mask = x[..., None, :] >= xp[..., :, None]
+
+        def find_interval(v):
+            v0 = torch.max(torch.where(mask, v[..., None], v[..., :1, None]), -2).values
+            v1 = torch.min(torch.where(~mask, v[..., None], v[..., -1:, None]), -2).values
+            return v0, v1
+        fp0, fp1 = find_interval(fp)
+        xp0, xp1 = find_interval(xp)
+        off = torch.clip(torch.nan_to_num((x - xp0) / (xp1 - xp0), 0), 0, 1)
+        return fp0 + off * (fp1 - fp0)
+
+    t, w = sdist, weights
+    p = w / (t[..., 1:] - t[..., :-1]).clamp_min(eps)
+    t0, t1 = t[..., :-1] - dilation, t[..., 1:] + dilation
+    td = torch.clip(torch.sort(torch.cat([t, t0, t1], dim=-1), dim=-1).values, *domain)
+    pd = torch.max(torch.where((t0[..., None, :] <= td[..., None]) & (t1[..., None, :] > td[..., None]),
+                               p[..., None, :], torch.zeros_like(p[..., None, :])), dim=-1).values[..., :-1]
+    wd = pd * (td[..., 1:] - td[..., :-1])
+    wd = wd / torch.sum(wd, dim=-1, keepdim=True).clamp_min(eps)
+    t, w = td[..., 1:-1], wd[..., 1:-1]
+    logits = torch.where(t[..., 1:] > t[..., :-1], torch.log(w + padding), -torch.inf)
+    u_max = eps + (1 - eps) / num_samples
+    max_jitter = (1 - u_max) / (num_samples - 1) - eps
+    u = torch.linspace(0, 1 - u_max, num_samples, device=t.device) + \
+        torch.rand(t.shape[:-1] + (1,), device=t.device) * max_jitter
+    wsm = torch.softmax(logits, dim=-1)
+    cw = torch.cumsum(wsm[..., :-1], dim=-1).clamp_max(1)
+    shape = cw.shape[:-1] + (1,)
+    cw = torch.cat([torch.zeros(shape, device=t.device), cw, torch.ones(shape, device=t.device)], dim=-1)
+    centers = sorted_interp(u, cw, t)
+    mid = (centers[..., 1:] + centers[..., :-1]) / 2
+    first = (2 * centers[..., :1] - mid[..., :1]).clamp_min(domain[0])
+    last = (2 * centers[..., -1:] - mid[..., -1:]).clamp_max(domain[1])
+    return torch.cat([first, mid, last], dim=-1)
+
+
 def run_ops(args, rank, local):
     """Each operator at a stated size, events around ``args.steps`` calls after
     ``args.warmup``; one JSON line with per-op ms and algorithmic GB/s."""
@@ -1056,15 +1122,21 @@ def run_ops(args, rank, local):
     def softmax_fb():
         d_, c_ = strokes.compose_strokes(a_req, c, dp, "softmax_density_weighted")
         (d_.sum() + c_.sum()).backward()
-    timed("compose softmax_density_weighted fwd+bwd (65536 x 256)", softmax_fb, P * S * 32)
+
+    def softmax_ref():
+        d_, c_ = _ref_softmax_density_weighted(a_req, c, dp)
+        (d_.sum() + c_.sum()).backward()
+    timed("compose softmax_density_weighted fwd+bwd (65536 x 256)", softmax_fb, P * S * 32, softmax_ref)
     # colour field: SH3 on 128 spheres
     sph = scenes.make_strokes(["sphere"] * 128, g)
     sh = torch.randn(128, 27, generator=g).to(dev)
     a2, c2 = torch.empty(P, 128, device=dev), torch.empty(P, 128, 3, device=dev)
     vdn = torch.nn.functional.normalize(vd, dim=-1)
+    sph_ps = sph.shape_params[:, :4].contiguous().to(dev)
     timed("stroke_forward sphere + SH3 colour (65536 x 128)", lambda: strokelib.stroke_forward(
-        a2, c2, none, none, x, r, vdn, sph.shape_params[:, :4].contiguous().to(dev), sh, scenes.SDF_ID["sphere"], 3,
-        0.02, True, True), P * 128 * 16)
+        a2, c2, none, none, x, r, vdn, sph_ps, sh, scenes.SDF_ID["sphere"], 3, 0.02, True, True), P * 128 * 16,
+        R(lambda: ref.stroke_forward(a2, c2, none, none, x, r, vdn, sph_ps, sh, scenes.SDF_ID["sphere"], 3, 0.02,
+                                     True, True)))
     # texture on the cube pairs
     tex = textures.ImageTexture(torch.rand(256, 256, 3, generator=g) * 255, (256, 256)).to(dev)
     tc = torch.rand(P, S, 2, device=dev)
@@ -1073,13 +1145,19 @@ def run_ops(args, rank, local):
     def tex_fb():
         co, al = tex(tc, c_req, a)
         co.sum().backward()
-    timed("ImageTexture fwd+bwd (65536 x 256)", tex_fb, P * S * (40 + 20))
+    image = tex.image_texture if hasattr(tex, "image_texture") else None
+
+    def tex_ref():
+        co, al = _ref_image_texture(image, tc, c_req, a)
+        co.sum().backward()
+    timed("ImageTexture fwd+bwd (65536 x 256)", tex_fb, P * S * (40 + 20), tex_ref if image is not None else None)
     # proposal resampling: 65,536 rays, 64 bins -> 32 samples, dilation
     sd = torch.sort(torch.rand(65536, 65, device=dev), -1).values
     sd[:, 0], sd[:, -1] = 0, 1
     wts = torch.rand(65536, 64, device=dev)
     timed("resample_intervals (65536 rays, 64 -> 32, dilation)", lambda: stepfun.resample_intervals(
-        sd, wts, 32, rand=True, dilation=0.01, resample_padding=0.01), 65536 * (65 + 64 + 33) * 4)
+        sd, wts, 32, rand=True, dilation=0.01, resample_padding=0.01), 65536 * (65 + 64 + 33) * 4,
+        lambda: _ref_resample(sd, wts, 32, 0.01, 0.01))
     # stroke insertion: 2000 strokes, 30,000 error points
     ins = StrokeInserter("sphere", max_num_strokes=2000, init_num_strokes=10, device=dev)
     ec, _ = ins.sample_error_coords()
@@ -1101,8 +1179,9 @@ def run_ops(args, rank, local):
         ms = time_of(fn)
         item = {"op": name, "ms": round(ms, 4), "bytes": int(nbytes),
                 "gbs": round(nbytes / ms / 1e6, 1) if nbytes else None}
-        if ref_fn is not None:  # the reference's operator on the same tensors
+        if ref_fn is not None:  # the reference's operator (or torch formulation) on the same tensors
             item["reference_ms"] = round(time_of(ref_fn), 4)
+            item["speedup"] = round(item["reference_ms"] / ms, 1)
         res.append(item)
     torch.cuda.profiler.stop()
     if rank == 0:

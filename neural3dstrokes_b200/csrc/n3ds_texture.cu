@@ -132,6 +132,81 @@ __global__ void texture_bwd_kernel(float* grad_colors, float* grad_alphas, const
   }
 }
 
+// Packed texture, four pairs per thread: texcoords as two float4, colours and the
+// outputs as three float4 (12 floats = four RGB triples), alphas as one. For
+// 16-byte-aligned arrays; pairs past 4 * n4 go to the scalar kernels.
+__device__ __forceinline__ void tints4(const Tex& t, const float4& ta, const float4& tb, float (&tn)[12]) {
+  const float u[4] = {ta.x, ta.z, tb.x, tb.z}, v[4] = {ta.y, ta.w, tb.y, tb.w};
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    float tk[3];
+    tint_at<true>(t, u[k], v[k], tk);
+    tn[3 * k] = tk[0];
+    tn[3 * k + 1] = tk[1];
+    tn[3 * k + 2] = tk[2];
+  }
+}
+
+__device__ __forceinline__ float mean_tint(const Tex& t, const float (&tn)[12], int k) {
+  return t.C == 1 ? tn[3 * k] : (tn[3 * k] + tn[3 * k + 1] + tn[3 * k + 2]) / 3.f;
+}
+
+__global__ void texture_fwd_vec_kernel(float4* color_out, float4* alpha_out, const float4* texcoords,
+                                       const float4* colors, const float4* alphas, long long n4, Tex t,
+                                       float tint_ratio, int modulate) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n4; q += (long long)gridDim.x * blockDim.x) {
+    float tn[12];
+    tints4(t, texcoords[2 * q], texcoords[2 * q + 1], tn);
+    const float base = 1.f - tint_ratio;
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      const float4 c = colors[3 * q + j];
+      color_out[3 * q + j] = make_float4((c.x * tint_ratio + base) * tn[4 * j], (c.y * tint_ratio + base) * tn[4 * j + 1],
+                                         (c.z * tint_ratio + base) * tn[4 * j + 2],
+                                         (c.w * tint_ratio + base) * tn[4 * j + 3]);
+    }
+    if (alpha_out) {
+      float4 a = alphas[q];
+      if (modulate) {
+        a.x *= mean_tint(t, tn, 0);
+        a.y *= mean_tint(t, tn, 1);
+        a.z *= mean_tint(t, tn, 2);
+        a.w *= mean_tint(t, tn, 3);
+      }
+      alpha_out[q] = a;
+    }
+  }
+}
+
+__global__ void texture_bwd_vec_kernel(float4* grad_colors, float4* grad_alphas, const float4* g_color,
+                                       const float4* g_alpha, const float4* texcoords, long long n4, Tex t,
+                                       float tint_ratio, int modulate) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n4; q += (long long)gridDim.x * blockDim.x) {
+    float tn[12];
+    tints4(t, texcoords[2 * q], texcoords[2 * q + 1], tn);
+    if (grad_colors) {
+#pragma unroll
+      for (int j = 0; j < 3; j++) {
+        const float4 g = g_color ? g_color[3 * q + j] : make_float4(0.f, 0.f, 0.f, 0.f);
+        grad_colors[3 * q + j] = make_float4(g.x * tn[4 * j] * tint_ratio, g.y * tn[4 * j + 1] * tint_ratio,
+                                             g.z * tn[4 * j + 2] * tint_ratio, g.w * tn[4 * j + 3] * tint_ratio);
+      }
+    }
+    if (grad_alphas) {
+      float4 g = g_alpha ? g_alpha[q] : make_float4(0.f, 0.f, 0.f, 0.f);
+      if (modulate) {
+        g.x *= mean_tint(t, tn, 0);
+        g.y *= mean_tint(t, tn, 1);
+        g.z *= mean_tint(t, tn, 2);
+        g.w *= mean_tint(t, tn, 3);
+      }
+      grad_alphas[q] = g;
+    }
+  }
+}
+
+bool al16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
 // [C, H, W] -> [H, W] float4 texels (r, g, b, 0), grayscale replicated.
 __global__ void texture_pack_kernel(float4* packed, const float* image, int C, int H, int W) {
   const long long hw = (long long)H * W;
@@ -217,8 +292,21 @@ extern "C" int n3ds_texture_forward_packed(float* color_out, float* alpha_out, c
     return n3ds::report_error(N3DS_ERR_INVALID, "texture: packed must be 16-byte aligned");
   if (n == 0) return N3DS_OK;
   Tex t{packed, channels, height, width};
-  texture_fwd_kernel<true><<<grid_for(n), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
-      color_out, alpha_out, texcoords, colors, alphas, n, t, tint_ratio, modulate_alpha != 0);
+  const cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  long long done = 0;
+  if (al16(color_out) && al16(texcoords) && al16(colors) && (!alpha_out || (al16(alpha_out) && al16(alphas)))) {
+    const long long n4 = n / 4;
+    if (n4 > 0)
+      texture_fwd_vec_kernel<<<grid_for(n4), 256, 0, st>>>(
+          reinterpret_cast<float4*>(color_out), reinterpret_cast<float4*>(alpha_out),
+          reinterpret_cast<const float4*>(texcoords), reinterpret_cast<const float4*>(colors),
+          reinterpret_cast<const float4*>(alphas), n4, t, tint_ratio, modulate_alpha != 0);
+    done = 4 * n4;
+  }
+  if (done < n)
+    texture_fwd_kernel<true><<<grid_for(n - done), 256, 0, st>>>(
+        color_out + 3 * done, alpha_out ? alpha_out + done : nullptr, texcoords + 2 * done, colors + 3 * done,
+        alphas ? alphas + done : nullptr, n - done, t, tint_ratio, modulate_alpha != 0);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return n3ds::report_error(N3DS_ERR_CUDA, std::string("texture forward: ") + cudaGetErrorString(e));
   return N3DS_OK;
@@ -234,8 +322,23 @@ extern "C" int n3ds_texture_backward_packed(float* grad_colors, float* grad_alph
     return n3ds::report_error(N3DS_ERR_INVALID, "texture: packed must be 16-byte aligned");
   if (n == 0 || (!grad_colors && !grad_alphas)) return N3DS_OK;
   Tex t{packed, channels, height, width};
-  texture_bwd_kernel<true><<<grid_for(n), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
-      grad_colors, grad_alphas, grad_color_out, grad_alpha_out, texcoords, n, t, tint_ratio, modulate_alpha != 0);
+  const cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  long long done = 0;
+  if (al16(texcoords) && (!grad_colors || al16(grad_colors)) && (!grad_color_out || al16(grad_color_out)) &&
+      (!grad_alphas || al16(grad_alphas)) && (!grad_alpha_out || al16(grad_alpha_out))) {
+    const long long n4 = n / 4;
+    if (n4 > 0)
+      texture_bwd_vec_kernel<<<grid_for(n4), 256, 0, st>>>(
+          reinterpret_cast<float4*>(grad_colors), reinterpret_cast<float4*>(grad_alphas),
+          reinterpret_cast<const float4*>(grad_color_out), reinterpret_cast<const float4*>(grad_alpha_out),
+          reinterpret_cast<const float4*>(texcoords), n4, t, tint_ratio, modulate_alpha != 0);
+    done = 4 * n4;
+  }
+  if (done < n)
+    texture_bwd_kernel<true><<<grid_for(n - done), 256, 0, st>>>(
+        grad_colors ? grad_colors + 3 * done : nullptr, grad_alphas ? grad_alphas + done : nullptr,
+        grad_color_out ? grad_color_out + 3 * done : nullptr, grad_alpha_out ? grad_alpha_out + done : nullptr,
+        texcoords + 2 * done, n - done, t, tint_ratio, modulate_alpha != 0);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return n3ds::report_error(N3DS_ERR_CUDA, std::string("texture backward: ") + cudaGetErrorString(e));
   return N3DS_OK;

@@ -34,6 +34,9 @@ def _load_image(src) -> torch.Tensor:
 
 
 class _TextureFn(torch.autograd.Function):
+    """Tinted colours (and, with modulate_alpha, modulated alphas; else no alpha
+    output: the caller passes its alphas through, as the reference does)."""
+
     @staticmethod
     def forward(ctx, texcoords, colors, alphas, image, tint_ratio, modulate_alpha):
         n = colors.numel() // 3
@@ -43,7 +46,7 @@ class _TextureFn(torch.autograd.Function):
         img = image.contiguous().float()
         C, H, W = img.shape
         col_out = torch.empty_like(col)
-        al_out = torch.empty_like(al)
+        al_out = torch.empty_like(al) if modulate_alpha else None
         # texels interleaved as float4 (r, g, b, 0): one load per bilinear corner
         packed = torch.empty(H, W, 4, device=col.device)
         lib = _lib.load()
@@ -55,11 +58,13 @@ class _TextureFn(torch.autograd.Function):
                                                        float(tint_ratio), int(bool(modulate_alpha)), st))
         ctx.save_for_backward(tc, packed)
         ctx.meta = (float(tint_ratio), bool(modulate_alpha), colors.shape, alphas.shape, C)
+        if not modulate_alpha:
+            return col_out.reshape(colors.shape)
         return col_out.reshape(colors.shape), al_out.reshape(alphas.shape)
 
     @staticmethod
     @once_differentiable
-    def backward(ctx, g_col, g_al):
+    def backward(ctx, g_col, g_al=None):
         tc, packed = ctx.saved_tensors
         tint_ratio, modulate, cshape, ashape, C = ctx.meta
         n = tc.shape[0]
@@ -67,7 +72,7 @@ class _TextureFn(torch.autograd.Function):
         gc = None if g_col is None else g_col.contiguous().float().reshape(n, 3)
         ga = None if g_al is None else g_al.contiguous().float().reshape(n)
         gcol = torch.empty(n, 3, device=tc.device) if ctx.needs_input_grad[1] else None
-        gal = torch.empty(n, device=tc.device) if ctx.needs_input_grad[2] else None
+        gal = torch.empty(n, device=tc.device) if (modulate and ctx.needs_input_grad[2]) else None
         lib = _lib.load()
         with torch.cuda.device(tc.device):
             _lib.check(lib.n3ds_texture_backward_packed(_lib.ptr(gcol), _lib.ptr(gal), _lib.ptr(gc), _lib.ptr(ga),
@@ -108,8 +113,9 @@ class ImageTexture(StrokeTexture):
         if not colors.is_cuda:
             raise RuntimeError("ImageTexture runs on CUDA tensors")
         image = self.image_texture[0].to(colors.device)
-        return _TextureFn.apply(texcoords.detach(), colors, alphas, image, float(self.tint_ratio),
-                                bool(self.modulate_alpha))
+        if not self.modulate_alpha:  # alphas pass through unchanged (the same tensor, as in the reference)
+            return _TextureFn.apply(texcoords.detach(), colors, alphas, image, float(self.tint_ratio), False), alphas
+        return _TextureFn.apply(texcoords.detach(), colors, alphas, image, float(self.tint_ratio), True)
 
 
 def get_stroke_texture(stroke_texture: str = "none", texture_image_path: Optional[str] = None,

@@ -109,3 +109,31 @@ def test_packed_texture_equals_planar(cuda, C, modulate):
     torch.cuda.synchronize(cuda)
     for a, b in zip(*outs):
         assert rel(a, b) < 1e-6
+
+
+@pytest.mark.parametrize("P,offset", [(301, 0), (300, 1)])
+@pytest.mark.parametrize("modulate", [False, True])
+def test_texture_tail_and_unaligned_arrays(cuda, P, offset, modulate):
+    """The kernels take four pairs per thread on 16-byte-aligned arrays and the rest
+    one by one: a pair count that is not a multiple of four and colours one float into
+    a buffer (the whole call on the scalar path) give the oracle's values too."""
+    tc, col, al, img = make(3, P=P, seed=3)
+    tex = textures.ImageTexture(img[0].permute(1, 2, 0).numpy(), img.shape[2:], tint_ratio=0.7,
+                                modulate_alpha=modulate)
+    buf = torch.empty(col.numel() + offset, device=cuda)
+    buf[offset:] = col.reshape(-1).to(cuda)
+    colc = buf[offset:].view(col.shape).detach().requires_grad_(True)
+    alc = al.to(cuda).requires_grad_(True)
+    out_c, out_a = tex(tc.to(cuda), colc, alc)
+    if not modulate:
+        assert out_a is alc  # the reference returns its alphas unchanged
+    g = torch.Generator().manual_seed(6)
+    gc = torch.randn(out_c.shape, generator=g)
+    (out_c * gc.to(cuda)).sum().backward()
+    img64 = tex.image_texture[0].double()
+    col64 = col.double().requires_grad_(True)
+    ref_c, ref_a = orr.image_texture(tc.double().reshape(-1, 2), col64.reshape(-1, 3), al.double().reshape(-1), img64,
+                                     0.7, modulate)
+    (ref_c * gc.double().reshape(-1, 3)).sum().backward()
+    assert rel(out_c.reshape(-1, 3), ref_c) < 1e-5 and rel(out_a.reshape(-1), ref_a) < 1e-5
+    assert rel(colc.grad, col64.grad) < 1e-5
