@@ -49,3 +49,24 @@ def test_single_rank_is_local_time():
     import bench
     v, s = bench.replica_throughput(0.5, 100, 1, torch.device("cpu"))
     assert s == 0.5 and v == 200
+
+
+def test_reference_arm_under_torchrun_two_ranks():
+    """bench.py --impl reference launched as the multi-GPU runs launch it (torchrun,
+    world size 2, here over gloo): rank 0 alone times the reference's CPU path and
+    prints one JSON line; rank 1 exits 0 without work."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    out = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+                          "--master-addr", "127.0.0.1", "--master-port", str(_free_port()), "bench.py",
+                          "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0", "--config", "0"],
+                         cwd=root, env=env, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [json.loads(l) for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    line = lines[0]
+    assert line["impl"] == "reference" and line["value"] > 0 and line["n_gpus"] == 2
+    assert line["cpu_baseline"]["kind"] == "port" and line["e2e"]["h2d_bytes_per_step"] == 0
