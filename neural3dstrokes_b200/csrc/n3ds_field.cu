@@ -322,11 +322,14 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_con
             kill[lane] = 0u;
             __syncwarp();
           }
-          // 3: evaluate the survivors block by block in compositing order
-          for (int k = 0; k < nblk; k++) {
+          // 3: evaluate the survivors block by block in compositing order, visiting only
+          // the blocks with survivors (lane k's word is block k's, lanes >= nblk hold 0)
+          unsigned todo = __ballot_sync(0xffffffffu, my_mask != 0u);
+          while (todo) {
+            const int k = __ffs(todo) - 1;
+            todo &= todo - 1u;
             const int hi = sc.chunk_n - 1 - 32 * k;
             unsigned mask = __shfl_sync(0xffffffffu, my_mask, k);
-            const bool any = mask != 0;
             unsigned kept = 0;  // this lane's strokes of the block whose adjoint the backward needs
             while (mask) {
               const int b = __ffs(mask) - 1;
@@ -344,7 +347,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_con
               cb += col.z * w;
             }
             // the words start at zero (cleared before the launch): store the non-empty ones
-            if (RECORD && any) {
+            if (RECORD) {
               kept = __reduce_or_sync(0xffffffffu, c.active ? kept : 0u);
               if (lane == 0 && kept) bm[(sc.n_strokes - 1 - (sc.chunk_lo + hi)) >> 5] = kept;
             }
@@ -509,16 +512,26 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
           const unsigned* bm =
               masks ? masks + sc.mask_begin + (long long)(ray_local * L.segs_per_ray + g) * sc.mask_words : nullptr;
           const unsigned nact = __popc(__ballot_sync(0xffffffffu, c.active));
-          unsigned held = 0;  // mask words (w & ~31) + lane of the current group of 32
-          for (int hi = sc.chunk_n - 1; hi >= 0; hi -= 32) {
+          // The chunk's blocks (at most 32: stages hold at most 1024 strokes, in multiples
+          // of 32) are mask words w0 .. w0 + nblk - 1 of the segment; lane k holds block
+          // k's word, and only the blocks with a kept stroke are visited. Without masks
+          // every block is visited and culled.
+          const int nblk = (sc.chunk_n + 31) >> 5;
+          unsigned held = 0u, todo;
+          if (bm) {
+            const int w0 = (sc.n_strokes - sc.chunk_lo - sc.chunk_n) >> 5;
+            held = lane < nblk ? bm[w0 + lane] : 0u;
+            todo = __ballot_sync(0xffffffffu, held != 0u);
+          } else {
+            todo = nblk >= 32 ? 0xffffffffu : (1u << nblk) - 1u;
+          }
+          while (todo) {
+            const int k = __ffs(todo) - 1;
+            todo &= todo - 1u;
+            const int hi = sc.chunk_n - 1 - 32 * k;
             unsigned mask;
             if (bm) {
-              const int w = (sc.n_strokes - 1 - (sc.chunk_lo + hi)) >> 5;
-              if (hi == sc.chunk_n - 1 || (w & 31) == 0) {
-                const int wl = (w & ~31) + lane;
-                held = wl < sc.mask_words ? bm[wl] : 0u;
-              }
-              mask = __shfl_sync(0xffffffffu, held, w & 31);
+              mask = __shfl_sync(0xffffffffu, held, k);
               if (hi < 31) mask &= (2u << hi) - 1u;  // only strokes hi .. 0 exist in the last block
             } else {
               unsigned unused;
