@@ -114,8 +114,6 @@ __device__ __forceinline__ bool polytope_reachable(const float* rec, const SegCt
   return !out && lo <= hi + 1e-6f;
 }
 
-// Sphere test of one 32-stroke block; *poly gets the survivors flagged for the
-// polytope test (the forward batches those tests, see seg_fwd_kernel).
 // Ellipsoid reach test (flagged per-axis-scaled spheres): the chord, in the stroke's
 // local frame, must pass within 1 + R_PLANE r_max of the origin; the samples' distance
 // rho to the chord grows by at most 1 / s_min in that frame.
@@ -202,19 +200,30 @@ __device__ __forceinline__ bool curve_reachable(const float* rec, const SegCtx& 
   return false;
 }
 
-__device__ __forceinline__ unsigned cull_block_sphere(const Stage& S, const SegCtx& c, int hi, int lane,
-                                                      unsigned* poly) {
+// Sphere test of one 32-stroke block (lane j: stroke hi - j) against the segment's
+// capsule; the ballot of the survivors. The survivors flagged for an exact reach test
+// are these and the block's flag word (flagged_words); the forward batches those tests.
+__device__ __forceinline__ unsigned cull_block_sphere(const Stage& S, const SegCtx& c, int hi, int lane) {
   const int sl = hi - lane;
-  bool cand = false, flagged = false;
+  bool cand = false;
   if (sl >= 0) {
     float4 ca = S.cull_a[sl];
     float d = seg_dist(v3(ca.x, ca.y, ca.z), c.A, c.AB, c.invL2);
-    const float cb = S.cull_b[sl];
-    cand = !(d - c.rho > ca.w + fabsf(cb) * c.rmax);
-    flagged = cand && __float_as_int(cb) < 0;
+    cand = !(d - c.rho > ca.w + fabsf(S.cull_b[sl]) * c.rmax);
   }
-  *poly = __ballot_sync(0xffffffffu, flagged);
   return __ballot_sync(0xffffffffu, cand);
+}
+
+// The strokes of the staged chunk flagged for an exact reach test (the margin's sign
+// bit, set by the prep kernel), one word per 32-stroke block: lane k returns block k's.
+__device__ __forceinline__ unsigned flagged_words(const Stage& S, int chunk_n, int lane) {
+  unsigned mine = 0u;
+  for (int k = 0; 32 * k < chunk_n; k++) {
+    const int sl = chunk_n - 1 - 32 * k - lane;
+    const unsigned f = __ballot_sync(0xffffffffu, sl >= 0 && __float_as_int(S.cull_b[sl]) < 0);
+    if (lane == k) mine = f;
+  }
+  return mine;
 }
 
 // ================================================================== forward
@@ -246,6 +255,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_con
       return;
     }
     const SceneDesc& sc = L.sc[sci];
+    const unsigned my_flag = flagged_words(S, sc.chunk_n, lane);
     int* counter = L.tile_counter + sci;
     int item = 0;
     if (lane == 0) item = atomicAdd(counter, L.rays_per_item);
@@ -269,15 +279,12 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_fwd_kernel(const __grid_con
           // Culling in three steps. 1: the sphere test of every block of the chunk (at most
           // 32 blocks); lane k keeps block k's survivors and its polytope-flagged subset.
           const int nblk = (sc.chunk_n + 31) >> 5;
-          unsigned my_mask = 0u, my_poly = 0u;
+          unsigned my_mask = 0u;
           for (int k = 0; k < nblk; k++) {
-            unsigned pm;
-            const unsigned m = cull_block_sphere(S, c, sc.chunk_n - 1 - 32 * k, lane, &pm);
-            if (lane == k) {
-              my_mask = m;
-              my_poly = pm;
-            }
+            const unsigned m = cull_block_sphere(S, c, sc.chunk_n - 1 - 32 * k, lane);
+            if (lane == k) my_mask = m;
           }
+          const unsigned my_poly = my_mask & my_flag;
           // 2: the flagged candidates of all blocks, 32 per pass, one per lane: the owner
           // block is the last with prefix count <= the candidate's index (5-step binary
           // search over the lanes), the stroke its n-th flagged bit; rejections are
@@ -534,8 +541,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
               mask = __shfl_sync(0xffffffffu, held, k);
               if (hi < 31) mask &= (2u << hi) - 1u;  // only strokes hi .. 0 exist in the last block
             } else {
-              unsigned unused;
-              mask = cull_block_sphere(S, c, hi, lane, &unused);  // conservative: no polytope test here
+              mask = cull_block_sphere(S, c, hi, lane);  // conservative: no exact reach tests here
             }
             while (mask) {
               const int b = __ffs(mask) - 1;

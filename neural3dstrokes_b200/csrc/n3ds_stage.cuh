@@ -57,7 +57,9 @@ __device__ __forceinline__ void fence_proxy_async() {
 
 __device__ __forceinline__ float seg_dist(V3 c, V3 A, V3 AB, float invL2) {
   V3 w = c - A;
-  float tt = clampf(dot(w, AB) * invL2, 0.f, 1.f);
+  // clamp to the chord [0, 1] as the multiply's saturation (a NaN product comes from
+  // non-finite coordinates, whose distance is not finite with either clamp)
+  float tt = __saturatef(dot(w, AB) * invL2);
   V3 d = w - AB * tt;
   return sqrtf(dot(d, d));
 }
