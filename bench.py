@@ -1285,7 +1285,8 @@ def main():
     if args.schedule == "auto" and not args.no_tune:
         from neural3dstrokes_b200 import autotune
         tuned = autotune.tune(field, reps=2, use_cache=False)
-        tune_table = [[f"{o.schedule} w{o.warps}/{o.warps_bwd} c{o.chunk_fwd}/{o.chunk_bwd}", round(ms, 3)]
+        tune_table = [[f"{o.schedule} w{o.warps}/{o.warps_bwd} c{o.chunk_fwd}/{o.chunk_bwd}"
+                       + (f" rays/claim {o.rays_per_item}" if o.rays_per_item > 1 else ""), round(ms, 3)]
                       for ms, o in autotune.last_results]
     segments = field.options.schedule != "runs"
 
@@ -1423,6 +1424,7 @@ def main():
                        "launch": {"schedule": "segments" if segments else "runs", "warps": field.options.warps,
                                   "warps_bwd": field.options.warps_bwd, "chunk_fwd": field.options.chunk_fwd,
                                   "chunk_bwd": field.options.chunk_bwd,
+                                  "rays_per_claim": max(1, field.options.rays_per_item),
                                   "picked_by": "autotuner" if tuned is not None else "flags",
                                   "tried_ms": tune_table}},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "accuracy": accuracy,
