@@ -449,8 +449,10 @@ __device__ __forceinline__ void compose_skip(const float* rec, float a, CompAdj&
 }
 
 // GX: the sample-position gradient is wanted (L.grad_x non-null); without it the
-// kernel carries no position gradient at all.
-template <int WARPS, bool GX>
+// kernel carries no position gradient at all. COMPAT: L.compat as a constant (the
+// reference's gradient formulas, 1, or the exact adjoint, 0), so that the adjoint's
+// formula choices are made at compile time.
+template <int WARPS, bool GX, int COMPAT>
 __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_constant__ SegLaunch L) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t bar;
@@ -465,7 +467,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
   for (int i = threadIdx.x; i < L.chunk_cap * GRAD_SLOTS; i += nthr) S.gacc[i] = 0.f;
   __syncthreads();
   uint32_t phase = 0;
-  const int compat = L.compat;
+  constexpr int compat = COMPAT;
   const unsigned* masks = (L.block_masks && *L.mask_tag == __float_as_int(L.skip_alpha)) ? L.block_masks : nullptr;
   unsigned long long bcount = 0;  // lane 0: evaluated (sample, stroke) pairs
 
@@ -1252,7 +1254,8 @@ static cudaError_t launch_fwd_w(const SegLaunch& L, int grid, size_t smem, cudaS
 }
 template <int W>
 static cudaError_t launch_bwd_w(const SegLaunch& L, int grid, size_t smem, cudaStream_t st) {
-  auto* k = L.grad_x ? seg_bwd_kernel<W, true> : seg_bwd_kernel<W, false>;
+  auto* k = L.compat ? (L.grad_x ? seg_bwd_kernel<W, true, 1> : seg_bwd_kernel<W, false, 1>)
+                     : (L.grad_x ? seg_bwd_kernel<W, true, 0> : seg_bwd_kernel<W, false, 0>);
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   k<<<grid, W * 32, smem, st>>>(L);
