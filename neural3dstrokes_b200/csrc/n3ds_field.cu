@@ -52,6 +52,21 @@ struct SegCtx {
   float invL2, rho, rmax;
 };
 
+// Culling geometry of a segment whose lanes 0 .. cnt - 1 hold its samples: the chord
+// A..B, the samples' spread rho about it and the largest sample radius.
+__device__ __forceinline__ void seg_geometry(SegCtx& c, int cnt) {
+  c.A = shfl3(c.x, 0);
+  V3 B = shfl3(c.x, cnt - 1);
+  c.AB = B - c.A;
+  float l2 = dot(c.AB, c.AB);
+  c.invL2 = l2 > 0.f ? 1.f / l2 : 0.f;
+  c.rho = warp_max(c.active ? seg_dist(c.x, c.A, c.AB, c.invL2) : 0.f);
+  c.rmax = warp_max(c.active ? fabsf(c.r) : 0.f);
+}
+
+// GEOM: with the culling geometry (a backward that reads the forward's block masks
+// needs none).
+template <bool GEOM = true>
 __device__ __forceinline__ SegCtx seg_setup(const SegLaunch& L, const SceneDesc& sc, int seg, int lane) {
   SegCtx c;
   const int spr = L.segs_per_ray;
@@ -64,13 +79,7 @@ __device__ __forceinline__ SegCtx seg_setup(const SegLaunch& L, const SceneDesc&
   c.si = ray * L.n_samples + i0 + (c.active ? lane : 0);
   load_sample(L, ray, i0 + (c.active ? lane : 0), c.si, c.x, c.r);
   c.rinv = 1.f / c.r;
-  c.A = shfl3(c.x, 0);
-  V3 B = shfl3(c.x, cnt - 1);
-  c.AB = B - c.A;
-  float l2 = dot(c.AB, c.AB);
-  c.invL2 = l2 > 0.f ? 1.f / l2 : 0.f;
-  c.rho = warp_max(c.active ? seg_dist(c.x, c.A, c.AB, c.invL2) : 0.f);
-  c.rmax = warp_max(c.active ? fabsf(c.r) : 0.f);
+  if (GEOM) seg_geometry(c, cnt);
   return c;
 }
 
@@ -451,8 +460,11 @@ __device__ __forceinline__ void compose_skip(const float* rec, float a, CompAdj&
 // GX: the sample-position gradient is wanted (L.grad_x non-null); without it the
 // kernel carries no position gradient at all. COMPAT: L.compat as a constant (the
 // reference's gradient formulas, 1, or the exact adjoint, 0), so that the adjoint's
-// formula choices are made at compile time.
-template <int WARPS, bool GX, int COMPAT>
+// formula choices are made at compile time. MASKS: the forward recorded stroke-block
+// masks (L.block_masks non-null); the kernel then carries no culling code. If the
+// masks were recorded at another threshold (their tag), it visits every block: the
+// per-candidate test of the skip threshold makes the decisions culling would make.
+template <int WARPS, bool GX, int COMPAT, bool MASKS>
 __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_constant__ SegLaunch L) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t bar;
@@ -468,7 +480,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
   __syncthreads();
   uint32_t phase = 0;
   constexpr int compat = COMPAT;
-  const unsigned* masks = (L.block_masks && *L.mask_tag == __float_as_int(L.skip_alpha)) ? L.block_masks : nullptr;
+  const bool tag_ok = MASKS && *L.mask_tag == __float_as_int(L.skip_alpha);
+  constexpr bool kGeom = !MASKS;  // the culling geometry only where the kernel culls
   unsigned long long bcount = 0;  // lane 0: evaluated (sample, stroke) pairs
 
   auto flush = [&](int sci) {
@@ -498,7 +511,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
       const int item_end = min(item + L.rays_per_item, sc.n_rays);
       for (int ray_local = item; ray_local < item_end; ray_local++) {
         for (int g = 0; g < L.segs_per_ray; g++) {
-          SegCtx c = seg_setup(L, sc, ray_local * L.segs_per_ray + g, lane);
+          SegCtx c = seg_setup<kGeom>(L, sc, ray_local * L.segs_per_ray + g, lane);
           CompAdj s;
           {
             const float* st = L.state + 5 * c.si;
@@ -518,8 +531,6 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
             s.T = b[0]; s.Ps = b[1]; s.Pr = b[2]; s.Pg = b[3]; s.Pb = b[4];
             gx = GX ? v3(b[5], b[6], b[7]) : v3(0.f, 0.f, 0.f);
           }
-          const unsigned* bm =
-              masks ? masks + sc.mask_begin + (long long)(ray_local * L.segs_per_ray + g) * sc.mask_words : nullptr;
           const unsigned nact = __popc(__ballot_sync(0xffffffffu, c.active));
           // The chunk's blocks (at most 32: stages hold at most 1024 strokes, in multiples
           // of 32) are mask words w0 .. w0 + nblk - 1 of the segment; lane k holds block
@@ -527,9 +538,15 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
           // every block is visited and culled.
           const int nblk = (sc.chunk_n + 31) >> 5;
           unsigned held = 0u, todo;
-          if (bm) {
-            const int w0 = (sc.n_strokes - sc.chunk_lo - sc.chunk_n) >> 5;
-            held = lane < nblk ? bm[w0 + lane] : 0u;
+          if (MASKS) {
+            if (tag_ok) {
+              const unsigned* bm = L.block_masks + sc.mask_begin +
+                                   (long long)(ray_local * L.segs_per_ray + g) * sc.mask_words;
+              const int w0 = (sc.n_strokes - sc.chunk_lo - sc.chunk_n) >> 5;
+              held = lane < nblk ? bm[w0 + lane] : 0u;
+            } else {
+              held = lane < nblk ? 0xffffffffu : 0u;
+            }
             todo = __ballot_sync(0xffffffffu, held != 0u);
           } else {
             todo = nblk >= 32 ? 0xffffffffu : (1u << nblk) - 1u;
@@ -539,7 +556,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
             todo &= todo - 1u;
             const int hi = sc.chunk_n - 1 - 32 * k;
             unsigned mask;
-            if (bm) {
+            if (MASKS) {
               mask = __shfl_sync(0xffffffffu, held, k);
               if (hi < 31) mask &= (2u << hi) - 1u;  // only strokes hi .. 0 exist in the last block
             } else {
@@ -1254,8 +1271,11 @@ static cudaError_t launch_fwd_w(const SegLaunch& L, int grid, size_t smem, cudaS
 }
 template <int W>
 static cudaError_t launch_bwd_w(const SegLaunch& L, int grid, size_t smem, cudaStream_t st) {
-  auto* k = L.compat ? (L.grad_x ? seg_bwd_kernel<W, true, 1> : seg_bwd_kernel<W, false, 1>)
-                     : (L.grad_x ? seg_bwd_kernel<W, true, 0> : seg_bwd_kernel<W, false, 0>);
+  auto* k = L.block_masks
+                ? (L.compat ? (L.grad_x ? seg_bwd_kernel<W, true, 1, true> : seg_bwd_kernel<W, false, 1, true>)
+                            : (L.grad_x ? seg_bwd_kernel<W, true, 0, true> : seg_bwd_kernel<W, false, 0, true>))
+                : (L.compat ? (L.grad_x ? seg_bwd_kernel<W, true, 1, false> : seg_bwd_kernel<W, false, 1, false>)
+                            : (L.grad_x ? seg_bwd_kernel<W, true, 0, false> : seg_bwd_kernel<W, false, 0, false>));
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   k<<<grid, W * 32, smem, st>>>(L);

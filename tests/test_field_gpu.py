@@ -173,8 +173,9 @@ def test_empty_scene_and_rays(cuda):
 
 def test_backward_without_matching_block_masks(cuda):
     """The backward reads the forward's stroke-block masks only when they were written
-    with its skip threshold; after a forward of the run schedule (which writes none)
-    it culls by itself and gives the same gradients."""
+    with its skip threshold; after a forward of the run schedule (which writes none),
+    a forward-only pass, or a forward at another threshold, it visits every block and
+    gives the same gradients."""
     from neural3dstrokes_b200.train import BatchedField
     sc, rays = small_workload("every", n_strokes=90, n_rays=128, n_samples=64, seed=8)
     f = BatchedField([sc], [rays], device=cuda)
@@ -183,10 +184,12 @@ def test_backward_without_matching_block_masks(cuda):
     f.g_acc.copy_(torch.randn(f.g_acc.shape, generator=g))
     f.step()
     ref = [t.clone() for t in (f.grad_x, f.grad_shape, f.grad_color, f.grad_density, f.grad_delta)]
-    for first in (FieldOptions(schedule="runs"), FieldOptions(forward_only=True)):
+    seg = FieldOptions(schedule="segments")
+    for first, second in ((FieldOptions(schedule="runs"), seg), (FieldOptions(forward_only=True), seg),
+                          (seg, FieldOptions(schedule="segments", cull_alpha=1e-8))):
         f.c_opt = first.c()
         f.forward()
-        f.c_opt = FieldOptions(schedule="segments").c()
+        f.c_opt = second.c()
         f.backward()
         for a, b in zip((f.grad_x, f.grad_shape, f.grad_color, f.grad_density, f.grad_delta), ref):
             assert rel(a, b) < 1e-5
