@@ -464,7 +464,8 @@ __device__ __forceinline__ void compose_skip(const float* rec, float a, CompAdj&
 // masks (L.block_masks non-null); the kernel then carries no culling code. If the
 // masks were recorded at another threshold (their tag), it visits every block: the
 // per-candidate test of the skip threshold makes the decisions culling would make.
-template <int WARPS, bool GX, int COMPAT, bool MASKS>
+// STATS: count the evaluated pairs into L.stats (non-null).
+template <int WARPS, bool GX, int COMPAT, bool MASKS, bool STATS>
 __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_constant__ SegLaunch L) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t bar;
@@ -568,7 +569,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
               const int sl = hi - b;
               const float* rec = S.recs + size_t(sl) * REC_FLOATS;
               float* row = S.gacc + size_t(sl) * GRAD_SLOTS;
-              bcount += nact;
+              if (STATS) bcount += nact;
               const float4 h = rec4(rec)[0];
               const int kind = __float_as_int(h.x);
               const int base = kind & 15;
@@ -665,7 +666,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) seg_bwd_kernel(const __grid_con
     __syncthreads();
     sci = s_scene;
   }
-  if (L.stats && lane == 0 && bcount) atomicAdd(L.stats, bcount);
+  if (STATS && lane == 0 && bcount) atomicAdd(L.stats, bcount);
 }
 
 // ============================================================== ray kernels
@@ -1269,17 +1270,24 @@ template <int W>
 static cudaError_t launch_fwd_w(const SegLaunch& L, int grid, size_t smem, cudaStream_t st) {
   return L.common_only ? launch_fwd_wc<W, true>(L, grid, smem, st) : launch_fwd_wc<W, false>(L, grid, smem, st);
 }
-template <int W>
-static cudaError_t launch_bwd_w(const SegLaunch& L, int grid, size_t smem, cudaStream_t st) {
-  auto* k = L.block_masks
-                ? (L.compat ? (L.grad_x ? seg_bwd_kernel<W, true, 1, true> : seg_bwd_kernel<W, false, 1, true>)
-                            : (L.grad_x ? seg_bwd_kernel<W, true, 0, true> : seg_bwd_kernel<W, false, 0, true>))
-                : (L.compat ? (L.grad_x ? seg_bwd_kernel<W, true, 1, false> : seg_bwd_kernel<W, false, 1, false>)
-                            : (L.grad_x ? seg_bwd_kernel<W, true, 0, false> : seg_bwd_kernel<W, false, 0, false>));
+template <int W, bool STATS>
+static cudaError_t launch_bwd_ws(const SegLaunch& L, int grid, size_t smem, cudaStream_t st) {
+  auto* k = L.block_masks ? (L.compat ? (L.grad_x ? seg_bwd_kernel<W, true, 1, true, STATS>
+                                                  : seg_bwd_kernel<W, false, 1, true, STATS>)
+                                      : (L.grad_x ? seg_bwd_kernel<W, true, 0, true, STATS>
+                                                  : seg_bwd_kernel<W, false, 0, true, STATS>))
+                          : (L.compat ? (L.grad_x ? seg_bwd_kernel<W, true, 1, false, STATS>
+                                                  : seg_bwd_kernel<W, false, 1, false, STATS>)
+                                      : (L.grad_x ? seg_bwd_kernel<W, true, 0, false, STATS>
+                                                  : seg_bwd_kernel<W, false, 0, false, STATS>));
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   k<<<grid, W * 32, smem, st>>>(L);
   return cudaGetLastError();
+}
+template <int W>
+static cudaError_t launch_bwd_w(const SegLaunch& L, int grid, size_t smem, cudaStream_t st) {
+  return L.stats ? launch_bwd_ws<W, true>(L, grid, smem, st) : launch_bwd_ws<W, false>(L, grid, smem, st);
 }
 
 cudaError_t launch_seg_fwd(const SegLaunch& L, int grid, int warps, size_t smem, cudaStream_t st) {
