@@ -245,8 +245,9 @@ def test_backward_warp_counts_agree(cuda, chunk):
 @pytest.mark.parametrize("kind", ["mixed_primitives", "ellipsoid", "capsule"])
 def test_common_primitive_build_matches_general_build(cuda, kind):
     """A field whose strokes are all common primitives (its kind list gives the base
-    hint) runs the forward build that carries only their code; it matches the general
-    build (render_strokes passes no hint) on the same inputs."""
+    hint) runs the forward build that carries only their code; its outputs and the
+    batched field's gradients match the general build (render_strokes passes no hint)
+    on the same inputs."""
     from neural3dstrokes_b200.train import BatchedField
     g = torch.Generator().manual_seed(41)
     kinds = ([scenes.MIXED_PRIMS[i % 6] for i in range(60)] if kind == "mixed_primitives" else [kind] * 60)
@@ -254,8 +255,14 @@ def test_common_primitive_build_matches_general_build(cuda, kind):
     rays = scenes.make_rays(80, 64, g)
     f = BatchedField([sc], [rays], device=cuda)
     assert f.c_strokes.base_mask != 0
-    f.forward()
+    up = [torch.randn(t.shape, generator=g).to(cuda) for t in (f.g_rgb, f.g_acc, f.g_depth)]
+    for dst, u in zip((f.g_rgb, f.g_acc, f.g_depth), up):
+        dst.copy_(u)
+    f.step()
     torch.cuda.synchronize()
-    (rgb, acc, depth), _ = run_field(sc, rays, cuda)
+    (rgb, acc, depth), leaves = run_field(sc, rays, cuda, requires_grad=True)
     assert rel(f.rgb, rgb) < 1e-6 and rel(f.acc, acc) < 1e-6
     assert f.status()[0] == 0
+    torch.autograd.backward([rgb, acc, depth], up)
+    for ours, leaf in zip((f.grad_x, f.grad_shape, f.grad_color, f.grad_density, f.grad_delta), leaves):
+        assert rel(ours, leaf.grad) < 1e-5
