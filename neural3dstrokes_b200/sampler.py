@@ -79,6 +79,8 @@ def sample_rays(origins: torch.Tensor, directions: torch.Tensor, radii: torch.Te
     n_levels = len(prop_mlps) + 1
     for i in range(n_levels):
         is_prop = i < n_levels - 1
+        if is_prop and num_prop_samples == 0:  # no proposal sampling (models.py:137-138)
+            continue
         n = num_prop_samples if is_prop else num_nerf_samples
         dilation = dilation_bias + dilation_multiplier * (init_s_far - init_s_near) / prod_num_samples
         prod_num_samples *= n

@@ -149,3 +149,16 @@ def test_rejects_mismatched_rays(cuda):
         sampler.sample_rays(o[:8], d, radii, near, far, nets)
     with pytest.raises(ValueError):
         sampler.sample_rays(o, d, radii[:8], near, far, nets)
+
+
+def test_without_proposal_samples_the_last_level_samples_the_whole_ray(cuda):
+    """num_prop_samples = 0 skips the proposal levels (models.py:137-138): the last
+    level dilates (i_level > 0) and resamples the initial single interval, i.e. centred
+    samples over [near, far]."""
+    R = 8
+    o, d, radii, near, far = rays(cuda, R)
+    out = sampler.sample_rays(o, d, radii, near, far, prop_nets(cuda), num_prop_samples=0, num_nerf_samples=N_NERF)
+    assert out.levels == []
+    ref_s, _ = ost.resample_level(torch.tensor([[0.0, 1.0]]).expand(R, 2), torch.ones(R, 1), N_NERF, None, True,
+                                  DIL_BIAS + DIL_MULT, 0.0, (0.0, 1.0), near.cpu()[:, None], far.cpu()[:, None])
+    assert torch.allclose(out.sdist.cpu(), ref_s, atol=1e-6)
