@@ -159,8 +159,12 @@ __global__ void __launch_bounds__(UF_WARPS * 32, 6) uf_stroke_fwd_kernel(const U
   }
 }
 
-template <int NV>
+// CLS: the call's curve class (one sdf_id per call), so that the kernel carries only
+// that class's evaluation and adjoint; COMPAT: L.compat as a constant.
+template <int CLS, int COMPAT>
 __global__ void __launch_bounds__(UF_WARPS * 32) uf_stroke_bwd_kernel(const UfStroke L) {
+  constexpr int NV = CLS == UF_CUBIC ? 32 : 16;
+  constexpr int compat = COMPAT;
   // padded stride (17 float4): rows stay 16-byte aligned and lane-indexed 128-bit
   // record loads of a quarter warp hit distinct banks
   constexpr int RS = REC_FLOATS + 4;
@@ -224,11 +228,11 @@ __global__ void __launch_bounds__(UF_WARPS * 32) uf_stroke_bwd_kernel(const UfSt
     V3 pl;
     QuadFwd qf;
     CubicFwd cf;
-    if (base <= B_TETRAHEDRON) {
+    if (CLS == UF_PRIM) {
       pl = prim_local(rec, x);
       sdf = prim_sdf(base, pl, rec);
       if (kind & K_S3FAC) f = s3_factor(base, pl, xyz(rec4(rec)[R_S / 4]), rec);
-    } else if (base == B_QUAD_BEZIER) {
+    } else if (CLS == UF_QUAD) {
       sdf = quad_eval(rec, x, qf);
     } else {
       sdf = cubic_eval(rec, x, cf, base == B_CATMULL_ROM);
@@ -239,7 +243,7 @@ __global__ void __launch_bounds__(UF_WARPS * 32) uf_stroke_bwd_kernel(const UfSt
     if (mode == STEP_HARD) {
       dsdf = gs;
       K = 0.f;
-    } else if (L.compat) {
+    } else if (compat) {
       // strokes_backward.cu:85-94: dAlpha/dSDF from the saved alpha
       const float dad = mode == STEP_LAPLACE ? (a < 0.5f ? a : 1.0f - a) * -kk
                                              : ((a > 0.f && a < 0.9999f) ? -kk : 0.f);
@@ -252,13 +256,13 @@ __global__ void __launch_bounds__(UF_WARPS * 32) uf_stroke_bwd_kernel(const UfSt
     }
     v[G_K] += K;
     V3 gx;
-    if (base <= B_TETRAHEDRON) {
-      gx = prim_backprop(rec, kind, pl, dsdf, K, v, L.compat);
-    } else if (base == B_QUAD_BEZIER) {
+    if (CLS == UF_PRIM) {
+      gx = prim_backprop(rec, kind, pl, dsdf, K, v, compat);
+    } else if (CLS == UF_QUAD) {
       gx = quad_adjoint(rec, qf, dsdf, v + G_CTRL);
     } else {
-      gx = cubic_adjoint(rec, x, cf, dsdf, v + G_CTRL, L.compat, base == B_CATMULL_ROM);
-      if (L.compat) gx = gx * dsdf;  // the reference multiplies by dL/dSDF again
+      gx = cubic_adjoint(rec, x, cf, dsdf, v + G_CTRL, compat, base == B_CATMULL_ROM);
+      if (compat) gx = gx * dsdf;  // the reference multiplies by dL/dSDF again
     }
     if (L.grad_x) {
       const float sx = warp_sum(gx.x), sy = warp_sum(gx.y), sz = warp_sum(gx.z);
@@ -1034,10 +1038,11 @@ cudaError_t launch_uf_stroke_bwd(const UfStroke& L, int base, cudaStream_t st) {
   if (want > cap) want = cap;
   if (want < 1) want = 1;
   dim3 grid((unsigned)want, sblocks);
-  if (base_is_cubic_curve(base))
-    uf_stroke_bwd_kernel<32><<<grid, UF_WARPS * 32, 0, st>>>(L);
-  else
-    uf_stroke_bwd_kernel<16><<<grid, UF_WARPS * 32, 0, st>>>(L);
+  const int cls = base_is_cubic_curve(base) ? UF_CUBIC : (base == B_QUAD_BEZIER ? UF_QUAD : UF_PRIM);
+  auto* k = cls == UF_PRIM ? (L.compat ? uf_stroke_bwd_kernel<UF_PRIM, 1> : uf_stroke_bwd_kernel<UF_PRIM, 0>)
+            : cls == UF_QUAD ? (L.compat ? uf_stroke_bwd_kernel<UF_QUAD, 1> : uf_stroke_bwd_kernel<UF_QUAD, 0>)
+                             : (L.compat ? uf_stroke_bwd_kernel<UF_CUBIC, 1> : uf_stroke_bwd_kernel<UF_CUBIC, 0>);
+  k<<<grid, UF_WARPS * 32, 0, st>>>(L);
   return cudaGetLastError();
 }
 
