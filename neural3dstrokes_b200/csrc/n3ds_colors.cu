@@ -302,41 +302,43 @@ __global__ void __launch_bounds__(COL_WARPS * 32) uf_texcoord_kernel(const UfCol
   }
 }
 
-dim3 color_grid(const UfColor& L) {
+// one wave of the kernel's resident blocks over the stroke blocks
+template <typename K>
+cudaError_t color_grid(const UfColor& L, K kernel, dim3* grid) {
   const int sblocks = (L.n_strokes + 31) / 32;
-  long long want = (148LL * 8 + sblocks - 1) / sblocks;
-  const long long cap = (L.n_points + COL_WARPS - 1) / COL_WARPS;
-  if (want > cap) want = cap;
-  if (want < 1) want = 1;
-  return dim3((unsigned)want, sblocks);
+  long long want = 1;
+  cudaError_t e = one_wave_blocks(kernel, COL_WARPS * 32, sblocks, (L.n_points + COL_WARPS - 1) / COL_WARPS, &want);
+  *grid = dim3((unsigned)want, sblocks);
+  return e;
 }
 
 }  // namespace
 
 cudaError_t launch_uf_color_fwd(const UfColor& L, cudaStream_t st) {
-  const dim3 grid = color_grid(L);
-  switch (L.color_id) {
-    case 1: uf_color_fwd_kernel<1><<<grid, COL_WARPS * 32, 0, st>>>(L); break;
-    case 2: uf_color_fwd_kernel<2><<<grid, COL_WARPS * 32, 0, st>>>(L); break;
-    case 3: uf_color_fwd_kernel<3><<<grid, COL_WARPS * 32, 0, st>>>(L); break;
-    default: return cudaErrorInvalidValue;
-  }
+  if (L.color_id < 1 || L.color_id > 3) return cudaErrorInvalidValue;
+  auto* k = L.color_id == 1 ? uf_color_fwd_kernel<1> : L.color_id == 2 ? uf_color_fwd_kernel<2> : uf_color_fwd_kernel<3>;
+  dim3 grid;
+  cudaError_t e = color_grid(L, k, &grid);
+  if (e != cudaSuccess) return e;
+  k<<<grid, COL_WARPS * 32, 0, st>>>(L);
   return cudaGetLastError();
 }
 
 cudaError_t launch_uf_texcoord(const UfColor& L, float* texcoord, cudaStream_t st) {
-  uf_texcoord_kernel<<<color_grid(L), COL_WARPS * 32, 0, st>>>(L, texcoord);
+  dim3 grid;
+  cudaError_t e = color_grid(L, uf_texcoord_kernel, &grid);
+  if (e != cudaSuccess) return e;
+  uf_texcoord_kernel<<<grid, COL_WARPS * 32, 0, st>>>(L, texcoord);
   return cudaGetLastError();
 }
 
 cudaError_t launch_uf_color_bwd(const UfColor& L, cudaStream_t st) {
-  const dim3 grid = color_grid(L);
-  switch (L.color_id) {
-    case 1: uf_color_bwd_kernel<1><<<grid, COL_WARPS * 32, 0, st>>>(L); break;
-    case 2: uf_color_bwd_kernel<2><<<grid, COL_WARPS * 32, 0, st>>>(L); break;
-    case 3: uf_color_bwd_kernel<3><<<grid, COL_WARPS * 32, 0, st>>>(L); break;
-    default: return cudaErrorInvalidValue;
-  }
+  if (L.color_id < 1 || L.color_id > 3) return cudaErrorInvalidValue;
+  auto* k = L.color_id == 1 ? uf_color_bwd_kernel<1> : L.color_id == 2 ? uf_color_bwd_kernel<2> : uf_color_bwd_kernel<3>;
+  dim3 grid;
+  cudaError_t e = color_grid(L, k, &grid);
+  if (e != cudaSuccess) return e;
+  k<<<grid, COL_WARPS * 32, 0, st>>>(L);
   return cudaGetLastError();
 }
 

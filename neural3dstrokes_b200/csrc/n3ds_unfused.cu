@@ -1035,19 +1035,11 @@ cudaError_t launch_uf_stroke_bwd(const UfStroke& L, int base, cudaStream_t st) {
   auto* k = cls == UF_PRIM ? (L.compat ? uf_stroke_bwd_kernel<UF_PRIM, 1> : uf_stroke_bwd_kernel<UF_PRIM, 0>)
             : cls == UF_QUAD ? (L.compat ? uf_stroke_bwd_kernel<UF_QUAD, 1> : uf_stroke_bwd_kernel<UF_QUAD, 0>)
                              : (L.compat ? uf_stroke_bwd_kernel<UF_CUBIC, 1> : uf_stroke_bwd_kernel<UF_CUBIC, 0>);
-  // one wave of sample-parallel blocks: the SMs times the blocks of this build that fit
-  // on one (registers decide it), spread over the stroke blocks; each warp then strides
-  // over the samples, so a second, partial wave would idle most of the machine
-  int dev = 0, sms = 148, per_sm = 4;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, UF_WARPS * 32, 0);
-  if (e != cudaSuccess) return e;
+  // one wave of sample-parallel blocks (registers decide how many fit)
   const int sblocks = (L.n_strokes + 31) / 32;
-  long long want = ((long long)sms * (per_sm > 0 ? per_sm : 1) + sblocks - 1) / sblocks;
-  long long cap = (L.n_points + UF_WARPS - 1) / UF_WARPS;
-  if (want > cap) want = cap;
-  if (want < 1) want = 1;
+  long long want = 1;
+  cudaError_t e = one_wave_blocks(k, UF_WARPS * 32, sblocks, (L.n_points + UF_WARPS - 1) / UF_WARPS, &want);
+  if (e != cudaSuccess) return e;
   dim3 grid((unsigned)want, sblocks);
   k<<<grid, UF_WARPS * 32, 0, st>>>(L);
   return cudaGetLastError();

@@ -71,6 +71,24 @@ struct UfCompose {
   int compat;
 };
 
+// Blocks per 32-stroke block for a kernel whose warps stride over the samples: one wave
+// of the blocks of `kernel` that fit on the device together (threads per block given,
+// no dynamic shared memory), spread over `sblocks` stroke blocks, at most `cap`. A
+// grid sized for more blocks than fit leaves a second, partial wave that idles most
+// of the machine.
+template <typename K>
+inline cudaError_t one_wave_blocks(K kernel, int threads, int sblocks, long long cap, long long* out) {
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
+  if (e != cudaSuccess) return e;
+  long long want = ((long long)sms * (per_sm > 0 ? per_sm : 1) + sblocks - 1) / sblocks;
+  if (want > cap) want = cap;
+  *out = want < 1 ? 1 : want;
+  return cudaSuccess;
+}
+
 cudaError_t launch_uf_stroke_fwd(const UfStroke& L, int base, cudaStream_t st);
 cudaError_t launch_uf_stroke_bwd(const UfStroke& L, int base, cudaStream_t st);
 cudaError_t launch_uf_compose_fwd(const UfCompose& L, cudaStream_t st);
