@@ -227,9 +227,20 @@ int check_texture(int64_t n, const float* texcoords, const float* image, int32_t
   return N3DS_OK;
 }
 
-unsigned grid_for(long long n) {
+// Blocks of 256 threads for n items of a grid-stride kernel: at most one wave of the
+// blocks of `kernel` that fit on the device together (a capped grid larger than that
+// leaves a partial last wave).
+template <typename K>
+unsigned grid_for(K kernel, long long n) {
   const long long blocks = (n + 255) / 256;
-  return (unsigned)std::max<long long>(1, std::min<long long>(blocks, 148LL * 16));
+  int dev = 0, sms = 148, per_sm = 8;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
+                                                 cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0) != cudaSuccess || per_sm < 1) {
+    sms = 148;
+    per_sm = 8;
+  }
+  return (unsigned)std::max<long long>(1, std::min<long long>(blocks, (long long)sms * per_sm));
 }
 
 }  // namespace
@@ -244,7 +255,8 @@ extern "C" int n3ds_texture_forward(float* color_out, float* alpha_out, const fl
   if (n > 0 && alpha_out && !alphas) return n3ds::report_error(N3DS_ERR_INVALID, "texture: alpha_out needs alphas");
   if (n == 0) return N3DS_OK;
   Tex t{image, channels, height, width};
-  texture_fwd_kernel<false><<<grid_for(n), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+  const unsigned grid = grid_for(texture_fwd_kernel<false>, n);
+  texture_fwd_kernel<false><<<grid, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
       color_out, alpha_out, texcoords, colors, alphas, n, t, tint_ratio, modulate_alpha != 0);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return n3ds::report_error(N3DS_ERR_CUDA, std::string("texture forward: ") + cudaGetErrorString(e));
@@ -259,7 +271,8 @@ extern "C" int n3ds_texture_backward(float* grad_colors, float* grad_alphas, con
   if (rc) return rc;
   if (n == 0 || (!grad_colors && !grad_alphas)) return N3DS_OK;
   Tex t{image, channels, height, width};
-  texture_bwd_kernel<false><<<grid_for(n), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+  const unsigned grid = grid_for(texture_bwd_kernel<false>, n);
+  texture_bwd_kernel<false><<<grid, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
       grad_colors, grad_alphas, grad_color_out, grad_alpha_out, texcoords, n, t, tint_ratio, modulate_alpha != 0);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return n3ds::report_error(N3DS_ERR_CUDA, std::string("texture backward: ") + cudaGetErrorString(e));
@@ -273,7 +286,8 @@ extern "C" int n3ds_texture_pack(float* packed, const float* image, int32_t chan
   if (!packed || !image) return n3ds::report_error(N3DS_ERR_INVALID, "texture pack: image and packed required");
   if (reinterpret_cast<uintptr_t>(packed) % 16)
     return n3ds::report_error(N3DS_ERR_INVALID, "texture pack: packed must be 16-byte aligned");
-  texture_pack_kernel<<<grid_for((long long)height * width), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+  const unsigned grid = grid_for(texture_pack_kernel, (long long)height * width);
+  texture_pack_kernel<<<grid, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
       reinterpret_cast<float4*>(packed), image, channels, height, width);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return n3ds::report_error(N3DS_ERR_CUDA, std::string("texture pack: ") + cudaGetErrorString(e));
@@ -297,14 +311,14 @@ extern "C" int n3ds_texture_forward_packed(float* color_out, float* alpha_out, c
   if (al16(color_out) && al16(texcoords) && al16(colors) && (!alpha_out || (al16(alpha_out) && al16(alphas)))) {
     const long long n4 = n / 4;
     if (n4 > 0)
-      texture_fwd_vec_kernel<<<grid_for(n4), 256, 0, st>>>(
+      texture_fwd_vec_kernel<<<grid_for(texture_fwd_vec_kernel, n4), 256, 0, st>>>(
           reinterpret_cast<float4*>(color_out), reinterpret_cast<float4*>(alpha_out),
           reinterpret_cast<const float4*>(texcoords), reinterpret_cast<const float4*>(colors),
           reinterpret_cast<const float4*>(alphas), n4, t, tint_ratio, modulate_alpha != 0);
     done = 4 * n4;
   }
   if (done < n)
-    texture_fwd_kernel<true><<<grid_for(n - done), 256, 0, st>>>(
+    texture_fwd_kernel<true><<<grid_for(texture_fwd_kernel<true>, n - done), 256, 0, st>>>(
         color_out + 3 * done, alpha_out ? alpha_out + done : nullptr, texcoords + 2 * done, colors + 3 * done,
         alphas ? alphas + done : nullptr, n - done, t, tint_ratio, modulate_alpha != 0);
   cudaError_t e = cudaGetLastError();
@@ -328,14 +342,14 @@ extern "C" int n3ds_texture_backward_packed(float* grad_colors, float* grad_alph
       (!grad_alphas || al16(grad_alphas)) && (!grad_alpha_out || al16(grad_alpha_out))) {
     const long long n4 = n / 4;
     if (n4 > 0)
-      texture_bwd_vec_kernel<<<grid_for(n4), 256, 0, st>>>(
+      texture_bwd_vec_kernel<<<grid_for(texture_bwd_vec_kernel, n4), 256, 0, st>>>(
           reinterpret_cast<float4*>(grad_colors), reinterpret_cast<float4*>(grad_alphas),
           reinterpret_cast<const float4*>(grad_color_out), reinterpret_cast<const float4*>(grad_alpha_out),
           reinterpret_cast<const float4*>(texcoords), n4, t, tint_ratio, modulate_alpha != 0);
     done = 4 * n4;
   }
   if (done < n)
-    texture_bwd_kernel<true><<<grid_for(n - done), 256, 0, st>>>(
+    texture_bwd_kernel<true><<<grid_for(texture_bwd_kernel<true>, n - done), 256, 0, st>>>(
         grad_colors ? grad_colors + 3 * done : nullptr, grad_alphas ? grad_alphas + done : nullptr,
         grad_color_out ? grad_color_out + 3 * done : nullptr, grad_alpha_out ? grad_alpha_out + done : nullptr,
         texcoords + 2 * done, n - done, t, tint_ratio, modulate_alpha != 0);
